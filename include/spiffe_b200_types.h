@@ -1,0 +1,172 @@
+/* spiffe_b200_types.h
+ *
+ * Plain-C descriptions of the state of one spiffe problem, shared by every
+ * entry point of libspiffe_b200 (no C++ or torch types).  They mirror the
+ * reference data model (spiffe.h:28-131 FIELDS, :201-221 BEAM, :341-352
+ * SCREEN) with one change of representation: every mesh array is a single
+ * contiguous (nz+1) x (nr+1) block indexed [iz*(nr+1) + ir] (ir fastest, the
+ * order of the reference's zarray_2d rows) instead of a row-pointer array.
+ * Array stagger, units and flag bits are the reference's (spiffe.h:50-100).
+ */
+#ifndef SPIFFE_B200_TYPES_H
+#define SPIFFE_B200_TYPES_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* mode bits, spiffe.h:50-56 */
+#define SPIFFE_FL_TM_FIELDS 1u
+#define SPIFFE_FL_TE_FIELDS 2u
+#define SPIFFE_FL_SPACE_CHARGE 4u
+#define SPIFFE_FL_RADIAL_INTERP 8u
+#define SPIFFE_FL_LONGIT_INTERP 16u
+#define SPIFFE_FL_RADIAL_SMEAR 32u
+#define SPIFFE_FL_LONGIT_SMEAR 64u
+
+/* metal-flag bits, spiffe.h:90-100 */
+#define SPIFFE_FL_IS_SURFACE 1
+#define SPIFFE_FL_IS_INSIDE 2
+#define SPIFFE_FL_EZ_ZERO 4
+#define SPIFFE_FL_ER_ZERO 8
+#define SPIFFE_FL_IS_VACUUM 16
+#define SPIFFE_FL_BPHI_ZERO 32
+#define SPIFFE_FL_EPHI_ZERO 64
+#define SPIFFE_FL_BZ_ZERO 128
+#define SPIFFE_FL_BR_ZERO 256
+#define SPIFFE_FL_IS_METAL (SPIFFE_FL_IS_SURFACE | SPIFFE_FL_IS_INSIDE)
+#define SPIFFE_FL_LAST_ACTIVE_PT 512
+
+/* boundary conditions, spiffe.h:38-39 */
+#define SPIFFE_DIRICHLET 0
+#define SPIFFE_NEUMANN 1
+
+/* particle status bits, spiffe.h:219-220 */
+#define SPIFFE_PART_ACTIVE 0x0001ull
+#define SPIFFE_PART_LOST 0x0002ull
+
+/* Mesh, time and uniform-field description (FIELDS scalars, spiffe.h:30-75,
+ * :117-120).  dz=(zmax-zmin)/(nz-1), dr=rmax/(nr-1) as geometry.c:75-76. */
+typedef struct spiffe_mesh {
+  int32_t nz, nr;
+  double zmin, zmax, rmax, dz, dr;
+  int32_t lower_bc, upper_bc, right_bc, left_bc;
+  uint32_t modes;
+  double dt, start_time, time;
+  int64_t time_step;
+  double constant_E[3]; /* Ez, Er, Ephi */
+  double constant_B[3]; /* Bz, Br, Bphi */
+  int16_t turn_off[6];  /* Ez, Er, Ephi, Bz, Br, Bphi */
+  int32_t has_solenoid; /* BzImposed/BrImposed take part in the gather */
+  double imposed_ramp_time, imposed_flat_top_time;
+} spiffe_mesh;
+
+/* Mesh arrays, each (nz+1)*(nr+1) doubles or NULL when absent. */
+typedef struct spiffe_field_set {
+  int16_t *flags;
+  double *Ez, *Er, *Bphi, *Bphi2, *Jz, *Jr;
+  double *Ephi, *Jphi, *Br, *Br2, *Bz, *Bz2;
+  double *EzImposed, *ErImposed, *PsiImposed;
+  double *BzImposed, *BrImposed;
+  double *Psi, *Q;
+} spiffe_field_set;
+
+/* Structure-of-arrays beam (BEAM, spiffe.h:201-221); arrays hold `capacity`
+ * slots of which the first np are live. */
+typedef struct spiffe_beam_set {
+  int64_t np, npActive, capacity;
+  int32_t nextParticleID;
+  double QoMC, stiffness;
+  double *z, *r, *pz, *pr, *r_pphi, *vz, *vr, *vphi, *Q;
+  double *r0, *z0, *t0, *rmin, *rmax, *zmin, *zmax;
+  int32_t *particleID;
+  int16_t *generation;
+  uint64_t *status;
+} spiffe_beam_set;
+
+/* Screen crossing records (SCREEN, spiffe.h:341-352; columns of screens.c:18). */
+#define SPIFFE_SCREEN_QUANS 8 /* r, pz, pr, pphi, t, q, r0, t0 */
+typedef struct spiffe_screen_set {
+  double z_position;
+  int32_t direction; /* +1 forward, -1 backward */
+  int64_t nb, capacity;
+  double *col[SPIFFE_SCREEN_QUANS];
+  double *rmin, *rmax, *zmin, *zmax;
+  int16_t *generation;
+  int32_t *particleID;
+} spiffe_screen_set;
+
+/* Lost-particle removal.  SPIFFE_COMPACT_REFERENCE reproduces
+ * advance_particles.c:491-518 as it behaves: the loop tests is_lost[ip] but
+ * never moves is_lost with the particle it copies down, so the first lost
+ * index ends the beam (np becomes that index).  SPIFFE_COMPACT_SWAP removes
+ * exactly the lost particles, each slot refilled from the end of the array.
+ * SPIFFE_COMPACT_ANY removes exactly the lost particles in any order (the
+ * cell-sorted single-precision form). */
+#define SPIFFE_COMPACT_REFERENCE 0
+#define SPIFFE_COMPACT_SWAP 1
+#define SPIFFE_COMPACT_ANY 2
+
+/* Screen momentum interpolation.  SPIFFE_SCREEN_REFERENCE reproduces
+ * advance_particles.c:383-385 as it behaves: pz0/pr0/r_pphi0 are function
+ * scope (:79) and hold the pre-kick values of the last particle of the push
+ * loop.  SPIFFE_SCREEN_PARTICLE uses each particle's own pre-kick values. */
+#define SPIFFE_SCREEN_REFERENCE 0
+#define SPIFFE_SCREEN_PARTICLE 1
+
+/* Options of advance_particles (advance_particles.c:67-76 arguments and the
+ * test-beam forced-acceleration mode, :289-311). */
+typedef struct spiffe_push_options {
+  double z_forces_start; /* integrate.nl:18, -1 = off */
+  double tb_electrons_per_macroparticle;
+  double tb_z_force, tb_r_force;
+  double tb_z_start_deceleration, tb_r_start_deceleration;
+  int32_t compaction;      /* SPIFFE_COMPACT_* */
+  int32_t screen_momentum; /* SPIFFE_SCREEN_* */
+} spiffe_push_options;
+
+/* Poisson correction command (poisson_correction.nl; defaults from
+ * setup_poisson_correction, poisson_correction.c:38-46). */
+typedef struct spiffe_poisson_options {
+  double start_time;
+  int64_t step_interval;
+  double accuracy;
+  double error_charge_threshold;
+  int64_t maximum_iterations;
+  int32_t verbosity;
+  int32_t guess_code; /* 0 none, 1 line-charge, 2 point-charge, 3 zero */
+} spiffe_poisson_options;
+
+/* define_cathode command (cathode.nl:8-40, defaults cathode.c:32-40).  A
+ * time profile, when given, is n_profile (t, factor) pairs in increasing t. */
+typedef struct spiffe_cathode_options {
+  double z_position, inner_radius, outer_radius;
+  double current_density, temperature, work_function;
+  int32_t field_emission;
+  double field_emission_beta;
+  double electrons_per_macroparticle;
+  double start_time, stop_time, time_offset;
+  int32_t autophase;
+  double number_per_step, initial_pz, initial_omega, stiffness;
+  int32_t discretize_radii, random_number_seed;
+  int32_t distribution_correction_interval, spread_over_dt, zoned_emission;
+  int32_t n_profile;
+  const double *profile_t, *profile_A;
+} spiffe_cathode_options;
+
+/* Result of one Poisson correction (the quantities the reference prints,
+ * poisson_correction.c:254-256, :284). */
+typedef struct spiffe_poisson_report {
+  int32_t ran;        /* 0 when skipped by interval or threshold */
+  int64_t iterations; /* solve_poisson_cyl return value */
+  double Qreal, Qerror, Qsurface;
+  double residual, driving; /* final sum|residual|, sum|rhs| of the solve */
+} spiffe_poisson_report;
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

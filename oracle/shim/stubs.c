@@ -1,0 +1,85 @@
+/* oracle/shim/stubs.c -- TEST INFRASTRUCTURE (checker only, never shipped).
+ *
+ * No-op stand-ins for reference functions that perform_integration()
+ * (integrate.c:149-193) calls every step but that lie outside the checked
+ * per-step PIC path: field sampling/saving/output, beam snapshots, arbitrary-
+ * surface emitters, resistors and the moving window.  Each is inert when its
+ * command was never given, which is how the checked configurations run; the
+ * ones that would act bomb instead, so a checker can never silently skip
+ * work.  compose_filename() stands in for the one in spiffe.c, which is not
+ * compiled.
+ */
+#include "spiffe.h"
+
+char *compose_filename(char *template, char *root_name)
+{
+  char *ptr;
+  if (template && root_name && str_in(template, "%s")) {
+    ptr = tmalloc(sizeof(char) * (strlen(template) + strlen(root_name) + 1));
+    replace_string(ptr, template, "%s", root_name);
+    return ptr;
+  }
+  return template;
+}
+
+void sample_fields(SAMPLE_DEFN *sample_defn, long n_sample_defns, FIELDS *EM_problem)
+{
+  (void)sample_defn;
+  (void)EM_problem;
+  if (n_sample_defns)
+    bomb("field sampling is not part of the checked path", NULL);
+}
+
+void save_fields(FIELD_SAVING *saving_defn, FIELDS *EM_problem, long final_call)
+{
+  (void)EM_problem;
+  (void)final_call;
+  if (saving_defn && saving_defn->filename)
+    bomb("field saving is not part of the checked path", NULL);
+}
+
+void output_fields(FIELD_OUTPUT *output_defn, FIELDS *EM_problem)
+{
+  (void)EM_problem;
+  if (output_defn && output_defn->filename)
+    bomb("field output is not part of the checked path", NULL);
+}
+
+void take_beam_snapshot(SNAPSHOT *snapshot_defn, BEAM *beam, FIELDS *EM_problem)
+{
+  (void)beam;
+  (void)EM_problem;
+  if (snapshot_defn && snapshot_defn->filename)
+    bomb("beam snapshots are not part of the checked path", NULL);
+}
+
+void emit_electrons_from_emitter(BEAM *beam, EMITTER *emitter, FIELDS *EM_problem)
+{
+  (void)beam;
+  (void)emitter;
+  (void)EM_problem;
+  bomb("surface emitters are not part of the checked path", NULL);
+}
+
+void setEmitterCurrentDensity(EMITTER *emitter, FIELDS *EM_problem)
+{
+  (void)emitter;
+  (void)EM_problem;
+  bomb("surface emitters are not part of the checked path", NULL);
+}
+
+void add_resistor_currents(FIELDS *EM_problem, RESISTOR *resistor)
+{
+  (void)EM_problem;
+  (void)resistor;
+  bomb("resistors are not part of the checked path", NULL);
+}
+
+void translate_problem(BEAM *beam, FIELDS *EM_problem, ANTENNA *antenna, long n_antennae, RESISTOR *resistor)
+{
+  (void)beam;
+  (void)EM_problem;
+  (void)antenna;
+  (void)n_antennae;
+  (void)resistor;
+}

@@ -1,0 +1,156 @@
+"""Synthetic workloads of the benchmark configurations, as spiffe input.
+
+Each builder returns spiffe namelist commands (the reference's command
+surface: define_geometry with a boundary file of &po points, define_cathode,
+define_screen, poisson_correction, integrate) plus any analytic initial field,
+with the sizes, seeds and parameters of the configuration it names.  No
+dataset is involved; every value is derived from the numbers below.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+C_MKS = 2.99792458e8
+E_MKS = 1.602176634e-19
+
+
+def po_lines(points):
+    """&po boundary points: list of dicts of &po variables (geometry.nl:40-55)."""
+    out = []
+    for p in points:
+        body = ", ".join(f"{k}={v!r}" if not isinstance(v, str) else f'{k}="{v}"' for k, v in p.items())
+        out.append(f"&po {body} &end")
+    return "\n".join(out) + "\n"
+
+
+def pillbox_geo(R, L):
+    """Closed PEC pillbox of radius R and length L with its axis on r=0."""
+    return po_lines([dict(x=0.0, y=0.0), dict(x=0.0, y=R), dict(x=L, y=R), dict(x=L, y=0.0), dict(x=0.0, y=0.0)])
+
+
+def dc_gun_geo(cathode_radius=5e-3, gap=10e-3, hole=3e-3, plate=0.2e-3, wall=20e-3, length=30e-3, voltage=300e3):
+    """Axisymmetric DC gun: cathode plane at z=0 (0 V), anode plate at z=gap
+    with a hole of radius `hole` at `voltage`, outer PEC wall of radius `wall`
+    whose potential ramps linearly from 0 to `voltage` between cathode and
+    anode (ramp_potential, grid_drawing.c draw_line startPotential), drift
+    region to z=length.  The emitting disk (cathode_radius) is the cathode
+    command's business, not the boundary's."""
+    v = float(voltage)
+    return po_lines([
+        dict(x=0.0, y=0.0, potential=0.0),
+        dict(x=0.0, y=wall, potential=0.0),
+        dict(x=gap, y=wall, potential=v, ramp_potential=1),
+        dict(x=gap, y=hole, potential=v),
+        dict(x=gap + plate, y=hole, potential=v),
+        dict(x=gap + plate, y=wall, potential=v),
+        dict(x=length, y=wall, potential=v),
+        dict(x=length, y=0.0, potential=v),
+        dict(x=0.0, y=0.0, potential=0.0),
+    ])
+
+
+def gun16_geo(half_cell=17.5e-3, full_cell=52.5e-3, cavity_r=41e-3, iris_r=10e-3, iris_t=5e-3,
+              pipe_r=10e-3, length=150e-3):
+    """1.6-cell RF gun: a half cell (length `half_cell`) and a full cell (length
+    `full_cell`), both of radius `cavity_r`, separated by an iris of radius
+    `iris_r` and thickness `iris_t`, an exit iris of the same size, then a beam
+    pipe of radius `pipe_r` out to z=`length`.  Cell lengths are measured
+    between iris faces."""
+    z1 = half_cell
+    z2 = z1 + iris_t
+    z3 = z2 + full_cell
+    z4 = z3 + iris_t
+    return po_lines([
+        dict(x=0.0, y=0.0), dict(x=0.0, y=cavity_r),
+        dict(x=z1, y=cavity_r), dict(x=z1, y=iris_r), dict(x=z2, y=iris_r), dict(x=z2, y=cavity_r),
+        dict(x=z3, y=cavity_r), dict(x=z3, y=iris_r), dict(x=z4, y=iris_r), dict(x=z4, y=pipe_r),
+        dict(x=length, y=pipe_r), dict(x=length, y=0.0), dict(x=0.0, y=0.0),
+    ])
+
+
+def geometry_command(nz, nr, zmin, zmax, rmax, boundary, **extra):
+    args = dict(nz=nz, nr=nr, zmin=zmin, zmax=zmax, rmax=rmax)
+    args.update(extra)
+    body = ", ".join(f"{k}={v}" for k, v in args.items())
+    return f'&define_geometry {body}, boundary="{boundary}" &end'
+
+
+def namelist(group, **kw):
+    parts = []
+    for k, v in kw.items():
+        parts.append(f'{k}="{v}"' if isinstance(v, str) else f"{k}={v!r}")
+    return f"&{group} " + ", ".join(parts) + " &end"
+
+
+def tm010_ez(nz, nr, dr, R, E0):
+    """Ez = E0 J0(2.405 r/R) on the Ez nodes (r = ir*dr), uniform in z."""
+    from scipy.special import j0, jn_zeros
+
+    x01 = float(jn_zeros(0, 1)[0])
+    r = np.arange(nr + 1) * dr
+    prof = E0 * j0(x01 * r / R)
+    prof[r > R] = 0.0
+    return np.repeat(prof[None, :], nz + 1, axis=0)
+
+
+class PillboxConfig:
+    """Closed PEC pillbox: radius 40 mm (the 40.1 mm of the specification
+    snapped to the 0.25 mm mesh), length 26 mm (26.2 mm snapped), 161 x 105
+    nodes, TM010 standing wave of 80 MV/m at t=0, a 1 mm cathode on the z=0
+    wall emitting 1 nC as 20,000 macroparticles with a Gaussian 3 ps rms time
+    profile centred at RF phase 30 degrees, dt = 0.5 x Courant."""
+
+    def __init__(self, nz=105, nr=161, R=0.040, L=0.026, E0=-80e6, charge=1e-9, n_macro=20000,
+                 sigma_t=3e-12, cathode_radius=1e-3, seed=987654321, dt_factor=0.5, space_charge=1):
+        self.nz, self.nr, self.R, self.L = nz, nr, R, L
+        self.zmin, self.zmax, self.rmax = 0.0, L, R
+        self.dz = L / (nz - 1)
+        self.dr = R / (nr - 1)
+        self.E0 = E0
+        self.charge, self.n_macro, self.sigma_t = charge, n_macro, sigma_t
+        self.cathode_radius, self.seed = cathode_radius, seed
+        self.dt = dt_factor * min(self.dz, self.dr) / C_MKS / math.sqrt(2.0)
+        self.space_charge = space_charge
+        f = 2.405 * C_MKS / (2 * math.pi * R)
+        self.t_centre = (30.0 / 360.0) / f
+        self.epm = charge / E_MKS / n_macro
+
+    def geo_text(self):
+        return pillbox_geo(self.R, self.L)
+
+    def geometry(self, boundary="pillbox.geo"):
+        return geometry_command(self.nz, self.nr, self.zmin, self.zmax, self.rmax, boundary)
+
+    def initial_ez(self):
+        return tm010_ez(self.nz, self.nr, self.dr, self.R, self.E0)
+
+    def profile(self, n=161, nsig=4.0):
+        t = self.t_centre + np.linspace(-nsig, nsig, n) * self.sigma_t
+        return t, np.exp(-0.5 * ((t - self.t_centre) / self.sigma_t) ** 2)
+
+    def peak_current_density(self):
+        return self.charge / (math.sqrt(2 * math.pi) * self.sigma_t * math.pi * self.cathode_radius ** 2)
+
+    def cathode_options(self):
+        from . import abi
+
+        t, A = self.profile()
+        self._profile = (np.ascontiguousarray(t), np.ascontiguousarray(A))
+        o = abi.CathodeOptions()
+        o.z_position = 0.0
+        o.outer_radius = self.cathode_radius
+        o.current_density = self.peak_current_density()
+        o.electrons_per_macroparticle = self.epm
+        o.stiffness = 1.0
+        o.zoned_emission = 1
+        o.random_number_seed = self.seed
+        o.field_emission_beta = 1.0
+        o.n_profile = len(t)
+        o.profile_t = self._profile[0].ctypes.data_as(abi.D)
+        o.profile_A = self._profile[1].ctypes.data_as(abi.D)
+        return o
+
+    def screen_z(self):
+        return self.L - self.dz
