@@ -1,0 +1,118 @@
+/* spiffe_b200.h -- C ABI of libspiffe_b200, the B200 implementation of
+ * spiffe's per-timestep particle-in-cell loop.
+ *
+ * One spiffe problem (FIELDS + BEAM + screens, spiffe.h:28-131, :201-221,
+ * :341-352) lives on the GPU as a spiffe_gpu_instance.  The calls below are
+ * the reference's hot-path functions, one entry point each, so a host loop
+ * shaped like perform_integration (integrate.c:134-194) can drive the GPU
+ * step by step; spiffe_gpu_run_steps runs that whole loop on the device.
+ * All arrays cross the boundary as contiguous (nz+1)x(nr+1) blocks, ir
+ * fastest (spiffe_b200_types.h).
+ *
+ * Every function returns 0 on success or a negative error code;
+ * spiffe_gpu_last_error() then describes the failure (thread-local).
+ * Instances are independent; one instance must not be used by two host
+ * threads at the same time.
+ */
+#ifndef SPIFFE_B200_H
+#define SPIFFE_B200_H
+
+#include <stdint.h>
+
+#include "spiffe_b200_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPIFFE_PRECISION_F64 0     /* plain FP64, bit-faithful to the reference */
+#define SPIFFE_PRECISION_SPLIT32 1 /* FP32 fields and push, split positions, fixed-point J */
+
+#define SPIFFE_ERR_INVALID -1
+#define SPIFFE_ERR_CUDA -2
+#define SPIFFE_ERR_CAPACITY -3
+#define SPIFFE_ERR_DEVICE -4
+#define SPIFFE_ERR_UNSUPPORTED -5
+#define SPIFFE_ERR_NOMEM -6
+
+typedef struct spiffe_gpu_instance spiffe_gpu_instance;
+
+/* Description of the last error on this thread. */
+const char *spiffe_gpu_last_error(void);
+
+/* Library version string. */
+const char *spiffe_gpu_version(void);
+
+/* Creates an instance for `mesh` with metal flags `flags` ((nz+1)*(nr+1)
+ * values as geometry.c:319-362 sets them) and room for `particle_capacity`
+ * macroparticles (grown on demand, like the reference's trealloc in
+ * cathode.c:427-456).  Replaces: the allocations of process_geometry_definition
+ * (geometry.c:78-107). */
+int spiffe_gpu_create(const spiffe_mesh *mesh, const int16_t *flags, int32_t precision, int64_t particle_capacity,
+                      spiffe_gpu_instance **out);
+int spiffe_gpu_destroy(spiffe_gpu_instance *inst);
+
+/* Time, dt, uniform fields and switches; the mesh geometry must not change. */
+int spiffe_gpu_set_mesh(spiffe_gpu_instance *inst, const spiffe_mesh *mesh);
+int spiffe_gpu_get_mesh(spiffe_gpu_instance *inst, spiffe_mesh *mesh);
+
+/* Copies every non-NULL array of `host` to / from the device. */
+int spiffe_gpu_upload_fields(spiffe_gpu_instance *inst, const spiffe_field_set *host);
+int spiffe_gpu_download_fields(spiffe_gpu_instance *inst, spiffe_field_set *host);
+int spiffe_gpu_upload_beam(spiffe_gpu_instance *inst, const spiffe_beam_set *host);
+int spiffe_gpu_download_beam(spiffe_gpu_instance *inst, spiffe_beam_set *host);
+
+/* 0: FP64 atomics (default); 1: deposit in particle order, bit-identical to
+ * the serial reference (space_charge.c:130-137). */
+int spiffe_gpu_set_deposit_order(spiffe_gpu_instance *inst, int32_t ordered);
+
+/* zero_current_arrays, integrate.c:210 */
+int spiffe_gpu_zero_current_arrays(spiffe_gpu_instance *inst);
+/* advance_field_solutions, integrate.c:277 */
+int spiffe_gpu_advance_field_solutions(spiffe_gpu_instance *inst);
+/* add_particle_currents, space_charge.c:34 */
+int spiffe_gpu_add_particle_currents(spiffe_gpu_instance *inst);
+/* advance_particles, advance_particles.c:67 (screens added with
+ * spiffe_gpu_add_screen; lost-particle logging is not produced) */
+int spiffe_gpu_advance_particles(spiffe_gpu_instance *inst, const spiffe_push_options *opt);
+/* solve_poisson_cyl, poisson.c:17: target 0 solves Psi with driving term Q,
+ * target 1 solves PsiImposed with no driving term.  *iterations receives the
+ * reference's return value (half-sweeps, or -1 at the limit). */
+int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *inst, int32_t target, double accuracy, int64_t iteration_limit,
+                                 int64_t *iterations);
+/* add_poisson_correction, poisson_correction.c:73 (interval and start-step
+ * tests included; `report` may be NULL) */
+int spiffe_gpu_add_poisson_correction(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_poisson_options *opt,
+                                      spiffe_poisson_report *report);
+/* compute_imposed_Efield, poisson_correction.c:456 */
+int spiffe_gpu_compute_imposed_efield(spiffe_gpu_instance *inst, const spiffe_poisson_options *opt, int32_t initialize);
+
+/* define_screen (screens.c:29): records accumulate on the device until cleared. */
+int spiffe_gpu_add_screen(spiffe_gpu_instance *inst, double z_position, int32_t direction, int64_t capacity);
+int spiffe_gpu_screen_count(spiffe_gpu_instance *inst, int32_t screen, int64_t *nb);
+int spiffe_gpu_download_screen(spiffe_gpu_instance *inst, int32_t screen, spiffe_screen_set *host);
+int spiffe_gpu_clear_screens(spiffe_gpu_instance *inst);
+
+/* define_cathode (cathode.c:21) and define_antenna (antenna.c:18) for the
+ * device integration loop; waveform times must already include time_offset. */
+int spiffe_gpu_add_cathode(spiffe_gpu_instance *inst, const spiffe_cathode_options *opt);
+int spiffe_gpu_add_antenna(spiffe_gpu_instance *inst, int32_t direction, int64_t istart, int64_t iend,
+                           int64_t iposition, double current, double frequency, double phase, const double *t,
+                           const double *W, int64_t n_points);
+
+/* perform_integration (integrate.c:24-194) on the device: configure, the
+ * setup before the loop (:125-133), then any number of loop steps. */
+int spiffe_gpu_configure_run(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_push_options *push,
+                             const spiffe_poisson_options *poisson);
+int spiffe_gpu_run_begin(spiffe_gpu_instance *inst, spiffe_poisson_report *report);
+int spiffe_gpu_run_steps(spiffe_gpu_instance *inst, int64_t n_steps);
+
+/* Waits for queued work and reports device-side errors. */
+int spiffe_gpu_synchronize(spiffe_gpu_instance *inst);
+int spiffe_gpu_counts(spiffe_gpu_instance *inst, int64_t *np, int64_t *np_active);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,94 @@
+// spiffe_b200/csrc/common.cuh -- device-side data model shared by all kernels.
+//
+// One problem ("instance") lives on the device as contiguous (nz+1)x(nr+1)
+// arrays, ir fastest, at row pitch `pitch` elements.  The plain FP64 form uses
+// pitch = nr+1 (the reference's zarray_2d rows, spiffe.h:60-71); the
+// single-precision form pads rows to a multiple of 32 elements so every row
+// starts on a 128-byte boundary.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/spiffe_b200_constants.h"
+#include "../../include/spiffe_b200_types.h"
+
+#define SPIFFE_MAX_SCREENS 8
+
+// Per-instance scalars every kernel needs (the FIELDS scalars of spiffe.h).
+struct DevMesh {
+  int nz, nr, pitch;
+  double zmin, zmax, rmax, dz, dr, dt;
+  int lower_bc, upper_bc, right_bc, left_bc;
+  unsigned modes;
+  double constE[3], constB[3];
+  short turn_off[6];
+  int has_solenoid;
+};
+
+template <typename T>
+struct DevFields {
+  const int16_t *flags;
+  T *Ez, *Er, *Bphi, *Bphi2, *Jz, *Jr;
+  T *Ephi, *Jphi, *Br, *Br2, *Bz, *Bz2;
+  T *EzImposed, *ErImposed, *PsiImposed, *BzImposed, *BrImposed;
+  T *Psi, *Q;
+};
+
+// FP64 structure-of-arrays beam (BEAM, spiffe.h:201-221).
+struct DevBeam64 {
+  double *z, *r, *pz, *pr, *r_pphi, *vz, *vr, *vphi, *Q;
+  double *r0, *z0, *t0, *rmin, *rmax, *zmin, *zmax;
+  int32_t *particleID;
+  int16_t *generation;
+  uint64_t *status;
+  int64_t capacity;
+};
+
+// Screen record buffers, one set per screen (SCREEN, spiffe.h:341-352).
+struct DevScreen {
+  double z_position;
+  int direction;
+  int64_t capacity;
+  double *col[SPIFFE_SCREEN_QUANS];
+  double *rmin, *rmax, *zmin, *zmax;
+  int16_t *generation;
+  int32_t *particleID;
+};
+
+struct DevScreens {
+  int n;
+  DevScreen s[SPIFFE_MAX_SCREENS];
+};
+
+// Counters kept on the device so a step needs no host round trip.
+struct DevCounts {
+  long long np, npActive;
+  long long nextParticleID;
+  long long first_lost; // smallest lost index this step (reference compaction)
+  long long n_lost;     // particles lost this step
+  long long new_active; // activations this step
+  long long screen_nb[SPIFFE_MAX_SCREENS];
+  long long screen_overflow;
+  double last_pz0, last_pr0, last_rpphi0; // pre-kick momenta of particle np-1
+  unsigned int error;                     // SPIFFE_DEV_ERR_* bits
+  unsigned int pad;
+};
+
+#define SPIFFE_DEV_ERR_CAPACITY 1u
+#define SPIFFE_DEV_ERR_SCREEN 2u
+#define SPIFFE_DEV_ERR_BARRIER 4u
+#define SPIFFE_DEV_ERR_INDEX 8u
+
+__host__ __device__ inline size_t node(int iz, int ir, int pitch) { return (size_t)iz * (size_t)pitch + (size_t)ir; }
+
+#ifdef __CUDACC__
+// signed 64-bit atomic add through the unsigned overload (two's complement)
+__device__ __forceinline__ long long atomic_add_ll(long long *p, long long v)
+{
+  return (long long)atomicAdd((unsigned long long *)p, (unsigned long long)v);
+}
+#endif
+
+// Host-side launch helpers.
+inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }

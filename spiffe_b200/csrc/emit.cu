@@ -1,0 +1,153 @@
+// spiffe_b200/csrc/emit.cu -- cathode births and antenna current on the device.
+//
+// The host decides how many macroparticles a cathode emits this step (the
+// reference's count logic, cathode.c:349-422, runs in runtime.cu with the
+// shared counter-based generator); this kernel writes the births straight
+// into the device beam, one thread per birth, drawing radius k from the
+// generator at counter base+k+1 so the stream is consumed exactly as the
+// serial reference consumes it (cathode.c:464-659).  Built with -fmad=false.
+#include "common.cuh"
+
+#include "../../include/spiffe_b200_rng.h"
+
+struct BirthBin {
+  long long start, count; // births [start, start+count) belong to this annulus
+  double area, rmin;
+};
+
+struct BirthParams {
+  long long total;
+  uint64_t key, counter_base; // draw k uses counter_base + k + 1
+  int mode;                   // 0 uniform in r^2, 1 per-annulus (correction), 2 discrete radii
+  int spread;                 // spread_over_dt
+  double z_position, inner_radius, outer_radius, inner_r2, dr2;
+  double initial_vz, initial_omega, Q, time, dt, QoMC, stiffness;
+  const BirthBin *bins;
+  int n_bins;
+};
+
+namespace {
+
+constexpr int T = 256;
+
+__global__ void __launch_bounds__(T) k_births(DevMesh m, DevFields<double> f, DevBeam64 b, BirthParams p, DevCounts *cnt)
+{
+  const long long k = (long long)blockIdx.x * T + threadIdx.x;
+  if (k >= p.total)
+    return;
+  const long long np = cnt->np;
+  if (np + p.total > b.capacity) {
+    if (k == 0)
+      atomicOr(&cnt->error, SPIFFE_DEV_ERR_CAPACITY);
+    return;
+  }
+  const long long ip = np + k;
+  const double c = SPIFFE_C_MKS;
+  double r, dte = 0;
+  if (p.mode == 1) {
+    int bin = 0;
+    while (bin + 1 < p.n_bins && k >= p.bins[bin + 1].start)
+      bin++;
+    const BirthBin B = p.bins[bin];
+    r = sqrt(spiffe_rng_uniform(p.key, p.counter_base + (uint64_t)k + 1) * B.area / SPIFFE_PI + B.rmin * B.rmin);
+    dte = m.dt * (double)(k - B.start) / (1.0 * B.count);
+  } else if (p.mode == 0) {
+    const double rn = spiffe_rng_uniform(p.key, p.counter_base + (uint64_t)k + 1);
+    r = sqrt(rn * (p.outer_radius * p.outer_radius - p.inner_radius * p.inner_radius) + p.inner_radius * p.inner_radius);
+    dte = m.dt * (double)k / (1.0 * p.total);
+  } else {
+    r = sqrt(p.inner_r2 + (double)(k + 1) * p.dr2);
+    dte = m.dt * (double)k / (1.0 * p.total);
+  }
+  // cathode.c:466-488
+  double vz = p.initial_vz, vr = 0, vphi = p.initial_omega * r;
+  double gamma = 1 / sqrt(1 - (vz / c) * (vz / c) - (vr / c) * (vr / c) - (vphi / c) * (vphi / c));
+  double pz = vz / c * gamma, pr = vr / c * gamma, r_pphi = r * vphi / c * gamma;
+  double z = p.z_position, t0 = p.time;
+  if (p.spread) {
+    // cathode.c:490-518: partial kick by the local Ez, Er over dte
+    const int P = m.pitch;
+    long iz = (long)((p.z_position - m.zmin) / m.dz);
+    if (iz <= 0)
+      iz = 1;
+    if (iz > m.nz)
+      iz = m.nz;
+    long ir = (long)(r / m.dr);
+    double Ez = m.constE[0], Er = m.constE[1];
+    if (m.modes & SPIFFE_FL_TM_FIELDS)
+      Ez = f.Ez[node((int)iz, (int)ir, P)] + f.EzImposed[node((int)iz, (int)ir, P)];
+    ir += 1;
+    iz -= 1;
+    if (m.modes & SPIFFE_FL_TM_FIELDS)
+      Er = f.Er[node((int)iz, (int)ir, P)] + f.ErImposed[node((int)iz, (int)ir, P)];
+    t0 -= dte;
+    const double pphi = (r ? r_pphi / r : 0);
+    z += vz * dte;
+    r += vr * dte;
+    pr += dte * p.QoMC * Er / p.stiffness;
+    pz += dte * p.QoMC * Ez / p.stiffness;
+    gamma = sqrt(pz * pz + pr * pr + pphi * pphi + 1);
+    vz = c * pz / gamma;
+    vr = c * pr / gamma;
+  }
+  b.particleID[ip] = (int32_t)(cnt->nextParticleID + k);
+  b.rmin[ip] = b.zmin[ip] = 1.7976931348623157e308;
+  b.rmax[ip] = b.zmax[ip] = -1.7976931348623157e308;
+  b.z[ip] = z;
+  b.z0[ip] = z;
+  b.r[ip] = r;
+  b.r0[ip] = r;
+  b.t0[ip] = t0;
+  b.generation[ip] = 0;
+  b.Q[ip] = p.Q;
+  b.vz[ip] = vz;
+  b.vr[ip] = vr;
+  b.vphi[ip] = vphi;
+  b.pz[ip] = pz;
+  b.pr[ip] = pr;
+  b.r_pphi[ip] = r_pphi;
+  b.status[ip] = SPIFFE_PART_ACTIVE;
+}
+
+__global__ void k_births_commit(long long total, long long capacity, DevCounts *cnt)
+{
+  if (cnt->np + total > capacity)
+    return;
+  cnt->np += total;
+  cnt->npActive += total;
+  cnt->nextParticleID += total;
+}
+
+__global__ void k_antenna(double *J, int P, int direction, long istart, long iend, long iposition, double value)
+{
+  const long i = istart + (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > iend)
+    return;
+  // antenna.c:398-415
+  if (direction == 1)
+    J[node((int)iposition, (int)i, P)] += value;
+  else
+    J[node((int)i, (int)iposition, P)] += value;
+}
+
+} // namespace
+
+extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const BirthParams *p,
+                               DevCounts *cnt, cudaStream_t s)
+{
+  if (p->total <= 0)
+    return 0;
+  k_births<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt);
+  k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, cnt);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int spiffe_antenna64(double *J, int pitch, int direction, long istart, long iend, long iposition, double value,
+                                cudaStream_t s)
+{
+  if (iend < istart)
+    return 0;
+  const long n = iend - istart + 1;
+  k_antenna<<<blocks_for(n, 128), 128, 0, s>>>(J, pitch, direction, istart, iend, iposition, value);
+  return (int)cudaGetLastError();
+}

@@ -1,0 +1,678 @@
+// spiffe_b200/csrc/poisson_f64.cu -- plain FP64 Poisson correction.
+//
+// add_poisson_correction (poisson_correction.c:73-454), solve_poisson_cyl
+// (poisson.c:17-130) and compute_imposed_Efield (poisson_correction.c:
+// 456-562) as device kernels.  The decision whether to solve (the error-
+// charge threshold, :258-265) is taken on the device, so a correction needs
+// no host round trip.  The red-black SOR runs as one persistent cooperative
+// kernel: each half-sweep updates one colour (the reference's colour test,
+// poisson.c:70), every block reduces its |residual| sum, and after a grid
+// barrier all blocks add the per-block sums in the same fixed order and take
+// the same stop decision (poisson.c:120-121).  Node updates are bit-identical
+// to the reference (a colour's nodes read only the other colour); the stop
+// sum is reduced in a fixed tree order rather than the reference's serial
+// order, which changes the half-sweep count only if the sum lands within
+// rounding distance of the threshold.  Built with -fmad=false.
+#include "common.cuh"
+
+#include <cooperative_groups.h>
+
+namespace {
+
+constexpr int BX = 32, BY = 8, RT = 256;
+
+// Fixed-order block reduction of one double per thread (blockDim.x*y <= 1024).
+__device__ double block_sum(double v, double *sh)
+{
+  const int t = threadIdx.y * blockDim.x + threadIdx.x, n = blockDim.x * blockDim.y;
+  sh[t] = v;
+  __syncthreads();
+  for (int s = 512; s > 0; s >>= 1) {
+    if (t < s && t + s < n)
+      sh[t] += sh[t + s];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+struct PcState {
+  double Qreal, Qerror, Qsurface, centroid, driving, residual;
+  long long iterations;
+  int do_solve, pad;
+};
+
+__device__ bool surface_cell(const DevMesh &m, int16_t fl, int iz, int ir)
+{
+  return (fl & SPIFFE_FL_IS_METAL) || (iz == 0 && m.left_bc == SPIFFE_NEUMANN) ||
+         (iz == m.nz - 1 && m.right_bc == SPIFFE_NEUMANN) || (ir == m.nr - 1 && m.upper_bc == SPIFFE_NEUMANN);
+}
+
+// Apparent charge from the flux of E through each cell (:141-182, second pass
+// :335-375, where the top-row surface term changes sign).  Per-block partial
+// sums of Qsurface and the centroid numerator go to part[2*block+{0,1}].
+__global__ void __launch_bounds__(BX *BY) k_apparent_charge(DevMesh m, DevFields<double> f, const double *Az_,
+                                                             const double *Ari, const double *Aro, int second,
+                                                             double *part)
+{
+  __shared__ double sh[BX * BY];
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  const double eps = SPIFFE_EPSILON_O;
+  double qs = 0, cen = 0;
+  if (ir < nr && iz < nz) {
+    const size_t i = node(iz, ir, P);
+    const double Az = Az_[ir], Ar_inner = Ari[ir], Ar_outer = Aro[ir];
+    double dQ;
+    if (ir == 0)
+      dQ = (f.Er[i + 1] * Ar_outer + (f.Ez[i + P] - f.Ez[i]) * Az) * eps;
+    else
+      dQ = (f.Er[i + 1] * Ar_outer - f.Er[i] * Ar_inner + (f.Ez[i + P] - f.Ez[i]) * Az) * eps;
+    if (surface_cell(m, f.flags[i], iz, ir)) {
+      if (iz == 0)
+        dQ += f.Ez[i] * Az * eps;
+      if (iz == nz - 1)
+        dQ -= f.Ez[i + P] * Az * eps;
+      if (ir == nr - 1) {
+        if (second)
+          dQ -= f.Ez[i + 1] * Ar_outer * eps;
+        else
+          dQ += f.Ez[i + 1] * Ar_outer * eps;
+      }
+      qs = dQ;
+      f.Q[i] = 0;
+    } else {
+      f.Q[i] = dQ;
+      cen = dQ * (iz * m.dz + m.zmin);
+    }
+  }
+  const double s0 = block_sum(qs, sh), s1 = block_sum(cen, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int b = blockIdx.y * gridDim.x + blockIdx.x;
+    part[2 * b] = s0;
+    part[2 * b + 1] = s1;
+  }
+}
+
+// Removal of the particles' own charge (:190-242), FP64 atomics; Qreal partial
+// sums per block.
+__global__ void __launch_bounds__(RT) k_remove_charge(DevMesh m, DevFields<double> f, DevBeam64 b,
+                                                       const DevCounts *cnt, double *part)
+{
+  __shared__ double sh[RT];
+  const long ip = (long)blockIdx.x * RT + threadIdx.x;
+  double qreal = 0;
+  if (ip < (long)cnt->np && (b.status[ip] & SPIFFE_PART_ACTIVE)) {
+    const long nz = m.nz, nr = m.nr;
+    const int P = m.pitch;
+    const double dz = m.dz, dr = m.dr;
+    const bool lsm = m.modes & SPIFFE_FL_LONGIT_SMEAR, rsm = m.modes & SPIFFE_FL_RADIAL_SMEAR;
+    const bool ln = m.left_bc == SPIFFE_NEUMANN, rn = m.right_bc == SPIFFE_NEUMANN, un = m.upper_bc == SPIFFE_NEUMANN;
+    const double z = b.z[ip], r = b.r[ip], Q = b.Q[ip];
+    const long iz = lsm ? (long)((z - m.zmin) / dz) : (long)((z - m.zmin) / dz + 0.5);
+    const long ir = rsm ? (long)(r / dr) : (long)(r / dr + 0.5);
+    if (iz >= 0 && iz < nz && ir >= 0 && ir < nr) {
+      double fa, fb, fr, fl;
+      if (rsm && ir != nr - 1) {
+        fa = r / dr - ir;
+        fb = 1 - fa;
+      } else {
+        fb = 1;
+        fa = 0;
+      }
+      if (lsm && iz != nz - 1) {
+        fr = (z - m.zmin) / dz - iz;
+        fl = 1 - fr;
+      } else {
+        fl = 1;
+        fr = 0;
+      }
+      const int16_t *F = f.flags;
+      if (!((F[node(iz, ir, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr - 1 && un))) {
+        atomicAdd(f.Q + node(iz, ir, P), -(Q * fb * fl));
+        qreal += Q * fb * fl;
+      }
+      if (!((F[node(iz + 1, ir, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr - 1 && un))) {
+        atomicAdd(f.Q + node(iz + 1, ir, P), -(Q * fb * fr));
+        qreal += Q * fb * fr;
+      }
+      if (!((F[node(iz, ir + 1, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr && un))) {
+        atomicAdd(f.Q + node(iz, ir + 1, P), -(Q * fa * fl));
+        qreal += Q * fa * fl;
+      }
+      if (!((F[node(iz + 1, ir + 1, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr && un))) {
+        atomicAdd(f.Q + node(iz + 1, ir + 1, P), -(Q * fa * fr));
+        qreal += Q * fa * fr;
+      }
+    }
+  }
+  const double s = block_sum(qreal, sh);
+  if (threadIdx.x == 0)
+    part[blockIdx.x] = s;
+}
+
+// Sum over a (rows x cols) window of a pitched array, |x| when absval.
+__global__ void __launch_bounds__(BX *BY) k_region_sum(const double *a, int rows, int cols, int P, int absval,
+                                                        double *part)
+{
+  __shared__ double sh[BX * BY];
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  double v = 0;
+  if (ir < cols && iz < rows) {
+    v = a[node(iz, ir, P)];
+    if (absval)
+      v = fabs(v);
+  }
+  const double s = block_sum(v, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+}
+
+// Serial fixed-order sum of n partials (strided by `stride`) into *out.
+__global__ void k_finish_sum(const double *part, int n, int stride, double *out)
+{
+  __shared__ double sh[1024];
+  double v = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    v += part[(size_t)i * stride];
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    *out = sh[0];
+}
+
+// error-charge threshold test (:258-265)
+__global__ void k_pc_decide(PcState *st, double threshold)
+{
+  const double Qerror = st->Qerror, Qreal = st->Qreal;
+  int skip = (threshold > 0 && fabs(Qerror) < threshold) ||
+             (threshold < 0 && (Qreal == 0 || fabs(Qerror / Qreal) < fabs(threshold)));
+  st->do_solve = !skip;
+}
+
+// Q -> -Q/(V eps0) over iz < nz, ir < nr (:268-274)
+__global__ void __launch_bounds__(BX *BY) k_scale_rhs(DevMesh m, DevFields<double> f, const double *volume,
+                                                       const PcState *st)
+{
+  if (!st->do_solve)
+    return;
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  if (ir < m.nr && iz < m.nz) {
+    const size_t i = node(iz, ir, m.pitch);
+    f.Q[i] = -f.Q[i] / (volume[ir] * SPIFFE_EPSILON_O);
+  }
+}
+
+// poisson_guess (:564-615)
+__global__ void __launch_bounds__(BX *BY) k_guess(DevMesh m, DevFields<double> f, int code, const PcState *st)
+{
+  if (!st->do_solve)
+    return;
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  if (ir >= m.nr || iz >= m.nz)
+    return;
+  const size_t i = node(iz, ir, m.pitch);
+  const double charge = st->Qerror;
+  if (code == 1)
+    f.Psi[i] = charge / (SPIFFE_PIx2 * SPIFFE_EPSILON_O) * log((ir ? ir : 0.5) * m.dr);
+  else if (code == 2) {
+    const double zz = (iz * m.dz + m.zmin) - st->centroid, rr = m.dr * (ir + 0.5);
+    const double dist = sqrt(zz * zz + rr * rr);
+    f.Psi[i] = charge / (4 * SPIFFE_PI * SPIFFE_EPSILON_O * dist);
+  } else if (code == 3)
+    f.Psi[i] = 0;
+}
+
+// Bounded grid barrier for a cooperative launch: returns false (and raises
+// the device error bit) if the other blocks do not arrive within `limit` polls.
+__device__ bool grid_barrier(unsigned *count, unsigned *gen, unsigned nblocks, DevCounts *cnt)
+{
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    ok = 1;
+    volatile unsigned *vgen = gen;
+    const unsigned g = *vgen;
+    __threadfence();
+    if (atomicAdd(count, 1u) == nblocks - 1) {
+      atomicExch(count, 0u);
+      __threadfence();
+      atomicAdd(gen, 1u);
+    } else {
+      unsigned long long polls = 0;
+      while (*vgen == g) {
+        if (++polls > (1ull << 26)) {
+          ok = 0;
+          atomicOr(&cnt->error, SPIFFE_DEV_ERR_BARRIER);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok;
+}
+
+struct SorArgs {
+  double *Psi;
+  const double *rhs; // null for the Laplace solve of the imposed potential
+  const int16_t *flags;
+  const double *omega; // omega[n] for half-sweep n
+  double a, e, accuracy;
+  const double *driving; // sum |rhs|
+  long long limit;
+  double *partials; // 2*gridDim.x doubles
+  unsigned *bar_count, *bar_gen;
+  PcState *st; // iterations and final residual; do_solve gate (may be null)
+  long long *iterations_out;
+};
+
+// solve_poisson_cyl (poisson.c:17-130): rows 0..nr-2, iz over the rows the
+// boundary conditions leave free; colour (ir+iz)%2 == n%2 on half-sweep n.
+__global__ void __launch_bounds__(RT) k_sor(DevMesh m, SorArgs s, DevCounts *cnt)
+{
+  __shared__ double sh[RT];
+  if (s.st && !s.st->do_solve)
+    return;
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  const int lo = m.left_bc == SPIFFE_DIRICHLET ? 0 : 1, hi = m.right_bc == SPIFFE_DIRICHLET ? nz - 1 : nz - 2;
+  const int cols = nr - 1, rows = hi - lo + 1;
+  const long long work = (long long)rows * cols;
+  const double dr = m.dr, a = s.a, e = s.e, inv_dr2 = 1 / (dr * dr);
+  const double thr = s.accuracy * *s.driving;
+  long long result = -1;
+  double total = 0;
+  for (long long n = 0; n < s.limit; n++) {
+    const double omega = s.omega[n];
+    const int colour = (int)(n % 2);
+    double acc = 0;
+    for (long long w = (long long)blockIdx.x * RT + threadIdx.x; w < work; w += (long long)gridDim.x * RT) {
+      const int iz = lo + (int)(w / cols), ir = (int)(w % cols);
+      if ((ir + iz) % 2 != colour)
+        continue;
+      const size_t i = node(iz, ir, P);
+      if (s.flags[i] & SPIFFE_FL_IS_METAL)
+        continue;
+      // Psi written by other blocks last half-sweep: load through L2 only
+      double left, right;
+      if (iz == 0 && lo == 0)
+        left = right = __ldcg(s.Psi + i + P);
+      else if (iz == nz - 1 && hi == nz - 1)
+        left = right = __ldcg(s.Psi + i - P);
+      else {
+        left = __ldcg(s.Psi + i + P);
+        right = __ldcg(s.Psi + i - P);
+      }
+      const double drive = s.rhs ? s.rhs[i] : 0;
+      const double self = __ldcg(s.Psi + i);
+      double residual;
+      if (ir == 0) {
+        const double c = inv_dr2;
+        residual = a * (left + right) + 4 * c * __ldcg(s.Psi + i + 1) + (e - 2 * c) * self - drive;
+        __stcg(s.Psi + i, self - omega * residual / (e - 2 * c));
+      } else {
+        const double c = inv_dr2 * (1 + 1. / (2 * ir)), d = inv_dr2 * (1 - 1. / (2 * ir));
+        residual = a * (left + right) + c * __ldcg(s.Psi + i + 1) + d * __ldcg(s.Psi + i - 1) + e * self - drive;
+        __stcg(s.Psi + i, self - omega * residual / e);
+      }
+      acc += fabs(residual);
+    }
+    // partial sums alternate between two halves of the buffer, so a block
+    // that runs ahead cannot overwrite sums another block is still reading
+    double *part = s.partials + (size_t)(n % 2) * gridDim.x;
+    const double bs = block_sum(acc, sh);
+    if (threadIdx.x == 0)
+      __stcg(part + blockIdx.x, bs);
+    __threadfence();
+    if (!grid_barrier(s.bar_count, s.bar_gen, gridDim.x, cnt))
+      return;
+    total = 0;
+    for (unsigned b = 0; b < gridDim.x; b++)
+      total += __ldcg(part + b);
+    if (n > 0 && (total < thr || total == 0)) {
+      result = n;
+      break;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (s.iterations_out)
+      *s.iterations_out = result;
+    if (s.st) {
+      s.st->iterations = result;
+      s.st->residual = total;
+    }
+  }
+}
+
+// Ez, Er -= grad Psi (:288-326) with the FDTD boundary copies; one writer per node.
+__global__ void __launch_bounds__(BX *BY) k_subtract_gradient(DevMesh m, DevFields<double> f, const PcState *st)
+{
+  if (!st->do_solve)
+    return;
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  if (ir > nr || iz > nz)
+    return;
+  const size_t i = node(iz, ir, P);
+  const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
+  if (ir < nr && iz >= 1 && iz <= nz - 1) {
+    double v = f.Ez[i];
+    if (!(f.flags[i] & SPIFFE_FL_EZ_ZERO))
+      v -= -(f.Psi[i] - f.Psi[i - P]) / m.dz;
+    if (ir == nr - 1)
+      v = 0.0;
+    f.Ez[i] = v;
+    if (iz == 1)
+      f.Ez[node(0, ir, P)] = ir == nr - 1 ? 0.0 : (leftN ? v : -v);
+    if (iz == nz - 1)
+      f.Ez[node(nz, ir, P)] = ir == nr - 1 ? 0.0 : (rightN ? v : -v);
+  }
+  if (iz <= nz - 1) {
+    const bool zero_row = (leftN && iz == 0) || (rightN && iz == nz - 1);
+    if (ir >= 1) {
+      double v = f.Er[i];
+      if (!(f.flags[i] & SPIFFE_FL_ER_ZERO))
+        v -= -(f.Psi[i] - f.Psi[i - 1]) / m.dr;
+      f.Er[i] = zero_row ? 0.0 : v;
+      if (ir == 1)
+        f.Er[node(iz, 0, P)] = zero_row ? 0.0 : -v;
+    }
+  }
+}
+
+// EzImposed, ErImposed = -factor grad PsiImposed (:523-561).
+__global__ void __launch_bounds__(BX *BY) k_imposed_field(DevMesh m, DevFields<double> f, double ff)
+{
+  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  if (ir > nr || iz > nz)
+    return;
+  const size_t i = node(iz, ir, P);
+  const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
+  if (ir < nr && iz >= 1 && iz <= nz - 1) {
+    double v = f.EzImposed[i];
+    if (!(f.flags[i] & SPIFFE_FL_EZ_ZERO))
+      v = -ff * (f.PsiImposed[i] - f.PsiImposed[i - P]) / m.dz;
+    if (ir == nr - 1)
+      v = 0.0;
+    f.EzImposed[i] = v;
+    if (iz == 1)
+      f.EzImposed[node(0, ir, P)] = ir == nr - 1 ? 0.0 : (leftN ? v : -v);
+    if (iz == nz - 1)
+      f.EzImposed[node(nz, ir, P)] = ir == nr - 1 ? 0.0 : (rightN ? v : -v);
+  }
+  if (iz <= nz - 1) {
+    const bool zero_row = (leftN && iz == 0) || (rightN && iz == nz - 1);
+    if (ir >= 1) {
+      double v = f.ErImposed[i];
+      if (!(f.flags[i] & SPIFFE_FL_ER_ZERO))
+        v = -ff * (f.PsiImposed[i] - f.PsiImposed[i - 1]) / m.dr;
+      f.ErImposed[i] = zero_row ? 0.0 : v;
+      if (ir == 1)
+        f.ErImposed[node(iz, 0, P)] = zero_row ? 0.0 : -v;
+    }
+  }
+}
+
+__global__ void k_set_state(PcState *st, double *qs_cen, double *qreal, double *qerr, int space_charge)
+{
+  st->Qsurface = qs_cen[0];
+  st->centroid = qs_cen[1];
+  st->Qreal = space_charge ? *qreal : 0.0;
+  st->Qerror = *qerr;
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- host side
+
+struct Poisson64Work {
+  double *Az = nullptr, *Ari = nullptr, *Aro = nullptr, *volume = nullptr;
+  double *part = nullptr;    // block partials
+  double *scalars = nullptr; // [0..1] Qsurface/centroid, [2] Qreal, [3] Qerror, [4] driving
+  double *omega = nullptr;
+  long long omega_n = 0;
+  unsigned *bar = nullptr;
+  PcState *st = nullptr;
+  long long *iters = nullptr;
+  int sor_grid = 0;
+  size_t part_n = 0;
+};
+
+extern "C" int spiffe_poisson64_setup(const DevMesh *m, Poisson64Work *w, long long np_capacity, cudaStream_t s)
+{
+  const int nr = m->nr, nz = m->nz;
+  const double dr = m->dr, dz = m->dz, dr2 = dr * dr, drdz = dr * dz;
+  double *Az = new double[nr + 1], *Ari = new double[nr + 1], *Aro = new double[nr + 1], *vol = new double[nr + 1];
+  for (int ir = 0; ir <= nr; ir++) {
+    if (ir == 0) {
+      Ari[ir] = Aro[ir] = SPIFFE_PI * drdz;
+      Az[ir] = dr2 / 4 * SPIFFE_PI;
+    } else {
+      Ari[ir] = SPIFFE_PI * (2 * ir - 1) * drdz;
+      Aro[ir] = SPIFFE_PI * (2 * ir + 1) * drdz;
+      Az[ir] = SPIFFE_PI * dr2 / 4 * (double)((long)(2 * ir + 1) * (2 * ir + 1) - (long)(2 * ir - 1) * (2 * ir - 1));
+    }
+    vol[ir] = Az[ir] * dz;
+  }
+  cudaError_t e = cudaSuccess;
+  const size_t gx = (nr + 1 + BX - 1) / BX, gy = (nz + 1 + BY - 1) / BY;
+  size_t parts = 2 * gx * gy;
+  const size_t pblocks = (size_t)blocks_for(np_capacity > 0 ? np_capacity : 1, RT);
+  if (pblocks > parts)
+    parts = pblocks;
+  if (parts < 4096)
+    parts = 4096;
+  if (!w->Az) {
+    e = cudaMalloc(&w->Az, sizeof(double) * (nr + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&w->Ari, sizeof(double) * (nr + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&w->Aro, sizeof(double) * (nr + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&w->volume, sizeof(double) * (nr + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&w->scalars, sizeof(double) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&w->bar, sizeof(unsigned) * 2);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w->bar, 0, sizeof(unsigned) * 2, s);
+    if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(PcState));
+    if (e == cudaSuccess) e = cudaMemsetAsync(w->st, 0, sizeof(PcState), s);
+    if (e == cudaSuccess) e = cudaMalloc(&w->iters, sizeof(long long));
+  }
+  if (e == cudaSuccess && w->part_n < parts) {
+    cudaFree(w->part);
+    e = cudaMalloc(&w->part, sizeof(double) * parts);
+    w->part_n = parts;
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->Az, Az, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->Ari, Ari, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->Aro, Aro, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->volume, vol, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  delete[] Az;
+  delete[] Ari;
+  delete[] Aro;
+  delete[] vol;
+  if (e == cudaSuccess && !w->sor_grid) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sor, RT, 0);
+    if (per > 4)
+      per = 4;
+    w->sor_grid = sms * (per > 0 ? per : 1);
+    if ((size_t)(2 * w->sor_grid) > w->part_n)
+      w->sor_grid = (int)(w->part_n / 2);
+  }
+  return (int)e;
+}
+
+extern "C" void spiffe_poisson64_free(Poisson64Work *w)
+{
+  cudaFree(w->Az);
+  cudaFree(w->Ari);
+  cudaFree(w->Aro);
+  cudaFree(w->volume);
+  cudaFree(w->part);
+  cudaFree(w->scalars);
+  cudaFree(w->omega);
+  cudaFree(w->bar);
+  cudaFree(w->st);
+  cudaFree(w->iters);
+  *w = Poisson64Work();
+}
+
+// Chebyshev over-relaxation sequence, poisson.c:342-344, :416-419.
+static int ensure_omega(const DevMesh *m, Poisson64Work *w, long long limit, cudaStream_t s)
+{
+  if (w->omega && w->omega_n >= limit)
+    return 0;
+  cudaFree(w->omega);
+  const double rz = m->dz / m->dr;
+  const double rj = (cos(SPIFFE_PI / m->nz) + rz * rz * cos(SPIFFE_PI / m->nr)) / (1 + rz * rz);
+  double *om = new double[limit];
+  double omega = 1.0;
+  for (long long n = 0; n < limit; n++) {
+    om[n] = omega;
+    if (n == 0)
+      omega = 1.0 / (1 - rj * rj / 2);
+    else
+      omega = 1.0 / (1 - rj * rj * omega / 4);
+  }
+  cudaError_t e = cudaMalloc(&w->omega, sizeof(double) * limit);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->omega, om, sizeof(double) * limit, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  delete[] om;
+  w->omega_n = limit;
+  return (int)e;
+}
+
+static int sum_region(const double *a, int rows, int cols, int P, int absval, Poisson64Work *w, double *out,
+                      cudaStream_t s)
+{
+  dim3 block(BX, BY), grid((cols + BX - 1) / BX, (rows + BY - 1) / BY);
+  if (grid.x * grid.y == 0) {
+    cudaMemsetAsync(out, 0, sizeof(double), s);
+    return 0;
+  }
+  k_region_sum<<<grid, block, 0, s>>>(a, rows, cols, P, absval, w->part);
+  k_finish_sum<<<1, 1024, 0, s>>>(w->part, grid.x * grid.y, 1, out);
+  return 0;
+}
+
+static int launch_sor(const DevMesh *m, Poisson64Work *w, double *Psi, const double *rhs, const int16_t *flags,
+                      double accuracy, long long limit, PcState *st, long long *iters, DevCounts *cnt, cudaStream_t s)
+{
+  int rc = ensure_omega(m, w, limit, s);
+  if (rc)
+    return rc;
+  // sum |rhs| over iz < nz, ir < nr-1 (poisson.c:333-336)
+  if (rhs)
+    sum_region(rhs, m->nz, m->nr - 1, m->pitch, 1, w, w->scalars + 4, s);
+  else
+    cudaMemsetAsync(w->scalars + 4, 0, sizeof(double), s);
+  SorArgs a;
+  a.Psi = Psi;
+  a.rhs = rhs;
+  a.flags = flags;
+  a.omega = w->omega;
+  a.a = 1 / (m->dz * m->dz);
+  a.e = -2 * (1 / (m->dz * m->dz) + 1 / (m->dr * m->dr));
+  a.accuracy = accuracy;
+  a.driving = w->scalars + 4;
+  a.limit = limit;
+  a.partials = w->part;
+  a.bar_count = w->bar;
+  a.bar_gen = w->bar + 1;
+  a.st = st;
+  a.iterations_out = iters;
+  DevMesh mm = *m;
+  void *args[] = {&mm, &a, &cnt};
+  cudaError_t e = cudaLaunchCooperativeKernel((void *)k_sor, dim3(w->sor_grid), dim3(RT), args, 0, s);
+  return (int)e;
+}
+
+// solve_poisson_cyl on device arrays; *iterations receives the reference's
+// return value (n, or -1 when the limit was reached) after the stream syncs.
+extern "C" int spiffe_sor64(const DevMesh *m, Poisson64Work *w, double *Psi, const double *rhs, const int16_t *flags,
+                            double accuracy, long long limit, DevCounts *cnt, long long *iterations, cudaStream_t s)
+{
+  int rc = launch_sor(m, w, Psi, rhs, flags, accuracy, limit, nullptr, w->iters, cnt, s);
+  if (rc)
+    return rc;
+  if (iterations) {
+    cudaMemcpyAsync(iterations, w->iters, sizeof(long long), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+  }
+  return (int)cudaGetLastError();
+}
+
+struct PoissonHostOptions {
+  double accuracy, error_charge_threshold;
+  long long maximum_iterations;
+  int guess_code, space_charge;
+};
+
+// One add_poisson_correction pass (the interval test is the caller's).
+extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b,
+                                           DevCounts *cnt, long long np_bound, const PoissonHostOptions *o,
+                                           Poisson64Work *w, cudaStream_t s)
+{
+  dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
+  const int nblk = grid.x * grid.y;
+  // apparent charge, then the particles' own charge
+  k_apparent_charge<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 0, w->part);
+  k_finish_sum<<<1, 1024, 0, s>>>(w->part, nblk, 2, w->scalars + 0);
+  k_finish_sum<<<1, 1024, 0, s>>>(w->part + 1, nblk, 2, w->scalars + 1);
+  if (o->space_charge && np_bound > 0) {
+    const unsigned pb = blocks_for(np_bound, RT);
+    k_remove_charge<<<pb, RT, 0, s>>>(*m, *f, *b, cnt, w->part);
+    k_finish_sum<<<1, 1024, 0, s>>>(w->part, (int)pb, 1, w->scalars + 2);
+  } else {
+    cudaMemsetAsync(w->scalars + 2, 0, sizeof(double), s);
+  }
+  sum_region(f->Q, m->nz, m->nr, m->pitch, 0, w, w->scalars + 3, s);
+  k_set_state<<<1, 1, 0, s>>>(w->st, w->scalars, w->scalars + 2, w->scalars + 3, o->space_charge);
+  k_pc_decide<<<1, 1, 0, s>>>(w->st, o->error_charge_threshold);
+  k_scale_rhs<<<grid, block, 0, s>>>(*m, *f, w->volume, w->st);
+  if (o->guess_code)
+    k_guess<<<grid, block, 0, s>>>(*m, *f, o->guess_code, w->st);
+  int rc = launch_sor(m, w, f->Psi, f->Q, f->flags, o->accuracy, o->maximum_iterations, w->st, w->iters, cnt, s);
+  if (rc)
+    return rc;
+  k_subtract_gradient<<<grid, block, 0, s>>>(*m, *f, w->st);
+  // the reference recomputes the apparent charge afterwards (:333-439)
+  k_apparent_charge<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 1, w->part);
+  if (o->space_charge && np_bound > 0)
+    k_remove_charge<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, w->part);
+  return (int)cudaGetLastError();
+}
+
+// Downloads the last correction's report (synchronises the stream).
+extern "C" int spiffe_poisson64_report(Poisson64Work *w, spiffe_poisson_report *rep, cudaStream_t s)
+{
+  PcState st;
+  cudaMemcpyAsync(&st, w->st, sizeof(st), cudaMemcpyDeviceToHost, s);
+  cudaError_t e = cudaStreamSynchronize(s);
+  rep->ran = st.do_solve;
+  rep->iterations = st.iterations;
+  rep->Qreal = st.Qreal;
+  rep->Qerror = st.Qerror;
+  rep->Qsurface = st.Qsurface;
+  rep->residual = st.residual;
+  double drv = 0;
+  cudaMemcpy(&drv, w->scalars + 4, sizeof(double), cudaMemcpyDeviceToHost);
+  rep->driving = drv;
+  return (int)e;
+}
+
+extern "C" int spiffe_imposed_field64(const DevMesh *m, const DevFields<double> *f, double factor, cudaStream_t s)
+{
+  dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
+  k_imposed_field<<<grid, block, 0, s>>>(*m, *f, factor);
+  return (int)cudaGetLastError();
+}

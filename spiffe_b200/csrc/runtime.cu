@@ -1,0 +1,1245 @@
+// spiffe_b200/csrc/runtime.cu -- host runtime behind the C ABI (spiffe_b200.h).
+//
+// Owns the device mirror of one spiffe problem and drives the kernels in the
+// order perform_integration uses (integrate.c:134-194).  The host keeps only
+// what the reference keeps on the host between steps and what is cheap to
+// decide there: time, the emission counts of each cathode with the shared
+// counter-based generator (cathode.c:349-422), the antenna current
+// (antenna.c:374-418) and the Poisson interval test (poisson_correction.c:
+// 116-119).  Particle counts live on the device; the host tracks an upper
+// bound for launch sizes and reads the true count only when it must.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+#include "../../include/spiffe_b200.h"
+#include "../../include/spiffe_b200_rng.h"
+
+// ------------------------------------------------------- kernel modules
+struct Fdtd64Tables {
+  double *cpz = nullptr, *cmz = nullptr, *bzf = nullptr;
+  int *cut0 = nullptr, *cut1 = nullptr;
+  double fEr = 0, topf = 0, fEphi = 0;
+};
+extern "C" int spiffe_fdtd64_tables(const DevMesh *m, const int16_t *host_flags, Fdtd64Tables *t, cudaStream_t s);
+extern "C" void spiffe_fdtd64_tables_free(Fdtd64Tables *t);
+extern "C" int spiffe_fdtd64_step(const DevMesh *m, const DevFields<double> *f, const Fdtd64Tables *t, cudaStream_t s);
+
+struct Particles64Work {
+  uint8_t *lost = nullptr;
+  int *surv = nullptr, *surv_before = nullptr, *map = nullptr;
+  int *keys = nullptr, *keys_alt = nullptr;
+  double *vals = nullptr, *vals_alt = nullptr;
+  void *cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  long long capacity = 0;
+};
+extern "C" int spiffe_particles64_work(Particles64Work *w, long long capacity, bool ordered);
+extern "C" void spiffe_particles64_work_free(Particles64Work *w);
+extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const DevCounts *cnt,
+                                long long np_bound, bool ordered, Particles64Work *w, cudaStream_t s);
+struct PushHostParams {
+  double time, z_forces_start, QoMC, stiffness;
+  double tb_epm, tb_z_force, tb_r_force, tb_z_decel, tb_r_decel;
+  int screen_momentum, compaction;
+};
+extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const PushHostParams *hp,
+                             const DevScreens *scr, DevCounts *cnt, long long np_bound, Particles64Work *w,
+                             cudaStream_t s);
+
+struct PcState;
+struct Poisson64Work {
+  double *Az = nullptr, *Ari = nullptr, *Aro = nullptr, *volume = nullptr;
+  double *part = nullptr;
+  double *scalars = nullptr;
+  double *omega = nullptr;
+  long long omega_n = 0;
+  unsigned *bar = nullptr;
+  PcState *st = nullptr;
+  long long *iters = nullptr;
+  int sor_grid = 0;
+  size_t part_n = 0;
+};
+struct PoissonHostOptions {
+  double accuracy, error_charge_threshold;
+  long long maximum_iterations;
+  int guess_code, space_charge;
+};
+extern "C" int spiffe_poisson64_setup(const DevMesh *m, Poisson64Work *w, long long np_capacity, cudaStream_t s);
+extern "C" void spiffe_poisson64_free(Poisson64Work *w);
+extern "C" int spiffe_sor64(const DevMesh *m, Poisson64Work *w, double *Psi, const double *rhs, const int16_t *flags,
+                            double accuracy, long long limit, DevCounts *cnt, long long *iterations, cudaStream_t s);
+extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b,
+                                           DevCounts *cnt, long long np_bound, const PoissonHostOptions *o,
+                                           Poisson64Work *w, cudaStream_t s);
+extern "C" int spiffe_poisson64_report(Poisson64Work *w, spiffe_poisson_report *rep, cudaStream_t s);
+extern "C" int spiffe_imposed_field64(const DevMesh *m, const DevFields<double> *f, double factor, cudaStream_t s);
+
+struct BirthBin {
+  long long start, count;
+  double area, rmin;
+};
+struct BirthParams {
+  long long total;
+  uint64_t key, counter_base;
+  int mode;
+  int spread;
+  double z_position, inner_radius, outer_radius, inner_r2, dr2;
+  double initial_vz, initial_omega, Q, time, dt, QoMC, stiffness;
+  const BirthBin *bins;
+  int n_bins;
+};
+extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const BirthParams *p,
+                               DevCounts *cnt, cudaStream_t s);
+extern "C" int spiffe_antenna64(double *J, int pitch, int direction, long istart, long iend, long iposition,
+                                double value, cudaStream_t s);
+
+// ---------------------------------------------------------------- errors
+static thread_local std::string g_error;
+
+static int fail(int code, const char *fmt, ...)
+{
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_error = buf;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                          \
+  do {                                                                                       \
+    cudaError_t e_ = (x);                                                                    \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(SPIFFE_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString(e_));            \
+  } while (0)
+
+// Kernel-module helpers return a CUDA error code (> 0) or 0; runtime helpers
+// return 0 or a SPIFFE_ERR_* code with the message already set.
+#define RC_TRY(x)                                                                            \
+  do {                                                                                       \
+    const int rc_ = (x);                                                                     \
+    if (rc_ > 0)                                                                             \
+      return fail(SPIFFE_ERR_CUDA, "%s failed: %s", #x, cudaGetErrorString((cudaError_t)rc_)); \
+    if (rc_ < 0)                                                                             \
+      return rc_;                                                                            \
+  } while (0)
+
+// ------------------------------------------------------------- host state
+
+// One cathode as the reference holds it (CATHODE, spiffe.h:236-262).
+struct HostCathode {
+  spiffe_cathode_options o;
+  std::vector<double> prof_t, prof_A;
+  double initial_vz = 0, QoMC = 0, Q = 0, inner_r2 = 0, outer_r2 = 0, ref_current_density = 0, current_density = 0;
+  double totalArea = 0, start_time = 0, stop_time = 0, number_per_step = 0, electrons_per_macroparticle = 0;
+  long long start_step = -1, stop_step = 0, step_emission_started = -1, n_bins = 0, correction_interval = 0;
+  long long zoned_emission = 0;
+  std::vector<long> distribution, deficit;
+  std::vector<double> area, rmin;
+};
+
+struct HostAntenna {
+  int direction;
+  long istart, iend, iposition;
+  double current, frequency, phase;
+  std::vector<double> t, W;
+  long last_index = 0;
+};
+
+struct spiffe_gpu_instance {
+  int precision = SPIFFE_PRECISION_F64;
+  spiffe_mesh mesh{};
+  DevMesh dm{};
+  cudaStream_t stream = nullptr;
+  size_t nodes = 0;
+  std::vector<int16_t> h_flags;
+  int16_t *d_flags = nullptr;
+  DevFields<double> f{};
+  DevBeam64 b{};
+  long long capacity = 0, np_upper = 0;
+  DevCounts *cnt = nullptr, *h_cnt = nullptr;
+  DevScreens screens{};
+  Fdtd64Tables fdtd;
+  double fdtd_dt = -1;
+  Particles64Work pw;
+  Poisson64Work pcw;
+  bool pc_ready = false;
+  int deposit_ordered = 0;
+  // integration state
+  int space_charge = 0;
+  spiffe_push_options push{};
+  spiffe_poisson_options pc{};
+  long long pc_start_step = -1;
+  double last_imposed_factor = -1;
+  std::vector<HostCathode> cathodes;
+  uint64_t rng_key = 0, rng_counter = 0;
+  std::vector<HostAntenna> antennas;
+  double QoMC = 0, stiffness = 1;
+  BirthBin *d_bins = nullptr, *h_bins = nullptr;
+  size_t bins_n = 0;
+  double *h_probe = nullptr; // pinned scratch for single values
+};
+
+// ------------------------------------------------------------- utilities
+
+static void set_devmesh(spiffe_gpu_instance *in)
+{
+  const spiffe_mesh &m = in->mesh;
+  DevMesh &d = in->dm;
+  d.nz = m.nz;
+  d.nr = m.nr;
+  d.pitch = m.nr + 1;
+  d.zmin = m.zmin;
+  d.zmax = m.zmax;
+  d.rmax = m.rmax;
+  d.dz = m.dz;
+  d.dr = m.dr;
+  d.dt = m.dt;
+  d.lower_bc = m.lower_bc;
+  d.upper_bc = m.upper_bc;
+  d.right_bc = m.right_bc;
+  d.left_bc = m.left_bc;
+  d.modes = m.modes;
+  for (int k = 0; k < 3; k++) {
+    d.constE[k] = m.constant_E[k];
+    d.constB[k] = m.constant_B[k];
+  }
+  for (int k = 0; k < 6; k++)
+    d.turn_off[k] = m.turn_off[k];
+  d.has_solenoid = m.has_solenoid && in->f.BzImposed != nullptr;
+}
+
+static int alloc_field(double **p, size_t n, cudaStream_t s)
+{
+  CUDA_TRY(cudaMalloc(p, n * sizeof(double)));
+  CUDA_TRY(cudaMemsetAsync(*p, 0, n * sizeof(double), s));
+  return 0;
+}
+
+static int alloc_beam(DevBeam64 *b, long long n)
+{
+#define BA(x) CUDA_TRY(cudaMalloc(&b->x, sizeof(*b->x) * (size_t)n))
+  BA(z); BA(r); BA(pz); BA(pr); BA(r_pphi); BA(vz); BA(vr); BA(vphi); BA(Q);
+  BA(r0); BA(z0); BA(t0); BA(rmin); BA(rmax); BA(zmin); BA(zmax);
+  BA(particleID); BA(generation); BA(status);
+#undef BA
+  b->capacity = n;
+  return 0;
+}
+
+static void free_beam(DevBeam64 *b)
+{
+  void *p[] = {b->z, b->r, b->pz, b->pr, b->r_pphi, b->vz, b->vr, b->vphi, b->Q, b->r0, b->z0, b->t0,
+               b->rmin, b->rmax, b->zmin, b->zmax, b->particleID, b->generation, b->status};
+  for (void *q : p)
+    cudaFree(q);
+  *b = DevBeam64{};
+}
+
+// Grows the particle arrays so `need` particles fit (trealloc of cathode.c:427-456).
+static int grow_beam(spiffe_gpu_instance *in, long long need)
+{
+  if (need <= in->capacity)
+    return 0;
+  long long cap = in->capacity * 3 / 2;
+  if (cap < need + need / 10 + 1)
+    cap = need + need / 10 + 1;
+  DevBeam64 nb{};
+  RC_TRY(alloc_beam(&nb, cap));
+  const size_t n = (size_t)in->capacity;
+  cudaStream_t s = in->stream;
+#define CP(x) CUDA_TRY(cudaMemcpyAsync(nb.x, in->b.x, sizeof(*nb.x) * n, cudaMemcpyDeviceToDevice, s))
+  CP(z); CP(r); CP(pz); CP(pr); CP(r_pphi); CP(vz); CP(vr); CP(vphi); CP(Q);
+  CP(r0); CP(z0); CP(t0); CP(rmin); CP(rmax); CP(zmin); CP(zmax);
+  CP(particleID); CP(generation); CP(status);
+#undef CP
+  CUDA_TRY(cudaStreamSynchronize(s));
+  free_beam(&in->b);
+  in->b = nb;
+  in->capacity = cap;
+  RC_TRY(spiffe_particles64_work(&in->pw, cap, in->deposit_ordered));
+  if (in->pc_ready)
+    RC_TRY(spiffe_poisson64_setup(&in->dm, &in->pcw, cap, s));
+  return 0;
+}
+
+static int read_counts(spiffe_gpu_instance *in)
+{
+  CUDA_TRY(cudaMemcpyAsync(in->h_cnt, in->cnt, sizeof(DevCounts), cudaMemcpyDeviceToHost, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  in->np_upper = in->h_cnt->np;
+  if (in->h_cnt->error & SPIFFE_DEV_ERR_CAPACITY)
+    return fail(SPIFFE_ERR_CAPACITY, "particle capacity exceeded on the device");
+  if (in->h_cnt->error & SPIFFE_DEV_ERR_BARRIER)
+    return fail(SPIFFE_ERR_DEVICE, "Poisson solver grid barrier timed out");
+  if (in->h_cnt->screen_overflow)
+    return fail(SPIFFE_ERR_CAPACITY, "screen record capacity exceeded (%lld records dropped)",
+                in->h_cnt->screen_overflow);
+  return 0;
+}
+
+static int ensure_fdtd(spiffe_gpu_instance *in)
+{
+  if (in->fdtd_dt == in->mesh.dt)
+    return 0;
+  RC_TRY(spiffe_fdtd64_tables(&in->dm, in->h_flags.data(), &in->fdtd, in->stream));
+  in->fdtd_dt = in->mesh.dt;
+  return 0;
+}
+
+static int ensure_poisson(spiffe_gpu_instance *in)
+{
+  if (in->pc_ready)
+    return 0;
+  RC_TRY(spiffe_poisson64_setup(&in->dm, &in->pcw, in->capacity, in->stream));
+  in->pc_ready = true;
+  return 0;
+}
+
+// ------------------------------------------------------------------ C ABI
+
+extern "C" const char *spiffe_gpu_last_error(void) { return g_error.c_str(); }
+extern "C" const char *spiffe_gpu_version(void) { return "spiffe_b200 0.1 (sm_100a)"; }
+
+extern "C" int spiffe_gpu_create(const spiffe_mesh *mesh, const int16_t *flags, int32_t precision,
+                                 int64_t particle_capacity, spiffe_gpu_instance **out)
+{
+  if (!mesh || !flags || !out)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (precision != SPIFFE_PRECISION_F64)
+    return fail(SPIFFE_ERR_UNSUPPORTED, "this entry point builds the FP64 form; use spiffe_gpu_create_split32");
+  if (mesh->nz < 3 || mesh->nr < 4)
+    return fail(SPIFFE_ERR_INVALID, "mesh too small (nz=%d nr=%d; need nz>=3, nr>=4)", mesh->nz, mesh->nr);
+  if (!(mesh->dz > 0) || !(mesh->dr > 0))
+    return fail(SPIFFE_ERR_INVALID, "dz and dr must be positive");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(SPIFFE_ERR_CUDA, "no CUDA device available");
+  spiffe_gpu_instance *in = new spiffe_gpu_instance();
+  in->precision = precision;
+  in->mesh = *mesh;
+  in->nodes = (size_t)(mesh->nz + 1) * (size_t)(mesh->nr + 1);
+  in->h_flags.assign(flags, flags + in->nodes);
+  int rc = 0;
+  auto bail = [&](int code) {
+    spiffe_gpu_destroy(in);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&in->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_CUDA, "stream creation failed"));
+  cudaStream_t s = in->stream;
+  const size_t n = in->nodes;
+  if (cudaMalloc(&in->d_flags, n * sizeof(int16_t)) != cudaSuccess ||
+      cudaMemcpyAsync(in->d_flags, flags, n * sizeof(int16_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_NOMEM, "flag allocation failed"));
+  DevFields<double> &f = in->f;
+  f.flags = in->d_flags;
+  double **tm[] = {&f.Ez, &f.Er, &f.Bphi, &f.Bphi2, &f.Jz, &f.Jr, &f.EzImposed, &f.ErImposed, &f.PsiImposed, &f.Psi, &f.Q};
+  for (double **p : tm)
+    if ((rc = alloc_field(p, n, s)))
+      return bail(rc);
+  if (mesh->modes & SPIFFE_FL_TE_FIELDS) {
+    double **te[] = {&f.Ephi, &f.Jphi, &f.Br, &f.Br2, &f.Bz, &f.Bz2};
+    for (double **p : te)
+      if ((rc = alloc_field(p, n, s)))
+        return bail(rc);
+  }
+  in->capacity = particle_capacity > 1024 ? particle_capacity : 1024;
+  if ((rc = alloc_beam(&in->b, in->capacity)))
+    return bail(rc);
+  if (cudaMalloc(&in->cnt, sizeof(DevCounts)) != cudaSuccess ||
+      cudaMallocHost(&in->h_cnt, sizeof(DevCounts)) != cudaSuccess ||
+      cudaMallocHost(&in->h_probe, 8 * sizeof(double)) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_NOMEM, "counter allocation failed"));
+  memset(in->h_cnt, 0, sizeof(DevCounts));
+  in->h_cnt->nextParticleID = 1;
+  in->h_cnt->first_lost = 0x7fffffffffffffffLL;
+  if (cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_CUDA, "counter upload failed"));
+  if ((rc = spiffe_particles64_work(&in->pw, in->capacity, false)))
+    return bail(fail(SPIFFE_ERR_NOMEM, "particle work allocation failed"));
+  set_devmesh(in);
+  if (cudaStreamSynchronize(s) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_CUDA, "instance setup failed: %s", cudaGetErrorString(cudaGetLastError())));
+  *out = in;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return 0;
+  if (in->stream)
+    cudaStreamSynchronize(in->stream);
+  DevFields<double> &f = in->f;
+  void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
+               f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
+               in->cnt, in->d_bins};
+  for (void *q : p)
+    cudaFree(q);
+  for (int k = 0; k < in->screens.n; k++) {
+    DevScreen &sc = in->screens.s[k];
+    for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
+      cudaFree(sc.col[c]);
+    cudaFree(sc.rmin);
+    cudaFree(sc.rmax);
+    cudaFree(sc.zmin);
+    cudaFree(sc.zmax);
+    cudaFree(sc.generation);
+    cudaFree(sc.particleID);
+  }
+  free_beam(&in->b);
+  spiffe_fdtd64_tables_free(&in->fdtd);
+  spiffe_particles64_work_free(&in->pw);
+  spiffe_poisson64_free(&in->pcw);
+  if (in->h_cnt)
+    cudaFreeHost(in->h_cnt);
+  if (in->h_bins)
+    cudaFreeHost(in->h_bins);
+  if (in->h_probe)
+    cudaFreeHost(in->h_probe);
+  if (in->stream)
+    cudaStreamDestroy(in->stream);
+  delete in;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_mesh(spiffe_gpu_instance *in, const spiffe_mesh *m)
+{
+  if (!in || !m)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (m->nz != in->mesh.nz || m->nr != in->mesh.nr || m->dz != in->mesh.dz || m->dr != in->mesh.dr ||
+      m->zmin != in->mesh.zmin || (m->modes & 3u) != (in->mesh.modes & 3u))
+    return fail(SPIFFE_ERR_INVALID, "set_mesh cannot change the mesh geometry or field modes");
+  in->mesh = *m;
+  set_devmesh(in);
+  return 0;
+}
+
+extern "C" int spiffe_gpu_get_mesh(spiffe_gpu_instance *in, spiffe_mesh *m)
+{
+  if (!in || !m)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  *m = in->mesh;
+  return 0;
+}
+
+#define FIELD_LIST(X) X(Ez) X(Er) X(Bphi) X(Bphi2) X(Jz) X(Jr) X(Ephi) X(Jphi) X(Br) X(Br2) X(Bz) X(Bz2) \
+  X(EzImposed) X(ErImposed) X(PsiImposed) X(BzImposed) X(BrImposed) X(Psi) X(Q)
+
+extern "C" int spiffe_gpu_upload_fields(spiffe_gpu_instance *in, const spiffe_field_set *h)
+{
+  if (!in || !h)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const size_t bytes = in->nodes * sizeof(double);
+  cudaStream_t s = in->stream;
+  if (h->BzImposed && !in->f.BzImposed) {
+    RC_TRY(alloc_field(&in->f.BzImposed, in->nodes, s));
+    RC_TRY(alloc_field(&in->f.BrImposed, in->nodes, s));
+  }
+#define UP(x)                                                                                   \
+  if (h->x) {                                                                                   \
+    if (!in->f.x)                                                                               \
+      return fail(SPIFFE_ERR_INVALID, "array " #x " is not part of this instance's field modes"); \
+    CUDA_TRY(cudaMemcpyAsync(in->f.x, h->x, bytes, cudaMemcpyHostToDevice, s));                 \
+  }
+  FIELD_LIST(UP)
+#undef UP
+  set_devmesh(in);
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_download_fields(spiffe_gpu_instance *in, spiffe_field_set *h)
+{
+  if (!in || !h)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const size_t bytes = in->nodes * sizeof(double);
+  cudaStream_t s = in->stream;
+#define DOWN(x)                                                                 \
+  if (h->x && in->f.x)                                                          \
+    CUDA_TRY(cudaMemcpyAsync(h->x, in->f.x, bytes, cudaMemcpyDeviceToHost, s));
+  FIELD_LIST(DOWN)
+#undef DOWN
+  if (h->flags)
+    CUDA_TRY(cudaMemcpyAsync(h->flags, in->d_flags, in->nodes * sizeof(int16_t), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+#define BEAM_LIST(X) X(z) X(r) X(pz) X(pr) X(r_pphi) X(vz) X(vr) X(vphi) X(Q) X(r0) X(z0) X(t0) \
+  X(rmin) X(rmax) X(zmin) X(zmax) X(particleID) X(generation) X(status)
+
+extern "C" int spiffe_gpu_upload_beam(spiffe_gpu_instance *in, const spiffe_beam_set *h)
+{
+  if (!in || !h)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (h->np < 0)
+    return fail(SPIFFE_ERR_INVALID, "negative particle count");
+  RC_TRY(grow_beam(in, h->np));
+  cudaStream_t s = in->stream;
+  const size_t n = (size_t)h->np;
+#define UPB(x)                                                                                 \
+  if (n) {                                                                                     \
+    if (!h->x)                                                                                 \
+      return fail(SPIFFE_ERR_INVALID, "beam array " #x " missing");                            \
+    CUDA_TRY(cudaMemcpyAsync(in->b.x, h->x, sizeof(*h->x) * n, cudaMemcpyHostToDevice, s));    \
+  }
+  BEAM_LIST(UPB)
+#undef UPB
+  RC_TRY(read_counts(in));
+  in->h_cnt->np = h->np;
+  in->h_cnt->npActive = h->npActive;
+  in->h_cnt->nextParticleID = h->nextParticleID;
+  CUDA_TRY(cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  in->np_upper = h->np;
+  in->QoMC = h->QoMC;
+  in->stiffness = h->stiffness;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_download_beam(spiffe_gpu_instance *in, spiffe_beam_set *h)
+{
+  if (!in || !h)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(read_counts(in));
+  const long long np = in->h_cnt->np;
+  if (np > h->capacity)
+    return fail(SPIFFE_ERR_CAPACITY, "host beam holds %lld particles, device has %lld", (long long)h->capacity, np);
+  cudaStream_t s = in->stream;
+  const size_t n = (size_t)np;
+#define DOWNB(x)                                                                                \
+  if (n && h->x)                                                                                \
+    CUDA_TRY(cudaMemcpyAsync(h->x, in->b.x, sizeof(*h->x) * n, cudaMemcpyDeviceToHost, s));
+  BEAM_LIST(DOWNB)
+#undef DOWNB
+  CUDA_TRY(cudaStreamSynchronize(s));
+  h->np = np;
+  h->npActive = in->h_cnt->npActive;
+  h->nextParticleID = (int32_t)in->h_cnt->nextParticleID;
+  h->QoMC = in->QoMC;
+  h->stiffness = in->stiffness;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_deposit_order(spiffe_gpu_instance *in, int32_t ordered)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  in->deposit_ordered = ordered ? 1 : 0;
+  RC_TRY(spiffe_particles64_work(&in->pw, in->capacity, in->deposit_ordered));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_zero_current_arrays(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const size_t bytes = in->nodes * sizeof(double);
+  if (in->mesh.modes & SPIFFE_FL_TM_FIELDS) {
+    CUDA_TRY(cudaMemsetAsync(in->f.Jz, 0, bytes, in->stream));
+    CUDA_TRY(cudaMemsetAsync(in->f.Jr, 0, bytes, in->stream));
+  }
+  if (in->mesh.modes & SPIFFE_FL_TE_FIELDS)
+    CUDA_TRY(cudaMemsetAsync(in->f.Jphi, 0, bytes, in->stream));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_advance_field_solutions(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(ensure_fdtd(in));
+  const int rc = spiffe_fdtd64_step(&in->dm, &in->f, &in->fdtd, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "FDTD launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_add_particle_currents(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const int rc = spiffe_deposit64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, in->deposit_ordered, &in->pw,
+                                  in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "deposition launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiffe_push_options *o)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (o->tb_electrons_per_macroparticle)
+    in->stiffness = 1; // advance_particles.c:280-281
+  PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
+                   o->tb_z_force, o->tb_r_force, o->tb_z_start_deceleration, o->tb_r_start_deceleration,
+                   o->screen_momentum, o->compaction};
+  const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *in, int32_t target, double accuracy,
+                                            int64_t limit, int64_t *iterations)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (accuracy <= 0)
+    return fail(SPIFFE_ERR_INVALID, "accuracy is <= 0 in solve_poisson_cyl"); // poisson.c:27-28
+  if (limit <= 1)
+    return fail(SPIFFE_ERR_INVALID, "iteration_limit is <= 1 in solve_poisson_cyl"); // poisson.c:29-30
+  RC_TRY(ensure_poisson(in));
+  long long it = 0;
+  double *psi = target ? in->f.PsiImposed : in->f.Psi;
+  const double *rhs = target ? nullptr : in->f.Q;
+  const int rc = spiffe_sor64(&in->dm, &in->pcw, psi, rhs, in->d_flags, accuracy, limit, in->cnt, &it, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "SOR launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  RC_TRY(read_counts(in));
+  if (iterations)
+    *iterations = it;
+  return 0;
+}
+
+static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const spiffe_poisson_options *o)
+{
+  // poisson_correction.c:84-119
+  if (o->maximum_iterations <= 0)
+    return 0;
+  if (in->pc_start_step == -1) {
+    if (in->mesh.dt <= 0)
+      return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (add_poisson_correction)");
+    in->pc_start_step = (long long)((o->start_time - in->mesh.start_time) / in->mesh.dt);
+  }
+  if (o->step_interval <= 0 || in->mesh.time_step % o->step_interval != 0 || in->pc_start_step > in->mesh.time_step)
+    return 0;
+  RC_TRY(ensure_poisson(in));
+  PoissonHostOptions h{o->accuracy, o->error_charge_threshold, o->maximum_iterations, o->guess_code, space_charge};
+  const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 1;
+}
+
+extern "C" int spiffe_gpu_add_poisson_correction(spiffe_gpu_instance *in, int32_t space_charge,
+                                                 const spiffe_poisson_options *o, spiffe_poisson_report *rep)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const int ran = poisson_correction(in, space_charge, o);
+  if (ran < 0)
+    return ran;
+  if (rep) {
+    memset(rep, 0, sizeof(*rep));
+    if (ran) {
+      RC_TRY(spiffe_poisson64_report(&in->pcw, rep, in->stream));
+      RC_TRY(read_counts(in));
+    }
+  }
+  return 0;
+}
+
+// compute_imposed_Efield, poisson_correction.c:456-562
+static int imposed_efield(spiffe_gpu_instance *in, const spiffe_poisson_options *o, int initialize)
+{
+  if (o->maximum_iterations <= 0)
+    return 0;
+  if (in->pc_start_step == -1) {
+    if (in->mesh.dt <= 0)
+      return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (compute_imposed_Efield)");
+    in->pc_start_step = (long long)((o->start_time - in->mesh.start_time) / in->mesh.dt);
+  }
+  if (initialize) {
+    RC_TRY(ensure_poisson(in));
+    const int rc = spiffe_sor64(&in->dm, &in->pcw, in->f.PsiImposed, nullptr, in->d_flags, o->accuracy,
+                                o->maximum_iterations, in->cnt, nullptr, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "SOR launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  }
+  const double T = in->mesh.imposed_ramp_time, F = in->mesh.imposed_flat_top_time, t = in->mesh.time;
+  double ff = 1;
+  if (T) {
+    if (t < T)
+      ff = t / T;
+    else if (t < (T + F))
+      ff = 1;
+    else if (t < (2 * T + F))
+      ff = ((2 * T + F) - t) / T;
+    else
+      ff = 0;
+    if (ff < 0)
+      ff = 0;
+  }
+  if (ff == in->last_imposed_factor)
+    return 0;
+  in->last_imposed_factor = ff;
+  const int rc = spiffe_imposed_field64(&in->dm, &in->f, ff, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "imposed field launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_compute_imposed_efield(spiffe_gpu_instance *in, const spiffe_poisson_options *o,
+                                                 int32_t initialize)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(imposed_efield(in, o, initialize));
+  return 0;
+}
+
+// ----------------------------------------------------------------- screens
+
+extern "C" int spiffe_gpu_add_screen(spiffe_gpu_instance *in, double z_position, int32_t direction, int64_t capacity)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->screens.n >= SPIFFE_MAX_SCREENS)
+    return fail(SPIFFE_ERR_INVALID, "at most %d screens", SPIFFE_MAX_SCREENS);
+  if (direction != 1 && direction != -1)
+    return fail(SPIFFE_ERR_INVALID, "screen direction must be +1 or -1");
+  if (capacity <= 0)
+    return fail(SPIFFE_ERR_INVALID, "screen capacity must be positive");
+  DevScreen &sc = in->screens.s[in->screens.n];
+  sc = DevScreen{};
+  sc.z_position = z_position;
+  sc.direction = direction;
+  sc.capacity = capacity;
+  const size_t n = (size_t)capacity;
+  for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
+    CUDA_TRY(cudaMalloc(&sc.col[c], n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&sc.rmin, n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&sc.rmax, n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&sc.zmin, n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&sc.zmax, n * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&sc.generation, n * sizeof(int16_t)));
+  CUDA_TRY(cudaMalloc(&sc.particleID, n * sizeof(int32_t)));
+  in->screens.n++;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_screen_count(spiffe_gpu_instance *in, int32_t is, int64_t *nb)
+{
+  if (!in || !nb || is < 0 || is >= in->screens.n)
+    return fail(SPIFFE_ERR_INVALID, "bad screen index");
+  RC_TRY(read_counts(in));
+  const long long n = in->h_cnt->screen_nb[is];
+  *nb = n < in->screens.s[is].capacity ? n : in->screens.s[is].capacity;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_download_screen(spiffe_gpu_instance *in, int32_t is, spiffe_screen_set *h)
+{
+  int64_t nb = 0;
+  RC_TRY(spiffe_gpu_screen_count(in, is, &nb));
+  if (nb > h->capacity)
+    return fail(SPIFFE_ERR_CAPACITY, "host screen buffer holds %lld records, device has %lld", (long long)h->capacity,
+                (long long)nb);
+  const DevScreen &sc = in->screens.s[is];
+  cudaStream_t s = in->stream;
+  const size_t n = (size_t)nb;
+  if (n) {
+    for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
+      if (h->col[c])
+        CUDA_TRY(cudaMemcpyAsync(h->col[c], sc.col[c], n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->rmin) CUDA_TRY(cudaMemcpyAsync(h->rmin, sc.rmin, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->rmax) CUDA_TRY(cudaMemcpyAsync(h->rmax, sc.rmax, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->zmin) CUDA_TRY(cudaMemcpyAsync(h->zmin, sc.zmin, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->zmax) CUDA_TRY(cudaMemcpyAsync(h->zmax, sc.zmax, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->generation)
+      CUDA_TRY(cudaMemcpyAsync(h->generation, sc.generation, n * sizeof(int16_t), cudaMemcpyDeviceToHost, s));
+    if (h->particleID)
+      CUDA_TRY(cudaMemcpyAsync(h->particleID, sc.particleID, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  h->nb = nb;
+  h->z_position = sc.z_position;
+  h->direction = sc.direction;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_clear_screens(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(read_counts(in));
+  for (int k = 0; k < SPIFFE_MAX_SCREENS; k++)
+    in->h_cnt->screen_nb[k] = 0;
+  in->h_cnt->screen_overflow = 0;
+  CUDA_TRY(cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  return 0;
+}
+
+// ---------------------------------------------------------------- cathodes
+
+// process_cathode_definition, cathode.c:21-237.
+extern "C" int spiffe_gpu_add_cathode(spiffe_gpu_instance *in, const spiffe_cathode_options *o)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const spiffe_mesh &m = in->mesh;
+  if (o->z_position < m.zmin || o->z_position > m.zmax)
+    return fail(SPIFFE_ERR_INVALID, "cathode is outside of simulation region");
+  if (o->inner_radius > o->outer_radius)
+    return fail(SPIFFE_ERR_INVALID, "cathode has negative radial extent");
+  if (o->inner_radius == o->outer_radius && o->current_density != 0)
+    return fail(SPIFFE_ERR_INVALID, "cathode has zero radial extent--specify electrons_per_macroparticle instead of current_density");
+  if (o->inner_radius < 0 || o->outer_radius > m.rmax)
+    return fail(SPIFFE_ERR_INVALID, "all or part of cathode is outside of simulation region");
+  if (!o->field_emission && o->current_density <= 0 && o->electrons_per_macroparticle == 0 && o->temperature <= 0)
+    return fail(SPIFFE_ERR_INVALID, "either field_emission, current_density, electrons_per_macroparticle, or temperature must be non-zero");
+  if (o->current_density < 0)
+    return fail(SPIFFE_ERR_INVALID, "the current density should be a positive quantity");
+  if (o->electrons_per_macroparticle < 0)
+    return fail(SPIFFE_ERR_INVALID, "electrons_per_macroparticle should be a positive quantity");
+  if (o->stop_time && o->start_time > o->stop_time)
+    return fail(SPIFFE_ERR_INVALID, "stop_time is non-zero and less than start_time");
+  if (o->distribution_correction_interval < 0)
+    return fail(SPIFFE_ERR_INVALID, "distribution_correction_interval < 0");
+  if (o->distribution_correction_interval && o->discretize_radii)
+    return fail(SPIFFE_ERR_INVALID, "distribution correction and discrete radii are incompatible");
+  if (o->stiffness <= 0)
+    return fail(SPIFFE_ERR_INVALID, "stiffness <= 0");
+  if (std::fabs(o->initial_omega * o->outer_radius) >= SPIFFE_C_MKS)
+    return fail(SPIFFE_ERR_INVALID, "initial_omega*outer_radius >= c---unphysical");
+  if (o->random_number_seed == 0)
+    return fail(SPIFFE_ERR_INVALID, "random_number_seed must be non-zero (a clock seed is not reproducible)");
+  if (o->n_profile) {
+    if (o->distribution_correction_interval)
+      return fail(SPIFFE_ERR_INVALID, "can't do distribution correction with an emission profile");
+    for (int i = 1; i < o->n_profile; i++)
+      if (o->profile_t[i - 1] >= o->profile_t[i])
+        return fail(SPIFFE_ERR_INVALID, "profile data is not ordered by increasing time values");
+  }
+  long n = 1;
+  if (o->field_emission) {
+    if (o->inner_radius != 0)
+      n = (long)((o->outer_radius - o->inner_radius) / m.dr);
+    else
+      n = (long)((o->outer_radius - o->inner_radius + m.dr / 2) / m.dr);
+  }
+  const long seed = o->random_number_seed < 0 ? -(long)o->random_number_seed : o->random_number_seed;
+  in->rng_key = spiffe_rng_key((uint64_t)seed); // random_1(-abs(seed)), cathode.c:90
+  in->rng_counter = 0;
+  for (long i = 0; i < n; i++) {
+    HostCathode c;
+    c.o = *o;
+    if (o->n_profile) {
+      c.prof_t.assign(o->profile_t, o->profile_t + o->n_profile);
+      c.prof_A.assign(o->profile_A, o->profile_A + o->n_profile);
+    }
+    c.o.profile_t = c.o.profile_A = nullptr;
+    if (o->field_emission) {
+      c.o.outer_radius = (i + 0.5) * m.dr;
+      if ((c.o.inner_radius = c.o.outer_radius - m.dr) < 0)
+        c.o.inner_radius = 0;
+      if (i == n - 1)
+        c.o.outer_radius = o->outer_radius;
+      if (c.o.outer_radius > o->outer_radius)
+        c.o.outer_radius = o->outer_radius;
+      if (c.o.inner_radius < o->inner_radius)
+        c.o.inner_radius = o->inner_radius;
+    }
+    c.initial_vz = o->initial_pz / std::sqrt(1 + o->initial_pz * o->initial_pz) * SPIFFE_C_MKS;
+    c.current_density = o->current_density;
+    c.start_time = o->start_time;
+    c.stop_time = o->stop_time;
+    c.number_per_step = o->number_per_step;
+    c.QoMC = -SPIFFE_E_MKS / (SPIFFE_ME_MKS * SPIFFE_C_MKS);
+    c.correction_interval = o->distribution_correction_interval;
+    c.electrons_per_macroparticle = o->electrons_per_macroparticle;
+    c.zoned_emission = o->zoned_emission;
+    if (o->discretize_radii)
+      c.correction_interval = 0;
+    if (o->field_emission)
+      c.zoned_emission = 0;
+    if (!c.zoned_emission)
+      c.correction_interval = 0;
+    in->cathodes.push_back(std::move(c));
+  }
+  return 0;
+}
+
+static double profile_value(const HostCathode &c, double t)
+{
+  const long n = (long)c.prof_t.size();
+  long lo = 0, hi = n - 1;
+  if (t <= c.prof_t[0])
+    return c.prof_A[0];
+  if (t >= c.prof_t[hi])
+    return c.prof_A[hi];
+  while (hi - lo > 1) {
+    const long mid = (lo + hi) / 2;
+    if (c.prof_t[mid] <= t)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return c.prof_A[lo] + (c.prof_A[hi] - c.prof_A[lo]) / (c.prof_t[hi] - c.prof_t[lo]) * (t - c.prof_t[lo]);
+}
+
+static double rng_next(spiffe_gpu_instance *in) { return spiffe_rng_uniform(in->rng_key, ++in->rng_counter); }
+
+static int ensure_bins(spiffe_gpu_instance *in, size_t n)
+{
+  if (in->bins_n >= n)
+    return 0;
+  cudaFree(in->d_bins);
+  if (in->h_bins)
+    cudaFreeHost(in->h_bins);
+  CUDA_TRY(cudaMalloc(&in->d_bins, n * sizeof(BirthBin)));
+  CUDA_TRY(cudaMallocHost(&in->h_bins, n * sizeof(BirthBin)));
+  in->bins_n = n;
+  return 0;
+}
+
+// emit_electrons_from_cathode, cathode.c:239-671: counts on the host, births on the device.
+static int emit(spiffe_gpu_instance *in)
+{
+  const spiffe_mesh &m = in->mesh;
+  for (HostCathode &c : in->cathodes) {
+    if (c.number_per_step == 0 && c.electrons_per_macroparticle == 0)
+      continue;
+    if (c.start_step == -1) {
+      if (c.current_density <= 1. / std::sqrt(1.7976931348623157e308))
+        continue;
+      c.ref_current_density = c.current_density;
+      if (c.o.autophase) {
+        c.stop_time = (c.stop_time - c.start_time) + m.time + c.o.time_offset;
+        c.start_time = m.time + c.o.time_offset;
+      }
+      if (m.dt <= 0)
+        return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (emit_electrons_from_cathode)");
+      c.inner_r2 = c.o.inner_radius * c.o.inner_radius;
+      c.outer_r2 = c.o.outer_radius * c.o.outer_radius;
+      double area;
+      if ((area = SPIFFE_PI * (c.outer_r2 - c.inner_r2)) != 0) {
+        if (c.electrons_per_macroparticle) {
+          c.number_per_step = area * m.dt * c.current_density / (SPIFFE_E_MKS * c.electrons_per_macroparticle);
+          if (c.number_per_step == 0)
+            continue;
+        } else
+          c.electrons_per_macroparticle = area * m.dt * c.current_density / (SPIFFE_E_MKS * c.number_per_step);
+      } else {
+        c.correction_interval = 0;
+        c.n_bins = 1;
+      }
+      c.start_step = (long long)((c.start_time - m.start_time) / m.dt);
+      if (c.stop_time && c.stop_time > m.start_time)
+        c.stop_step = (long long)((c.stop_time - m.start_time) / m.dt);
+      else
+        c.stop_step = 0x7fffffffffffffffLL;
+      c.Q = -SPIFFE_E_MKS * c.electrons_per_macroparticle;
+      c.n_bins = (long long)((c.o.outer_radius - c.o.inner_radius) / m.dr + 1);
+      c.distribution.assign((size_t)c.n_bins, 0);
+      c.deficit.assign((size_t)c.n_bins, 0);
+      c.area.assign((size_t)c.n_bins, 0);
+      c.rmin.assign((size_t)c.n_bins, 0);
+      c.totalArea = 0;
+      for (long long ib = 0; ib < c.n_bins; ib++) {
+        const long ir = (long)(c.o.inner_radius / m.dr + ib);
+        if (ir == 0) {
+          const double r_max = m.dr / 2;
+          c.area[ib] = r_max * r_max * SPIFFE_PI;
+          c.rmin[ib] = 0;
+        } else {
+          const double r_min = m.dr * (ir - 0.5), r_max = m.dr * (ir + 0.5);
+          c.area[ib] = SPIFFE_PI * (r_max * r_max - r_min * r_min);
+          c.rmin[ib] = r_min;
+          c.totalArea += c.area[ib];
+        }
+      }
+    }
+    double profile_factor = 1;
+    if (!c.prof_t.empty()) {
+      if (m.time >= c.prof_t.front() && m.time <= c.prof_t.back())
+        profile_factor = profile_value(c, m.time);
+      else
+        profile_factor = 0;
+    }
+    if (c.start_step > m.time_step || c.stop_step < m.time_step)
+      continue;
+    if (c.step_emission_started < 0)
+      c.step_emission_started = m.time_step;
+    const double dr2 = (c.outer_r2 - c.inner_r2) / c.number_per_step;
+    const double total_area = c.totalArea;
+    const double totalNominal = c.number_per_step * (c.current_density / c.ref_current_density);
+    long long total;
+    if (c.correction_interval && m.time_step % c.correction_interval == 0) {
+      total = 0;
+      for (long long ib = 0; ib < c.n_bins; ib++) {
+        if ((c.deficit[ib] = (long)((m.time_step - c.step_emission_started + 1) * (c.area[ib] / total_area) *
+                                        totalNominal +
+                                    0.5) -
+                             c.distribution[ib]) <= 0)
+          c.deficit[ib] = 0;
+        total += c.deficit[ib];
+      }
+    } else if (c.zoned_emission) {
+      total = 0;
+      for (long long ib = 0; ib < c.n_bins; ib++) {
+        if (total_area) {
+          double fnumber = profile_factor * (c.area[ib] / total_area) * totalNominal;
+          if (fnumber > 1) {
+            c.deficit[ib] = (long)fnumber;
+            fnumber -= c.deficit[ib];
+          } else
+            c.deficit[ib] = 0;
+          if (fnumber && fnumber > rng_next(in))
+            c.deficit[ib] += 1;
+          total += c.deficit[ib];
+        }
+      }
+    } else {
+      double fnumber = totalNominal * profile_factor;
+      total = (long)fnumber;
+      fnumber -= (long)fnumber;
+      if (fnumber && fnumber > rng_next(in))
+        total += 1;
+    }
+    if (total < 0)
+      return fail(SPIFFE_ERR_INVALID, "negative number of particles created!");
+    if (!total)
+      continue;
+    // make room: the bound is exact enough unless many particles were lost
+    if (in->np_upper + total > in->capacity) {
+      RC_TRY(read_counts(in));
+      RC_TRY(grow_beam(in, in->h_cnt->np + total));
+    }
+    BirthParams p{};
+    p.total = total;
+    p.key = in->rng_key;
+    p.counter_base = in->rng_counter;
+    p.spread = c.o.spread_over_dt;
+    p.z_position = c.o.z_position;
+    p.inner_radius = c.o.inner_radius;
+    p.outer_radius = c.o.outer_radius;
+    p.inner_r2 = c.inner_r2;
+    p.dr2 = dr2;
+    p.initial_vz = c.initial_vz;
+    p.initial_omega = c.o.initial_omega;
+    p.Q = c.Q;
+    p.time = m.time;
+    p.dt = m.dt;
+    p.QoMC = c.QoMC;
+    p.stiffness = c.o.stiffness;
+    if (c.correction_interval) {
+      RC_TRY(ensure_bins(in, (size_t)c.n_bins));
+      CUDA_TRY(cudaStreamSynchronize(in->stream)); // the pinned bin table may still be in flight
+      long long start = 0;
+      for (long long ib = 0; ib < c.n_bins; ib++) {
+        in->h_bins[ib] = BirthBin{start, c.deficit[ib], c.area[ib], c.rmin[ib]};
+        start += c.deficit[ib];
+        c.distribution[ib] += c.deficit[ib];
+      }
+      CUDA_TRY(cudaMemcpyAsync(in->d_bins, in->h_bins, (size_t)c.n_bins * sizeof(BirthBin), cudaMemcpyHostToDevice,
+                               in->stream));
+      p.mode = 1;
+      p.bins = in->d_bins;
+      p.n_bins = (int)c.n_bins;
+      in->rng_counter += (uint64_t)total;
+    } else if (!c.o.discretize_radii) {
+      p.mode = 0;
+      in->rng_counter += (uint64_t)total;
+    } else {
+      p.mode = 2;
+    }
+    const int rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "birth launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    in->np_upper += total;
+    in->QoMC = c.QoMC; // cathode.c:661-663
+    in->stiffness = c.o.stiffness;
+  }
+  return 0;
+}
+
+// set_current_density, cathode.c:673-715
+static int set_current_density(spiffe_gpu_instance *in)
+{
+  const spiffe_mesh &m = in->mesh;
+  for (HostCathode &c : in->cathodes) {
+    const bool schottky = c.o.temperature > 0 && c.o.work_function;
+    if (!schottky && !c.o.field_emission)
+      continue;
+    long iz = (long)((c.o.z_position - m.zmin) / m.dz + 1.5), ir = (long)((c.o.inner_radius + c.o.outer_radius) / 2 / m.dr);
+    if (iz <= 0)
+      iz = 1;
+    double Ez = m.constant_E[0];
+    if (m.modes & SPIFFE_FL_TM_FIELDS) {
+      const size_t i = node((int)iz, (int)ir, m.nr + 1);
+      CUDA_TRY(cudaMemcpyAsync(in->h_probe, in->f.Ez + i, sizeof(double), cudaMemcpyDeviceToHost, in->stream));
+      CUDA_TRY(cudaMemcpyAsync(in->h_probe + 1, in->f.EzImposed + i, sizeof(double), cudaMemcpyDeviceToHost, in->stream));
+      CUDA_TRY(cudaStreamSynchronize(in->stream));
+      Ez += in->h_probe[0] + in->h_probe[1];
+    }
+    if (Ez >= 0 && c.initial_vz <= 0)
+      continue;
+    if (schottky) {
+      double wf = 0.012 * std::sqrt(std::fabs(Ez * 1e-5));
+      if (wf > c.o.work_function)
+        wf = c.o.work_function;
+      c.current_density = 60e4 * c.o.temperature * c.o.temperature *
+                          std::exp(-(c.o.work_function - wf) / (c.o.temperature * SPIFFE_KB_MKS / SPIFFE_E_MKS));
+    } else {
+      double E = std::fabs(Ez) * c.o.field_emission_beta;
+      const double y = 3.79e-5 * std::sqrt(E) / c.o.work_function;
+      const double t = ((-0.0020 * y + 0.0131) * y + 0.1091) * y + 0.9899;
+      const double v = ((0.0445 * y - 0.6782) * y - 0.4091) * y + 1.0437;
+      c.current_density = 1.54e-6 * E * E / (c.o.work_function * t * t) *
+                          std::exp(-6.83e9 * v * std::pow(c.o.work_function, 1.5) / E);
+    }
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_add_antenna(spiffe_gpu_instance *in, int32_t direction, int64_t istart, int64_t iend,
+                                      int64_t iposition, double current, double frequency, double phase,
+                                      const double *t, const double *W, int64_t n)
+{
+  if (!in || !t || !W)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (n <= 2)
+    return fail(SPIFFE_ERR_INVALID, "SDDS waveform file empty or invalid");
+  if (frequency <= 0)
+    return fail(SPIFFE_ERR_INVALID, "antenna frequency <= 0");
+  if (direction < 0 || direction > 2 || (direction == 2 && !(in->mesh.modes & SPIFFE_FL_TE_FIELDS)))
+    return fail(SPIFFE_ERR_INVALID, "bad antenna direction");
+  const long lim_a = direction == 1 ? in->mesh.nr : in->mesh.nz, lim_b = direction == 1 ? in->mesh.nz : in->mesh.nr;
+  if (istart < 0 || iend > lim_a || iposition < 0 || iposition > lim_b)
+    return fail(SPIFFE_ERR_INVALID, "antenna indices out of range");
+  for (int64_t i = 1; i < n; i++)
+    if (t[i - 1] >= t[i])
+      return fail(SPIFFE_ERR_INVALID, "waveform data is not ordered by increasing time index");
+  HostAntenna a;
+  a.direction = direction;
+  a.istart = (long)istart;
+  a.iend = (long)iend;
+  a.iposition = (long)iposition;
+  a.current = current;
+  a.frequency = frequency;
+  a.phase = phase;
+  a.t.assign(t, t + n);
+  a.W.assign(W, W + n);
+  in->antennas.push_back(std::move(a));
+  return 0;
+}
+
+// add_antenna_excitation, antenna.c:374-418
+static int antennas(spiffe_gpu_instance *in, double time)
+{
+  for (HostAntenna &a : in->antennas) {
+    const long n_pts = (long)a.t.size();
+    double J;
+    if (time <= a.t[0])
+      J = a.W[0];
+    else if (time > a.t[n_pts - 1] || a.last_index >= (n_pts - 1))
+      J = a.W[n_pts - 1];
+    else {
+      long i = a.last_index;
+      while (i < n_pts - 2 && time >= a.t[i + 1])
+        i++;
+      a.last_index = i;
+      J = (a.W[i + 1] - a.W[i]) / (a.t[i + 1] - a.t[i]) * (time - a.t[i]) + a.W[i];
+    }
+    J *= a.current * std::sin(SPIFFE_PIx2 * a.frequency * time + a.phase);
+    double *arr = a.direction == 0 ? in->f.Jz : (a.direction == 1 ? in->f.Jr : in->f.Jphi);
+    const int rc = spiffe_antenna64(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "antenna launch failed");
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_configure_run(spiffe_gpu_instance *in, int32_t space_charge, const spiffe_push_options *push,
+                                        const spiffe_poisson_options *pc)
+{
+  if (!in || !push)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  in->space_charge = space_charge;
+  in->push = *push;
+  if (pc)
+    in->pc = *pc;
+  else
+    memset(&in->pc, 0, sizeof(in->pc));
+  if (space_charge)
+    in->mesh.modes |= SPIFFE_FL_SPACE_CHARGE;
+  set_devmesh(in);
+  return 0;
+}
+
+// setup before the loop, integrate.c:125-133
+extern "C" int spiffe_gpu_run_begin(spiffe_gpu_instance *in, spiffe_poisson_report *rep)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(imposed_efield(in, &in->pc, 1));
+  const int ran = poisson_correction(in, in->space_charge, &in->pc);
+  if (ran < 0)
+    return ran;
+  if (rep) {
+    memset(rep, 0, sizeof(*rep));
+    if (ran)
+      RC_TRY(spiffe_poisson64_report(&in->pcw, rep, in->stream));
+  }
+  RC_TRY(set_current_density(in));
+  return 0;
+}
+
+// The perform_integration loop body, integrate.c:136-193.
+extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  spiffe_mesh &m = in->mesh;
+  for (int64_t k = 0; k < n_steps; k++) {
+    if (m.imposed_ramp_time > 0)
+      RC_TRY(imposed_efield(in, &in->pc, 0));
+    m.time = m.time_step * m.dt + m.start_time;
+    RC_TRY(emit(in));
+    RC_TRY(spiffe_gpu_zero_current_arrays(in));
+    if (in->space_charge)
+      RC_TRY(spiffe_gpu_add_particle_currents(in));
+    RC_TRY(antennas(in, m.time + m.dt / 2));
+    const int ran = poisson_correction(in, in->space_charge, &in->pc);
+    if (ran < 0)
+      return ran;
+    RC_TRY(spiffe_gpu_advance_field_solutions(in));
+    RC_TRY(spiffe_gpu_advance_particles(in, &in->push));
+    RC_TRY(set_current_density(in));
+    m.time_step++;
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_synchronize(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(read_counts(in));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_counts(spiffe_gpu_instance *in, int64_t *np, int64_t *np_active)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(read_counts(in));
+  if (np)
+    *np = in->h_cnt->np;
+  if (np_active)
+    *np_active = in->h_cnt->npActive;
+  return 0;
+}

@@ -1,0 +1,219 @@
+"""Python binding of libspiffe_b200 (the CUDA implementation, C ABI).
+
+`GpuInstance` mirrors the reference's per-step functions on one device-
+resident problem: advance_field_solutions, add_particle_currents,
+advance_particles, solve_poisson_cyl, add_poisson_correction and the whole
+perform_integration loop.  State moves through abi.Fields / abi.Beam /
+abi.Screen.  There is no fallback: if the shared library or a GPU is
+missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libspiffe_b200.so")
+
+PRECISION_F64 = 0
+PRECISION_SPLIT32 = 1
+
+_lib = None
+P = C.POINTER
+H = C.c_void_p
+
+
+class SpiffeGpuError(RuntimeError):
+    pass
+
+
+def load():
+    """Loads libspiffe_b200.so (raises when it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise SpiffeGpuError(f"{LIB_PATH} is missing: build it with `make -C spiffe_b200/csrc`")
+    lib = C.CDLL(LIB_PATH)
+    M, F, B, S = P(abi.Mesh), P(abi.FieldSet), P(abi.BeamSet), P(abi.ScreenSet)
+    sig = {
+        "spiffe_gpu_last_error": ([], C.c_char_p),
+        "spiffe_gpu_version": ([], C.c_char_p),
+        "spiffe_gpu_create": ([M, P(C.c_int16), C.c_int32, C.c_int64, P(H)], C.c_int),
+        "spiffe_gpu_destroy": ([H], C.c_int),
+        "spiffe_gpu_set_mesh": ([H, M], C.c_int),
+        "spiffe_gpu_get_mesh": ([H, M], C.c_int),
+        "spiffe_gpu_upload_fields": ([H, F], C.c_int),
+        "spiffe_gpu_download_fields": ([H, F], C.c_int),
+        "spiffe_gpu_upload_beam": ([H, B], C.c_int),
+        "spiffe_gpu_download_beam": ([H, B], C.c_int),
+        "spiffe_gpu_set_deposit_order": ([H, C.c_int32], C.c_int),
+        "spiffe_gpu_zero_current_arrays": ([H], C.c_int),
+        "spiffe_gpu_advance_field_solutions": ([H], C.c_int),
+        "spiffe_gpu_add_particle_currents": ([H], C.c_int),
+        "spiffe_gpu_advance_particles": ([H, P(abi.PushOptions)], C.c_int),
+        "spiffe_gpu_solve_poisson_cyl": ([H, C.c_int32, C.c_double, C.c_int64, P(C.c_int64)], C.c_int),
+        "spiffe_gpu_add_poisson_correction": ([H, C.c_int32, P(abi.PoissonOptions), P(abi.PoissonReport)], C.c_int),
+        "spiffe_gpu_compute_imposed_efield": ([H, P(abi.PoissonOptions), C.c_int32], C.c_int),
+        "spiffe_gpu_add_screen": ([H, C.c_double, C.c_int32, C.c_int64], C.c_int),
+        "spiffe_gpu_screen_count": ([H, C.c_int32, P(C.c_int64)], C.c_int),
+        "spiffe_gpu_download_screen": ([H, C.c_int32, S], C.c_int),
+        "spiffe_gpu_clear_screens": ([H], C.c_int),
+        "spiffe_gpu_add_cathode": ([H, P(abi.CathodeOptions)], C.c_int),
+        "spiffe_gpu_add_antenna": ([H, C.c_int32, C.c_int64, C.c_int64, C.c_int64, C.c_double, C.c_double,
+                                    C.c_double, P(C.c_double), P(C.c_double), C.c_int64], C.c_int),
+        "spiffe_gpu_configure_run": ([H, C.c_int32, P(abi.PushOptions), P(abi.PoissonOptions)], C.c_int),
+        "spiffe_gpu_run_begin": ([H, P(abi.PoissonReport)], C.c_int),
+        "spiffe_gpu_run_steps": ([H, C.c_int64], C.c_int),
+        "spiffe_gpu_synchronize": ([H], C.c_int),
+        "spiffe_gpu_counts": ([H, P(C.c_int64), P(C.c_int64)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise SpiffeGpuError(f"spiffe_b200 error {rc}: {load().spiffe_gpu_last_error().decode()}")
+
+
+class GpuInstance:
+    """One spiffe problem resident on the GPU."""
+
+    def __init__(self, fields, capacity=1 << 16, precision=PRECISION_F64):
+        lib = load()
+        self.lib = lib
+        self.precision = precision
+        self.shape = fields.shape
+        self.mesh = abi.Mesh.from_buffer_copy(fields.mesh)
+        h = H()
+        flags = np.ascontiguousarray(fields.flags, np.int16)
+        _check(lib.spiffe_gpu_create(C.byref(self.mesh), flags.ctypes.data_as(P(C.c_int16)), precision,
+                                     int(capacity), C.byref(h)))
+        self.h = h
+        self.upload_fields(fields)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.spiffe_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_mesh(self, mesh=None):
+        if mesh is not None:
+            self.mesh = abi.Mesh.from_buffer_copy(mesh)
+        _check(self.lib.spiffe_gpu_set_mesh(self.h, C.byref(self.mesh)))
+
+    def get_mesh(self):
+        m = abi.Mesh()
+        _check(self.lib.spiffe_gpu_get_mesh(self.h, C.byref(m)))
+        return m
+
+    def upload_fields(self, fields):
+        _check(self.lib.spiffe_gpu_upload_fields(self.h, C.byref(fields.c())))
+
+    def download_fields(self, fields):
+        _check(self.lib.spiffe_gpu_download_fields(self.h, C.byref(fields.c())))
+        return fields
+
+    def fields(self, like):
+        out = like.copy()
+        return self.download_fields(out)
+
+    def upload_beam(self, beam):
+        _check(self.lib.spiffe_gpu_upload_beam(self.h, C.byref(beam.c())))
+
+    def download_beam(self, beam):
+        bs = beam.c()
+        _check(self.lib.spiffe_gpu_download_beam(self.h, C.byref(bs)))
+        beam.take(bs)
+        return beam
+
+    def set_deposit_order(self, ordered):
+        _check(self.lib.spiffe_gpu_set_deposit_order(self.h, int(ordered)))
+
+    def zero_currents(self):
+        _check(self.lib.spiffe_gpu_zero_current_arrays(self.h))
+
+    def advance_fields(self):
+        _check(self.lib.spiffe_gpu_advance_field_solutions(self.h))
+
+    def deposit(self):
+        _check(self.lib.spiffe_gpu_add_particle_currents(self.h))
+
+    def advance_particles(self, opts=None):
+        opts = opts or abi.push_options()
+        _check(self.lib.spiffe_gpu_advance_particles(self.h, C.byref(opts)))
+
+    def solve_poisson(self, target, accuracy, limit):
+        n = C.c_int64()
+        _check(self.lib.spiffe_gpu_solve_poisson_cyl(self.h, target, accuracy, limit, C.byref(n)))
+        return n.value
+
+    def poisson_correction(self, space_charge, opts):
+        rep = abi.PoissonReport()
+        _check(self.lib.spiffe_gpu_add_poisson_correction(self.h, space_charge, C.byref(opts), C.byref(rep)))
+        return rep
+
+    def imposed_efield(self, opts, initialize):
+        _check(self.lib.spiffe_gpu_compute_imposed_efield(self.h, C.byref(opts), int(initialize)))
+
+    def add_screen(self, z_position, direction=1, capacity=1 << 16):
+        _check(self.lib.spiffe_gpu_add_screen(self.h, z_position, direction, int(capacity)))
+
+    def screen(self, index, capacity=None):
+        n = C.c_int64()
+        _check(self.lib.spiffe_gpu_screen_count(self.h, index, C.byref(n)))
+        sc = abi.Screen(0.0, 1, capacity=max(1, n.value if capacity is None else capacity))
+        ss = sc.c()
+        _check(self.lib.spiffe_gpu_download_screen(self.h, index, C.byref(ss)))
+        sc.nb, sc.z_position, sc.direction = ss.nb, ss.z_position, ss.direction
+        return sc
+
+    def clear_screens(self):
+        _check(self.lib.spiffe_gpu_clear_screens(self.h))
+
+    def add_cathode(self, opts):
+        _check(self.lib.spiffe_gpu_add_cathode(self.h, C.byref(opts)))
+
+    def add_antenna(self, direction, istart, iend, iposition, current, frequency, phase, t, W):
+        t = np.ascontiguousarray(t, np.float64)
+        W = np.ascontiguousarray(W, np.float64)
+        _check(self.lib.spiffe_gpu_add_antenna(self.h, direction, istart, iend, iposition, current, frequency, phase,
+                                               t.ctypes.data_as(P(C.c_double)), W.ctypes.data_as(P(C.c_double)),
+                                               len(t)))
+
+    def configure_run(self, space_charge=1, push=None, poisson=None):
+        self._push = push or abi.push_options()
+        self._pc = poisson
+        _check(self.lib.spiffe_gpu_configure_run(self.h, space_charge, C.byref(self._push),
+                                                 C.byref(poisson) if poisson is not None else None))
+
+    def run_begin(self):
+        rep = abi.PoissonReport()
+        _check(self.lib.spiffe_gpu_run_begin(self.h, C.byref(rep)))
+        return rep
+
+    def run_steps(self, n):
+        _check(self.lib.spiffe_gpu_run_steps(self.h, int(n)))
+
+    def synchronize(self):
+        _check(self.lib.spiffe_gpu_synchronize(self.h))
+
+    def counts(self):
+        a, b = C.c_int64(), C.c_int64()
+        _check(self.lib.spiffe_gpu_counts(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value

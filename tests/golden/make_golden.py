@@ -1,0 +1,164 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Each fixture is produced by the reference spiffe's own code, compiled in
+place from its sources by oracle/Makefile into oracle/_ref/libspiffe_ref.so
+(one thread, so the OpenMP push loop is deterministic), on the project's
+synthetic inputs (spiffe_b200.workloads).  Inputs and outputs are stored
+together so the oracle and the CUDA path can be checked without the
+reference present.  Run from the repository root:
+
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import pyoracle  # noqa: E402
+from spiffe_b200 import abi, workloads  # noqa: E402
+
+MODES = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP
+QoMC = -1.602176634e-19 / (9.1093837015e-31 * 2.99792458e8)
+
+
+def save(name, **arrays):
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    print("wrote", name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes raw")
+
+
+def geometry(cmd, geo_name, geo_text):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, geo_name), "w") as f:
+        f.write(geo_text)
+    mesh, flags, psi = pyoracle.run_reference([("command", cmd), ("mesh",), ("get_flags",), ("get_field", "PsiImposed")],
+                                              cwd=d)
+    return d, mesh, flags, psi
+
+
+def mesh_arrays(mesh):
+    return dict(nz=mesh["nz"], nr=mesh["nr"], zmin=mesh["zmin"], zmax=mesh["zmax"], rmax=mesh["rmax"],
+                dz=mesh["dz"], dr=mesh["dr"], bcs=np.array([mesh["lower_bc"], mesh["upper_bc"], mesh["right_bc"],
+                                                             mesh["left_bc"]]))
+
+
+def random_beam(rng, n, zlo, zhi, rhi, active_frac=0.9):
+    z = rng.uniform(zlo, zhi, n)
+    r = rng.uniform(-0.05 * rhi, 1.02 * rhi, n)
+    pz = rng.normal(size=n)
+    pr = rng.normal(size=n) * 0.1
+    rpp = rng.normal(size=n) * 1e-5
+    rs = np.where(r != 0, r, 1.0)
+    g = np.sqrt(1 + pz ** 2 + pr ** 2 + (rpp / rs) ** 2)
+    c = 2.99792458e8
+    status = np.where(rng.uniform(size=n) < active_frac, 1, 0).astype(np.uint64)
+    return dict(z=z, r=r, pz=pz, pr=pr, r_pphi=rpp, vz=c * pz / g, vr=c * pr / g, vphi=c * rpp / rs / g,
+                Q=np.full(n, -1e-14), r0=r.copy(), z0=z.copy(), t0=np.zeros(n), rmin=r - 1e-4, rmax=r + 1e-4,
+                zmin=z - 1e-4, zmax=z + 1e-4, particleID=np.arange(1, n + 1, dtype=np.int32),
+                generation=np.zeros(n, np.int16), status=status)
+
+
+def beam_out(rb):
+    return {"out_" + k: rb[k] for k in abi.BEAM_DOUBLES + ["particleID", "status"]} | {
+        "out_np": rb["np"], "out_npActive": rb["npActive"]}
+
+
+def main():
+    rng = np.random.default_rng(20261203)
+
+    # --- config-1 pillbox: geometry, and the cavity ringing 400 steps
+    cfg = workloads.PillboxConfig()
+    d, mesh, flags, _ = geometry(cfg.geometry(), "pillbox.geo", cfg.geo_text())
+    ez0 = cfg.initial_ez()
+    steps = 400
+    prog = [("command", cfg.geometry()), ("set_time", cfg.dt, 0.0, 0, MODES), ("set_field", "Ez", ez0)]
+    prog += [("call", "ref_advance_field_solutions")] * steps
+    prog += [("get_field", n) for n in ("Ez", "Er", "Bphi", "Bphi2")]
+    out = pyoracle.run_reference(prog, cwd=d)[-4:]
+    save("pillbox_fdtd", flags=flags, geo=np.array(cfg.geo_text()), dt=cfg.dt, steps=steps, Ez0=ez0,
+         Ez=out[0], Er=out[1], Bphi=out[2], Bphi2=out[3], **mesh_arrays(mesh))
+
+    # --- one push + deposition on disturbed fields with a solenoid and a screen
+    shape = flags.shape
+    fields = {n: rng.normal(size=shape) * (1e7 if n[0] == "E" else 0.05) for n in ("Ez", "Er", "Bphi", "Bphi2")}
+    fields["EzImposed"] = rng.normal(size=shape) * 1e6
+    fields["ErImposed"] = rng.normal(size=shape) * 1e6
+    fields["BzImposed"] = rng.normal(size=shape) * 0.1
+    fields["BrImposed"] = rng.normal(size=shape) * 0.1
+    N = 1500
+    beam = random_beam(rng, N, -0.0003, cfg.L + 0.0003, cfg.R)
+    tstep = 37
+    modes = MODES | abi.FL_SPACE_CHARGE
+    zs = cfg.L / 2
+    for comp, tag in ((0, "ref"), (1, "swap")):
+        prog = [("command", cfg.geometry()), ("command", workloads.namelist("define_screen", filename="s", z_position=zs)),
+                ("set_time", cfg.dt, 0.0, tstep, modes)]
+        prog += [("set_field", n, a) for n, a in fields.items()]
+        prog += [("set_beam", (N, int(beam["status"].sum()), 0, N + 1), (QoMC, 1.0), beam),
+                 ("call", "ref_zero_current_arrays"), ("call", "ref_add_particle_currents"), ("get_field", "Jz"),
+                 ("get_field", "Jr"), ("call", "ref_advance_particles", -1.0), ("get_beam",), ("screen", 0)]
+        if tag == "swap":
+            continue  # the reference has one compaction behaviour; "swap" is checked against the oracle
+        res = pyoracle.run_reference(prog, cwd=d)
+        Jz, Jr, rb, rs = res[-5], res[-4], res[-2], res[-1]
+        save("pillbox_push", flags=flags, dt=cfg.dt, time_step=tstep, modes=modes, screen_z=zs, QoMC=QoMC,
+             **{"f_" + k: v for k, v in fields.items()}, **{"in_" + k: v for k, v in beam.items()},
+             Jz=Jz, Jr=Jr, **beam_out(rb), **{"screen_" + k: v for k, v in rs.items()}, **mesh_arrays(mesh))
+
+    # --- DC gun (coarse): imposed Laplace solve and a Poisson correction
+    geo = workloads.dc_gun_geo()
+    cmd = workloads.geometry_command(151, 101, 0.0, 0.030, 0.020, "dc.geo")
+    d2, mesh2, flags2, psi_imp0 = geometry(cmd, "dc.geo", geo)
+    pc = workloads.namelist("poisson_correction", step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+    shape2 = flags2.shape
+    Ez = rng.normal(size=shape2) * 1e5
+    Er = rng.normal(size=shape2) * 1e5
+    N2 = 1200
+    beam2 = dict(z=rng.uniform(0, 0.03, N2), r=rng.uniform(0, 0.02, N2), Q=np.full(N2, -1e-13),
+                 status=np.ones(N2, np.uint64))
+    dt2 = 1e-13
+    prog = [("command", cmd), ("command", pc), ("set_time", dt2, 0.0, 0, modes), ("call", "ref_compute_imposed_Efield", 1),
+            ("get_field", "PsiImposed"), ("get_field", "EzImposed"), ("get_field", "ErImposed"),
+            ("set_field", "Ez", Ez), ("set_field", "Er", Er), ("set_beam", (N2, N2, 0, 1), (0.0, 1.0), beam2),
+            ("call", "ref_add_poisson_correction", 1), ("get_field", "Ez"), ("get_field", "Er"), ("get_field", "Psi"),
+            ("get_field", "Q")]
+    res = pyoracle.run_reference(prog, cwd=d2)
+    save("dcgun_poisson", flags=flags2, dt=dt2, PsiImposed0=psi_imp0, PsiImposed=res[1], EzImposed=res[2],
+         ErImposed=res[3], Ez0=Ez, Er0=Er, **{"in_" + k: v for k, v in beam2.items()}, Ez=res[-4], Er=res[-3],
+         Psi=res[-2], Q=res[-1], **mesh_arrays(mesh2))
+
+    # --- config-1 loop with emission through perform_integration, 220 steps
+    t, A = cfg.profile()
+    with open(os.path.join(d, "prof.sdds"), "w") as f:
+        f.write("SDDS1\n&column name=t type=double &end\n&column name=A type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(t, A):
+            f.write("%.17g %.17g\n" % (a, b))
+    nsteps = 220
+    cath = workloads.namelist("define_cathode", z_position=0.0, outer_radius=cfg.cathode_radius,
+                              current_density=cfg.peak_current_density(), electrons_per_macroparticle=cfg.epm,
+                              profile="prof.sdds", profile_time_name="t", profile_factor_name="A",
+                              random_number_seed=cfg.seed)
+    scr = workloads.namelist("define_screen", filename="exit", z_position=0.004)
+    integ = workloads.namelist("integrate", dt_integration=cfg.dt, finish_time=(nsteps + 0.5) * cfg.dt, space_charge=1)
+    res = pyoracle.run_reference([("command", cfg.geometry()), ("set_field", "Ez", ez0), ("command", cath),
+                                  ("command", scr), ("command", integ), ("get_field", "Ez"), ("get_field", "Er"),
+                                  ("get_field", "Bphi"), ("get_field", "Jz"), ("get_field", "Jr"), ("get_beam",),
+                                  ("screen", 0), ("rng_counter",)], cwd=d, capacity=40000)
+    Ezf, Erf, Bpf, Jzf, Jrf, rb, rs, rc = res
+    save("pillbox_loop", flags=flags, dt=cfg.dt, steps=nsteps, Ez0=ez0, prof_t=t, prof_A=A, screen_z=0.004,
+         Ez=Ezf, Er=Erf, Bphi=Bpf, Jz=Jzf, Jr=Jrf, rng_counter=rc, **beam_out(rb),
+         **{"screen_" + k: v for k, v in rs.items()}, **mesh_arrays(mesh))
+
+    # --- geometry rasterisation of the other two configurations' shapes
+    _, mesh3, flags3, psi3 = geometry(workloads.geometry_command(301, 83, 0.0, 0.150, 0.041, "gun.geo"), "gun.geo",
+                                      workloads.gun16_geo())
+    save("gun16_geometry", flags=flags3, geo=np.array(workloads.gun16_geo()), **mesh_arrays(mesh3))
+    save("dcgun_geometry", flags=flags2, PsiImposed=psi_imp0, geo=np.array(geo), **mesh_arrays(mesh2))
+
+
+if __name__ == "__main__":
+    main()

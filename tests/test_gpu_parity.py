@@ -1,0 +1,220 @@
+"""Parity of the plain FP64 CUDA path with the reference, through the C ABI.
+
+Bit-exact where the arithmetic is order-free (FDTD, push, SOR updates,
+ordered deposition); within a stated tolerance where the device sums in a
+different order (FP64 atomics: relative L2 <= 1e-12 after one step).
+"""
+import numpy as np
+import pytest
+
+from spiffe_b200 import abi, gpu, workloads
+from oracle import pyoracle
+from helpers import MODES, beam_from, by_id, fields_from, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+ATOMIC_TOL = 1e-12
+
+
+def push_fixture_state(fx):
+    f = fields_from(fx, modes=int(fx["modes"]), dt=float(fx["dt"]))
+    f.mesh.time_step = int(fx["time_step"])
+    f.mesh.time = f.mesh.time_step * f.mesh.dt
+    for k in ("Ez", "Er", "Bphi", "Bphi2", "EzImposed", "ErImposed", "BzImposed", "BrImposed"):
+        f[k] = fx["f_" + k]
+    return f, beam_from(fx)
+
+
+def test_fdtd_pillbox_bit_exact():
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    g = gpu.GpuInstance(f)
+    for _ in range(int(fx["steps"])):
+        g.advance_fields()
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Bphi2"):
+        assert np.array_equal(out[n], fx[n]), n
+
+
+def test_fdtd_te_fields_match_oracle(oracle):
+    fx = load("gun16_geometry")
+    modes = MODES | abi.FL_TE_FIELDS
+    f = fields_from(fx, modes=modes, dt=2e-13)
+    rng = np.random.default_rng(3)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Bz", "Br2", "Bz2", "Jz", "Jr", "Jphi"):
+        f[n] = rng.normal(size=f.shape)
+    ref = f.copy()
+    g = gpu.GpuInstance(f)
+    for _ in range(25):
+        g.advance_fields()
+        oracle.advance_fields(ref)
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Br2", "Bz", "Bz2"):
+        assert np.array_equal(out[n], ref[n]), n
+
+
+@pytest.mark.parametrize("ordered", [1, 0])
+def test_deposit(ordered):
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    g = gpu.GpuInstance(f)
+    g.set_deposit_order(ordered)
+    g.upload_beam(b)
+    g.zero_currents()
+    g.deposit()
+    out = g.fields(f)
+    for n in ("Jz", "Jr"):
+        if ordered:
+            assert np.array_equal(out[n], fx[n]), n
+        else:
+            assert rel_l2(out[n], fx[n]) <= ATOMIC_TOL, n
+
+
+def test_push_reference_policies_bit_exact():
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    g = gpu.GpuInstance(f)
+    g.upload_beam(b)
+    g.add_screen(float(fx["screen_z"]))
+    g.advance_particles(abi.push_options(compaction=abi.COMPACT_REFERENCE, screen_momentum=abi.SCREEN_REFERENCE))
+    out = g.download_beam(abi.Beam(b.capacity))
+    assert out.np == int(fx["out_np"]) and out.npActive == int(fx["out_npActive"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(out[k], fx["out_" + k]), k
+    rec = by_id(g.screen(0).records())
+    ref = by_id({c: fx["screen_" + c] for c in abi.SCREEN_COLUMNS} | {"particleID": fx["screen_particleID"]})
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rec[c], ref[c]), c
+
+
+def test_push_swap_compaction_matches_oracle(oracle):
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    opts = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
+    g = gpu.GpuInstance(f)
+    g.upload_beam(b)
+    g.add_screen(float(fx["screen_z"]))
+    g.advance_particles(opts)
+    out = g.download_beam(abi.Beam(b.capacity))
+    ref_b = b.copy()
+    sc = abi.Screen(float(fx["screen_z"]))
+    oracle.advance_particles(f.copy(), ref_b, [sc], opts)
+    assert out.np == ref_b.np and out.npActive == ref_b.npActive
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(out[k], ref_b[k]), k
+    rec, ref = by_id(g.screen(0).records()), by_id(sc.records())
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rec[c], ref[c]), c
+
+
+def test_single_test_particle_trajectory(oracle):
+    """A single electron in the pillbox's TM010 field for 600 steps."""
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    b = abi.Beam(4)
+    b.set(1, z=[0.002], r=[0.003], pz=[0.0], pr=[0.0], r_pphi=[0.0], vz=[0.0], vr=[0.0], vphi=[0.0], Q=[-1e-15],
+          r0=[0.003], z0=[0.002], t0=[0.0], rmin=[1e300], rmax=[-1e300], zmin=[1e300], zmax=[-1e300],
+          particleID=[1], generation=[0], status=[1])
+    b.npActive, b.nextParticleID, b.QoMC, b.stiffness = 1, 2, abi_qomc(), 1.0
+    g = gpu.GpuInstance(f)
+    g.upload_beam(b)
+    ref_f, ref_b = f.copy(), b.copy()
+    opts = abi.push_options(compaction=abi.COMPACT_SWAP)
+    traj_g, traj_o = [], []
+    for step in range(600):
+        ref_f.mesh.time = step * ref_f.mesh.dt
+        g.mesh.time = ref_f.mesh.time
+        g.set_mesh()
+        g.advance_fields()
+        oracle.advance_fields(ref_f)
+        g.advance_particles(opts)
+        oracle.advance_particles(ref_f, ref_b, [], opts)
+        if step % 100 == 99:
+            out = g.download_beam(abi.Beam(4))
+            traj_g.append([out["z"][0], out["r"][0], out["pz"][0], out["pr"][0]])
+            traj_o.append([ref_b["z"][0], ref_b["r"][0], ref_b["pz"][0], ref_b["pr"][0]])
+    traj_g, traj_o = np.array(traj_g), np.array(traj_o)
+    assert np.max(np.abs(traj_g - traj_o) / np.maximum(np.abs(traj_o), 1e-30)) <= 1e-9
+    assert np.array_equal(traj_g, traj_o)  # the FP64 form is bit-faithful
+
+
+def abi_qomc():
+    return -1.602176634e-19 / (9.1093837015e-31 * 2.99792458e8)
+
+
+def test_imposed_field_and_sor_bit_exact():
+    fx = load("dcgun_poisson")
+    f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
+    f["PsiImposed"] = fx["PsiImposed0"]
+    g = gpu.GpuInstance(f)
+    opts = abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+    g.imposed_efield(opts, 1)
+    out = g.fields(f)
+    for n in ("PsiImposed", "EzImposed", "ErImposed"):
+        assert np.array_equal(out[n], fx[n]), n
+
+
+def test_poisson_correction(oracle):
+    fx = load("dcgun_poisson")
+    modes = MODES | abi.FL_SPACE_CHARGE
+    f = fields_from(fx, modes=modes, dt=float(fx["dt"]))
+    f["PsiImposed"] = fx["PsiImposed"]
+    f["EzImposed"], f["ErImposed"] = fx["EzImposed"], fx["ErImposed"]
+    f["Ez"], f["Er"] = fx["Ez0"], fx["Er0"]
+    b = beam_from(fx)
+    opts = abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+    # without particles the correction is order-free: bit-exact against the oracle
+    g0 = gpu.GpuInstance(f)
+    rep0 = g0.poisson_correction(0, opts)
+    ref0 = f.copy()
+    orep0 = oracle.poisson_correction(ref0, abi.Beam(1), 0, opts)
+    assert rep0.ran == orep0.ran == 1 and rep0.iterations == orep0.iterations
+    out0 = g0.fields(f)
+    for n in ("Ez", "Er", "Psi", "Q"):
+        assert np.array_equal(out0[n], ref0[n]), n
+    # with particles the charge is scattered with FP64 atomics
+    g = gpu.GpuInstance(f)
+    g.upload_beam(b)
+    rep = g.poisson_correction(1, opts)
+    assert rep.ran == 1 and abs(rep.iterations - 527) <= 1
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Psi"):
+        assert rel_l2(out[n], fx[n]) <= ATOMIC_TOL, n
+
+
+def test_loop_with_emission_bit_exact():
+    """perform_integration for 220 steps with emission and space charge."""
+    fx = load("pillbox_loop")
+    cfg = workloads.PillboxConfig()
+    f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    g = gpu.GpuInstance(f, capacity=40000)
+    g.set_deposit_order(1)
+    g.add_screen(float(fx["screen_z"]), capacity=40000)
+    g.add_cathode(cfg.cathode_options())
+    g.configure_run(space_charge=1, push=abi.push_options())
+    g.run_begin()
+    g.run_steps(int(fx["steps"]))
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Jz", "Jr"):
+        assert np.array_equal(out[n], fx[n]), n
+    b = g.download_beam(abi.Beam(40000))
+    assert b.np == int(fx["out_np"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k], fx["out_" + k]), k
+    rec = by_id(g.screen(0, capacity=40000).records())
+    ref = by_id({c: fx["screen_" + c] for c in abi.SCREEN_COLUMNS} | {"particleID": fx["screen_particleID"]})
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rec[c], ref[c]), c
+
+
+def test_device_errors_are_reported():
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]))
+    g = gpu.GpuInstance(f)
+    with pytest.raises(gpu.SpiffeGpuError):
+        g.solve_poisson(0, -1.0, 10)  # accuracy <= 0 is rejected as the reference does (poisson.c:27)
+    with pytest.raises(gpu.SpiffeGpuError):
+        g.add_screen(0.01, direction=2)
