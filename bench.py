@@ -1,0 +1,404 @@
+#!/usr/bin/env python
+"""Benchmark of spiffe's per-timestep PIC loop on one B200 (or N replicas).
+
+Workload: the 1.6-cell RF gun -- 3001 x 821 nodes at 50 um, 1,000,000
+macroparticles of a 1 nC, 2 ps bunch, solenoid, Poisson correction every 20
+steps (spiffe_b200.workloads.Gun16Config).  One step is one pass of the
+perform_integration loop body (integrate.c:136-193): J zero and deposit,
+Poisson correction when due, FDTD, gather and push with wall losses and the
+exit screen.  The metric is active particles pushed per second (with cell
+updates per second beside it), measured on the device with CUDA events on
+the library's stream, maximum over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+--impl reference times the reference spiffe's own CPU code (compiled from
+its sources into oracle/_ref) on the same state, with all host threads.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s & cell-updates/s per B200 at ≤0.5% moment error vs FP64; p50/p99"
+UNIT = "particle-steps/s"
+QoMC = -1.602176634e-19 / (9.1093837015e-31 * 2.99792458e8)
+
+# algorithmic bytes per unit (FP64 form): the compulsory traffic of each phase
+BYTES = {
+    "fdtd": 74.0,     # per node-step: read Ez,Er,Bphi,Jz,Jr (40) + flags (2); write Ez,Er,Bphi,Bphi2 (32)
+    "push": 144.0,    # per particle-step: read 9 doubles + status (80); write 8 doubles (64)
+    "deposit": 80.0,  # per particle-step: z, r, v, Q, status for Jz and again for Jr
+    "sor": 13.0,      # per node and half-sweep: read Psi, rhs, flags; write half of Psi
+    "correction": 110.0,  # per node and correction: two flux passes, rhs scaling, gradient update
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=600)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--precision", default="f64", choices=["f64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-steps", type=int, default=20, help="reference steps timed for the CPU baseline")
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            with open(self.path) as f:
+                for line in f:
+                    parts = [x.strip() for x in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm.append(float(parts[1]))
+                        mx = float(parts[2])
+                    except ValueError:
+                        continue
+                    for n, v in zip(names, parts[5:9]):
+                        if v.lower() == "active":
+                            reasons.add(n)
+            os.unlink(self.path)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def build_state(cfg):
+    """Mesh flags from the product's define_geometry, the analytic field, the
+    solenoid and the beam, as abi containers."""
+    from spiffe_b200 import abi, geometry
+
+    modes = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP | abi.FL_SPACE_CHARGE
+    f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(), modes=modes)
+    f.mesh.dt = cfg.dt
+    f["Ez"] = cfg.initial_ez(f.flags)
+    bz, br = cfg.solenoid()
+    f["BzImposed"] = bz
+    f["BrImposed"] = br
+    arrays = cfg.beam_arrays()
+    n = len(arrays["z"])
+    b = abi.Beam(int(n * 1.25))
+    b.set(n, **arrays)
+    b.npActive, b.nextParticleID, b.QoMC, b.stiffness = n, n + 1, QoMC, 1.0
+    return f, b
+
+
+def pinned_like(arr):
+    import torch
+
+    t = torch.empty(arr.shape, dtype=getattr(torch, str(arr.dtype).replace("uint64", "int64")), pin_memory=True)
+    out = t.numpy().view(arr.dtype)
+    out[...] = arr
+    return out, t
+
+
+def reference_sample(cfg, steps, warmup=1, threads=None):
+    """The reference's own perform_integration loop body (integrate.c:136-193,
+    compiled from its sources) on the same state; returns timing per step."""
+    from oracle import pyoracle
+    from spiffe_b200 import abi, workloads
+
+    threads = threads or os.cpu_count()
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "gun.geo"), "w") as fgeo:
+        fgeo.write(cfg.geo_text())
+    geom = workloads.geometry_command(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, "gun.geo")
+    pc = workloads.namelist("poisson_correction", step_interval=cfg.step_interval, accuracy=1e-6,
+                            maximum_iterations=1000)
+    scr = workloads.namelist("define_screen", filename="exit", z_position=cfg.screen_z())
+    modes = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP | abi.FL_SPACE_CHARGE
+    flags_prog = [("command", geom), ("get_flags",)]
+    flags = pyoracle.run_reference(flags_prog, cwd=d, threads=threads)[0]
+    arrays = cfg.beam_arrays()
+    n = len(arrays["z"])
+    bz, br = cfg.solenoid()
+    prog = [("command", geom), ("command", pc), ("command", scr), ("set_time", cfg.dt, 0.0, 0, modes),
+            ("set_field", "Ez", cfg.initial_ez(flags)), ("set_field", "BzImposed", bz), ("set_field", "BrImposed", br),
+            ("set_beam", (n, n, 0, n + 1), (QoMC, 1.0), arrays), ("call", "ref_calculate_areas_and_setup"),
+            ("call", "ref_compute_imposed_Efield", 1), ("call", "ref_add_poisson_correction", 1),
+            ("time_steps", warmup, 1, -1.0), ("time_steps", steps, 1, -1.0)]
+    res = pyoracle.run_reference(prog, cwd=d, capacity=int(n * 1.25), threads=threads, timeout=3600)
+    timed = res[-1]
+    secs = sum(t for t, _ in timed)
+    psteps = sum(a for _, a in timed)
+    return {"seconds": secs, "particle_steps": psteps, "steps": steps, "threads": threads,
+            "value": psteps / secs if secs else 0.0,
+            "cell_updates_per_s": cfg.nz * cfg.nr * steps / secs if secs else 0.0}
+
+
+def gpu_arm(args):
+    import torch
+
+    from spiffe_b200 import abi, gpu, workloads
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    gpu.select_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = td
+    cfg = workloads.Gun16Config()
+    f, b = build_state(cfg)
+    K, W = args.steps, args.warmup
+    push = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
+
+    # --- device-resident throughput
+    g = gpu.GpuInstance(f, capacity=b.capacity)
+    g.upload_beam(b)
+    g.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
+    g.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
+    g.run_begin()
+    g.run_steps(W)
+    g.synchronize()
+    # host copy of the post-warm-up state, for the end-to-end run
+    host_f, host_b = f.copy(), abi.Beam(b.capacity)
+    g.download_fields(host_f)
+    g.download_beam(host_b)
+    mesh_w = g.get_mesh()
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    g.set_profiling(True)
+    w0 = g.work_counters()
+    l0 = gpu.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0.record(stream)
+    g.run_steps(K)
+    ev1.record(stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = gpu.launch_count() - l0
+    w1 = g.work_counters()
+    phases = g.phase_times()
+    g.set_profiling(False)
+    psteps = w1["particle_steps"] - w0["particle_steps"]
+    halfsweeps = w1["sor_halfsweeps"] - w0["sor_halfsweeps"]
+    solves = w1["sor_solves"] - w0["sor_solves"]
+    np_end, _ = g.counts()
+    g.close()
+
+    # --- end to end through the public API from pinned host buffers: upload
+    # the state, K steps each reading the particle count back, download
+    pin = {}
+    for k, v in host_f.a.items():
+        host_f.a[k], pin[k] = pinned_like(v)
+    for k, v in host_b.a.items():
+        host_b.a[k], pin["b" + k] = pinned_like(v)
+    g2 = gpu.GpuInstance(f, capacity=b.capacity)
+    g2.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
+    g2.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
+    g2.set_mesh(mesh_w)
+    stream2 = torch.cuda.ExternalStream(g2.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    state_bytes = sum(v.nbytes for v in host_f.a.values()) + sum(
+        v[: host_b.np].nbytes for v in host_b.a.values()) + host_b.np * (4 + 2 + 8)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream2)
+    g2.upload_fields(host_f)
+    g2.upload_beam(host_b)
+    wb0 = g2.work_counters()
+    for _ in range(K):
+        g2.run_steps(1)
+        g2.counts()
+    wb1 = g2.work_counters()
+    g2.download_beam(host_b)
+    g2.download_fields(host_f)
+    e1.record(stream2)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_psteps = wb1["particle_steps"] - wb0["particle_steps"]
+    g2.close()
+
+    # --- totals over ranks (max time, summed work)
+    if dist:
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        w = torch.tensor([psteps, e2e_psteps], dtype=torch.float64, device="cuda")
+        dist.all_reduce(w, op=dist.ReduceOp.SUM)
+        ms, e2e_ms = float(t[0]), float(t[1])
+        psteps_all, e2e_all = float(w[0]), float(w[1])
+    else:
+        psteps_all, e2e_all = psteps, e2e_psteps
+    sec = ms / 1e3
+    value = psteps_all / sec
+    cells = cfg.nz * cfg.nr * K * world / sec
+
+    # --- roofline of the dominant phase
+    peak, peak_kind = measured_peak()
+    nodes = (cfg.nz + 1) * (cfg.nr + 1)
+    sor_nodes = cfg.nz * (cfg.nr - 1)
+    work_bytes = {
+        "fdtd": BYTES["fdtd"] * nodes * phases["fdtd"][1],
+        "push": BYTES["push"] * psteps,
+        "deposit": BYTES["deposit"] * psteps,
+        "poisson": BYTES["sor"] * sor_nodes * halfsweeps + BYTES["correction"] * nodes * solves,
+        "emission": 0.0,
+    }
+    total_ms = sum(v[0] for v in phases.values()) or 1.0
+    breakdown = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_ms, 4),
+                     "gbs": round(work_bytes[k] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None}
+                 for k, v in phases.items()}
+    dom = max(phases, key=lambda k: phases[k][0])
+    dom_units = {"fdtd": phases["fdtd"][1], "push": phases["push"][1], "deposit": phases["deposit"][1],
+                 "poisson": max(solves, 1), "emission": 1}[dom]
+    achieved = work_bytes[dom] / (phases[dom][0] / 1e3) / 1e9 if phases[dom][0] > 0 else 0.0
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as ft:
+            traffic = json.load(ft).get(dom)
+    except (OSError, ValueError):
+        pass
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                "traffic": traffic, "bytes_per_launch": round(work_bytes[dom] / max(dom_units, 1)),
+                "avg_launch_ms": round(phases[dom][0] / max(dom_units, 1), 4)}
+
+    line = {
+        "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "1.6-cell RF gun, 3001x821 nodes at 50um, 1,000,000 macroparticles, "
+                               "Poisson correction every 20 steps, solenoid",
+                   "form": "plain FP64 (bit-faithful to the reference)",
+                   "field": "analytic pi-mode standing wave, 100 MV/m on the cathode",
+                   "particles": cfg.n_macro, "nodes": cfg.nz * cfg.nr, "steps_timed": K,
+                   "l2": "no flush: the resident state (fields ~%d MB, beam ~%d MB) exceeds the 126 MB L2"
+                         % (sum(v.nbytes for v in f.a.values()) // 2 ** 20, sum(v.nbytes for v in b.a.values()) // 2 ** 20),
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "cell_updates_per_s": round(cells, 1),
+        "particles_end": np_end,
+        "phases": breakdown,
+        "roofline": roofline,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": {"value": round(e2e_all / (e2e_ms / 1e3), 1), "unit": UNIT,
+                "h2d_bytes_per_step": int(state_bytes / K), "d2h_bytes_per_step": int((state_bytes + 8 * K) / K),
+                "how": "public API from pinned host buffers: state upload, K single-step calls each reading the "
+                       "particle count back, state download"},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            s = reference_sample(cfg, args.cpu_steps)
+            line["cpu_baseline"] = {"value": round(s["value"], 1), "unit": UNIT, "cores": s["threads"],
+                                    "kind": "reference",
+                                    "sample": "%d perform_integration steps of the reference (one Poisson interval) "
+                                              "on the same 1M-particle state, after 1 warm-up step, %.1f s"
+                                              % (s["steps"], s["seconds"])}
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": "unavailable: %s" % str(e)[:200]}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def reference_arm(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    from oracle import pyoracle
+    from spiffe_b200 import workloads
+
+    if not pyoracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspiffe_ref.so was not built"}))
+        return
+    cfg = workloads.Gun16Config()
+    steps = min(args.steps, args.cpu_steps)
+    s = reference_sample(cfg, steps, warmup=max(1, min(args.warmup, 1)))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(s["value"], 1), "unit": UNIT, "n_gpus": world,
+        "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * s["seconds"] / steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "1.6-cell RF gun, 3001x821 nodes at 50um, 1,000,000 macroparticles, "
+                               "Poisson correction every 20 steps, solenoid",
+                   "form": "reference spiffe CPU code (OpenMP push)", "steps_timed": steps},
+        "cell_updates_per_s": round(s["cell_updates_per_s"], 1),
+        "cpu_baseline": {"value": round(s["value"], 1), "unit": UNIT, "cores": s["threads"], "kind": "reference",
+                         "sample": "%d perform_integration steps (a bounded sample of the K requested)" % steps},
+        "e2e": {"value": round(s["value"], 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -111,6 +111,20 @@ int spiffe_gpu_run_steps(spiffe_gpu_instance *inst, int64_t n_steps);
 int spiffe_gpu_synchronize(spiffe_gpu_instance *inst);
 int spiffe_gpu_counts(spiffe_gpu_instance *inst, int64_t *np, int64_t *np_active);
 
+/* Measurement (no counterpart in the reference, which has no timers): the device used by instances created afterwards on
+ * this thread; the instance's CUDA stream (a cudaStream_t); per-phase device
+ * time with CUDA events on that stream, in the order emission, deposition,
+ * Poisson correction, FDTD, push (ms[5], count[5]; reading restarts the
+ * accumulation); and the number of kernels this library has queued. */
+int spiffe_gpu_select_device(int32_t device);
+int spiffe_gpu_stream(spiffe_gpu_instance *inst, void **stream);
+int spiffe_gpu_set_profiling(spiffe_gpu_instance *inst, int32_t on);
+int spiffe_gpu_phase_times(spiffe_gpu_instance *inst, double *ms, int64_t *count);
+int64_t spiffe_gpu_launch_count(void);
+/* Work done so far: out[0] particle-steps (active particles summed over
+ * pushes), out[1] SOR half-sweeps, out[2] SOR solves, out[3] FDTD steps. */
+int spiffe_gpu_work_counters(spiffe_gpu_instance *inst, int64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -308,6 +308,20 @@ def _child(program, capacity, cwd):
             out.append((e[0], e[1]))
         elif kind == "rng_counter":
             out.append(lib.ref_rng_counter())
+        elif kind == "time_steps":
+            # (seconds, active particles) of each perform_integration loop step
+            import time
+
+            n, space_charge, zfs = args
+            res = []
+            for _ in range(n):
+                counts = (C.c_int64 * 4)()
+                sc = (C.c_double * 2)()
+                lib.ref_get_beam_counts(counts, sc)
+                t0 = time.perf_counter()
+                lib.ref_step(space_charge, zfs)
+                res.append((time.perf_counter() - t0, counts[1]))
+            out.append(res)
         else:
             raise ValueError(kind)
     return out

@@ -71,6 +71,8 @@ struct DevCounts {
   long long screen_nb[SPIFFE_MAX_SCREENS];
   long long screen_overflow;
   double last_pz0, last_pr0, last_rpphi0; // pre-kick momenta of particle np-1
+  long long pushed;                       // sum over pushes of the active count (particle-steps)
+  long long sor_halfsweeps, sor_solves;   // red-black half-sweeps and solves run
   unsigned int error;                     // SPIFFE_DEV_ERR_* bits
   unsigned int pad;
 };
@@ -92,3 +94,7 @@ __device__ __forceinline__ long long atomic_add_ll(long long *p, long long v)
 
 // Host-side launch helpers.
 inline unsigned blocks_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+// Every host wrapper reports the kernels it queued (a process-wide count the
+// benchmark reads around its timed region).
+extern "C" void spiffe_note_launches(int n);

@@ -138,7 +138,9 @@ extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, con
   if (p->total <= 0)
     return 0;
   k_births<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt);
+  spiffe_note_launches(1);
   k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, cnt);
+  spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }
 
@@ -149,5 +151,6 @@ extern "C" int spiffe_antenna64(double *J, int pitch, int direction, long istart
     return 0;
   const long n = iend - istart + 1;
   k_antenna<<<blocks_for(n, 128), 128, 0, s>>>(J, pitch, direction, istart, iend, iposition, value);
+  spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

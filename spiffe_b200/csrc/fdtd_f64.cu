@@ -289,11 +289,15 @@ extern "C" int spiffe_fdtd64_step(const DevMesh *m, const DevFields<double> *f, 
   dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
   if (m->modes & SPIFFE_FL_TM_FIELDS) {
     k_tm_e<<<grid, block, 0, s>>>(*m, *f, c);
+    spiffe_note_launches(1);
     k_tm_b<<<grid, block, 0, s>>>(*m, *f, c);
+    spiffe_note_launches(1);
   }
   if (m->modes & SPIFFE_FL_TE_FIELDS) {
     k_te_e<<<grid, block, 0, s>>>(*m, *f, c);
+    spiffe_note_launches(1);
     k_te_b<<<grid, block, 0, s>>>(*m, *f, c);
+    spiffe_note_launches(1);
   }
   return (int)cudaGetLastError();
 }

@@ -776,6 +776,7 @@ __global__ void k_reset_step_counts(DevCounts *cnt)
   cnt->first_lost = 0x7fffffffffffffffLL;
   cnt->n_lost = 0;
   cnt->new_active = 0;
+  cnt->pushed += cnt->npActive;
 }
 
 } // namespace
@@ -862,16 +863,19 @@ extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, co
       continue;
     if (!ordered) {
       k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, nullptr, nullptr);
+      spiffe_note_launches(1);
       continue;
     }
     const int n = (int)(4 * np_bound);
     k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, w->keys, w->vals);
+    spiffe_note_launches(1);
     // stable LSD radix sort keeps particle order inside each node's run;
     // the INT_MAX pad key sorts last within the 31-bit key space
     size_t bytes = w->cub_bytes;
     cub::DeviceRadixSort::SortPairs(w->cub_tmp, bytes, w->keys, w->keys_alt, w->vals, w->vals_alt, n, 0, 31, s);
     double *J = comp == 0 ? f->Jz : (comp == 1 ? f->Jr : f->Jphi);
     k_ordered_sum<<<blocks_for(n, T), T, 0, s>>>(w->keys_alt, w->vals_alt, n, J);
+    spiffe_note_launches(1);
     (void)bits;
   }
   return (int)cudaGetLastError();
@@ -888,23 +892,30 @@ extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const
                              const DevScreens *scr, DevCounts *cnt, long long np_bound, Particles64Work *w, cudaStream_t s)
 {
   k_reset_step_counts<<<1, 1, 0, s>>>(cnt);
+  spiffe_note_launches(1);
   if (np_bound > 0) {
     PushParams p{hp->time, hp->z_forces_start, hp->QoMC, hp->stiffness, hp->tb_epm, hp->tb_z_force,
                  hp->tb_r_force, hp->tb_z_decel, hp->tb_r_decel, hp->screen_momentum};
     if (scr->n && hp->screen_momentum == SPIFFE_SCREEN_REFERENCE)
-      k_snapshot_last<<<1, 1, 0, s>>>(*b, cnt);
+      { k_snapshot_last<<<1, 1, 0, s>>>(*b, cnt); spiffe_note_launches(1); }
     k_push<<<blocks_for(np_bound, T), T, 0, s>>>(*m, *f, *b, p, *scr, cnt, w->lost);
+    spiffe_note_launches(1);
   }
   if (hp->compaction == SPIFFE_COMPACT_REFERENCE || np_bound <= 0) {
     k_compact_reference<<<1, 1, 0, s>>>(cnt);
+    spiffe_note_launches(1);
   } else {
     const unsigned nb = blocks_for(np_bound, T);
     k_survivor_flags<<<nb, T, 0, s>>>(w->lost, cnt, w->surv, np_bound);
+    spiffe_note_launches(1);
     size_t bytes = w->cub_bytes;
     cub::DeviceScan::ExclusiveSum(w->cub_tmp, bytes, w->surv, w->surv_before, (int)np_bound, s);
     k_compact_swap_map<<<nb, T, 0, s>>>(w->lost, w->surv_before, cnt, w->map);
+    spiffe_note_launches(1);
     k_compact_swap_move<<<nb, T, 0, s>>>(*b, w->lost, w->surv_before, cnt, w->map);
+    spiffe_note_launches(1);
     k_compact_swap_finish<<<1, 1, 0, s>>>(cnt);
+    spiffe_note_launches(1);
   }
   return (int)cudaGetLastError();
 }

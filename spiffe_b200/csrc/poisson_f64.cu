@@ -349,6 +349,8 @@ __global__ void __launch_bounds__(RT) k_sor(DevMesh m, SorArgs s, DevCounts *cnt
       s.st->iterations = result;
       s.st->residual = total;
     }
+    cnt->sor_halfsweeps += result >= 0 ? result + 1 : s.limit;
+    cnt->sor_solves += 1;
   }
 }
 
@@ -560,7 +562,9 @@ static int sum_region(const double *a, int rows, int cols, int P, int absval, Po
     return 0;
   }
   k_region_sum<<<grid, block, 0, s>>>(a, rows, cols, P, absval, w->part);
+  spiffe_note_launches(1);
   k_finish_sum<<<1, 1024, 0, s>>>(w->part, grid.x * grid.y, 1, out);
+  spiffe_note_launches(1);
   return 0;
 }
 
@@ -593,6 +597,7 @@ static int launch_sor(const DevMesh *m, Poisson64Work *w, double *Psi, const dou
   DevMesh mm = *m;
   void *args[] = {&mm, &a, &cnt};
   cudaError_t e = cudaLaunchCooperativeKernel((void *)k_sor, dim3(w->sor_grid), dim3(RT), args, 0, s);
+  spiffe_note_launches(1);
   return (int)e;
 }
 
@@ -626,29 +631,39 @@ extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<dou
   const int nblk = grid.x * grid.y;
   // apparent charge, then the particles' own charge
   k_apparent_charge<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 0, w->part);
+  spiffe_note_launches(1);
   k_finish_sum<<<1, 1024, 0, s>>>(w->part, nblk, 2, w->scalars + 0);
+  spiffe_note_launches(1);
   k_finish_sum<<<1, 1024, 0, s>>>(w->part + 1, nblk, 2, w->scalars + 1);
+  spiffe_note_launches(1);
   if (o->space_charge && np_bound > 0) {
     const unsigned pb = blocks_for(np_bound, RT);
     k_remove_charge<<<pb, RT, 0, s>>>(*m, *f, *b, cnt, w->part);
+    spiffe_note_launches(1);
     k_finish_sum<<<1, 1024, 0, s>>>(w->part, (int)pb, 1, w->scalars + 2);
+    spiffe_note_launches(1);
   } else {
     cudaMemsetAsync(w->scalars + 2, 0, sizeof(double), s);
   }
   sum_region(f->Q, m->nz, m->nr, m->pitch, 0, w, w->scalars + 3, s);
   k_set_state<<<1, 1, 0, s>>>(w->st, w->scalars, w->scalars + 2, w->scalars + 3, o->space_charge);
+  spiffe_note_launches(1);
   k_pc_decide<<<1, 1, 0, s>>>(w->st, o->error_charge_threshold);
+  spiffe_note_launches(1);
   k_scale_rhs<<<grid, block, 0, s>>>(*m, *f, w->volume, w->st);
+  spiffe_note_launches(1);
   if (o->guess_code)
-    k_guess<<<grid, block, 0, s>>>(*m, *f, o->guess_code, w->st);
+    { k_guess<<<grid, block, 0, s>>>(*m, *f, o->guess_code, w->st); spiffe_note_launches(1); }
   int rc = launch_sor(m, w, f->Psi, f->Q, f->flags, o->accuracy, o->maximum_iterations, w->st, w->iters, cnt, s);
   if (rc)
     return rc;
   k_subtract_gradient<<<grid, block, 0, s>>>(*m, *f, w->st);
+  spiffe_note_launches(1);
   // the reference recomputes the apparent charge afterwards (:333-439)
   k_apparent_charge<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 1, w->part);
+  spiffe_note_launches(1);
   if (o->space_charge && np_bound > 0)
-    k_remove_charge<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, w->part);
+    { k_remove_charge<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, w->part); spiffe_note_launches(1); }
   return (int)cudaGetLastError();
 }
 
@@ -674,5 +689,6 @@ extern "C" int spiffe_imposed_field64(const DevMesh *m, const DevFields<double> 
 {
   dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
   k_imposed_field<<<grid, block, 0, s>>>(*m, *f, factor);
+  spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

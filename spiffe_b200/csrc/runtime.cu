@@ -8,6 +8,7 @@
 // (antenna.c:374-418) and the Poisson interval test (poisson_correction.c:
 // 116-119).  Particle counts live on the device; the host tracks an upper
 // bound for launch sizes and reads the true count only when it must.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -113,6 +114,45 @@ static int fail(int code, const char *fmt, ...)
   return code;
 }
 
+// lets the host-only modules (geometry, commands) report through the same channel
+extern "C" int spiffe_set_error(int code, const char *msg)
+{
+  g_error = msg ? msg : "";
+  return code;
+}
+
+// process-wide count of kernels queued by this library
+static std::atomic<long long> g_launches{0};
+extern "C" void spiffe_note_launches(int n) { g_launches += n; }
+extern "C" int64_t spiffe_gpu_launch_count(void) { return g_launches.load(); }
+
+// Phases of one step, timed with CUDA events on the instance's stream.
+enum Phase { PH_EMIT, PH_DEPOSIT, PH_POISSON, PH_FDTD, PH_PUSH, PH_COUNT };
+
+struct PhaseTimer {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool[PH_COUNT];
+  size_t used[PH_COUNT] = {};
+  cudaEvent_t take_start(int ph)
+  {
+    if (used[ph] == pool[ph].size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      pool[ph].push_back({a, b});
+    }
+    return pool[ph][used[ph]].first;
+  }
+  void release()
+  {
+    for (auto &v : pool)
+      for (auto &e : v) {
+        cudaEventDestroy(e.first);
+        cudaEventDestroy(e.second);
+      }
+  }
+};
+
 #define CUDA_TRY(x)                                                                          \
   do {                                                                                       \
     cudaError_t e_ = (x);                                                                    \
@@ -168,6 +208,7 @@ struct spiffe_gpu_instance {
   DevScreens screens{};
   Fdtd64Tables fdtd;
   double fdtd_dt = -1;
+  long long fdtd_steps = 0;
   Particles64Work pw;
   Poisson64Work pcw;
   bool pc_ready = false;
@@ -185,6 +226,25 @@ struct spiffe_gpu_instance {
   BirthBin *d_bins = nullptr, *h_bins = nullptr;
   size_t bins_n = 0;
   double *h_probe = nullptr; // pinned scratch for single values
+  PhaseTimer timer;
+};
+
+// Brackets one phase with events when profiling is on.
+struct PhaseScope {
+  spiffe_gpu_instance *in;
+  int ph;
+  PhaseScope(spiffe_gpu_instance *i, int p) : in(i), ph(p)
+  {
+    if (in->timer.on)
+      cudaEventRecord(in->timer.take_start(ph), in->stream);
+  }
+  ~PhaseScope()
+  {
+    if (in->timer.on) {
+      cudaEventRecord(in->timer.pool[ph][in->timer.used[ph]].second, in->stream);
+      in->timer.used[ph]++;
+    }
+  }
 };
 
 // ------------------------------------------------------------- utilities
@@ -399,6 +459,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   spiffe_fdtd64_tables_free(&in->fdtd);
   spiffe_particles64_work_free(&in->pw);
   spiffe_poisson64_free(&in->pcw);
+  in->timer.release();
   if (in->h_cnt)
     cudaFreeHost(in->h_cnt);
   if (in->h_bins)
@@ -558,6 +619,8 @@ extern "C" int spiffe_gpu_advance_field_solutions(spiffe_gpu_instance *in)
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
   RC_TRY(ensure_fdtd(in));
+  PhaseScope ps(in, PH_FDTD);
+  in->fdtd_steps++;
   const int rc = spiffe_fdtd64_step(&in->dm, &in->f, &in->fdtd, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "FDTD launch failed: %s", cudaGetErrorString((cudaError_t)rc));
@@ -568,6 +631,7 @@ extern "C" int spiffe_gpu_add_particle_currents(spiffe_gpu_instance *in)
 {
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  PhaseScope ps(in, PH_DEPOSIT);
   const int rc = spiffe_deposit64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, in->deposit_ordered, &in->pw,
                                   in->stream);
   if (rc)
@@ -584,6 +648,7 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
   PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
                    o->tb_z_force, o->tb_r_force, o->tb_z_start_deceleration, o->tb_r_start_deceleration,
                    o->screen_momentum, o->compaction};
+  PhaseScope ps(in, PH_PUSH);
   const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
@@ -626,6 +691,7 @@ static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const s
     return 0;
   RC_TRY(ensure_poisson(in));
   PoissonHostOptions h{o->accuracy, o->error_charge_threshold, o->maximum_iterations, o->guess_code, space_charge};
+  PhaseScope ps(in, PH_POISSON);
   const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
@@ -908,6 +974,7 @@ static int ensure_bins(spiffe_gpu_instance *in, size_t n)
 // emit_electrons_from_cathode, cathode.c:239-671: counts on the host, births on the device.
 static int emit(spiffe_gpu_instance *in)
 {
+  PhaseScope ps(in, PH_EMIT);
   const spiffe_mesh &m = in->mesh;
   for (HostCathode &c : in->cathodes) {
     if (c.number_per_step == 0 && c.electrons_per_macroparticle == 0)
@@ -1241,5 +1308,67 @@ extern "C" int spiffe_gpu_counts(spiffe_gpu_instance *in, int64_t *np, int64_t *
     *np = in->h_cnt->np;
   if (np_active)
     *np_active = in->h_cnt->npActive;
+  return 0;
+}
+
+// ------------------------------------------------------------ measurement
+
+extern "C" int spiffe_gpu_select_device(int32_t device)
+{
+  CUDA_TRY(cudaSetDevice(device));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_stream(spiffe_gpu_instance *in, void **stream)
+{
+  if (!in || !stream)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  *stream = (void *)in->stream;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_profiling(spiffe_gpu_instance *in, int32_t on)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  in->timer.on = on != 0;
+  for (int p = 0; p < PH_COUNT; p++)
+    in->timer.used[p] = 0;
+  return 0;
+}
+
+// Per-phase device time since profiling was (re)started: emission, deposit,
+// Poisson correction, FDTD, push.  Synchronises the stream and restarts.
+extern "C" int spiffe_gpu_phase_times(spiffe_gpu_instance *in, double *ms, int64_t *count)
+{
+  if (!in || !ms || !count)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  for (int p = 0; p < PH_COUNT; p++) {
+    double total = 0;
+    for (size_t k = 0; k < in->timer.used[p]; k++) {
+      float e = 0;
+      CUDA_TRY(cudaEventElapsedTime(&e, in->timer.pool[p][k].first, in->timer.pool[p][k].second));
+      total += e;
+    }
+    ms[p] = total;
+    count[p] = (int64_t)in->timer.used[p];
+    in->timer.used[p] = 0;
+  }
+  return 0;
+}
+
+// Work done so far: [0] particle-steps (active particles summed over pushes),
+// [1] SOR half-sweeps, [2] SOR solves, [3] FDTD steps.
+extern "C" int spiffe_gpu_work_counters(spiffe_gpu_instance *in, int64_t *out)
+{
+  if (!in || !out)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(read_counts(in));
+  out[0] = in->h_cnt->pushed;
+  out[1] = in->h_cnt->sor_halfsweeps;
+  out[2] = in->h_cnt->sor_solves;
+  out[3] = in->fdtd_steps;
   return 0;
 }

@@ -71,6 +71,12 @@ def load():
         "spiffe_gpu_run_steps": ([H, C.c_int64], C.c_int),
         "spiffe_gpu_synchronize": ([H], C.c_int),
         "spiffe_gpu_counts": ([H, P(C.c_int64), P(C.c_int64)], C.c_int),
+        "spiffe_gpu_select_device": ([C.c_int32], C.c_int),
+        "spiffe_gpu_stream": ([H, P(C.c_void_p)], C.c_int),
+        "spiffe_gpu_set_profiling": ([H, C.c_int32], C.c_int),
+        "spiffe_gpu_phase_times": ([H, P(C.c_double), P(C.c_int64)], C.c_int),
+        "spiffe_gpu_launch_count": ([], C.c_int64),
+        "spiffe_gpu_work_counters": ([H, P(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -78,6 +84,15 @@ def load():
         fn.restype = res
     _lib = lib
     return lib
+
+
+def select_device(device):
+    """Device used by instances created afterwards on this thread."""
+    _check(load().spiffe_gpu_select_device(int(device)))
+
+
+def launch_count():
+    return load().spiffe_gpu_launch_count()
 
 
 def _check(rc):
@@ -212,6 +227,28 @@ class GpuInstance:
 
     def synchronize(self):
         _check(self.lib.spiffe_gpu_synchronize(self.h))
+
+    PHASES = ("emission", "deposit", "poisson", "fdtd", "push")
+
+    def stream_handle(self):
+        p = C.c_void_p()
+        _check(self.lib.spiffe_gpu_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def set_profiling(self, on):
+        _check(self.lib.spiffe_gpu_set_profiling(self.h, int(on)))
+
+    def phase_times(self):
+        ms = (C.c_double * 5)()
+        cnt = (C.c_int64 * 5)()
+        _check(self.lib.spiffe_gpu_phase_times(self.h, ms, cnt))
+        return {n: (ms[i], cnt[i]) for i, n in enumerate(self.PHASES)}
+
+    def work_counters(self):
+        """particle-steps, SOR half-sweeps, SOR solves, FDTD steps so far."""
+        out = (C.c_int64 * 4)()
+        _check(self.lib.spiffe_gpu_work_counters(self.h, out))
+        return dict(particle_steps=out[0], sor_halfsweeps=out[1], sor_solves=out[2], fdtd_steps=out[3])
 
     def counts(self):
         a, b = C.c_int64(), C.c_int64()

@@ -154,3 +154,88 @@ class PillboxConfig:
 
     def screen_z(self):
         return self.L - self.dz
+
+
+class Gun16Config:
+    """The 1.6-cell RF gun workload: half cell 17.5 mm and full cell 52.5 mm
+    of radius 41 mm, 10 mm irises 5 mm thick, a 10 mm beam pipe to z=150 mm,
+    mesh dr=dz=50 um (3001 x 821 nodes), dt = 0.5 x Courant.  Field: a
+    pi-mode standing wave (TM010 profile in each cell, opposite signs) with
+    100 MV/m on the cathode at t=0 and B=0.  Solenoid: Gaussian on-axis Bz,
+    0.25 T peak at z=100 mm, sigma 20 mm, extended off axis to first order
+    (Br = -r/2 dBz/dz).  Beam: 1 nC as 1,000,000 macroparticles from a 1 mm
+    disk with a 2 ps rms Gaussian emission time, already emitted: a particle
+    emitted tau before t=0 sits where uniform acceleration by the cathode
+    field carries it.  Poisson correction every 20 steps (accuracy 1e-6, at
+    most 1000 iterations)."""
+
+    def __init__(self, nz=3001, nr=821, length=0.150, radius=0.041, n_macro=1_000_000, charge=1e-9,
+                 sigma_t=2e-12, cathode_radius=1e-3, E_cathode=100e6, B_peak=0.25, B_z=0.100, B_sigma=0.020,
+                 step_interval=20, seed=1234):
+        self.nz, self.nr, self.length, self.radius = nz, nr, length, radius
+        self.zmin, self.zmax, self.rmax = 0.0, length, radius
+        self.dz = length / (nz - 1)
+        self.dr = radius / (nr - 1)
+        self.dt = 0.5 * min(self.dz, self.dr) / C_MKS / math.sqrt(2.0)
+        self.n_macro, self.charge, self.sigma_t = n_macro, charge, sigma_t
+        self.cathode_radius, self.E_cathode = cathode_radius, E_cathode
+        self.B_peak, self.B_z, self.B_sigma = B_peak, B_z, B_sigma
+        self.step_interval, self.seed = step_interval, seed
+
+    def geo_text(self):
+        return gun16_geo(pipe_r=10e-3, length=self.length, cavity_r=self.radius)
+
+    def cell_spans(self):
+        return [(0.0, 17.5e-3, -1.0), (22.5e-3, 75e-3, 1.0)]
+
+    def initial_ez(self, flags):
+        from scipy.special import j0, jn_zeros
+
+        x01 = float(jn_zeros(0, 1)[0])
+        nz, nr = self.nz, self.nr
+        z = (np.arange(nz + 1) - 0.5) * self.dz + self.zmin  # Ez nodes, spiffe.h:60
+        r = np.arange(nr + 1) * self.dr
+        ez = np.zeros((nz + 1, nr + 1))
+        prof = j0(x01 * r / self.radius)
+        prof[r > self.radius] = 0
+        for z0, z1, sign in self.cell_spans():
+            sel = (z > z0) & (z < z1)
+            ez[sel, :] = sign * prof[None, :]
+        ez[(flags & 4) != 0] = 0.0  # FL_EZ_ZERO
+        ez *= self.E_cathode / abs(ez[1, 0])
+        return ez
+
+    def solenoid(self):
+        z = np.arange(self.nz + 1) * self.dz + self.zmin  # BzImposed nodes, spiffe.h:114
+        r = np.arange(self.nr + 1) * self.dr
+        bz0 = self.B_peak * np.exp(-0.5 * ((z - self.B_z) / self.B_sigma) ** 2)
+        dbz = -bz0 * (z - self.B_z) / self.B_sigma ** 2
+        bz = np.repeat(bz0[:, None], self.nr + 1, axis=1)
+        br = -0.5 * r[None, :] * dbz[:, None]
+        return bz, br
+
+    def beam_arrays(self):
+        rng = np.random.default_rng(self.seed)
+        n = self.n_macro
+        te = rng.normal(0.0, self.sigma_t, n)
+        te = np.clip(te, -4 * self.sigma_t, 4 * self.sigma_t)
+        tau = 4 * self.sigma_t - te
+        kappa = E_MKS * self.E_cathode / (9.1093837015e-31 * C_MKS)
+        pz = kappa * tau
+        gamma = np.sqrt(1 + pz ** 2)
+        z = C_MKS / kappa * (gamma - 1) + 1e-9
+        r = self.cathode_radius * np.sqrt(rng.uniform(0, 1, n))
+        vz = C_MKS * pz / gamma
+        zeros = np.zeros(n)
+        return dict(z=z, r=r, pz=pz, pr=zeros, r_pphi=zeros, vz=vz, vr=zeros, vphi=zeros,
+                    Q=np.full(n, -self.charge / n), r0=r.copy(), z0=np.zeros(n), t0=-tau, rmin=r.copy(),
+                    rmax=r.copy(), zmin=np.zeros(n), zmax=z.copy(), particleID=np.arange(1, n + 1, dtype=np.int32),
+                    generation=np.zeros(n, np.int16), status=np.ones(n, np.uint64))
+
+    def screen_z(self):
+        return self.length - self.dz
+
+    def poisson(self):
+        from . import abi
+
+        return abi.poisson_options(step_interval=self.step_interval, accuracy=1e-6, maximum_iterations=1000)
