@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--precision", default="f64", choices=["f64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-steps", type=int, default=20, help="reference steps timed for the CPU baseline")
+    p.add_argument("--scale", type=int, default=1,
+                   help="coarsen the mesh by this factor and the beam by its square (small profiling cases)")
     return p.parse_args()
 
 
@@ -184,6 +186,14 @@ def reference_sample(cfg, steps, warmup=1, threads=None):
             "cell_updates_per_s": cfg.nz * cfg.nr * steps / secs if secs else 0.0}
 
 
+def scaled_config(scale):
+    from spiffe_b200 import workloads
+
+    if scale <= 1:
+        return workloads.Gun16Config()
+    return workloads.Gun16Config(nz=3000 // scale + 1, nr=820 // scale + 1, n_macro=1_000_000 // scale ** 2)
+
+
 def gpu_arm(args):
     import torch
 
@@ -200,7 +210,7 @@ def gpu_arm(args):
 
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
         dist = td
-    cfg = workloads.Gun16Config()
+    cfg = scaled_config(args.scale)
     f, b = build_state(cfg)
     K, W = args.steps, args.warmup
     push = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
@@ -374,7 +384,7 @@ def reference_arm(args):
     if not pyoracle.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libspiffe_ref.so was not built"}))
         return
-    cfg = workloads.Gun16Config()
+    cfg = scaled_config(args.scale)
     steps = min(args.steps, args.cpu_steps)
     s = reference_sample(cfg, steps, warmup=max(1, min(args.warmup, 1)))
     line = {

@@ -6,25 +6,11 @@
 // into the device beam, one thread per birth, drawing radius k from the
 // generator at counter base+k+1 so the stream is consumed exactly as the
 // serial reference consumes it (cathode.c:464-659).  Built with -fmad=false.
-#include "common.cuh"
+#include "modules.cuh"
 
 #include "../../include/spiffe_b200_rng.h"
 
-struct BirthBin {
-  long long start, count; // births [start, start+count) belong to this annulus
-  double area, rmin;
-};
 
-struct BirthParams {
-  long long total;
-  uint64_t key, counter_base; // draw k uses counter_base + k + 1
-  int mode;                   // 0 uniform in r^2, 1 per-annulus (correction), 2 discrete radii
-  int spread;                 // spread_over_dt
-  double z_position, inner_radius, outer_radius, inner_r2, dr2;
-  double initial_vz, initial_omega, Q, time, dt, QoMC, stiffness;
-  const BirthBin *bins;
-  int n_bins;
-};
 
 namespace {
 

@@ -9,7 +9,7 @@
 // FL_LAST_ACTIVE_PT" rule (integrate.c:345-346) becomes a per-row cut-off
 // index computed once on the host.  Built with -fmad=false so every product
 // and sum rounds as the reference's does.
-#include "common.cuh"
+#include "modules.cuh"
 
 namespace {
 
@@ -205,11 +205,6 @@ __global__ void __launch_bounds__(BX *BY) k_te_b(DevMesh m, DevFields<double> f,
 } // namespace
 
 // Host-side coefficient tables, computed with the reference's expressions.
-struct Fdtd64Tables {
-  double *cpz = nullptr, *cmz = nullptr, *bzf = nullptr;
-  int *cut0 = nullptr, *cut1 = nullptr;
-  double fEr = 0, topf = 0, fEphi = 0;
-};
 
 extern "C" int spiffe_fdtd64_tables(const DevMesh *m, const int16_t *host_flags, Fdtd64Tables *t, cudaStream_t s)
 {

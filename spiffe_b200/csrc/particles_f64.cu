@@ -9,7 +9,7 @@
 // bit-identical to the reference's given the same fields.  Deposition sums
 // with FP64 atomics by default (order-dependent in the last bits) or, in the
 // ordered mode, in particle order exactly as the serial reference does.
-#include "common.cuh"
+#include "modules.cuh"
 
 namespace {
 
@@ -786,15 +786,6 @@ __global__ void k_reset_step_counts(DevCounts *cnt)
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
-struct Particles64Work {
-  uint8_t *lost = nullptr;
-  int *surv = nullptr, *surv_before = nullptr, *map = nullptr;
-  int *keys = nullptr, *keys_alt = nullptr;
-  double *vals = nullptr, *vals_alt = nullptr;
-  void *cub_tmp = nullptr;
-  size_t cub_bytes = 0;
-  long long capacity = 0;
-};
 
 extern "C" int spiffe_particles64_work(Particles64Work *w, long long capacity, bool ordered)
 {
@@ -881,11 +872,6 @@ extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, co
   return (int)cudaGetLastError();
 }
 
-struct PushHostParams {
-  double time, z_forces_start, QoMC, stiffness;
-  double tb_epm, tb_z_force, tb_r_force, tb_z_decel, tb_r_decel;
-  int screen_momentum, compaction;
-};
 
 // advance_particles: snapshot, push with screens, then compaction.
 extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const PushHostParams *hp,

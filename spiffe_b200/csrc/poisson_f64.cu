@@ -13,7 +13,7 @@
 // sum is reduced in a fixed tree order rather than the reference's serial
 // order, which changes the half-sweep count only if the sum lands within
 // rounding distance of the threshold.  Built with -fmad=false.
-#include "common.cuh"
+#include "modules.cuh"
 
 #include <cooperative_groups.h>
 
@@ -36,12 +36,6 @@ __device__ double block_sum(double v, double *sh)
   __syncthreads();
   return r;
 }
-
-struct PcState {
-  double Qreal, Qerror, Qsurface, centroid, driving, residual;
-  long long iterations;
-  int do_solve, pad;
-};
 
 __device__ bool surface_cell(const DevMesh &m, int16_t fl, int iz, int ir)
 {
@@ -265,9 +259,10 @@ struct SorArgs {
   double *Psi;
   const double *rhs; // null for the Laplace solve of the imposed potential
   const int16_t *flags;
-  const double *omega; // omega[n] for half-sweep n
-  double a, e, accuracy;
-  const double *driving; // sum |rhs|
+  const double *omega;       // omega[n] for half-sweep n
+  const double *crow, *drow; // c and d of each row ir >= 1 (poisson.c:357-358)
+  double a, e, c4_axis, e2c_axis, accuracy; // 4c and e-2c of the axis row (poisson.c:361, :386-387)
+  const double *driving;     // sum |rhs|
   long long limit;
   double *partials; // 2*gridDim.x doubles
   unsigned *bar_count, *bar_gen;
@@ -275,8 +270,12 @@ struct SorArgs {
   long long *iterations_out;
 };
 
-// solve_poisson_cyl (poisson.c:17-130): rows 0..nr-2, iz over the rows the
-// boundary conditions leave free; colour (ir+iz)%2 == n%2 on half-sweep n.
+// solve_poisson_cyl (poisson.c:17-130): rows ir = 0..nr-2 of the iz the
+// boundary conditions leave free; half-sweep n updates the nodes with
+// (ir+iz)%2 == n%2.  Each block owns whole iz rows (block-strided) and its
+// threads visit only that row's nodes of the current colour, so a warp reads
+// every other Psi of a row.  Psi of neighbouring rows was written by other
+// blocks in the previous half-sweep, so it is read through L2 (ld.cg).
 __global__ void __launch_bounds__(RT) k_sor(DevMesh m, SorArgs s, DevCounts *cnt)
 {
   __shared__ double sh[RT];
@@ -285,58 +284,54 @@ __global__ void __launch_bounds__(RT) k_sor(DevMesh m, SorArgs s, DevCounts *cnt
   const int nz = m.nz, nr = m.nr, P = m.pitch;
   const int lo = m.left_bc == SPIFFE_DIRICHLET ? 0 : 1, hi = m.right_bc == SPIFFE_DIRICHLET ? nz - 1 : nz - 2;
   const int cols = nr - 1, rows = hi - lo + 1;
-  const long long work = (long long)rows * cols;
-  const double dr = m.dr, a = s.a, e = s.e, inv_dr2 = 1 / (dr * dr);
+  const double a = s.a, e = s.e;
   const double thr = s.accuracy * *s.driving;
   long long result = -1;
   double total = 0;
   for (long long n = 0; n < s.limit; n++) {
     const double omega = s.omega[n];
-    const int colour = (int)(n % 2);
+    const int colour = (int)(n & 1);
     double acc = 0;
-    for (long long w = (long long)blockIdx.x * RT + threadIdx.x; w < work; w += (long long)gridDim.x * RT) {
-      const int iz = lo + (int)(w / cols), ir = (int)(w % cols);
-      if ((ir + iz) % 2 != colour)
-        continue;
-      const size_t i = node(iz, ir, P);
-      if (s.flags[i] & SPIFFE_FL_IS_METAL)
-        continue;
-      // Psi written by other blocks last half-sweep: load through L2 only
-      double left, right;
-      if (iz == 0 && lo == 0)
-        left = right = __ldcg(s.Psi + i + P);
-      else if (iz == nz - 1 && hi == nz - 1)
-        left = right = __ldcg(s.Psi + i - P);
-      else {
-        left = __ldcg(s.Psi + i + P);
-        right = __ldcg(s.Psi + i - P);
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+      const int iz = lo + row;
+      const int parity = (colour + iz) & 1; // ir with (ir+iz)%2 == colour
+      const size_t base = node(iz, 0, P);
+      // the left and right Dirichlet rows mirror their only neighbour (poisson.c:369-375, :404-410)
+      const long up = (iz == 0 && lo == 0) ? P : (iz == nz - 1 && hi == nz - 1 ? -P : P);
+      const long dn = (iz == 0 && lo == 0) ? P : -P;
+      for (int ir = 2 * threadIdx.x + parity; ir < cols; ir += 2 * RT) {
+        const size_t i = base + ir;
+        if (s.flags[i] & SPIFFE_FL_IS_METAL)
+          continue;
+        const double left = __ldcg(s.Psi + i + up), right = __ldcg(s.Psi + i + dn);
+        const double drive = s.rhs ? s.rhs[i] : 0;
+        const double self = __ldcg(s.Psi + i);
+        double residual;
+        if (ir == 0) {
+          residual = a * (left + right) + s.c4_axis * __ldcg(s.Psi + i + 1) + s.e2c_axis * self - drive;
+          __stcg(s.Psi + i, self - omega * residual / s.e2c_axis);
+        } else {
+          residual = a * (left + right) + s.crow[ir] * __ldcg(s.Psi + i + 1) + s.drow[ir] * __ldcg(s.Psi + i - 1) +
+                     e * self - drive;
+          __stcg(s.Psi + i, self - omega * residual / e);
+        }
+        acc += fabs(residual);
       }
-      const double drive = s.rhs ? s.rhs[i] : 0;
-      const double self = __ldcg(s.Psi + i);
-      double residual;
-      if (ir == 0) {
-        const double c = inv_dr2;
-        residual = a * (left + right) + 4 * c * __ldcg(s.Psi + i + 1) + (e - 2 * c) * self - drive;
-        __stcg(s.Psi + i, self - omega * residual / (e - 2 * c));
-      } else {
-        const double c = inv_dr2 * (1 + 1. / (2 * ir)), d = inv_dr2 * (1 - 1. / (2 * ir));
-        residual = a * (left + right) + c * __ldcg(s.Psi + i + 1) + d * __ldcg(s.Psi + i - 1) + e * self - drive;
-        __stcg(s.Psi + i, self - omega * residual / e);
-      }
-      acc += fabs(residual);
     }
     // partial sums alternate between two halves of the buffer, so a block
     // that runs ahead cannot overwrite sums another block is still reading
-    double *part = s.partials + (size_t)(n % 2) * gridDim.x;
+    double *part = s.partials + (size_t)(n & 1) * gridDim.x;
     const double bs = block_sum(acc, sh);
     if (threadIdx.x == 0)
       __stcg(part + blockIdx.x, bs);
     __threadfence();
     if (!grid_barrier(s.bar_count, s.bar_gen, gridDim.x, cnt))
       return;
-    total = 0;
-    for (unsigned b = 0; b < gridDim.x; b++)
-      total += __ldcg(part + b);
+    // every block forms the same fixed-order sum of the partials
+    double v = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += RT)
+      v += __ldcg(part + b);
+    total = block_sum(v, sh);
     if (n > 0 && (total < thr || total == 0)) {
       result = n;
       break;
@@ -436,18 +431,6 @@ __global__ void k_set_state(PcState *st, double *qs_cen, double *qreal, double *
 
 // ---------------------------------------------------------------- host side
 
-struct Poisson64Work {
-  double *Az = nullptr, *Ari = nullptr, *Aro = nullptr, *volume = nullptr;
-  double *part = nullptr;    // block partials
-  double *scalars = nullptr; // [0..1] Qsurface/centroid, [2] Qreal, [3] Qerror, [4] driving
-  double *omega = nullptr;
-  long long omega_n = 0;
-  unsigned *bar = nullptr;
-  PcState *st = nullptr;
-  long long *iters = nullptr;
-  int sor_grid = 0;
-  size_t part_n = 0;
-};
 
 extern "C" int spiffe_poisson64_setup(const DevMesh *m, Poisson64Work *w, long long np_capacity, cudaStream_t s)
 {
@@ -494,7 +477,22 @@ extern "C" int spiffe_poisson64_setup(const DevMesh *m, Poisson64Work *w, long l
   if (e == cudaSuccess) e = cudaMemcpyAsync(w->Ari, Ari, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w->Aro, Aro, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(w->volume, vol, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  // SOR row coefficients with the reference's expressions (poisson.c:355-361)
+  double *crow = new double[nr + 1], *drow = new double[nr + 1];
+  for (int ir = 0; ir <= nr; ir++) {
+    if (ir != 0) {
+      crow[ir] = 1 / (dr * dr) * (1 + 1. / (2 * ir));
+      drow[ir] = 1 / (dr * dr) * (1 - 1. / (2 * ir));
+    } else
+      crow[ir] = drow[ir] = 1 / (dr * dr);
+  }
+  if (e == cudaSuccess && !w->crow) e = cudaMalloc(&w->crow, sizeof(double) * (nr + 1));
+  if (e == cudaSuccess && !w->drow) e = cudaMalloc(&w->drow, sizeof(double) * (nr + 1));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->crow, crow, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(w->drow, drow, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  delete[] crow;
+  delete[] drow;
   delete[] Az;
   delete[] Ari;
   delete[] Aro;
@@ -525,6 +523,8 @@ extern "C" void spiffe_poisson64_free(Poisson64Work *w)
   cudaFree(w->bar);
   cudaFree(w->st);
   cudaFree(w->iters);
+  cudaFree(w->crow);
+  cudaFree(w->drow);
   *w = Poisson64Work();
 }
 
@@ -586,6 +586,11 @@ static int launch_sor(const DevMesh *m, Poisson64Work *w, double *Psi, const dou
   a.omega = w->omega;
   a.a = 1 / (m->dz * m->dz);
   a.e = -2 * (1 / (m->dz * m->dz) + 1 / (m->dr * m->dr));
+  a.crow = w->crow;
+  a.drow = w->drow;
+  const double c_axis = 1 / (m->dr * m->dr);
+  a.c4_axis = 4 * c_axis;
+  a.e2c_axis = a.e - 2 * c_axis;
   a.accuracy = accuracy;
   a.driving = w->scalars + 4;
   a.limit = limit;
@@ -616,11 +621,6 @@ extern "C" int spiffe_sor64(const DevMesh *m, Poisson64Work *w, double *Psi, con
   return (int)cudaGetLastError();
 }
 
-struct PoissonHostOptions {
-  double accuracy, error_charge_threshold;
-  long long maximum_iterations;
-  int guess_code, space_charge;
-};
 
 // One add_poisson_correction pass (the interval test is the caller's).
 extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b,
