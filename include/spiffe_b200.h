@@ -80,6 +80,22 @@ int spiffe_gpu_advance_particles(spiffe_gpu_instance *inst, const spiffe_push_op
  * reference's return value (half-sweeps, or -1 at the limit). */
 int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *inst, int32_t target, double accuracy, int64_t iteration_limit,
                                  int64_t *iterations);
+/* No counterpart in the reference.  The same SOR solve on device arrays the
+ * caller owns (Psi updated in place; rhs may be NULL; flags int16; all
+ * (nz+1)*(nr+1), ir fastest), allocating nothing: for callers that may not
+ * allocate device memory, such as a host application whose device memory
+ * belongs to another framework's pool, or a control loop that forbids
+ * allocation after start-up.  All scratch lives in one fixed 352 KB array
+ * that every GPU loading the library holds until exit; limits: iteration_limit
+ * <= 16384, nr <= 4096, ceil((nr-1)/32)*ceil(nz/8) <= 16384.  Larger sizes
+ * are rejected with an error.  The first call on a device looks up that
+ * array's device address (with the device current), so make that first call
+ * before any stream capture.  Every call shares the one array: calls that
+ * overlap on the GPU (other threads, other streams) race and must be
+ * serialised by the caller.  `stream` is a cudaStream_t (NULL: the default
+ * stream); the call waits for the solve to finish. */
+int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, double *psi, const double *rhs, const int16_t *flags,
+                                         double accuracy, int64_t iteration_limit, int64_t *iterations, void *stream);
 /* add_poisson_correction, poisson_correction.c:73 (interval and start-step
  * tests included; `report` may be NULL) */
 int spiffe_gpu_add_poisson_correction(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_poisson_options *opt,

@@ -692,3 +692,207 @@ extern "C" int spiffe_imposed_field64(const DevMesh *m, const DevFields<double> 
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }
+
+// ----------------------------------------------- allocation-free SOR solve
+//
+// spiffe_gpu_solve_poisson_cyl_noalloc runs the same red-black SOR as
+// spiffe_gpu_solve_poisson_cyl on device arrays the caller owns, for callers
+// that must not allocate device memory: a host application whose device
+// memory is owned by another framework's pool, which has reserved it and
+// whose budget a cudaMalloc would break; or a control or real-time loop that
+// forbids allocation after start-up so a solve can never fail for lack of
+// memory or stall in the allocator.  Every piece of scratch the solve needs
+// (the Chebyshev factors, the row coefficients, the block partial sums, the
+// grid-barrier words and a counter block) lives in the fixed array below,
+// which every GPU that loads this library holds until the process exits.
+
+#define SPIFFE_NOALLOC_MAX_HALFSWEEPS 16384 // iteration_limit
+#define SPIFFE_NOALLOC_MAX_NR 4096          // nr
+#define SPIFFE_NOALLOC_MAX_PARTS 16384      // blocks of the |rhs| sum: ceil((nr-1)/32) * ceil(nz/8)
+#define SPIFFE_NOALLOC_MAX_GRID 1024        // SOR blocks
+
+struct NoallocScratch {
+  double omega[SPIFFE_NOALLOC_MAX_HALFSWEEPS];
+  double crow[SPIFFE_NOALLOC_MAX_NR + 1], drow[SPIFFE_NOALLOC_MAX_NR + 1];
+  double part[SPIFFE_NOALLOC_MAX_PARTS];
+  double sor_part[2 * SPIFFE_NOALLOC_MAX_GRID];
+  double driving;
+  long long iterations;
+  unsigned bar[2];
+  DevCounts cnt;
+};
+
+#define SPIFFE_NOALLOC_SCRATCH_BYTES (352u * 1024u)
+static_assert(sizeof(NoallocScratch) <= SPIFFE_NOALLOC_SCRATCH_BYTES, "no-alloc scratch too small");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SPIFFE_NOALLOC_SCRATCH_BYTES];
+
+#include <cstdio>
+#include <mutex>
+
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mutex;
+NoallocScratch *g_noalloc_addr[NOALLOC_MAX_DEVICES];
+int g_noalloc_grid[NOALLOC_MAX_DEVICES];
+// host staging for the tables, static so the call allocates nothing
+double g_noalloc_omega[SPIFFE_NOALLOC_MAX_HALFSWEEPS];
+double g_noalloc_crow[SPIFFE_NOALLOC_MAX_NR + 1], g_noalloc_drow[SPIFFE_NOALLOC_MAX_NR + 1];
+} // namespace
+
+extern "C" int spiffe_set_error(int code, const char *msg);
+
+extern "C" int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, double *psi, const double *rhs,
+                                                    const int16_t *flags, double accuracy, int64_t iteration_limit,
+                                                    int64_t *iterations, void *stream)
+{
+  char msg[256];
+  if (!mesh || !psi || !flags)
+    return spiffe_set_error(-1, "null argument");
+  if (accuracy <= 0)
+    return spiffe_set_error(-1, "accuracy is <= 0 in solve_poisson_cyl");
+  if (iteration_limit <= 1)
+    return spiffe_set_error(-1, "iteration_limit is <= 1 in solve_poisson_cyl");
+  const int nz = mesh->nz, nr = mesh->nr;
+  if (nz < 3 || nr < 4)
+    return spiffe_set_error(-1, "mesh too small (need nz>=3, nr>=4)");
+  if (iteration_limit > SPIFFE_NOALLOC_MAX_HALFSWEEPS) {
+    snprintf(msg, sizeof(msg), "iteration_limit %lld exceeds the allocation-free maximum of %d",
+             (long long)iteration_limit, SPIFFE_NOALLOC_MAX_HALFSWEEPS);
+    return spiffe_set_error(-1, msg);
+  }
+  if (nr > SPIFFE_NOALLOC_MAX_NR) {
+    snprintf(msg, sizeof(msg), "nr=%d exceeds the allocation-free maximum of %d", nr, SPIFFE_NOALLOC_MAX_NR);
+    return spiffe_set_error(-1, msg);
+  }
+  const dim3 sblock(BX, BY), sgrid((nr - 1 + BX - 1) / BX, (nz + BY - 1) / BY);
+  if ((size_t)sgrid.x * sgrid.y > SPIFFE_NOALLOC_MAX_PARTS) {
+    snprintf(msg, sizeof(msg), "mesh of %d x %d nodes exceeds the allocation-free maximum of %d sum blocks", nz, nr,
+             SPIFFE_NOALLOC_MAX_PARTS);
+    return spiffe_set_error(-1, msg);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+    return spiffe_set_error(-2, "no current CUDA device");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  // once per device, with that device current: the device address of the
+  // scratch array (its host-side name is not a device address)
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) {
+      snprintf(msg, sizeof(msg), "cudaGetSymbolAddress of the solver scratch failed: %s", cudaGetErrorString(e));
+      return spiffe_set_error(-2, msg);
+    }
+    int sms = 0, per = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sor, RT, 0);
+    if (per > 4)
+      per = 4;
+    int grid = sms * (per > 0 ? per : 1);
+    if (grid > SPIFFE_NOALLOC_MAX_GRID)
+      grid = SPIFFE_NOALLOC_MAX_GRID;
+    g_noalloc_grid[dev] = grid;
+    g_noalloc_addr[dev] = (NoallocScratch *)p;
+  }
+  NoallocScratch *sc = g_noalloc_addr[dev];
+  // the tables, with the expressions of the instance path (poisson.c:342-361)
+  const double dz = mesh->dz, dr = mesh->dr;
+  const double rz = dz / dr;
+  const double rj = (cos(SPIFFE_PI / nz) + rz * rz * cos(SPIFFE_PI / nr)) / (1 + rz * rz);
+  double omega = 1.0;
+  for (long long n = 0; n < iteration_limit; n++) {
+    g_noalloc_omega[n] = omega;
+    omega = n == 0 ? 1.0 / (1 - rj * rj / 2) : 1.0 / (1 - rj * rj * omega / 4);
+  }
+  for (int ir = 0; ir <= nr; ir++) {
+    if (ir != 0) {
+      g_noalloc_crow[ir] = 1 / (dr * dr) * (1 + 1. / (2 * ir));
+      g_noalloc_drow[ir] = 1 / (dr * dr) * (1 - 1. / (2 * ir));
+    } else
+      g_noalloc_crow[ir] = g_noalloc_drow[ir] = 1 / (dr * dr);
+  }
+  cudaError_t e = cudaMemcpyAsync(sc->omega, g_noalloc_omega, sizeof(double) * iteration_limit,
+                                  cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sc->crow, g_noalloc_crow, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(sc->drow, g_noalloc_drow, sizeof(double) * (nr + 1), cudaMemcpyHostToDevice, s);
+  // the array keeps the previous call's contents: clear what must start at zero
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(sc->bar, 0, sizeof(sc->bar), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(&sc->cnt, 0, sizeof(DevCounts), s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(&sc->iterations, 0, sizeof(long long), s);
+  if (e != cudaSuccess) {
+    snprintf(msg, sizeof(msg), "staging the solver tables failed: %s", cudaGetErrorString(e));
+    return spiffe_set_error(-2, msg);
+  }
+  DevMesh m{};
+  m.nz = nz;
+  m.nr = nr;
+  m.pitch = nr + 1;
+  m.zmin = mesh->zmin;
+  m.zmax = mesh->zmax;
+  m.rmax = mesh->rmax;
+  m.dz = dz;
+  m.dr = dr;
+  m.dt = mesh->dt;
+  m.lower_bc = mesh->lower_bc;
+  m.upper_bc = mesh->upper_bc;
+  m.right_bc = mesh->right_bc;
+  m.left_bc = mesh->left_bc;
+  m.modes = mesh->modes;
+  // sum |rhs| over iz < nz, ir < nr-1 (poisson.c:333-336), as the instance path forms it
+  if (rhs) {
+    k_region_sum<<<sgrid, sblock, 0, s>>>(rhs, nz, nr - 1, nr + 1, 1, sc->part);
+    spiffe_note_launches(1);
+    k_finish_sum<<<1, 1024, 0, s>>>(sc->part, sgrid.x * sgrid.y, 1, &sc->driving);
+    spiffe_note_launches(1);
+  } else {
+    cudaMemsetAsync(&sc->driving, 0, sizeof(double), s);
+  }
+  SorArgs a;
+  a.Psi = psi;
+  a.rhs = rhs;
+  a.flags = flags;
+  a.omega = sc->omega;
+  a.a = 1 / (dz * dz);
+  a.e = -2 * (1 / (dz * dz) + 1 / (dr * dr));
+  a.crow = sc->crow;
+  a.drow = sc->drow;
+  const double c_axis = 1 / (dr * dr);
+  a.c4_axis = 4 * c_axis;
+  a.e2c_axis = a.e - 2 * c_axis;
+  a.accuracy = accuracy;
+  a.driving = &sc->driving;
+  a.limit = iteration_limit;
+  a.partials = sc->sor_part;
+  a.bar_count = sc->bar;
+  a.bar_gen = sc->bar + 1;
+  a.st = nullptr;
+  a.iterations_out = &sc->iterations;
+  DevCounts *cnt = &sc->cnt;
+  void *args[] = {&m, &a, &cnt};
+  e = cudaLaunchCooperativeKernel((void *)k_sor, dim3(g_noalloc_grid[dev]), dim3(RT), args, 0, s);
+  spiffe_note_launches(1);
+  long long it = 0;
+  unsigned err = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&it, &sc->iterations, sizeof(it), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&err, &sc->cnt.error, sizeof(err), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    snprintf(msg, sizeof(msg), "allocation-free SOR failed: %s", cudaGetErrorString(e));
+    return spiffe_set_error(-2, msg);
+  }
+  if (err & SPIFFE_DEV_ERR_BARRIER)
+    return spiffe_set_error(-4, "allocation-free SOR: grid barrier timed out");
+  if (iterations)
+    *iterations = it;
+  return 0;
+}
