@@ -33,13 +33,24 @@ METRIC = "particle-steps/s & cell-updates/s per B200 at ≤0.5% moment error vs 
 UNIT = "particle-steps/s"
 QoMC = -1.602176634e-19 / (9.1093837015e-31 * 2.99792458e8)
 
-# algorithmic bytes per unit (FP64 form): the compulsory traffic of each phase
+# algorithmic bytes per unit: the compulsory traffic of each phase in each form
 BYTES = {
-    "fdtd": 74.0,     # per node-step: read Ez,Er,Bphi,Jz,Jr (40) + flags (2); write Ez,Er,Bphi,Bphi2 (32)
-    "push": 144.0,    # per particle-step: read 9 doubles + status (80); write 8 doubles (64)
-    "deposit": 80.0,  # per particle-step: z, r, v, Q, status for Jz and again for Jr
-    "sor": 13.0,      # per node and half-sweep: read Psi, rhs, flags; write half of Psi
-    "correction": 110.0,  # per node and correction: two flux passes, rhs scaling, gradient update
+    "f64": {
+        "fdtd": 74.0,     # per node-step: read Ez,Er,Bphi,Jz,Jr (40) + flags (2); write Ez,Er,Bphi,Bphi2 (32)
+        "push": 144.0,    # per particle-step: read 9 doubles + status (80); write 8 doubles (64)
+        "deposit": 80.0,  # per particle-step: z, r, v, Q, status for Jz and again for Jr
+        "sor": 13.0,      # per node and half-sweep: read Psi, rhs, flags; write half of Psi
+        "correction": 110.0,  # per node and correction: two flux passes, rhs scaling, gradient update
+    },
+    "split32": {
+        "fdtd": 61.0,     # per node-step: read Ez,Er,Bphi (12) + int64 Jz,Jr (16) + mask (1); write Ez,Er,
+                          # Bphi,Bphi2 (16); zero Jz,Jr (16)
+        "push": 86.0,     # per particle-step: read cell,fz,fr,pz,pr,r_pphi,Q,status,4 extrema (45); write all
+                          # but Q (41); the next step's deposition is fused in (its J traffic stays in L2)
+        "deposit": 29.0,  # per particle-step (first step only): cell, offsets, momenta, Q, status
+        "sor": 7.0,       # per node and half-sweep: FP32 d and r0 (the bands live in shared memory)
+        "correction": 90.0,  # per node and correction: flux passes, charge combine, rhs scaling, FP64 r0 and fold
+    },
 }
 
 
@@ -49,8 +60,13 @@ def parse():
     p.add_argument("--steps", type=int, default=600)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    p.add_argument("--precision", default="f64", choices=["f64"])
+    p.add_argument("--precision", default="split32", choices=["split32", "f64"],
+                   help="split32: FP32 fields/push, split positions, fixed-point current (the form the metric is "
+                        "quoted on); f64: the plain FP64 drop-in")
+    p.add_argument("--f64-steps", type=int, default=100,
+                   help="steps of the plain FP64 form timed on the same state for comparison (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling captures)")
     p.add_argument("--cpu-steps", type=int, default=20, help="reference steps timed for the CPU baseline")
     p.add_argument("--scale", type=int, default=1,
                    help="coarsen the mesh by this factor and the beam by its square (small profiling cases)")
@@ -194,6 +210,47 @@ def scaled_config(scale):
     return workloads.Gun16Config(nz=3000 // scale + 1, nr=820 // scale + 1, n_macro=1_000_000 // scale ** 2)
 
 
+def e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist):
+    """The same K steps end to end through the public API from pinned host
+    buffers: state upload, K single-step calls each reading the particle
+    count back, state download.  Returns (ms, particle-steps, state bytes)."""
+    import torch
+
+    from spiffe_b200 import gpu
+
+    pin = {}
+    for k, v in host_f.a.items():
+        host_f.a[k], pin[k] = pinned_like(v)
+    for k, v in host_b.a.items():
+        host_b.a[k], pin["b" + k] = pinned_like(v)
+    g2 = gpu.GpuInstance(f, capacity=b.capacity, precision=prec)
+    g2.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
+    g2.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
+    g2.set_mesh(mesh_w)
+    stream2 = torch.cuda.ExternalStream(g2.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    state_bytes = sum(v.nbytes for v in host_f.a.values()) + sum(
+        v[: host_b.np].nbytes for v in host_b.a.values()) + host_b.np * (4 + 2 + 8)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream2)
+    g2.upload_fields(host_f)
+    g2.upload_beam(host_b)
+    wb0 = g2.work_counters()
+    for _ in range(K):
+        g2.run_steps(1)
+        g2.counts()
+    wb1 = g2.work_counters()
+    g2.download_beam(host_b)
+    g2.download_fields(host_f)
+    e1.record(stream2)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    g2.close()
+    return ms, wb1["particle_steps"] - wb0["particle_steps"], state_bytes
+
+
 def gpu_arm(args):
     import torch
 
@@ -214,9 +271,11 @@ def gpu_arm(args):
     f, b = build_state(cfg)
     K, W = args.steps, args.warmup
     push = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
+    prec = gpu.PRECISION_SPLIT32 if args.precision == "split32" else gpu.PRECISION_F64
+    nbytes = BYTES[args.precision]
 
     # --- device-resident throughput
-    g = gpu.GpuInstance(f, capacity=b.capacity)
+    g = gpu.GpuInstance(f, capacity=b.capacity, precision=prec)
     g.upload_beam(b)
     g.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
     g.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
@@ -255,39 +314,36 @@ def gpu_arm(args):
     np_end, _ = g.counts()
     g.close()
 
-    # --- end to end through the public API from pinned host buffers: upload
-    # the state, K steps each reading the particle count back, download
-    pin = {}
-    for k, v in host_f.a.items():
-        host_f.a[k], pin[k] = pinned_like(v)
-    for k, v in host_b.a.items():
-        host_b.a[k], pin["b" + k] = pinned_like(v)
-    g2 = gpu.GpuInstance(f, capacity=b.capacity)
-    g2.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
-    g2.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
-    g2.set_mesh(mesh_w)
-    stream2 = torch.cuda.ExternalStream(g2.stream_handle())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    state_bytes = sum(v.nbytes for v in host_f.a.values()) + sum(
-        v[: host_b.np].nbytes for v in host_b.a.values()) + host_b.np * (4 + 2 + 8)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0.record(stream2)
-    g2.upload_fields(host_f)
-    g2.upload_beam(host_b)
-    wb0 = g2.work_counters()
-    for _ in range(K):
-        g2.run_steps(1)
-        g2.counts()
-    wb1 = g2.work_counters()
-    g2.download_beam(host_b)
-    g2.download_fields(host_f)
-    e1.record(stream2)
-    e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    e2e_psteps = wb1["particle_steps"] - wb0["particle_steps"]
-    g2.close()
+    f64_form = None
+    if prec == gpu.PRECISION_SPLIT32 and args.f64_steps > 0:
+        # the plain FP64 drop-in on the same post-warm-up state, same GPU, same run
+        g3 = gpu.GpuInstance(f, capacity=b.capacity, precision=gpu.PRECISION_F64)
+        g3.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
+        g3.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
+        g3.upload_fields(host_f)
+        g3.upload_beam(host_b)
+        g3.set_mesh(mesh_w)
+        s3 = torch.cuda.ExternalStream(g3.stream_handle())
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        K3 = args.f64_steps
+        g3.run_steps(2)
+        g3.synchronize()
+        x0 = g3.work_counters()
+        f0.record(s3)
+        g3.run_steps(K3)
+        f1.record(s3)
+        f1.synchronize()
+        x1 = g3.work_counters()
+        f64_val = (x1["particle_steps"] - x0["particle_steps"]) / (f0.elapsed_time(f1) / 1e3)
+        f64_form = {"value": round(f64_val, 1), "unit": UNIT, "steps": K3,
+                    "ms_per_step": round(f0.elapsed_time(f1) / K3, 4),
+                    "how": "plain FP64 drop-in on the same post-warm-up state and GPU, right after the split-form "
+                           "run; its K steps hold the same share of Poisson corrections (one per 20 steps)"}
+        g3.close()
+    # --- end to end through the public API from pinned host buffers
+    e2e_ms, e2e_psteps, state_bytes = 0.0, 0, 0
+    if not args.no_e2e:
+        e2e_ms, e2e_psteps, state_bytes = e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist)
 
     # --- totals over ranks (max time, summed work)
     if dist:
@@ -308,10 +364,10 @@ def gpu_arm(args):
     nodes = (cfg.nz + 1) * (cfg.nr + 1)
     sor_nodes = cfg.nz * (cfg.nr - 1)
     work_bytes = {
-        "fdtd": BYTES["fdtd"] * nodes * phases["fdtd"][1],
-        "push": BYTES["push"] * psteps,
-        "deposit": BYTES["deposit"] * psteps,
-        "poisson": BYTES["sor"] * sor_nodes * halfsweeps + BYTES["correction"] * nodes * solves,
+        "fdtd": nbytes["fdtd"] * nodes * phases["fdtd"][1],
+        "push": nbytes["push"] * psteps,
+        "deposit": nbytes["deposit"] * psteps if prec == gpu.PRECISION_F64 else nbytes["deposit"] * cfg.n_macro * phases["deposit"][1],
+        "poisson": nbytes["sor"] * sor_nodes * halfsweeps + nbytes["correction"] * nodes * solves,
         "emission": 0.0,
     }
     total_ms = sum(v[0] for v in phases.values()) or 1.0
@@ -336,10 +392,12 @@ def gpu_arm(args):
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": round(ms / K, 4), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f32" if prec == gpu.PRECISION_SPLIT32 else "f64", "data": "synthetic",
         "config": {"workload": "1.6-cell RF gun, 3001x821 nodes at 50um, 1,000,000 macroparticles, "
                                "Poisson correction every 20 steps, solenoid",
-                   "form": "plain FP64 (bit-faithful to the reference)",
+                   "form": ("split precision: FP32 fields and push, cell+FP32-offset positions, 64-bit fixed-point "
+                            "current, FP32 SOR in FP64 iterative refinement") if prec == gpu.PRECISION_SPLIT32
+                   else "plain FP64 (bit-faithful to the reference)",
                    "field": "analytic pi-mode standing wave, 100 MV/m on the cathode",
                    "particles": cfg.n_macro, "nodes": cfg.nz * cfg.nr, "steps_timed": K,
                    "l2": "no flush: the resident state (fields ~%d MB, beam ~%d MB) exceeds the 126 MB L2"
@@ -351,11 +409,14 @@ def gpu_arm(args):
         "roofline": roofline,
         "gpu_launches": launches,
         "clocks": clk,
-        "e2e": {"value": round(e2e_all / (e2e_ms / 1e3), 1), "unit": UNIT,
+        "e2e": None if args.no_e2e else {"value": round(e2e_all / (e2e_ms / 1e3), 1), "unit": UNIT,
                 "h2d_bytes_per_step": int(state_bytes / K), "d2h_bytes_per_step": int((state_bytes + 8 * K) / K),
                 "how": "public API from pinned host buffers: state upload, K single-step calls each reading the "
                        "particle count back, state download"},
     }
+    if f64_form:
+        f64_form["split_over_f64"] = round(value / f64_form["value"], 3) if f64_form["value"] else None
+        line["f64_form"] = f64_form
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             s = reference_sample(cfg, args.cpu_steps)

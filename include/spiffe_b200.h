@@ -137,6 +137,11 @@ int spiffe_gpu_stream(spiffe_gpu_instance *inst, void **stream);
 int spiffe_gpu_set_profiling(spiffe_gpu_instance *inst, int32_t on);
 int spiffe_gpu_phase_times(spiffe_gpu_instance *inst, double *ms, int64_t *count);
 int64_t spiffe_gpu_launch_count(void);
+/* Split-precision form only (no counterpart in the reference): reorder the
+ * particles by mesh cell every n steps of spiffe_gpu_run_steps (default 20;
+ * 0 never), which keeps the gather and the deposition of neighbouring
+ * threads on the same nodes.  No effect on the FP64 form. */
+int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *inst, int64_t n);
 /* Work done so far: out[0] particle-steps (active particles summed over
  * pushes), out[1] SOR half-sweeps, out[2] SOR solves, out[3] FDTD steps. */
 int spiffe_gpu_work_counters(spiffe_gpu_instance *inst, int64_t *out);

@@ -512,14 +512,16 @@ __device__ void contrib_jz(const DevMesh &m, double z, double r, double v, doubl
   const int P = m.pitch;
   c.node[c.n] = (int)node((int)iz, (int)ir, P);
   c.val[c.n++] = fm * Jm;
-  if (lsm) {
+  // row iz+1 exists only for iz < nz; at iz == nz its weight is zero (the
+  // reference would index past the last row)
+  if (lsm && iz < nz) {
     c.node[c.n] = (int)node((int)iz + 1, (int)ir, P);
     c.val[c.n++] = fp * Jm;
   }
   if (rsm) {
     c.node[c.n] = (int)node((int)iz, (int)ir + 1, P);
     c.val[c.n++] = fm * Jp;
-    if (lsm) {
+    if (lsm && iz < nz) {
       c.node[c.n] = (int)node((int)iz + 1, (int)ir + 1, P);
       c.val[c.n++] = fp * Jp;
     }
@@ -572,14 +574,16 @@ __device__ void contrib_jr(const DevMesh &m, double z, double r, double v, doubl
   const int P = m.pitch;
   c.node[c.n] = (int)node((int)iz, (int)ir, P);
   c.val[c.n++] = fm * Jm;
-  if (lsm) {
+  // row iz+1 exists only for iz < nz; at iz == nz its weight is zero (the
+  // reference would index past the last row)
+  if (lsm && iz < nz) {
     c.node[c.n] = (int)node((int)iz + 1, (int)ir, P);
     c.val[c.n++] = fp * Jm;
   }
   if (rsm) {
     c.node[c.n] = (int)node((int)iz, (int)ir + 1, P);
     c.val[c.n++] = fm * Jp;
-    if (lsm) {
+    if (lsm && iz < nz) {
       c.node[c.n] = (int)node((int)iz + 1, (int)ir + 1, P);
       c.val[c.n++] = fp * Jp;
     }
@@ -632,14 +636,16 @@ __device__ void contrib_jphi(const DevMesh &m, double z, double r, double v, dou
   const int P = m.pitch;
   c.node[c.n] = (int)node((int)iz, (int)ir, P);
   c.val[c.n++] = fm * Jm;
-  if (lsm) {
+  // row iz+1 exists only for iz < nz; at iz == nz its weight is zero (the
+  // reference would index past the last row)
+  if (lsm && iz < nz) {
     c.node[c.n] = (int)node((int)iz + 1, (int)ir, P);
     c.val[c.n++] = fp * Jm;
   }
   if (rsm) {
     c.node[c.n] = (int)node((int)iz, (int)ir + 1, P);
     c.val[c.n++] = fm * Jp;
-    if (lsm) {
+    if (lsm && iz < nz) {
       c.node[c.n] = (int)node((int)iz + 1, (int)ir + 1, P);
       c.val[c.n++] = fp * Jp;
     }

@@ -22,6 +22,7 @@
 #include "../../include/spiffe_b200_rng.h"
 
 #include "modules.cuh"
+#include "split32.cuh"
 
 // ---------------------------------------------------------------- errors
 static thread_local std::string g_error;
@@ -116,8 +117,30 @@ struct HostAntenna {
   long last_index = 0;
 };
 
+// Device state of the split-precision form (split32.cuh).
+enum { S32_J_UNKNOWN = 0, S32_J_ZERO = 1, S32_J_DEPOSITED = 2 };
+struct S32State {
+  DevFields32 f{};
+  DevBeam32 b{};
+  uint8_t *umask = nullptr;
+  Fdtd32Tables fdtd;
+  double fdtd_dt = -1;
+  Particles32Work pw;
+  Poisson32Work pcw;
+  bool pc_ready = false;
+  int qexp = -60; // q_ref = 2^qexp bounds |Q| of every macroparticle (fixed-point scale)
+  S32Scales sc{};
+  // what J holds: unknown, zero, or exactly the deposit of the current
+  // particles (left by the push of the previous step inside the loop)
+  int j_state = S32_J_UNKNOWN;
+  long long sort_interval = 20, since_sort = 0;
+  double *staging = nullptr; // device FP64 staging for host transfers
+  size_t staging_n = 0;
+};
+
 struct spiffe_gpu_instance {
   int precision = SPIFFE_PRECISION_F64;
+  S32State *s32 = nullptr; // the split-precision form's device state (null for FP64)
   spiffe_mesh mesh{};
   DevMesh dm{};
   cudaStream_t stream = nullptr;
@@ -178,7 +201,7 @@ static void set_devmesh(spiffe_gpu_instance *in)
   DevMesh &d = in->dm;
   d.nz = m.nz;
   d.nr = m.nr;
-  d.pitch = m.nr + 1;
+  d.pitch = in->s32 ? (m.nr + 1 + 31) / 32 * 32 : m.nr + 1;
   d.zmin = m.zmin;
   d.zmax = m.zmax;
   d.rmax = m.rmax;
@@ -196,7 +219,7 @@ static void set_devmesh(spiffe_gpu_instance *in)
   }
   for (int k = 0; k < 6; k++)
     d.turn_off[k] = m.turn_off[k];
-  d.has_solenoid = m.has_solenoid && in->f.BzImposed != nullptr;
+  d.has_solenoid = m.has_solenoid && (in->s32 ? in->s32->f.BzImposed != nullptr : in->f.BzImposed != nullptr);
 }
 
 static int alloc_field(double **p, size_t n, cudaStream_t s)
@@ -226,11 +249,15 @@ static void free_beam(DevBeam64 *b)
   *b = DevBeam64{};
 }
 
+static int s32_grow(spiffe_gpu_instance *in, long long need);
+
 // Grows the particle arrays so `need` particles fit (trealloc of cathode.c:427-456).
 static int grow_beam(spiffe_gpu_instance *in, long long need)
 {
   if (need <= in->capacity)
     return 0;
+  if (in->s32)
+    return s32_grow(in, need);
   long long cap = in->capacity * 3 / 2;
   if (cap < need + need / 10 + 1)
     cap = need + need / 10 + 1;
@@ -262,6 +289,8 @@ static int read_counts(spiffe_gpu_instance *in)
     return fail(SPIFFE_ERR_CAPACITY, "particle capacity exceeded on the device");
   if (in->h_cnt->error & SPIFFE_DEV_ERR_BARRIER)
     return fail(SPIFFE_ERR_DEVICE, "Poisson solver grid barrier timed out");
+  if (in->h_cnt->error & SPIFFE_DEV_ERR_INDEX)
+    return fail(SPIFFE_ERR_INVALID, "a particle moved more than 32767 cells outside the mesh (split-precision cell range)");
   if (in->h_cnt->screen_overflow)
     return fail(SPIFFE_ERR_CAPACITY, "screen record capacity exceeded (%lld records dropped)",
                 in->h_cnt->screen_overflow);
@@ -286,6 +315,401 @@ static int ensure_poisson(spiffe_gpu_instance *in)
   return 0;
 }
 
+// ------------------------------------------------- split-precision form
+//
+// The same entry points on the split32.cuh representation.  Host arrays
+// cross the boundary as FP64 and are converted on the device through one
+// FP64 staging buffer; inside the integration loop the deposition of step
+// n+1 is fused into the push of step n (j_state tracks what J holds).
+
+static int s32_staging(spiffe_gpu_instance *in, size_t n)
+{
+  S32State &S = *in->s32;
+  if (S.staging_n >= n)
+    return 0;
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  cudaFree(S.staging);
+  S.staging = nullptr;
+  S.staging_n = 0;
+  CUDA_TRY(cudaMalloc(&S.staging, n * sizeof(double)));
+  S.staging_n = n;
+  return 0;
+}
+
+static void s32_scales(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  const spiffe_mesh &m = in->mesh;
+  const double q_ref = std::ldexp(1.0, S.qexp);
+  const double one_over = 1 / (SPIFFE_PI * m.dz * (m.dr * m.dr));
+  S.sc.s_charge = (float)std::ldexp(1.0, 38 - S.qexp);
+  S.sc.sq_charge = S.sc.s_charge;
+  S.sc.qJ = 4 * q_ref * SPIFFE_C_MKS * one_over * std::ldexp(1.0, -40);
+  S.sc.kJ = (float)(-m.dt * S.sc.qJ / SPIFFE_EPSILON_O);
+  S.sc.qQ = std::ldexp(1.0, S.qexp - 38);
+}
+
+static size_t s32_nodes(const spiffe_gpu_instance *in) { return (size_t)(in->mesh.nz + 1) * (size_t)in->dm.pitch; }
+
+// Makes the fixed-point scale cover a macroparticle charge |Q| = qabs: the
+// quantum grows by a power of two and the currents already accumulated are
+// rescaled to it.
+static int s32_cover_charge(spiffe_gpu_instance *in, double qabs)
+{
+  S32State &S = *in->s32;
+  if (!(qabs > std::ldexp(1.0, S.qexp)) || !std::isfinite(qabs))
+    return 0;
+  int e = 0;
+  std::frexp(qabs, &e); // qabs < 2^e
+  const int shift = e - S.qexp;
+  const size_t n = s32_nodes(in);
+  long long *J[] = {S.f.Jz, S.f.Jr, S.f.Jphi};
+  for (long long *a : J)
+    RC_TRY(s32_rescale_fixed(a, n, shift, in->stream));
+  S.qexp = e;
+  s32_scales(in);
+  return 0;
+}
+
+static int s32_alloc_f(float **p, size_t n, cudaStream_t s)
+{
+  CUDA_TRY(cudaMalloc(p, n * sizeof(float)));
+  CUDA_TRY(cudaMemsetAsync(*p, 0, n * sizeof(float), s));
+  return 0;
+}
+
+template <typename T> static int s32_alloc_z(T **p, size_t n, cudaStream_t s)
+{
+  CUDA_TRY(cudaMalloc(p, n * sizeof(T)));
+  CUDA_TRY(cudaMemsetAsync(*p, 0, n * sizeof(T), s));
+  return 0;
+}
+
+static int s32_create(spiffe_gpu_instance *in, const int16_t *flags)
+{
+  in->s32 = new S32State();
+  S32State &S = *in->s32;
+  set_devmesh(in);
+  const int nz = in->mesh.nz, nr = in->mesh.nr, P = in->dm.pitch;
+  const size_t n = s32_nodes(in);
+  cudaStream_t s = in->stream;
+  RC_TRY(s32_alloc_z(&in->d_flags, n, s));
+  CUDA_TRY(cudaMemcpy2DAsync(in->d_flags, (size_t)P * sizeof(int16_t), flags, (size_t)(nr + 1) * sizeof(int16_t),
+                             (size_t)(nr + 1) * sizeof(int16_t), (size_t)nz + 1, cudaMemcpyHostToDevice, s));
+  RC_TRY(s32_alloc_z(&S.umask, n, s));
+  S.f.flags = in->d_flags;
+  S.f.umask = S.umask;
+  if (in->mesh.modes & SPIFFE_FL_TM_FIELDS) {
+    float **tm[] = {&S.f.Ez, &S.f.Er, &S.f.Bphi, &S.f.Bphi2};
+    for (float **p : tm)
+      RC_TRY(s32_alloc_f(p, n, s));
+    RC_TRY(s32_alloc_z(&S.f.Jz, n, s));
+    RC_TRY(s32_alloc_z(&S.f.Jr, n, s));
+  }
+  if (in->mesh.modes & SPIFFE_FL_TE_FIELDS) {
+    float **te[] = {&S.f.Ephi, &S.f.Br, &S.f.Br2, &S.f.Bz, &S.f.Bz2};
+    for (float **p : te)
+      RC_TRY(s32_alloc_f(p, n, s));
+    RC_TRY(s32_alloc_z(&S.f.Jphi, n, s));
+  }
+  RC_TRY(s32_alloc_f(&S.f.EzImposed, n, s));
+  RC_TRY(s32_alloc_f(&S.f.ErImposed, n, s));
+  RC_TRY(s32_alloc_z(&S.f.Psi, n, s));
+  RC_TRY(s32_alloc_z(&S.f.PsiImposed, n, s));
+  RC_TRY(s32_alloc_z(&S.f.Q, n, s));
+  RC_TRY(s32_alloc_z(&S.f.Qp, n, s));
+  RC_TRY(s32_beam_alloc(&S.b, in->capacity));
+  RC_TRY(s32_particles_work(&S.pw, in->capacity));
+  RC_TRY(s32_fdtd_tables(&in->dm, in->h_flags.data(), &S.fdtd, S.umask, s));
+  S.fdtd_dt = in->mesh.dt;
+  s32_scales(in);
+  S.j_state = S32_J_ZERO;
+  return 0;
+}
+
+static void s32_destroy(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  void *p[] = {S.f.Ez, S.f.Er, S.f.Bphi, S.f.Bphi2, S.f.Ephi, S.f.Br, S.f.Br2, S.f.Bz, S.f.Bz2,
+               S.f.EzImposed, S.f.ErImposed, S.f.BzImposed, S.f.BrImposed, S.f.Jz, S.f.Jr, S.f.Jphi,
+               S.f.Psi, S.f.PsiImposed, S.f.Q, S.f.Qp, S.umask, S.staging};
+  for (void *q : p)
+    cudaFree(q);
+  s32_beam_free(&S.b);
+  s32_particles_work_free(&S.pw);
+  s32_poisson_free(&S.pcw);
+  s32_fdtd_tables_free(&S.fdtd);
+  delete in->s32;
+  in->s32 = nullptr;
+}
+
+static int s32_grow(spiffe_gpu_instance *in, long long need)
+{
+  S32State &S = *in->s32;
+  long long cap = in->capacity * 3 / 2;
+  if (cap < need + need / 10 + 1)
+    cap = need + need / 10 + 1;
+  DevBeam32 nb{};
+  RC_TRY(s32_beam_alloc(&nb, cap));
+  RC_TRY(s32_beam_copy(&nb, &S.b, in->capacity, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  s32_beam_free(&S.b);
+  S.b = nb;
+  in->capacity = cap;
+  RC_TRY(s32_particles_work(&S.pw, cap));
+  return 0;
+}
+
+static int s32_ensure_fdtd(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  if (S.fdtd_dt == in->mesh.dt)
+    return 0;
+  RC_TRY(s32_fdtd_tables(&in->dm, in->h_flags.data(), &S.fdtd, S.umask, in->stream));
+  S.fdtd_dt = in->mesh.dt;
+  s32_scales(in);
+  return 0;
+}
+
+static int s32_ensure_poisson(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  if (S.pc_ready)
+    return 0;
+  const int rc = s32_poisson_setup(&in->dm, &S.pcw, in->capacity, in->stream);
+  if (rc == (int)cudaErrorInvalidConfiguration)
+    return fail(SPIFFE_ERR_UNSUPPORTED,
+                "mesh %d x %d is too large for the shared-memory Poisson solver of the split-precision form",
+                in->mesh.nz, in->mesh.nr);
+  RC_TRY(rc);
+  S.pc_ready = true;
+  return 0;
+}
+
+#define S32_FLOAT_FIELDS(X) X(Ez) X(Er) X(Bphi) X(Bphi2) X(Ephi) X(Br) X(Br2) X(Bz) X(Bz2) \
+  X(EzImposed) X(ErImposed) X(BzImposed) X(BrImposed)
+#define S32_F64_FIELDS(X) X(Psi) X(PsiImposed) X(Q)
+#define S32_FIXED_FIELDS(X) X(Jz) X(Jr) X(Jphi)
+
+static int s32_upload_fields(spiffe_gpu_instance *in, const spiffe_field_set *h)
+{
+  S32State &S = *in->s32;
+  const size_t bytes = in->nodes * sizeof(double);
+  cudaStream_t s = in->stream;
+  RC_TRY(s32_staging(in, in->nodes));
+  if (h->BzImposed && !S.f.BzImposed) {
+    RC_TRY(s32_alloc_f(&S.f.BzImposed, s32_nodes(in), s));
+    RC_TRY(s32_alloc_f(&S.f.BrImposed, s32_nodes(in), s));
+  }
+#define UP(x, call)                                                                             \
+  if (h->x) {                                                                                   \
+    if (!S.f.x)                                                                                 \
+      return fail(SPIFFE_ERR_INVALID, "array " #x " is not part of this instance's field modes"); \
+    CUDA_TRY(cudaMemcpyAsync(S.staging, h->x, bytes, cudaMemcpyHostToDevice, s));               \
+    RC_TRY(call);                                                                               \
+  }
+#define UPF(x) UP(x, s32_to_f32(&in->dm, S.staging, S.f.x, s))
+#define UPD(x) UP(x, s32_to_f64p(&in->dm, S.staging, S.f.x, s))
+#define UPJ(x) UP(x, s32_to_fixed(&in->dm, S.staging, S.f.x, S.sc.qJ, s))
+  S32_FLOAT_FIELDS(UPF)
+  S32_F64_FIELDS(UPD)
+  S32_FIXED_FIELDS(UPJ)
+#undef UPF
+#undef UPD
+#undef UPJ
+#undef UP
+  if (h->Jz || h->Jr || h->Jphi)
+    S.j_state = S32_J_UNKNOWN;
+  set_devmesh(in);
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+static int s32_download_fields(spiffe_gpu_instance *in, spiffe_field_set *h)
+{
+  S32State &S = *in->s32;
+  const size_t bytes = in->nodes * sizeof(double);
+  cudaStream_t s = in->stream;
+  RC_TRY(s32_staging(in, in->nodes));
+#define DOWN(x, call)                                                           \
+  if (h->x && S.f.x) {                                                          \
+    RC_TRY(call);                                                               \
+    CUDA_TRY(cudaMemcpyAsync(h->x, S.staging, bytes, cudaMemcpyDeviceToHost, s)); \
+  }
+#define DOF(x) DOWN(x, s32_from_f32(&in->dm, S.f.x, S.staging, s))
+#define DOD(x) DOWN(x, s32_from_f64p(&in->dm, S.f.x, S.staging, s))
+#define DOJ(x) DOWN(x, s32_from_fixed(&in->dm, S.f.x, S.staging, S.sc.qJ, s))
+  S32_FLOAT_FIELDS(DOF)
+  S32_F64_FIELDS(DOD)
+  S32_FIXED_FIELDS(DOJ)
+#undef DOF
+#undef DOD
+#undef DOJ
+#undef DOWN
+  if (h->flags)
+    CUDA_TRY(cudaMemcpy2DAsync(h->flags, (size_t)(in->mesh.nr + 1) * sizeof(int16_t), in->d_flags,
+                               (size_t)in->dm.pitch * sizeof(int16_t), (size_t)(in->mesh.nr + 1) * sizeof(int16_t),
+                               (size_t)in->mesh.nz + 1, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  return 0;
+}
+
+static int s32_upload_beam(spiffe_gpu_instance *in, const spiffe_beam_set *h)
+{
+  S32State &S = *in->s32;
+  cudaStream_t s = in->stream;
+  const long long n = h->np;
+  const size_t nn = (size_t)n;
+  if (n) {
+    const void *need[] = {h->z, h->r, h->pz, h->pr, h->r_pphi, h->Q, h->r0, h->z0, h->t0, h->rmin, h->rmax,
+                          h->zmin, h->zmax, h->particleID, h->generation, h->status};
+    for (const void *p : need)
+      if (!p)
+        return fail(SPIFFE_ERR_INVALID, "beam array missing");
+    RC_TRY(s32_staging(in, 2 * nn));
+    CUDA_TRY(cudaMemcpyAsync(S.staging, h->z, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(S.staging + nn, h->r, nn * sizeof(double), cudaMemcpyHostToDevice, s));
+    RC_TRY(s32_beam_pack_pos(&in->dm, S.staging, S.staging + nn, &S.b, n, in->cnt, s));
+#define UPB(hx, dx)                                                                                 \
+  CUDA_TRY(cudaMemcpyAsync(S.staging, h->hx, nn * sizeof(double), cudaMemcpyHostToDevice, s));     \
+  RC_TRY(s32_d2f(S.staging, S.b.dx, n, s));
+    UPB(pz, pz) UPB(pr, pr) UPB(r_pphi, rpphi) UPB(Q, Q) UPB(zmin, zmin) UPB(zmax, zmax) UPB(rmin, rmin)
+    UPB(rmax, rmax)
+#undef UPB
+#define UPD(x) CUDA_TRY(cudaMemcpyAsync(S.b.x, h->x, nn * sizeof(*h->x), cudaMemcpyHostToDevice, s));
+    UPD(r0) UPD(z0) UPD(t0) UPD(particleID) UPD(generation)
+#undef UPD
+    CUDA_TRY(cudaMemcpyAsync(S.staging, h->status, nn * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+    RC_TRY(s32_status_pack((const uint64_t *)S.staging, S.b.status, n, s));
+    double qmax = 0;
+    for (size_t i = 0; i < nn; i++)
+      qmax = std::fmax(qmax, std::fabs(h->Q[i]));
+    RC_TRY(s32_cover_charge(in, qmax));
+  }
+  RC_TRY(read_counts(in));
+  in->h_cnt->np = h->np;
+  in->h_cnt->npActive = h->npActive;
+  in->h_cnt->nextParticleID = h->nextParticleID;
+  CUDA_TRY(cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  RC_TRY(read_counts(in));
+  in->np_upper = h->np;
+  in->QoMC = h->QoMC;
+  in->stiffness = h->stiffness;
+  S.j_state = S32_J_UNKNOWN;
+  return 0;
+}
+
+static int s32_download_beam(spiffe_gpu_instance *in, spiffe_beam_set *h)
+{
+  S32State &S = *in->s32;
+  RC_TRY(read_counts(in));
+  const long long np = in->h_cnt->np;
+  if (np > h->capacity)
+    return fail(SPIFFE_ERR_CAPACITY, "host beam holds %lld particles, device has %lld", (long long)h->capacity, np);
+  cudaStream_t s = in->stream;
+  const size_t n = (size_t)np;
+  if (n) {
+    RC_TRY(s32_staging(in, 3 * n));
+    double *a = S.staging, *b = S.staging + n, *c = S.staging + 2 * n;
+    RC_TRY(s32_beam_unpack_pos(&in->dm, &S.b, a, b, np, s));
+    if (h->z) CUDA_TRY(cudaMemcpyAsync(h->z, a, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->r) CUDA_TRY(cudaMemcpyAsync(h->r, b, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    RC_TRY(s32_beam_unpack_vel(&in->dm, &S.b, a, b, c, np, s));
+    if (h->vz) CUDA_TRY(cudaMemcpyAsync(h->vz, a, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->vr) CUDA_TRY(cudaMemcpyAsync(h->vr, b, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (h->vphi) CUDA_TRY(cudaMemcpyAsync(h->vphi, c, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+#define DNB(hx, dx)                                                                               \
+  if (h->hx) {                                                                                    \
+    RC_TRY(s32_f2d(S.b.dx, a, np, s));                                                            \
+    CUDA_TRY(cudaMemcpyAsync(h->hx, a, n * sizeof(double), cudaMemcpyDeviceToHost, s));           \
+  }
+    DNB(pz, pz) DNB(pr, pr) DNB(r_pphi, rpphi) DNB(Q, Q) DNB(zmin, zmin) DNB(zmax, zmax) DNB(rmin, rmin)
+    DNB(rmax, rmax)
+#undef DNB
+#define DND(x) if (h->x) CUDA_TRY(cudaMemcpyAsync(h->x, S.b.x, n * sizeof(*h->x), cudaMemcpyDeviceToHost, s));
+    DND(r0) DND(z0) DND(t0) DND(particleID) DND(generation)
+#undef DND
+    if (h->status) {
+      RC_TRY(s32_status_unpack(S.b.status, (uint64_t *)a, np, s));
+      CUDA_TRY(cudaMemcpyAsync(h->status, a, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(s));
+  h->np = np;
+  h->npActive = in->h_cnt->npActive;
+  h->nextParticleID = (int32_t)in->h_cnt->nextParticleID;
+  h->QoMC = in->QoMC;
+  h->stiffness = in->stiffness;
+  return 0;
+}
+
+static int s32_zero_j(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  const size_t bytes = s32_nodes(in) * sizeof(long long);
+  long long *J[] = {S.f.Jz, S.f.Jr, S.f.Jphi};
+  for (long long *a : J)
+    if (a)
+      CUDA_TRY(cudaMemsetAsync(a, 0, bytes, in->stream));
+  S.j_state = S32_J_ZERO;
+  return 0;
+}
+
+static int s32_fdtd(spiffe_gpu_instance *in, int zero_j)
+{
+  S32State &S = *in->s32;
+  RC_TRY(s32_ensure_fdtd(in));
+  PhaseScope ps(in, PH_FDTD);
+  in->fdtd_steps++;
+  const int rc = s32_fdtd_step(&in->dm, &S.f, &S.fdtd, S.sc.kJ, zero_j, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "FDTD launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  if (zero_j)
+    S.j_state = S32_J_ZERO;
+  return 0;
+}
+
+static int s32_deposit_all(spiffe_gpu_instance *in)
+{
+  S32State &S = *in->s32;
+  PhaseScope ps(in, PH_DEPOSIT);
+  const int rc = s32_deposit(&in->dm, &S.f, &S.b, in->cnt, in->np_upper, &S.sc, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "deposition launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, int deposit)
+{
+  S32State &S = *in->s32;
+  const spiffe_mesh &m = in->mesh;
+  if (o->tb_electrons_per_macroparticle)
+    in->stiffness = 1; // advance_particles.c:280-281
+  Push32Params p{};
+  p.time = m.time;
+  p.dt = (float)m.dt;
+  p.dt_dz = (float)(m.dt / m.dz);
+  p.dt_dr = (float)(m.dt / m.dr);
+  p.QoMC_dt = (float)(in->QoMC * m.dt);
+  p.stiff_inv = (float)(1 / in->stiffness);
+  p.z_forces_start = o->z_forces_start;
+  p.forced = o->tb_electrons_per_macroparticle && (o->tb_z_force || o->tb_r_force);
+  p.tb_z_force_dt = (float)(m.dt * o->tb_z_force);
+  p.tb_r_force_dt = (float)(m.dt * o->tb_r_force);
+  p.tb_z_decel = o->tb_z_start_deceleration;
+  p.tb_r_decel = o->tb_r_start_deceleration;
+  p.screen_momentum = o->screen_momentum;
+  p.deposit = deposit;
+  PhaseScope ps(in, PH_PUSH);
+  const int rc = s32_push(&in->dm, &S.f, &S.b, &p, &in->screens, in->cnt, in->np_upper, o->compaction, &S.sc, &S.pw,
+                          in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  S.j_state = deposit ? S32_J_DEPOSITED : S32_J_UNKNOWN;
+  return 0;
+}
+
 // ------------------------------------------------------------------ C ABI
 
 extern "C" const char *spiffe_gpu_last_error(void) { return g_error.c_str(); }
@@ -296,8 +720,8 @@ extern "C" int spiffe_gpu_create(const spiffe_mesh *mesh, const int16_t *flags, 
 {
   if (!mesh || !flags || !out)
     return fail(SPIFFE_ERR_INVALID, "null argument");
-  if (precision != SPIFFE_PRECISION_F64)
-    return fail(SPIFFE_ERR_UNSUPPORTED, "this entry point builds the FP64 form; use spiffe_gpu_create_split32");
+  if (precision != SPIFFE_PRECISION_F64 && precision != SPIFFE_PRECISION_SPLIT32)
+    return fail(SPIFFE_ERR_UNSUPPORTED, "unknown precision %d", (int)precision);
   if (mesh->nz < 3 || mesh->nr < 4)
     return fail(SPIFFE_ERR_INVALID, "mesh too small (nz=%d nr=%d; need nz>=3, nr>=4)", mesh->nz, mesh->nr);
   if (!(mesh->dz > 0) || !(mesh->dr > 0))
@@ -319,6 +743,26 @@ extern "C" int spiffe_gpu_create(const spiffe_mesh *mesh, const int16_t *flags, 
     return bail(fail(SPIFFE_ERR_CUDA, "stream creation failed"));
   cudaStream_t s = in->stream;
   const size_t n = in->nodes;
+  in->capacity = particle_capacity > 1024 ? particle_capacity : 1024;
+  if (cudaMalloc(&in->cnt, sizeof(DevCounts)) != cudaSuccess ||
+      cudaMallocHost(&in->h_cnt, sizeof(DevCounts)) != cudaSuccess ||
+      cudaMallocHost(&in->h_probe, 8 * sizeof(double)) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_NOMEM, "counter allocation failed"));
+  memset(in->h_cnt, 0, sizeof(DevCounts));
+  in->h_cnt->nextParticleID = 1;
+  in->h_cnt->first_lost = 0x7fffffffffffffffLL;
+  if (cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return bail(fail(SPIFFE_ERR_CUDA, "counter upload failed"));
+  if (precision == SPIFFE_PRECISION_SPLIT32) {
+    if (mesh->nz > 32767 || mesh->nr > 32767)
+      return bail(fail(SPIFFE_ERR_INVALID, "the split-precision form holds at most 32767 cells per axis"));
+    if ((rc = s32_create(in, flags)))
+      return bail(rc);
+    if (cudaStreamSynchronize(s) != cudaSuccess)
+      return bail(fail(SPIFFE_ERR_CUDA, "instance setup failed: %s", cudaGetErrorString(cudaGetLastError())));
+    *out = in;
+    return 0;
+  }
   if (cudaMalloc(&in->d_flags, n * sizeof(int16_t)) != cudaSuccess ||
       cudaMemcpyAsync(in->d_flags, flags, n * sizeof(int16_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
     return bail(fail(SPIFFE_ERR_NOMEM, "flag allocation failed"));
@@ -334,18 +778,8 @@ extern "C" int spiffe_gpu_create(const spiffe_mesh *mesh, const int16_t *flags, 
       if ((rc = alloc_field(p, n, s)))
         return bail(rc);
   }
-  in->capacity = particle_capacity > 1024 ? particle_capacity : 1024;
   if ((rc = alloc_beam(&in->b, in->capacity)))
     return bail(rc);
-  if (cudaMalloc(&in->cnt, sizeof(DevCounts)) != cudaSuccess ||
-      cudaMallocHost(&in->h_cnt, sizeof(DevCounts)) != cudaSuccess ||
-      cudaMallocHost(&in->h_probe, 8 * sizeof(double)) != cudaSuccess)
-    return bail(fail(SPIFFE_ERR_NOMEM, "counter allocation failed"));
-  memset(in->h_cnt, 0, sizeof(DevCounts));
-  in->h_cnt->nextParticleID = 1;
-  in->h_cnt->first_lost = 0x7fffffffffffffffLL;
-  if (cudaMemcpyAsync(in->cnt, in->h_cnt, sizeof(DevCounts), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    return bail(fail(SPIFFE_ERR_CUDA, "counter upload failed"));
   if ((rc = spiffe_particles64_work(&in->pw, in->capacity, false)))
     return bail(fail(SPIFFE_ERR_NOMEM, "particle work allocation failed"));
   set_devmesh(in);
@@ -361,6 +795,8 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
     return 0;
   if (in->stream)
     cudaStreamSynchronize(in->stream);
+  if (in->s32)
+    s32_destroy(in);
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
@@ -422,6 +858,8 @@ extern "C" int spiffe_gpu_upload_fields(spiffe_gpu_instance *in, const spiffe_fi
 {
   if (!in || !h)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_upload_fields(in, h);
   const size_t bytes = in->nodes * sizeof(double);
   cudaStream_t s = in->stream;
   if (h->BzImposed && !in->f.BzImposed) {
@@ -445,6 +883,8 @@ extern "C" int spiffe_gpu_download_fields(spiffe_gpu_instance *in, spiffe_field_
 {
   if (!in || !h)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_download_fields(in, h);
   const size_t bytes = in->nodes * sizeof(double);
   cudaStream_t s = in->stream;
 #define DOWN(x)                                                                 \
@@ -468,6 +908,8 @@ extern "C" int spiffe_gpu_upload_beam(spiffe_gpu_instance *in, const spiffe_beam
   if (h->np < 0)
     return fail(SPIFFE_ERR_INVALID, "negative particle count");
   RC_TRY(grow_beam(in, h->np));
+  if (in->s32)
+    return s32_upload_beam(in, h);
   cudaStream_t s = in->stream;
   const size_t n = (size_t)h->np;
 #define UPB(x)                                                                                 \
@@ -494,6 +936,8 @@ extern "C" int spiffe_gpu_download_beam(spiffe_gpu_instance *in, spiffe_beam_set
 {
   if (!in || !h)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_download_beam(in, h);
   RC_TRY(read_counts(in));
   const long long np = in->h_cnt->np;
   if (np > h->capacity)
@@ -518,6 +962,8 @@ extern "C" int spiffe_gpu_set_deposit_order(spiffe_gpu_instance *in, int32_t ord
 {
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return 0; // fixed-point deposition is order-independent already
   in->deposit_ordered = ordered ? 1 : 0;
   RC_TRY(spiffe_particles64_work(&in->pw, in->capacity, in->deposit_ordered));
   return 0;
@@ -527,6 +973,8 @@ extern "C" int spiffe_gpu_zero_current_arrays(spiffe_gpu_instance *in)
 {
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_zero_j(in);
   const size_t bytes = in->nodes * sizeof(double);
   if (in->mesh.modes & SPIFFE_FL_TM_FIELDS) {
     CUDA_TRY(cudaMemsetAsync(in->f.Jz, 0, bytes, in->stream));
@@ -541,6 +989,8 @@ extern "C" int spiffe_gpu_advance_field_solutions(spiffe_gpu_instance *in)
 {
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_fdtd(in, 0);
   RC_TRY(ensure_fdtd(in));
   PhaseScope ps(in, PH_FDTD);
   in->fdtd_steps++;
@@ -554,6 +1004,11 @@ extern "C" int spiffe_gpu_add_particle_currents(spiffe_gpu_instance *in)
 {
   if (!in)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32) {
+    RC_TRY(s32_deposit_all(in));
+    in->s32->j_state = S32_J_UNKNOWN;
+    return 0;
+  }
   PhaseScope ps(in, PH_DEPOSIT);
   const int rc = spiffe_deposit64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, in->deposit_ordered, &in->pw,
                                   in->stream);
@@ -566,6 +1021,8 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
 {
   if (!in || !o)
     return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (in->s32)
+    return s32_push_step(in, o, 0);
   if (o->tb_electrons_per_macroparticle)
     in->stiffness = 1; // advance_particles.c:280-281
   PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
@@ -587,6 +1044,20 @@ extern "C" int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *in, int32_t tar
     return fail(SPIFFE_ERR_INVALID, "accuracy is <= 0 in solve_poisson_cyl"); // poisson.c:27-28
   if (limit <= 1)
     return fail(SPIFFE_ERR_INVALID, "iteration_limit is <= 1 in solve_poisson_cyl"); // poisson.c:29-30
+  if (in->s32) {
+    S32State &S = *in->s32;
+    RC_TRY(s32_ensure_poisson(in));
+    const int rc = s32_sor(&in->dm, &S.pcw, target ? S.f.PsiImposed : S.f.Psi, target ? nullptr : S.f.Q, S.umask,
+                           accuracy, limit, nullptr, in->cnt, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "SOR launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    long long it = 0;
+    CUDA_TRY(cudaMemcpyAsync(&it, S.pcw.iters, sizeof(it), cudaMemcpyDeviceToHost, in->stream));
+    RC_TRY(read_counts(in));
+    if (iterations)
+      *iterations = it;
+    return 0;
+  }
   RC_TRY(ensure_poisson(in));
   long long it = 0;
   double *psi = target ? in->f.PsiImposed : in->f.Psi;
@@ -612,8 +1083,17 @@ static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const s
   }
   if (o->step_interval <= 0 || in->mesh.time_step % o->step_interval != 0 || in->pc_start_step > in->mesh.time_step)
     return 0;
-  RC_TRY(ensure_poisson(in));
   PoissonHostOptions h{o->accuracy, o->error_charge_threshold, o->maximum_iterations, o->guess_code, space_charge};
+  if (in->s32) {
+    S32State &S = *in->s32;
+    RC_TRY(s32_ensure_poisson(in));
+    PhaseScope ps(in, PH_POISSON);
+    const int rc = s32_poisson_correction(&in->dm, &S.f, &S.b, in->cnt, in->np_upper, &h, &S.sc, &S.pcw, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    return 1;
+  }
+  RC_TRY(ensure_poisson(in));
   PhaseScope ps(in, PH_POISSON);
   const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, in->stream);
   if (rc)
@@ -632,7 +1112,8 @@ extern "C" int spiffe_gpu_add_poisson_correction(spiffe_gpu_instance *in, int32_
   if (rep) {
     memset(rep, 0, sizeof(*rep));
     if (ran) {
-      RC_TRY(spiffe_poisson64_report(&in->pcw, rep, in->stream));
+      RC_TRY(in->s32 ? s32_poisson_report(&in->s32->pcw, rep, in->stream)
+                     : spiffe_poisson64_report(&in->pcw, rep, in->stream));
       RC_TRY(read_counts(in));
     }
   }
@@ -649,7 +1130,14 @@ static int imposed_efield(spiffe_gpu_instance *in, const spiffe_poisson_options 
       return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (compute_imposed_Efield)");
     in->pc_start_step = (long long)((o->start_time - in->mesh.start_time) / in->mesh.dt);
   }
-  if (initialize) {
+  if (initialize && in->s32) {
+    S32State &S = *in->s32;
+    RC_TRY(s32_ensure_poisson(in));
+    const int rc = s32_sor(&in->dm, &S.pcw, S.f.PsiImposed, nullptr, S.umask, o->accuracy, o->maximum_iterations,
+                           nullptr, in->cnt, in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "SOR launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  } else if (initialize) {
     RC_TRY(ensure_poisson(in));
     const int rc = spiffe_sor64(&in->dm, &in->pcw, in->f.PsiImposed, nullptr, in->d_flags, o->accuracy,
                                 o->maximum_iterations, in->cnt, nullptr, in->stream);
@@ -673,7 +1161,8 @@ static int imposed_efield(spiffe_gpu_instance *in, const spiffe_poisson_options 
   if (ff == in->last_imposed_factor)
     return 0;
   in->last_imposed_factor = ff;
-  const int rc = spiffe_imposed_field64(&in->dm, &in->f, ff, in->stream);
+  const int rc = in->s32 ? s32_imposed_field(&in->dm, &in->s32->f, ff, in->stream)
+                         : spiffe_imposed_field64(&in->dm, &in->f, ff, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "imposed field launch failed: %s", cudaGetErrorString((cudaError_t)rc));
   return 0;
@@ -1046,7 +1535,15 @@ static int emit(spiffe_gpu_instance *in)
     } else {
       p.mode = 2;
     }
-    const int rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+    int rc;
+    if (in->s32) {
+      S32State &S = *in->s32;
+      RC_TRY(s32_cover_charge(in, std::fabs(c.Q)));
+      rc = s32_births(&in->dm, &S.f, &S.b, &p, in->cnt, &S.sc,
+                      in->space_charge && S.j_state == S32_J_DEPOSITED ? 1 : 0, in->stream);
+    } else {
+      rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+    }
     if (rc)
       return fail(SPIFFE_ERR_CUDA, "birth launch failed: %s", cudaGetErrorString((cudaError_t)rc));
     in->np_upper += total;
@@ -1067,8 +1564,17 @@ static int set_current_density(spiffe_gpu_instance *in)
     long iz = (long)((c.o.z_position - m.zmin) / m.dz + 1.5), ir = (long)((c.o.inner_radius + c.o.outer_radius) / 2 / m.dr);
     if (iz <= 0)
       iz = 1;
+    if (iz > m.nz)
+      iz = m.nz; // a cathode at zmax would probe one row past the mesh
     double Ez = m.constant_E[0];
-    if (m.modes & SPIFFE_FL_TM_FIELDS) {
+    if ((m.modes & SPIFFE_FL_TM_FIELDS) && in->s32) {
+      const size_t i = node((int)iz, (int)ir, in->dm.pitch);
+      float *pf = (float *)in->h_probe;
+      CUDA_TRY(cudaMemcpyAsync(pf, in->s32->f.Ez + i, sizeof(float), cudaMemcpyDeviceToHost, in->stream));
+      CUDA_TRY(cudaMemcpyAsync(pf + 1, in->s32->f.EzImposed + i, sizeof(float), cudaMemcpyDeviceToHost, in->stream));
+      CUDA_TRY(cudaStreamSynchronize(in->stream));
+      Ez += (double)pf[0] + (double)pf[1];
+    } else if (m.modes & SPIFFE_FL_TM_FIELDS) {
       const size_t i = node((int)iz, (int)ir, m.nr + 1);
       CUDA_TRY(cudaMemcpyAsync(in->h_probe, in->f.Ez + i, sizeof(double), cudaMemcpyDeviceToHost, in->stream));
       CUDA_TRY(cudaMemcpyAsync(in->h_probe + 1, in->f.EzImposed + i, sizeof(double), cudaMemcpyDeviceToHost, in->stream));
@@ -1145,8 +1651,15 @@ static int antennas(spiffe_gpu_instance *in, double time)
       J = (a.W[i + 1] - a.W[i]) / (a.t[i + 1] - a.t[i]) * (time - a.t[i]) + a.W[i];
     }
     J *= a.current * std::sin(SPIFFE_PIx2 * a.frequency * time + a.phase);
-    double *arr = a.direction == 0 ? in->f.Jz : (a.direction == 1 ? in->f.Jr : in->f.Jphi);
-    const int rc = spiffe_antenna64(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->stream);
+    int rc;
+    if (in->s32) {
+      const DevFields32 &F = in->s32->f;
+      long long *arr = a.direction == 0 ? F.Jz : (a.direction == 1 ? F.Jr : F.Jphi);
+      rc = s32_antenna(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->s32->sc.qJ, in->stream);
+    } else {
+      double *arr = a.direction == 0 ? in->f.Jz : (a.direction == 1 ? in->f.Jr : in->f.Jphi);
+      rc = spiffe_antenna64(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->stream);
+    }
     if (rc)
       return fail(SPIFFE_ERR_CUDA, "antenna launch failed");
   }
@@ -1182,7 +1695,8 @@ extern "C" int spiffe_gpu_run_begin(spiffe_gpu_instance *in, spiffe_poisson_repo
   if (rep) {
     memset(rep, 0, sizeof(*rep));
     if (ran)
-      RC_TRY(spiffe_poisson64_report(&in->pcw, rep, in->stream));
+      RC_TRY(in->s32 ? s32_poisson_report(&in->s32->pcw, rep, in->stream)
+                     : spiffe_poisson64_report(&in->pcw, rep, in->stream));
   }
   RC_TRY(set_current_density(in));
   return 0;
@@ -1199,15 +1713,38 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
       RC_TRY(imposed_efield(in, &in->pc, 0));
     m.time = m.time_step * m.dt + m.start_time;
     RC_TRY(emit(in));
-    RC_TRY(spiffe_gpu_zero_current_arrays(in));
-    if (in->space_charge)
-      RC_TRY(spiffe_gpu_add_particle_currents(in));
+    S32State *S = in->s32;
+    if (!S) {
+      RC_TRY(spiffe_gpu_zero_current_arrays(in));
+      if (in->space_charge)
+        RC_TRY(spiffe_gpu_add_particle_currents(in));
+    } else if (!(in->space_charge && S->j_state == S32_J_DEPOSITED)) {
+      // J holds the previous push's deposit only when that push ran inside this loop
+      if (S->j_state != S32_J_ZERO)
+        RC_TRY(s32_zero_j(in));
+      if (in->space_charge) {
+        RC_TRY(s32_deposit_all(in));
+        S->j_state = S32_J_DEPOSITED;
+      }
+    }
     RC_TRY(antennas(in, m.time + m.dt / 2));
     const int ran = poisson_correction(in, in->space_charge, &in->pc);
     if (ran < 0)
       return ran;
-    RC_TRY(spiffe_gpu_advance_field_solutions(in));
-    RC_TRY(spiffe_gpu_advance_particles(in, &in->push));
+    if (!S) {
+      RC_TRY(spiffe_gpu_advance_field_solutions(in));
+      RC_TRY(spiffe_gpu_advance_particles(in, &in->push));
+    } else {
+      RC_TRY(s32_fdtd(in, 1)); // reads J and leaves it zero
+      RC_TRY(s32_push_step(in, &in->push, in->space_charge)); // deposits J for the next step
+      if (!in->space_charge)
+        S->j_state = S32_J_ZERO;
+      if (S->sort_interval > 0 && ++S->since_sort >= S->sort_interval) {
+        S->since_sort = 0;
+        PhaseScope ps(in, PH_PUSH);
+        RC_TRY(s32_sort(&in->dm, &S->b, in->cnt, in->np_upper, &S->pw, in->stream));
+      }
+    }
     RC_TRY(set_current_density(in));
     m.time_step++;
   }
@@ -1278,6 +1815,19 @@ extern "C" int spiffe_gpu_phase_times(spiffe_gpu_instance *in, double *ms, int64
     ms[p] = total;
     count[p] = (int64_t)in->timer.used[p];
     in->timer.used[p] = 0;
+  }
+  return 0;
+}
+
+// Split-precision form: reorder the particles by cell every n steps of the
+// integration loop (0: never).
+extern "C" int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *in, int64_t n)
+{
+  if (!in || n < 0)
+    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  if (in->s32) {
+    in->s32->sort_interval = n;
+    in->s32->since_sort = 0;
   }
   return 0;
 }

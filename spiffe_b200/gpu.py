@@ -160,6 +160,9 @@ class GpuInstance:
     def set_deposit_order(self, ordered):
         _check(self.lib.spiffe_gpu_set_deposit_order(self.h, int(ordered)))
 
+    def set_sort_interval(self, n):
+        _check(self.lib.spiffe_gpu_set_sort_interval(self.h, C.c_int64(int(n))))
+
     def zero_currents(self):
         _check(self.lib.spiffe_gpu_zero_current_arrays(self.h))
 

@@ -123,6 +123,7 @@ def test_single_test_particle_trajectory(oracle):
     ref_f, ref_b = f.copy(), b.copy()
     opts = abi.push_options(compaction=abi.COMPACT_SWAP)
     traj_g, traj_o = [], []
+    lost_at = None
     for step in range(600):
         ref_f.mesh.time = step * ref_f.mesh.dt
         g.mesh.time = ref_f.mesh.time
@@ -131,10 +132,16 @@ def test_single_test_particle_trajectory(oracle):
         oracle.advance_fields(ref_f)
         g.advance_particles(opts)
         oracle.advance_particles(ref_f, ref_b, [], opts)
-        if step % 100 == 99:
+        if step % 10 == 9 or ref_b.np == 0:
             out = g.download_beam(abi.Beam(4))
+            # the electron is absorbed by the cavity wall on the same step on both sides
+            assert out.np == ref_b.np, step
+            if ref_b.np == 0:
+                lost_at = step
+                break
             traj_g.append([out["z"][0], out["r"][0], out["pz"][0], out["pr"][0]])
             traj_o.append([ref_b["z"][0], ref_b["r"][0], ref_b["pz"][0], ref_b["pr"][0]])
+    assert len(traj_g) >= 10, lost_at
     traj_g, traj_o = np.array(traj_g), np.array(traj_o)
     assert np.max(np.abs(traj_g - traj_o) / np.maximum(np.abs(traj_o), 1e-30)) <= 1e-9
     assert np.array_equal(traj_g, traj_o)  # the FP64 form is bit-faithful

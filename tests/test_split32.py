@@ -1,0 +1,255 @@
+"""The split-precision form against the FP64 oracle and the FP64 GPU form.
+
+The split form computes fields, gather, push and deposition in FP32, keeps
+positions as an integer cell plus an FP32 offset and accumulates current in
+64-bit fixed point, so it is compared within stated tolerances:
+
+* fields after an FDTD run: relative L2 <= 1e-5 (FIELD_TOL);
+* one push: positions within 1e-5 of a cell, momenta within 1e-5 of the
+  largest momentum (PUSH_TOL), same particle count;
+* deposited current: relative L2 <= 1e-5;
+* a single test particle over 345 steps in the pillbox: relative <= 1e-5;
+* Poisson solves: Psi relative L2 <= 1e-6 (SOR_TOL), the same half-sweep
+  count within 2;
+* exit-plane moments of a full pillbox run: within 0.5% of the FP64 form
+  (MOMENT_TOL, the target of the split form).
+
+Fixed-point deposition makes a split-form run bit-reproducible: the same
+run twice gives identical fields, currents and particles.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from spiffe_b200 import abi, geometry, gpu, moments, workloads
+from helpers import MODES, QoMC, beam_from, by_id, fields_from, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TOL = 1e-5
+PUSH_TOL = 1e-5
+SOR_TOL = 1e-6
+MOMENT_TOL = 5e-3
+
+
+def split(f, **kw):
+    return gpu.GpuInstance(f, precision=gpu.PRECISION_SPLIT32, **kw)
+
+
+def push_fixture_state(fx):
+    f = fields_from(fx, modes=int(fx["modes"]), dt=float(fx["dt"]))
+    f.mesh.time_step = int(fx["time_step"])
+    f.mesh.time = f.mesh.time_step * f.mesh.dt
+    for k in ("Ez", "Er", "Bphi", "Bphi2", "EzImposed", "ErImposed", "BzImposed", "BrImposed"):
+        f[k] = fx["f_" + k]
+    return f, beam_from(fx)
+
+
+def test_fdtd_pillbox_within_tolerance():
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    g = split(f)
+    for _ in range(int(fx["steps"])):
+        g.advance_fields()
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Bphi2"):
+        assert rel_l2(out[n], fx[n]) <= FIELD_TOL, n
+
+
+def test_fdtd_te_fields_within_tolerance(oracle):
+    fx = load("gun16_geometry")
+    f = fields_from(fx, modes=MODES | abi.FL_TE_FIELDS, dt=2e-13)
+    rng = np.random.default_rng(3)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Bz", "Br2", "Bz2"):
+        f[n] = rng.normal(size=f.shape)
+    ref = f.copy()
+    g = split(f)
+    for _ in range(25):
+        g.advance_fields()
+        oracle.advance_fields(ref)
+    out = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Br2", "Bz", "Bz2"):
+        assert rel_l2(out[n], ref[n]) <= FIELD_TOL, n
+
+
+def test_beam_round_trip():
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    g = split(f)
+    g.upload_beam(b)
+    out = g.download_beam(abi.Beam(b.capacity))
+    assert out.np == b.np and out.npActive == b.npActive
+    assert np.max(np.abs(out["z"] - b["z"])) <= 1e-6 * f.mesh.dz
+    assert np.max(np.abs(out["r"] - b["r"])) <= 1e-6 * f.mesh.dr
+    for k in ("pz", "pr", "r_pphi", "Q"):
+        assert np.allclose(out[k], b[k], rtol=1e-7, atol=0), k
+    for k in ("r0", "z0", "t0", "particleID", "generation", "status"):
+        assert np.array_equal(out[k], b[k]), k
+
+
+def test_deposit_within_tolerance():
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    g = split(f)
+    g.upload_beam(b)
+    g.zero_currents()
+    g.deposit()
+    out = g.fields(f)
+    for n in ("Jz", "Jr"):
+        assert rel_l2(out[n], fx[n]) <= FIELD_TOL, n
+
+
+def test_push_within_tolerance(oracle):
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    opts = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
+    g = split(f)
+    g.upload_beam(b)
+    g.add_screen(float(fx["screen_z"]))
+    g.advance_particles(opts)
+    out = g.download_beam(abi.Beam(b.capacity))
+    ref_b = b.copy()
+    sc = abi.Screen(float(fx["screen_z"]))
+    oracle.advance_particles(f.copy(), ref_b, [sc], opts)
+    assert out.np == ref_b.np and out.npActive == ref_b.npActive
+    keys = ("z", "r", "pz", "pr", "particleID")
+    got, ref = by_id({k: out[k] for k in keys}), by_id({k: ref_b[k] for k in keys})
+    assert np.max(np.abs(got["z"] - ref["z"])) <= PUSH_TOL * f.mesh.dz
+    assert np.max(np.abs(got["r"] - ref["r"])) <= PUSH_TOL * f.mesh.dr
+    pmax = np.max(np.abs(ref["pz"]))
+    for k in ("pz", "pr"):
+        assert np.max(np.abs(got[k] - ref[k])) <= PUSH_TOL * pmax, k
+    assert len(g.screen(0).records()["r"]) == len(sc.records()["r"])
+
+
+def test_single_test_particle_trajectory(oracle):
+    """A single electron in the pillbox's TM010 field until the wall absorbs it."""
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    b = abi.Beam(4)
+    b.set(1, z=[0.002], r=[0.003], pz=[0.0], pr=[0.0], r_pphi=[0.0], vz=[0.0], vr=[0.0], vphi=[0.0], Q=[-1e-15],
+          r0=[0.003], z0=[0.002], t0=[0.0], rmin=[1e300], rmax=[-1e300], zmin=[1e300], zmax=[-1e300],
+          particleID=[1], generation=[0], status=[1])
+    b.npActive, b.nextParticleID, b.QoMC, b.stiffness = 1, 2, QoMC, 1.0
+    g = split(f)
+    g.upload_beam(b)
+    ref_f, ref_b = f.copy(), b.copy()
+    opts = abi.push_options(compaction=abi.COMPACT_SWAP)
+    err, lost_g, lost_o = 0.0, None, None
+    for step in range(600):
+        ref_f.mesh.time = step * ref_f.mesh.dt
+        g.mesh.time = ref_f.mesh.time
+        g.set_mesh()
+        g.advance_fields()
+        oracle.advance_fields(ref_f)
+        g.advance_particles(opts)
+        oracle.advance_particles(ref_f, ref_b, [], opts)
+        out = g.download_beam(abi.Beam(4))
+        if out.np == 0 and lost_g is None:
+            lost_g = step
+        if ref_b.np == 0 and lost_o is None:
+            lost_o = step
+        if out.np and ref_b.np:
+            for k in ("z", "r", "pz", "pr"):
+                scale = max(abs(ref_b[k][0]), 1e-3 if k in ("z", "r") else 1e-2)
+                err = max(err, abs(out[k][0] - ref_b[k][0]) / scale)
+        if lost_g is not None and lost_o is not None:
+            break
+    assert lost_o is not None and abs(lost_g - lost_o) <= 1, (lost_g, lost_o)
+    assert err <= PUSH_TOL, err
+
+
+def test_sor_within_tolerance(oracle):
+    fx = load("dcgun_poisson")
+    f = fields_from(fx, modes=MODES, dt=float(fx["dt"]))
+    rng = np.random.default_rng(5)
+    f["Q"] = rng.normal(size=f.shape) * 1e4
+    f["Psi"] = rng.normal(size=f.shape)
+    ref = f.copy()
+    g = split(f)
+    n_g = g.solve_poisson(0, 1e-6, 3000)
+    n_o, _, _ = oracle.solve_poisson(ref, ref["Psi"], ref["Q"], 1e-6, 3000)
+    out = g.fields(f)
+    assert n_o > 0 and abs(n_g - n_o) <= 2, (n_g, n_o)
+    assert rel_l2(out["Psi"], ref["Psi"]) <= SOR_TOL
+
+
+def test_imposed_field_within_tolerance():
+    fx = load("dcgun_poisson")
+    f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
+    f["PsiImposed"] = fx["PsiImposed0"]
+    g = split(f)
+    opts = abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+    g.imposed_efield(opts, 1)
+    out = g.fields(f)
+    assert rel_l2(out["PsiImposed"], fx["PsiImposed"]) <= SOR_TOL
+    for n in ("EzImposed", "ErImposed"):
+        assert rel_l2(out[n], fx[n]) <= FIELD_TOL, n
+
+
+def test_poisson_correction_within_tolerance():
+    fx = load("dcgun_poisson")
+    f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
+    f["PsiImposed"] = fx["PsiImposed"]
+    f["EzImposed"], f["ErImposed"] = fx["EzImposed"], fx["ErImposed"]
+    f["Ez"], f["Er"] = fx["Ez0"], fx["Er0"]
+    g = split(f)
+    g.upload_beam(beam_from(fx))
+    rep = g.poisson_correction(1, abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000))
+    assert rep.ran == 1 and abs(rep.iterations - 527) <= 2
+    out = g.fields(f)
+    for n in ("Ez", "Er"):
+        assert rel_l2(out[n], fx[n]) <= FIELD_TOL, n
+    assert rel_l2(out["Psi"], fx["Psi"]) <= 1e-5
+
+
+def pillbox_run(precision, steps, sort_interval=20):
+    cfg = workloads.PillboxConfig()
+    f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(),
+                            modes=MODES | abi.FL_SPACE_CHARGE)
+    f.mesh.dt = cfg.dt
+    f["Ez"] = cfg.initial_ez()
+    g = gpu.GpuInstance(f, capacity=cfg.n_macro + 4096, precision=precision)
+    if precision == gpu.PRECISION_SPLIT32:
+        g.set_sort_interval(sort_interval)
+    g.add_screen(cfg.screen_z(), capacity=cfg.n_macro + 4096)
+    g.add_cathode(cfg.cathode_options())
+    g.configure_run(space_charge=1, push=abi.push_options(abi.COMPACT_SWAP, abi.SCREEN_PARTICLE))
+    g.run_begin()
+    g.run_steps(steps)
+    rec = g.screen(0, capacity=cfg.n_macro + 4096).records()
+    return g, f, rec
+
+
+def test_split_run_is_bit_reproducible():
+    g1, f1, r1 = pillbox_run(gpu.PRECISION_SPLIT32, 300)
+    g2, f2, r2 = pillbox_run(gpu.PRECISION_SPLIT32, 300)
+    o1, o2 = g1.fields(f1), g2.fields(f2)
+    for n in ("Ez", "Er", "Bphi", "Jz", "Jr"):
+        assert np.array_equal(o1[n], o2[n]), n
+    b1, b2 = g1.download_beam(abi.Beam(24096)), g2.download_beam(abi.Beam(24096))
+    assert b1.np == b2.np
+    k1, k2 = np.argsort(b1["particleID"]), np.argsort(b2["particleID"])
+    for k in ("z", "r", "pz", "pr"):
+        assert np.array_equal(b1[k][k1], b2[k][k2]), k
+
+
+def test_pillbox_exit_moments_within_half_percent():
+    """Config 1 in full (4000 steps): exit-plane moments of the split form
+    within 0.5% of the FP64 form; the final fields' relative L2 is reported."""
+    g64, f64, r64 = pillbox_run(gpu.PRECISION_F64, 4000)
+    g32, f32, r32 = pillbox_run(gpu.PRECISION_SPLIT32, 4000)
+    m64, m32 = moments.exit_moments(r64), moments.exit_moments(r32)
+    assert m64["count"] > 100
+    err = moments.relative_errors(m32, m64)
+    print("exit moments FP64", m64)
+    print("exit moments split", m32)
+    print("relative errors", err)
+    o64, o32 = g64.fields(f64), g32.fields(f32)
+    print("field rel L2", {n: rel_l2(o32[n], o64[n]) for n in ("Ez", "Er", "Bphi")})
+    assert abs(m32["count"] - m64["count"]) <= max(2, 0.005 * m64["count"])
+    for k, v in err.items():
+        assert v <= MOMENT_TOL, (k, v)
