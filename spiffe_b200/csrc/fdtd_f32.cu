@@ -332,6 +332,12 @@ extern "C" int s32_fdtd_tables(const DevMesh *m, const int16_t *host_flags, Fdtd
       if (iz <= cut1[ir] && !(fl & SPIFFE_FL_BR_ZERO)) u |= S32_U_BR;
       if (iz <= cut0[ir] && !(fl & SPIFFE_FL_BZ_ZERO)) u |= S32_U_BZ;
       if (fl & SPIFFE_FL_IS_METAL) u |= S32_U_METAL;
+      bool clean = true;
+      for (int z = iz - 1; z <= iz + 1 && clean; z++)
+        for (int r = ir; r <= ir + 1 && clean; r++)
+          if (z >= 0 && z <= nz && r <= nr && host_flags[(size_t)z * (nr + 1) + r])
+            clean = false;
+      if (clean) u |= S32_U_CLEAN;
       um[(size_t)iz * P + ir] = u;
     }
   t->fEr = (float)(dti / (mu0 * eps0 * dz));

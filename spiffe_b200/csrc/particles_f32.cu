@@ -72,11 +72,16 @@ __device__ int loss_code32(const DevMesh &m, const int16_t *__restrict__ fl, int
 
 // interpolateFields (advance_particles.c:622-890) at ξz = iz+fz, ξr = ir+fr.
 // E = Ez, Er, Ephi, Bz, Br, Bphi.
+// DEF: the default field modes (TM fields, longitudinal and radial
+// interpolation, no TE, no switches), chosen on the host, so the mode tests
+// fold away.
+template <bool DEF>
 __device__ void gather32(const DevMesh &m, const DevFields32 &f, int iz0, float fz, int ir0, float fr, float *E)
 {
   const int nz = m.nz, nr = m.nr, P = m.pitch;
-  const bool longit = m.modes & SPIFFE_FL_LONGIT_INTERP, radial = m.modes & SPIFFE_FL_RADIAL_INTERP;
-  const bool tm = m.modes & SPIFFE_FL_TM_FIELDS, te = m.modes & SPIFFE_FL_TE_FIELDS;
+  const bool longit = DEF || (m.modes & SPIFFE_FL_LONGIT_INTERP), radial = DEF || (m.modes & SPIFFE_FL_RADIAL_INTERP);
+  const bool tm = DEF || (m.modes & SPIFFE_FL_TM_FIELDS), te = !DEF && (m.modes & SPIFFE_FL_TE_FIELDS);
+  const uint8_t *__restrict__ um = f.umask;
   const bool r_nonzero = ir0 != 0 || fr != 0.f;
   const int16_t *__restrict__ fl = f.flags;
   int iz, ir, iz1, ir1;
@@ -108,7 +113,9 @@ __device__ void gather32(const DevMesh &m, const DevFields32 &f, int iz0, float 
       iz1 = iz;
     if ((ir1 = ir + 1) >= nr)
       ir1 = ir;
-    if (LD(fl, N(iz, ir + 1)) & SPIFFE_FL_ER_ZERO && LD(fl, N(iz, ir)) & SPIFFE_FL_ER_ZERO) {
+    if (LD(um, N(iz, ir)) & S32_U_CLEAN) {
+      // no metal near this cell
+    } else if (LD(fl, N(iz, ir + 1)) & SPIFFE_FL_ER_ZERO && LD(fl, N(iz, ir)) & SPIFFE_FL_ER_ZERO) {
       if (iz > 0 && (LD(fl, N(iz - 1, ir)) || LD(fl, N(iz - 1, ir + 1))))
         iz = iz1;
       else
@@ -145,7 +152,9 @@ __device__ void gather32(const DevMesh &m, const DevFields32 &f, int iz0, float 
       ir = nr - 1;
     iz1 = iz + 1;
     ir1 = ir + 1;
-    if (LD(fl, N(iz + 1, ir)) & SPIFFE_FL_EZ_ZERO && LD(fl, N(iz, ir)) & SPIFFE_FL_EZ_ZERO)
+    if (LD(um, N(iz, ir)) & S32_U_CLEAN) {
+      // no metal near this cell
+    } else if (LD(fl, N(iz + 1, ir)) & SPIFFE_FL_EZ_ZERO && LD(fl, N(iz, ir)) & SPIFFE_FL_EZ_ZERO)
       ir = ir1;
     else if (LD(fl, N(iz + 1, ir + 1)) & SPIFFE_FL_EZ_ZERO && LD(fl, N(iz, ir + 1)) & SPIFFE_FL_EZ_ZERO)
       ir1 = ir;
@@ -220,12 +229,14 @@ __device__ void gather32(const DevMesh &m, const DevFields32 &f, int iz0, float 
   Bz += (float)m.constB[0];
   Br += (float)m.constB[1];
   Bphi += (float)m.constB[2];
-  if (m.turn_off[0]) Ez = 0;
-  if (m.turn_off[1]) Er = 0;
-  if (m.turn_off[2]) Ephi = 0;
-  if (m.turn_off[3]) Bz = 0;
-  if (m.turn_off[4]) Br = 0;
-  if (m.turn_off[5]) Bphi = 0;
+  if (!DEF) {
+    if (m.turn_off[0]) Ez = 0;
+    if (m.turn_off[1]) Er = 0;
+    if (m.turn_off[2]) Ephi = 0;
+    if (m.turn_off[3]) Bz = 0;
+    if (m.turn_off[4]) Br = 0;
+    if (m.turn_off[5]) Bphi = 0;
+  }
   // solenoid fields on nodes (:859-875)
   if (m.has_solenoid) {
     shift(iz0, fz, 0.f, iz, wr);
@@ -265,11 +276,12 @@ __device__ __forceinline__ void put(Contrib32 &c, int k, int nd, float v)
 }
 
 // component 0 Jz, 1 Jr, 2 Jphi
+template <bool DEF>
 __device__ void contrib32(const DevMesh &m, int comp, int iz0, float fz, int ir0, float fr, float qvg, Contrib32 &c)
 {
   c.node[0] = c.node[1] = c.node[2] = c.node[3] = -1;
   const int nz = m.nz, nr = m.nr, P = m.pitch;
-  const bool rsm = m.modes & SPIFFE_FL_RADIAL_SMEAR, lsm = m.modes & SPIFFE_FL_LONGIT_SMEAR;
+  const bool rsm = !DEF && (m.modes & SPIFFE_FL_RADIAL_SMEAR), lsm = !DEF && (m.modes & SPIFFE_FL_LONGIT_SMEAR);
   int iz, ir;
   float rfrac, zfrac;
   // radial index and fraction
@@ -364,17 +376,18 @@ __device__ __forceinline__ void warp_add(long long *J, int nd, long long v)
 
 // Deposits the three components of one particle (or nothing, when !on);
 // called by every lane of the warp.
+template <bool DEF>
 __device__ void deposit_particle(const DevMesh &m, const DevFields32 &f, bool on, int iz, float fz, int ir, float fr,
                                  float bz, float br, float bphi, float qs)
 {
-  const bool lsm = m.modes & SPIFFE_FL_LONGIT_SMEAR, rsm = m.modes & SPIFFE_FL_RADIAL_SMEAR;
-  const bool tm = m.modes & SPIFFE_FL_TM_FIELDS, te = m.modes & SPIFFE_FL_TE_FIELDS;
+  const bool lsm = !DEF && (m.modes & SPIFFE_FL_LONGIT_SMEAR), rsm = !DEF && (m.modes & SPIFFE_FL_RADIAL_SMEAR);
+  const bool tm = DEF || (m.modes & SPIFFE_FL_TM_FIELDS), te = !DEF && (m.modes & SPIFFE_FL_TE_FIELDS);
   Contrib32 c;
   for (int comp = 0; comp < 3; comp++) {
     if ((comp < 2 && !tm) || (comp == 2 && !te))
       continue;
     if (on)
-      contrib32(m, comp, iz, fz, ir, fr, (comp == 0 ? bz : comp == 1 ? br : bphi) * qs, c);
+      contrib32<DEF>(m, comp, iz, fz, ir, fr, (comp == 0 ? bz : comp == 1 ? br : bphi) * qs, c);
     else
       c.node[0] = c.node[1] = c.node[2] = c.node[3] = -1;
     long long *J = comp == 0 ? f.Jz : comp == 1 ? f.Jr : f.Jphi;
@@ -414,7 +427,7 @@ __global__ void __launch_bounds__(T) k_deposit32(DevMesh m, DevFields32 f, DevBe
     betas(b.pz[ip], b.pr[ip], b.rpphi[ip], ((float)ir + fr) * (float)m.dr, bz, br, bphi);
     qs = b.Q[ip] * sc.s_charge;
   }
-  deposit_particle(m, f, on, iz, fz, ir, fr, bz, br, bphi, qs);
+  deposit_particle<false>(m, f, on, iz, fz, ir, fr, bz, br, bphi, qs);
 }
 
 struct ScreenCtx {
@@ -451,7 +464,7 @@ __global__ void k_snapshot_last32(DevBeam32 b, DevCounts *cnt)
 
 // advance_particles (:131-339) and its screen loop (:362-434); with DEP the
 // pushed particle's current for the next step.
-template <bool DEP>
+template <bool DEP, bool DEF>
 __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBeam32 b, Push32Params p, DevScreens scr,
                                                DevCounts *cnt, int32_t *lost_list, S32Scales sc)
 {
@@ -566,7 +579,7 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
       // momentum kick with the old velocities (:270-287)
       float E[6];
       if (active)
-        gather32(m, f, iz, fz, ir, fr, E);
+        gather32<DEF>(m, f, iz, fz, ir, fr, E);
       else
         E[0] = E[1] = E[2] = E[3] = E[4] = E[5] = 0.f;
       const float ir_ = r != 0.f ? __frcp_rn(r) : 0.f;
@@ -668,7 +681,7 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
     }
   }
   if (DEP)
-    deposit_particle(m, f, dep_on, d_iz, d_fz, d_ir, d_fr, d_bz, d_br, d_bphi, d_qs);
+    deposit_particle<DEF>(m, f, dep_on, d_iz, d_fz, d_ir, d_fr, d_bz, d_br, d_bphi, d_qs);
 }
 
 // ---- compaction
@@ -905,7 +918,7 @@ __global__ void __launch_bounds__(T) k_births32(DevMesh m, DevFields32 f, DevBea
     qs = b.Q[ip] * sc.s_charge;
   }
   if (deposit)
-    deposit_particle(m, f, on, iz, fz, ir, fr, bz, br, bphi, qs);
+    deposit_particle<false>(m, f, on, iz, fz, ir, fr, bz, br, bphi, qs);
 }
 
 __global__ void k_births_commit32(long long total, long long capacity, DevCounts *cnt)
@@ -1100,10 +1113,23 @@ extern "C" int s32_push(const DevMesh *m, const DevFields32 *f, const DevBeam32 
       k_snapshot_last32<<<1, 1, 0, s>>>(*b, cnt);
       spiffe_note_launches(1);
     }
-    if (p->deposit)
-      k_push32<true><<<blocks_for(np_bound, T), T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, any ? w->lost_list : nullptr, *sc);
+    // the default field modes get a variant with the mode tests folded away
+    const unsigned def_modes = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_LONGIT_INTERP | SPIFFE_FL_RADIAL_INTERP;
+    const unsigned mode_bits = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_TE_FIELDS | SPIFFE_FL_LONGIT_INTERP |
+                               SPIFFE_FL_RADIAL_INTERP | SPIFFE_FL_LONGIT_SMEAR | SPIFFE_FL_RADIAL_SMEAR;
+    bool def = (m->modes & mode_bits) == def_modes;
+    for (int k = 0; k < 6; k++)
+      def = def && !m->turn_off[k];
+    int32_t *ll = any ? w->lost_list : nullptr;
+    const unsigned nb = blocks_for(np_bound, T);
+    if (p->deposit && def)
+      k_push32<true, true><<<nb, T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, ll, *sc);
+    else if (p->deposit)
+      k_push32<true, false><<<nb, T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, ll, *sc);
+    else if (def)
+      k_push32<false, true><<<nb, T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, ll, *sc);
     else
-      k_push32<false><<<blocks_for(np_bound, T), T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, any ? w->lost_list : nullptr, *sc);
+      k_push32<false, false><<<nb, T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, ll, *sc);
     spiffe_note_launches(1);
   }
   if (!any) {

@@ -287,9 +287,11 @@ struct Sor32Args {
   double a_d, e_d, c4_d, e2c_d, dr2_inv;
   double accuracy;
   long long limit;
-  float *xbuf;                  // exchange rows [2][grid][2][H]
-  unsigned long long *arrive;   // barrier arrivals (low byte) and fixed-point sum
-  unsigned long long *release;  // barrier generation (high 16 bits) and published sum (low 48)
+  float *xbuf;                  // exchange rows [2][grid][2 sides][2 rows][2 parities][H]
+  unsigned long long *arrive;   // barrier arrivals (low byte) and the first fixed-point sum
+  unsigned long long *release;  // barrier generation (high 16 bits) and the first sum (low 48)
+  unsigned long long *acc1;     // the second fixed-point sum
+  unsigned long long *pub1;     // the second sum, published by the last CTA to arrive
   double *dpart;                // [grid][2] |rhs| and |r0| partials
   PcState *st;
   long long *iters_out;
@@ -303,33 +305,39 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
   return v;
 }
 
-// Bounded grid barrier that also sums one fixed-point value per CTA: each
-// CTA adds (value << 8) | 1 to *arrive, so the low byte counts arrivals (at
-// most 255 CTAs) and the rest accumulates the sum; the last CTA to arrive
-// clears *arrive and stores the next generation (high 16 bits) with the
-// total (low 48 bits) in *release, which the others poll.  The fence before
-// the arrival releases the CTA's earlier writes; the acquire of *release (or
-// the fence after the last arrival) makes every CTA's writes visible.  `gen`
-// is the calling thread's count of barriers passed.  Returns false (and
-// raises the device error bit) when the others do not arrive within the
-// poll limit.
-__device__ bool grid_sync_sum(const Sor32Args &s, unsigned long long value, unsigned &gen, unsigned long long *total,
-                              DevCounts *cnt, int *ok_sh)
+// Bounded grid barrier that also sums two fixed-point values per CTA.  Each
+// CTA adds the second value to *acc1 and then (v0 << 8) | 1 to *arrive, so
+// the low byte of *arrive counts arrivals (at most 255 CTAs) and the rest
+// accumulates the first sum; the last CTA to arrive reads and clears both
+// accumulators, publishes the second sum in *pub1 and releases the others
+// by storing the next generation (high 16 bits) with the first sum (low 48
+// bits) in *release.  The fence before the arrival releases the CTA's
+// earlier writes; the acquire of *release (or the fence after the last
+// arrival) makes every CTA's writes visible.  `gen` counts the barriers the
+// calling thread has passed.  Returns false (and raises the device error
+// bit) when the others do not arrive within the poll limit.
+__device__ bool grid_sync_sum(const Sor32Args &s, unsigned long long v0, unsigned long long v1, unsigned &gen,
+                              unsigned long long *t0, unsigned long long *t1, DevCounts *cnt, int *ok_sh)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     gen = (gen + 1) & 0xffffu;
-    unsigned long long old, tot = 0;
-    const unsigned long long add = (value << 8) | 1ull;
+    unsigned long long old, tot0 = 0, tot1 = 0;
+    const unsigned long long add = (v0 << 8) | 1ull;
+    if (v1)
+      asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(s.acc1), "l"(v1) : "memory");
     asm volatile("fence.acq_rel.gpu;" ::: "memory");
     asm volatile("atom.relaxed.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(s.arrive), "l"(add) : "memory");
     if ((old & 0xffull) == gridDim.x - 1) {
-      tot = (old >> 8) + value;
-      const unsigned long long rel = ((unsigned long long)gen << 48) | (tot & 0xffffffffffffull);
+      asm volatile("fence.acq_rel.gpu;" ::: "memory");
+      tot0 = (old >> 8) + v0;
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(tot1) : "l"(s.acc1) : "memory");
+      const unsigned long long rel = ((unsigned long long)gen << 48) | (tot0 & 0xffffffffffffull);
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.acc1), "l"(0ull) : "memory");
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.pub1), "l"(tot1) : "memory");
       asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.arrive), "l"(0ull) : "memory");
       asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(s.release), "l"(rel) : "memory");
-      asm volatile("fence.acq_rel.gpu;" ::: "memory");
     } else {
       unsigned long long polls = 0, v;
       while (((v = ld_acquire64(s.release)) >> 48) != gen) {
@@ -341,10 +349,13 @@ __device__ bool grid_sync_sum(const Sor32Args &s, unsigned long long value, unsi
         if (polls > 256)
           __nanosleep(20);
       }
-      tot = v & 0xffffffffffffull;
+      tot0 = v & 0xffffffffffffull;
+      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(tot1) : "l"(s.pub1) : "memory");
     }
-    if (total)
-      *total = tot;
+    if (t0)
+      *t0 = tot0;
+    if (t1)
+      *t1 = tot1;
     *ok_sh = ok;
   }
   __syncthreads();
@@ -359,67 +370,60 @@ __device__ __forceinline__ void band(int rows, int b, int G, int &start, int &n)
   start = b * base + (b < rem ? b : rem);
 }
 
-// r0 = rhs - A Psi (FP64, Psi read through L2) for the band's rows, into B;
-// adds this thread's share of sum |rhs| to *drive and of sum |r0| to *rsum.
-__device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz_first, int nrow, double *drive,
-                        double *rsum)
+// r0 = rhs - A Psi (FP64, Psi read through L2) into B for the mesh rows
+// iz0 .. iz0+nb-1 (B row i = mesh row iz0+i) that the SOR updates; adds this
+// thread's share of sum |rhs| and sum |r0| over the band's own rows
+// [own_lo, own_hi] to *drive and *rsum.
+__device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0, int nb, int own_lo, int own_hi,
+                        double *drive, double *rsum)
 {
   const int nz = m.nz, P = m.pitch, H = s.H, cols = s.cols;
   double d = 0, q = 0;
-  for (int j = 1; j <= nrow; j++) {
-    const int iz = iz_first + j - 1;
+  for (int i = 0; i < nb; i++) {
+    const int iz = iz0 + i;
+    const bool upd = iz >= s.lo && iz <= s.hi, own = iz >= own_lo && iz <= own_hi;
     const long up = (iz == 0 && s.lo == 0) ? P : (iz == nz - 1 && s.hi == nz - 1 ? -P : P);
     const long dn = (iz == 0 && s.lo == 0) ? P : -P;
     for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
       const int p = t / H, k = t - p * H, ir = 2 * k + p;
       float r0 = 0.f;
-      if (ir < cols) {
-        const size_t i = node(iz, ir, P);
-        const double rh = s.rhs ? s.rhs[i] : 0.0;
-        d += fabs(rh);
-        if (!(s.umask[i] & S32_U_METAL)) {
-          const double psi = __ldcg(s.Psi + i), lr = __ldcg(s.Psi + i + up) + __ldcg(s.Psi + i + dn);
+      if (upd && ir < cols) {
+        const size_t j = node(iz, ir, P);
+        const double rh = s.rhs ? s.rhs[j] : 0.0;
+        if (own)
+          d += fabs(rh);
+        if (!(s.umask[j] & S32_U_METAL)) {
+          const double psi = __ldcg(s.Psi + j), lr = __ldcg(s.Psi + j + up) + __ldcg(s.Psi + j + dn);
           double ap;
           if (ir == 0)
-            ap = s.a_d * lr + s.c4_d * __ldcg(s.Psi + i + 1) + s.e2c_d * psi;
+            ap = s.a_d * lr + s.c4_d * __ldcg(s.Psi + j + 1) + s.e2c_d * psi;
           else
-            ap = s.a_d * lr + s.dr2_inv * (1 + 1. / (2 * ir)) * __ldcg(s.Psi + i + 1) +
-                 s.dr2_inv * (1 - 1. / (2 * ir)) * __ldcg(s.Psi + i - 1) + s.e_d * psi;
+            ap = s.a_d * lr + s.dr2_inv * (1 + 1. / (2 * ir)) * __ldcg(s.Psi + j + 1) +
+                 s.dr2_inv * (1 - 1. / (2 * ir)) * __ldcg(s.Psi + j - 1) + s.e_d * psi;
           r0 = (float)(rh - ap);
-          q += fabs(rh - ap);
+          if (own)
+            q += fabs(rh - ap);
         }
       }
-      B[((j - 1) * 2 + p) * H + k] = r0;
+      B[(i * 2 + p) * H + k] = r0;
     }
   }
   *drive += d;
   *rsum += q;
 }
 
-// Psi += d on the band's updated nodes (FP64)
-__device__ void fold_d(const Sor32Args &s, int P, const float *D, const uint8_t *M, int iz_first, int nrow)
-{
-  const int H = s.H, cols = s.cols;
-  for (int j = 1; j <= nrow; j++) {
-    const int iz = iz_first + j - 1;
-    for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
-      const int p = t / H, k = t - p * H, ir = 2 * k + p;
-      const float d = D[(j * 2 + p) * H + k];
-      if (ir < cols && M[((j - 1) * 2 + p) * H + k] && d != 0.f) {
-        const size_t i = node(iz, ir, P);
-        __stcg(s.Psi + i, __ldcg(s.Psi + i) + (double)d);
-      }
-    }
-  }
-}
-
-// One colour's update of four consecutive nodes of that colour in one row
-// (nodes ir = 2(k0+i) + p); returns the sum of their |residual|.
+// The SOR update of four consecutive nodes of one colour in one row (nodes
+// ir = 2(k0+i) + p): D row jd with neighbour rows uj, dj, B/M row jb.
+// Returns the sum of their |residual|.  With UNDO it instead restores the
+// values before that update: new = old(1-w) - w(nb - r0)/e, so
+// old = (new + w(nb - r0)/e)/(1-w) (w > 1 after the first half-sweep).
+template <bool UNDO>
 __device__ __forceinline__ float sweep4(const Sor32Args &s, float *D, const float *B, const uint8_t *M,
-                                        const float *CR, const float *DR, int j, int uj, int dj, int p, int k0, float w)
+                                        const float *CR, const float *DR, int jd, int uj, int dj, int jb, int p,
+                                        int k0, float w)
 {
   const int H = s.H;
-  const int rs = (j * 2 + p) * H + k0, ro = (j * 2 + (p ^ 1)) * H + k0, rb = ((j - 1) * 2 + p) * H + k0;
+  const int rs = (jd * 2 + p) * H + k0, ro = (jd * 2 + (p ^ 1)) * H + k0, rb = (jb * 2 + p) * H + k0;
   float4 sv = *reinterpret_cast<const float4 *>(D + rs);
   const float4 uv = *reinterpret_cast<const float4 *>(D + (uj * 2 + p) * H + k0);
   const float4 dv = *reinterpret_cast<const float4 *>(D + (dj * 2 + p) * H + k0);
@@ -451,43 +455,126 @@ __device__ __forceinline__ float sweep4(const Sor32Args &s, float *D, const floa
   }
   const float a = s.a, e = s.e, we = w * s.inv_e;
   float acc = 0.f;
-  if (mv.x) {
-    float res;
-    if (p == 0 && k0 == 0) { // the axis node (poisson.c:386-387)
-      res = a * (uv.x + dv.x) + s.c4 * r0 + s.e2c * sv.x - bv.x;
-      sv.x -= w * s.inv_e2c * res;
-    } else {
-      res = a * (uv.x + dv.x) + cr.x * r0 + dr.x * l0 + e * sv.x - bv.x;
-      sv.x -= we * res;
+  if (UNDO) {
+    const float inv1w = 1.f / (1.f - w);
+    if (mv.x) {
+      if (p == 0 && k0 == 0)
+        sv.x = (sv.x + w * s.inv_e2c * (a * (uv.x + dv.x) + s.c4 * r0 - bv.x)) * inv1w;
+      else
+        sv.x = (sv.x + we * (a * (uv.x + dv.x) + cr.x * r0 + dr.x * l0 - bv.x)) * inv1w;
     }
-    acc += fabsf(res);
-  }
-  if (mv.y) {
-    const float res = a * (uv.y + dv.y) + cr.y * r1 + dr.y * l1 + e * sv.y - bv.y;
-    sv.y -= we * res;
-    acc += fabsf(res);
-  }
-  if (mv.z) {
-    const float res = a * (uv.z + dv.z) + cr.z * r2 + dr.z * l2 + e * sv.z - bv.z;
-    sv.z -= we * res;
-    acc += fabsf(res);
-  }
-  if (mv.w) {
-    const float res = a * (uv.w + dv.w) + cr.w * r3 + dr.w * l3 + e * sv.w - bv.w;
-    sv.w -= we * res;
-    acc += fabsf(res);
+    if (mv.y)
+      sv.y = (sv.y + we * (a * (uv.y + dv.y) + cr.y * r1 + dr.y * l1 - bv.y)) * inv1w;
+    if (mv.z)
+      sv.z = (sv.z + we * (a * (uv.z + dv.z) + cr.z * r2 + dr.z * l2 - bv.z)) * inv1w;
+    if (mv.w)
+      sv.w = (sv.w + we * (a * (uv.w + dv.w) + cr.w * r3 + dr.w * l3 - bv.w)) * inv1w;
+  } else {
+    if (mv.x) {
+      float res;
+      if (p == 0 && k0 == 0) { // the axis node (poisson.c:386-387)
+        res = a * (uv.x + dv.x) + s.c4 * r0 + s.e2c * sv.x - bv.x;
+        sv.x -= w * s.inv_e2c * res;
+      } else {
+        res = a * (uv.x + dv.x) + cr.x * r0 + dr.x * l0 + e * sv.x - bv.x;
+        sv.x -= we * res;
+      }
+      acc += fabsf(res);
+    }
+    if (mv.y) {
+      const float res = a * (uv.y + dv.y) + cr.y * r1 + dr.y * l1 + e * sv.y - bv.y;
+      sv.y -= we * res;
+      acc += fabsf(res);
+    }
+    if (mv.z) {
+      const float res = a * (uv.z + dv.z) + cr.z * r2 + dr.z * l2 + e * sv.z - bv.z;
+      sv.z -= we * res;
+      acc += fabsf(res);
+    }
+    if (mv.w) {
+      const float res = a * (uv.w + dv.w) + cr.w * r3 + dr.w * l3 + e * sv.w - bv.w;
+      sv.w -= we * res;
+      acc += fabsf(res);
+    }
   }
   *reinterpret_cast<float4 *>(D + rs) = sv;
   return acc;
 }
 
-__global__ void __launch_bounds__(1024) k_sor32(DevMesh m, Sor32Args s, DevCounts *cnt)
+// One colour over D rows jlo..jhi (mesh row iz = iz_first + jd - 2; B/M row
+// jd - 1); |residual| summed over the own rows 2..nrow+1 only.
+template <bool UNDO>
+__device__ float sweep_rows(const DevMesh &m, const Sor32Args &s, float *D, const float *B, const uint8_t *M,
+                            const float *CR, const float *DR, int iz_first, int nrow, int jlo, int jhi, int c, float w)
+{
+  const int nz = m.nz, Q = s.H >> 2, NT = blockDim.x, tid = threadIdx.x;
+  const int slots = (jhi - jlo + 1) * Q, jstep = NT / Q, qstep = NT - jstep * Q;
+  int jd = jlo + tid / Q, q = tid - (tid / Q) * Q;
+  float acc = 0.f;
+  for (int t = tid; t < slots; t += NT) {
+    const int iz = iz_first + jd - 2;
+    const int p = (c + iz) & 1;
+    // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
+    const int uj = (iz == nz - 1 && s.hi == nz - 1) ? jd - 1 : jd + 1;
+    const int dj = (iz == 0 && s.lo == 0) ? jd + 1 : jd - 1;
+    const float r = sweep4<UNDO>(s, D, B, M, CR, DR, jd, uj, dj, jd - 1, p, q << 2, w);
+    if (jd >= 2 && jd <= nrow + 1)
+      acc += r;
+    q += qstep;
+    jd += jstep;
+    if (q >= Q) {
+      q -= Q;
+      jd++;
+    }
+  }
+  return acc;
+}
+
+// Psi += d on the band's own updated nodes (FP64)
+__device__ void fold_d(const Sor32Args &s, int P, const float *D, const uint8_t *M, int iz_first, int nrow)
+{
+  const int H = s.H, cols = s.cols;
+  for (int j = 2; j <= nrow + 1; j++) {
+    const int iz = iz_first + j - 2;
+    for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
+      const int p = t / H, k = t - p * H, ir = 2 * k + p;
+      const float d = D[(j * 2 + p) * H + k];
+      if (ir < cols && M[((j - 1) * 2 + p) * H + k] && d != 0.f) {
+        const size_t i = node(iz, ir, P);
+        __stcg(s.Psi + i, __ldcg(s.Psi + i) + (double)d);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double block_sum2(double v, double *red, int slot)
+{
+  for (int o = 16; o > 0; o >>= 1)
+    v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0)
+    red[slot * 32 + (threadIdx.x >> 5)] = v;
+  return v;
+}
+
+// solve_poisson_cyl (poisson.c:17-130) on the correction d of the warm
+// start.  Each round runs one half-sweep of each colour between two grid
+// barriers: a CTA's band carries two halo rows on each side, the colour-0
+// sweep also updates the nearer halo row (from exactly the inputs the
+// neighbour uses, so with the same result), and the colour-1 sweep then
+// needs nothing from the neighbours.  Both half-sweeps' |residual| sums
+// arrive with the barrier, so the reference's stop test runs after every
+// half-sweep; when it fires after colour 0, the colour-1 update of the
+// round is undone.
+constexpr int SOR_NT = 1024; // threads per CTA of the shared-memory kernel
+
+__global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCounts *cnt)
 {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[64];
-  __shared__ int ok_sh, stop_sh, rebase_sh;
-  __shared__ double total_sh, thr_sh, quantum_sh, partial_sh, base_sh;
-  __shared__ unsigned long long tf_sh;
+  __shared__ int ok_sh, stop_sh, undo_sh, rebase_sh;
+  __shared__ double total_sh, thr_sh, quantum_sh, base_sh, p0_sh, p1_sh;
+  __shared__ unsigned long long t0_sh, t1_sh;
+  __shared__ long long result_sh;
   if (s.st && !s.st->do_solve)
     return;
   const int nz = m.nz, P = m.pitch, H = s.H, Q = s.H >> 2, cols = s.cols, R = s.rows_per;
@@ -495,30 +582,34 @@ __global__ void __launch_bounds__(1024) k_sor32(DevMesh m, Sor32Args s, DevCount
   int start, nrow;
   band(s.hi - s.lo + 1, b, G, start, nrow);
   const int iz_first = s.lo + start;
-  // shared layout (32-bit offsets): D[(R+2)][2][H] d, B[R][2][H] r0,
-  // CR/DR[2][H] row coefficients, M[R][2][H] node mask; row j's nodes of
-  // parity p are the contiguous run (j*2+p)*H .. +H
+  // shared layout (32-bit offsets): D[(R+4)][2][H] d for mesh rows
+  // iz_first-2 .. iz_first+R+1 (D row iz - iz_first + 2), B[(R+2)][2][H] r0
+  // and M[(R+2)][2][H] node mask for rows iz_first-1 .. (B row iz -
+  // iz_first + 1), CR/DR[2][H] row coefficients; row j's nodes of parity p
+  // are the contiguous run (j*2+p)*H .. +H
   float *D = (float *)smem;
-  float *B = D + (R + 2) * 2 * H;
-  float *CR = B + R * 2 * H;
+  float *B = D + (R + 4) * 2 * H;
+  float *CR = B + (R + 2) * 2 * H;
   float *DR = CR + 2 * H;
   uint8_t *M = (uint8_t *)(DR + 2 * H);
-  for (int t = tid; t < (R + 2) * 2 * H; t += NT)
+  for (int t = tid; t < (R + 4) * 2 * H; t += NT)
     D[t] = 0.f;
   for (int t = tid; t < 2 * H; t += NT) {
     const int p = t / H, k = t - p * H, ir = 2 * k + p;
     CR[t] = ir < cols ? s.crow[ir] : 0.f;
     DR[t] = ir < cols ? s.drow[ir] : 0.f;
   }
-  for (int j = 1; j <= nrow; j++) {
-    const int iz = iz_first + j - 1;
+  for (int i = 0; i < nrow + 2; i++) {
+    const int iz = iz_first - 1 + i;
+    const bool upd = iz >= s.lo && iz <= s.hi;
     for (int t = tid; t < 2 * H; t += NT) {
       const int p = t / H, k = t - p * H, ir = 2 * k + p;
-      M[((j - 1) * 2 + p) * H + k] = ir < cols && !(s.umask[node(iz, ir, P)] & S32_U_METAL) ? 1 : 0;
+      M[(i * 2 + p) * H + k] = upd && ir < cols && !(s.umask[node(iz, ir, P)] & S32_U_METAL) ? 1 : 0;
     }
   }
+  const int iz_last = iz_first + nrow - 1;
   double drive = 0, r0sum = 0;
-  form_r0(m, s, B, iz_first, nrow, &drive, &r0sum);
+  form_r0(m, s, B, iz_first - 1, nrow + 2, iz_first, iz_last, &drive, &r0sum);
   // rows outside lo..hi that the driving sum still covers (iz < nz)
   if (s.rhs) {
     const bool first = b == 0, last = b == G - 1;
@@ -532,16 +623,81 @@ __global__ void __launch_bounds__(1024) k_sor32(DevMesh m, Sor32Args s, DevCount
     }
   }
   // fixed-order block sums of the |rhs| and |r0| partials
-  {
-    double v = drive, u = r0sum;
-    for (int o = 16; o > 0; o >>= 1) {
-      v += __shfl_down_sync(0xffffffffu, v, o);
-      u += __shfl_down_sync(0xffffffffu, u, o);
+  block_sum2(drive, red, 0);
+  block_sum2(r0sum, red, 1);
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0, t2 = 0;
+    for (int w = 0; w < (NT + 31) / 32; w++) {
+      t += red[w];
+      t2 += red[32 + w];
     }
-    if ((tid & 31) == 0) {
-      red[tid >> 5] = v;
-      red[32 + (tid >> 5)] = u;
+    if (G > 1) {
+      __stcg(s.dpart + 2 * b, t);
+      __stcg(s.dpart + 2 * b + 1, t2);
+    } else {
+      thr_sh = s.accuracy * t;
+      base_sh = t2;
     }
+  }
+  unsigned gen = 0;
+  if (G > 1) {
+    if (!grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
+      return;
+    if (tid == 0) {
+      double d = 0, qq = 0;
+      for (int i = 0; i < G; i++) {
+        d += __ldcg(s.dpart + 2 * i);
+        qq += __ldcg(s.dpart + 2 * i + 1);
+      }
+      thr_sh = s.accuracy * d;
+      base_sh = qq;
+    }
+  }
+  if (tid == 0) {
+    quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
+    rebase_sh = 0;
+    result_sh = -1;
+    total_sh = 0;
+  }
+  __syncthreads();
+  // sweeps of the first colour cover the nearer halo rows when there are neighbours
+  const int jlo0 = G > 1 ? 1 : 2, jhi0 = G > 1 ? nrow + 2 : nrow + 1;
+  for (long long n0 = 0; n0 < s.limit; n0 += 2) {
+    if (rebase_sh) {
+      // iterative refinement: Psi += d in FP64, r0 = rhs - A Psi in FP64 once
+      // every band has folded its d in, and the sweeps go on from d = 0
+      fold_d(s, P, D, M, iz_first, nrow);
+      if (G > 1) {
+        if (!grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
+          return;
+      } else {
+        __syncthreads();
+      }
+      double d0 = 0, q0 = 0;
+      form_r0(m, s, B, iz_first - 1, nrow + 2, iz_first, iz_last, &d0, &q0);
+      for (int t = tid; t < (R + 4) * 2 * H; t += NT)
+        D[t] = 0.f;
+      __syncthreads();
+    }
+    const bool two = n0 + 1 < s.limit;
+    const float w0 = s.omega[n0], w1 = two ? s.omega[n0 + 1] : 0.f;
+    const float acc0 = sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, jlo0, jhi0, 0, w0);
+    __syncthreads();
+    const float acc1 = two ? sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1) : 0.f;
+    __syncthreads();
+    if (G > 1) {
+      // own rows iz_first, iz_first+1 for the CTA above, iz_last-1, iz_last for the one below
+      float *xo = s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H + (size_t)b * 8 * H;
+      for (int t = tid; t < 8 * Q; t += NT) {
+        const int side = t / (4 * Q), r = t - side * 4 * Q; // r: (row, parity, k4) within the side
+        const int jd = (side == 0 ? 2 : nrow) + r / (2 * Q);
+        const float4 v = *reinterpret_cast<const float4 *>(D + jd * 2 * H + 4 * (r % (2 * Q)));
+        __stcg(reinterpret_cast<float4 *>(xo + side * 4 * H) + r, v);
+      }
+    }
+    block_sum2((double)acc0, red, 0);
+    block_sum2((double)acc1, red, 1);
     __syncthreads();
     if (tid == 0) {
       double t = 0, t2 = 0;
@@ -549,158 +705,90 @@ __global__ void __launch_bounds__(1024) k_sor32(DevMesh m, Sor32Args s, DevCount
         t += red[w];
         t2 += red[32 + w];
       }
-      if (G > 1) {
-        __stcg(s.dpart + 2 * b, t);
-        __stcg(s.dpart + 2 * b + 1, t2);
-      } else {
-        thr_sh = s.accuracy * t;
-        base_sh = t2;
-      }
-      rebase_sh = 0;
+      p0_sh = t;
+      p1_sh = t2;
     }
-    __syncthreads();
-  }
-  unsigned gen = 0;
-  const int slots = nrow * Q, jstep = NT / Q, qstep = NT - jstep * Q;
-  long long result = -1;
-  double total = 0;
-  for (long long n = 0; n < s.limit; n++) {
-    if (rebase_sh) {
-      // iterative refinement: Psi += d in FP64, r0 = rhs - A Psi in FP64 once
-      // every band has folded its d in, and the sweeps go on from d = 0
-      fold_d(s, P, D, M, iz_first, nrow);
-      if (G > 1) {
-        if (!grid_sync_sum(s, 0ull, gen, nullptr, cnt, &ok_sh))
-          return;
-      } else {
-        __syncthreads();
-      }
-      double d0 = 0, q0 = 0;
-      form_r0(m, s, B, iz_first, nrow, &d0, &q0);
-      for (int t = tid; t < (R + 2) * 2 * H; t += NT)
-        D[t] = 0.f;
-      __syncthreads();
-    }
-    const float w = s.omega[n];
-    const int c = (int)(n & 1);
-    float acc = 0.f;
-    int j = 1 + tid / Q, q = tid - (tid / Q) * Q;
-    for (int t = tid; t < slots; t += NT) {
-      const int iz = iz_first + j - 1;
-      const int p = (c + iz) & 1;
-      // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
-      const int uj = (iz == nz - 1 && s.hi == nz - 1) ? j - 1 : j + 1;
-      const int dj = (iz == 0 && s.lo == 0) ? j + 1 : j - 1;
-      const int k0 = q << 2;
-      acc += sweep4(s, D, B, M, CR, DR, j, uj, dj, p, k0, w);
-      if (G > 1 && (j == 1 || j == nrow)) {
-        const float4 v = *reinterpret_cast<const float4 *>(D + (j * 2 + p) * H + k0);
-        float *x = s.xbuf + ((size_t)((n & 1) * G + b) * 2 + (j == 1 ? 0 : 1)) * H + k0;
-        __stcg(reinterpret_cast<float4 *>(x), v);
-        if (j == 1 && nrow == 1)
-          __stcg(reinterpret_cast<float4 *>(x + H), v);
-      }
-      q += qstep;
-      j += jstep;
-      if (q >= Q) {
-        q -= Q;
-        j++;
-      }
-    }
-    // fixed-order block sum of |residual|
-    double v = (double)acc;
-    for (int o = 16; o > 0; o >>= 1)
-      v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((tid & 31) == 0)
-      red[tid >> 5] = v;
-    __syncthreads();
-    if (tid == 0) {
-      double t = 0;
-      for (int wi = 0; wi < (NT + 31) / 32; wi++)
-        t += red[wi];
-      partial_sh = t;
-    }
-    __syncthreads();
-    const double partial = partial_sh;
+    double total0, total1;
+    unsigned long long tf0 = 0, tf1 = 0;
     if (G > 1) {
-      // this CTA's |residual| sum in quanta of 2^-30 of the larger of the
+      // this CTA's |residual| sums in quanta of 2^-30 of the larger of the
       // refinement base and the stop threshold, capped at 2^40 quanta
-      unsigned long long pf = 0;
-      if (tid == 0 && n > 0 && partial != 0) {
-        const double x = partial / quantum_sh;
-        pf = x >= 1099511627776.0 ? 1099511627776ull : (unsigned long long)llrint(x);
-        if (pf == 0)
-          pf = 1;
-      }
-      if (!grid_sync_sum(s, pf, gen, &tf_sh, cnt, &ok_sh))
-        return;
-      // neighbour rows of the colour just updated
-      if (b > 0) {
-        const int ph = (c + iz_first - 1) & 1;
-        const float *x = s.xbuf + ((size_t)((n & 1) * G + (b - 1)) * 2 + 1) * H;
-        for (int k = tid; k < Q; k += NT)
-          *reinterpret_cast<float4 *>(D + ph * H + 4 * k) = __ldcg(reinterpret_cast<const float4 *>(x) + k);
-      }
-      if (b < G - 1) {
-        const int ph = (c + iz_first + nrow) & 1;
-        const float *x = s.xbuf + ((size_t)((n & 1) * G + (b + 1)) * 2 + 0) * H;
-        for (int k = tid; k < Q; k += NT)
-          *reinterpret_cast<float4 *>(D + ((nrow + 1) * 2 + ph) * H + 4 * k) =
-              __ldcg(reinterpret_cast<const float4 *>(x) + k);
-      }
+      unsigned long long q0 = 0, q1 = 0;
       if (tid == 0) {
-        if (n == 0) {
-          double d = 0, qq = 0;
-          for (int i = 0; i < G; i++) {
-            d += __ldcg(s.dpart + 2 * i);
-            qq += __ldcg(s.dpart + 2 * i + 1);
-          }
-          thr_sh = s.accuracy * d;
-          base_sh = qq;
-          stop_sh = 0;
-        } else {
-          const unsigned long long tf = tf_sh;
-          total_sh = (double)tf * quantum_sh;
-          stop_sh = total_sh < thr_sh || tf == 0;
+        const double x0 = p0_sh / quantum_sh, x1 = p1_sh / quantum_sh;
+        if (p0_sh != 0)
+          q0 = x0 >= 1099511627776.0 ? 1099511627776ull : ((unsigned long long)llrint(x0) | 1ull);
+        if (p1_sh != 0)
+          q1 = x1 >= 1099511627776.0 ? 1099511627776ull : ((unsigned long long)llrint(x1) | 1ull);
+      }
+      if (!grid_sync_sum(s, q0, q1, gen, &t0_sh, &t1_sh, cnt, &ok_sh))
+        return;
+      // the neighbours' rows into the halo rows
+      const float *xi = s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H;
+      for (int t = tid; t < 8 * Q; t += NT) {
+        const int side = t / (4 * Q), r = t - side * 4 * Q;
+        if (side == 0 && b > 0) {
+          const float4 v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)(b - 1) * 8 * H + 4 * H) + r);
+          *reinterpret_cast<float4 *>(D + (r / (2 * Q)) * 2 * H + 4 * (r % (2 * Q))) = v;
+        } else if (side == 1 && b < G - 1) {
+          const float4 v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)(b + 1) * 8 * H) + r);
+          *reinterpret_cast<float4 *>(D + (nrow + 2 + r / (2 * Q)) * 2 * H + 4 * (r % (2 * Q))) = v;
         }
       }
-    } else if (tid == 0) {
-      if (n > 0) {
-        total_sh = partial;
-        stop_sh = partial < thr_sh || partial == 0;
-      } else {
-        stop_sh = 0;
-      }
+      tf0 = t0_sh;
+      tf1 = t1_sh;
+      total0 = (double)tf0 * quantum_sh;
+      total1 = (double)tf1 * quantum_sh;
+    } else {
+      __syncthreads();
+      total0 = p0_sh;
+      total1 = p1_sh;
+      tf0 = total0 != 0;
+      tf1 = total1 != 0;
     }
     if (tid == 0) {
-      // Iterative refinement: once the residual has fallen 2^8-fold below the
-      // last FP64 residual (the base), fold d into Psi and form the residual
-      // again in FP64 before FP32 rounding of the growing d limits it.  The
-      // fixed-point quantum of the residual sums is 2^-30 of the larger of
-      // the base and the stop threshold, so the stop test keeps its
-      // resolution as the base follows the residual down; a per-CTA sum is
-      // capped at 2^40 quanta (the barrier word holds 255 of them).
-      rebase_sh = 0;
-      if (n > 0 && !stop_sh && total_sh < base_sh * (1.0 / 256)) {
-        rebase_sh = 1;
-        base_sh = total_sh;
+      const bool stop0 = n0 > 0 && (total0 < thr_sh || tf0 == 0);
+      const bool stop1 = two && (total1 < thr_sh || tf1 == 0);
+      stop_sh = stop0 || stop1;
+      undo_sh = stop0 && two;
+      if (stop0) {
+        result_sh = n0;
+        total_sh = total0;
+      } else if (stop1) {
+        result_sh = n0 + 1;
+        total_sh = total1;
+      } else {
+        total_sh = two ? total1 : total0;
+        // Iterative refinement: once the residual has fallen 2^8-fold below
+        // the last FP64 residual (the base), fold d into Psi and form the
+        // residual again in FP64 before FP32 rounding of the growing d
+        // limits it.  The fixed-point quantum of the residual sums is 2^-30
+        // of the larger of the base and the stop threshold, so the stop test
+        // keeps its resolution as the base follows the residual down; a
+        // per-CTA sum is capped at 2^40 quanta (a barrier word holds 255).
+        rebase_sh = total_sh < base_sh * (1.0 / 256);
+        if (rebase_sh)
+          base_sh = total_sh;
+        quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
       }
-      quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
     }
     __syncthreads();
-    total = total_sh;
-    if (n > 0 && stop_sh) {
-      result = n;
+    if (stop_sh) {
+      if (undo_sh) {
+        sweep_rows<true>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1);
+        __syncthreads();
+      }
       break;
     }
   }
   fold_d(s, P, D, M, iz_first, nrow);
   if (b == 0 && tid == 0) {
+    const long long result = result_sh;
     if (s.iters_out)
       *s.iters_out = result;
     if (s.st) {
       s.st->iterations = result;
-      s.st->residual = total;
+      s.st->residual = total_sh;
     }
     cnt->sor_halfsweeps += result >= 0 ? result + 1 : s.limit;
     cnt->sor_solves += 1;
@@ -781,12 +869,17 @@ __global__ void __launch_bounds__(BX *BY) k_imposed32(DevMesh m, DevFields32 f, 
   }
 }
 
-size_t sor_smem(int R, int H) { return (size_t)(R + 2) * 2 * H * 4 + (size_t)R * 2 * H * 4 + 2 * (size_t)2 * H * 4 + (size_t)R * 2 * H; }
+// shared bytes of a band of R rows: d with two halo rows a side, r0 and the
+// mask with one, the row coefficients
+size_t sor_smem(int R, int H)
+{
+  return (size_t)(R + 4) * 2 * H * 4 + (size_t)(R + 2) * 2 * H * 4 + 2 * (size_t)2 * H * 4 + (size_t)(R + 2) * 2 * H;
+}
 
 int sor_threads(int R, int H)
 {
-  const int slots = R * (H / 4);
-  return std::min(1024, std::max(128, (slots + 31) / 32 * 32));
+  const int slots = (R + 2) * (H / 4);
+  return std::min(SOR_NT, std::max(128, (slots + 31) / 32 * 32));
 }
 
 } // namespace
@@ -820,26 +913,29 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
   const int rows = (m->right_bc == SPIFFE_DIRICHLET ? nz - 1 : nz - 2) - (m->left_bc == SPIFFE_DIRICHLET ? 0 : 1) + 1;
   const int cols = nr - 1, H = ((cols + 2) / 2 + 3) / 4 * 4; // half-row (one colour), a multiple of 4
   const size_t budget = (size_t)max_smem - 1024;
+  // one CTA when the mesh fits one SM (no grid barriers); otherwise bands of
+  // at least two rows (the halo exchange carries two rows) over all SMs
   int G = 1;
   if (sor_smem(rows, H) > budget || (size_t)rows * 2 * H > 65536) {
-    G = std::min(sms, rows);
-    while (G < rows && sor_smem((rows + G - 1) / G, H) > budget)
+    G = std::min(sms, rows / 2);
+    while (G < rows / 2 && sor_smem((rows + G - 1) / G, H) > budget)
       G++;
   }
+  cudaError_t e = cudaSuccess;
+  int occ = 0;
   const int R = (rows + G - 1) / G;
-  if (G > sms || G > 255 || sor_smem(R, H) > budget)
+  if (G < 1 || G > sms || G > 255 || sor_smem(R, H) > budget)
     return (int)cudaErrorInvalidConfiguration; // the mesh does not fit the shared-memory bands
   w->grid = G;
   w->rows_per = R;
-  w->half = H;
   w->smem = sor_smem(R, H);
   w->threads = sor_threads(R, H);
-  cudaError_t e = cudaFuncSetAttribute(k_sor32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem);
-  int occ = 0;
+  e = cudaFuncSetAttribute(k_sor32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem);
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor32, w->threads, w->smem);
   if (e == cudaSuccess && occ < 1)
     e = cudaErrorInvalidConfiguration;
+  w->half = H;
   const size_t gx = (nr + 1 + BX - 1) / BX, gy = (nz + 1 + BY - 1) / BY;
   size_t parts = std::max<size_t>(2 * gx * gy, 4096);
   (void)np_capacity;
@@ -856,9 +952,9 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
     if (e == cudaSuccess) e = cudaMemsetAsync(w->st, 0, sizeof(PcState), s);
     if (e == cudaSuccess) e = cudaMalloc(&w->iters, sizeof(long long));
     if (e == cudaSuccess) e = cudaMalloc(&w->bar, sizeof(unsigned) * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&w->rsum, sizeof(unsigned long long) * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&w->rsum, sizeof(unsigned long long) * 4);
     if (e == cudaSuccess) e = cudaMalloc(&w->dpart, sizeof(double) * (size_t)sms * 2); // |rhs|, |r0| per CTA
-    if (e == cudaSuccess) e = cudaMalloc(&w->xbuf, sizeof(float) * (size_t)2 * sms * 2 * H);
+    if (e == cudaSuccess) e = cudaMalloc(&w->xbuf, sizeof(float) * (size_t)2 * sms * 8 * H); // exchange rows
     if (e == cudaSuccess) e = cudaMalloc(&w->part, sizeof(double) * parts);
     w->part_n = parts;
   }
@@ -936,6 +1032,8 @@ extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const do
   a.xbuf = w->xbuf;
   a.arrive = w->rsum;
   a.release = w->rsum + 1;
+  a.acc1 = w->rsum + 2;
+  a.pub1 = w->rsum + 3;
   a.dpart = w->dpart;
   a.st = st;
   a.iters_out = w->iters;
@@ -946,12 +1044,12 @@ extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const do
   a.rows_per = w->rows_per;
   cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(unsigned) * 2, s);
   if (e == cudaSuccess)
-    e = cudaMemsetAsync(w->rsum, 0, sizeof(unsigned long long) * 2, s);
+    e = cudaMemsetAsync(w->rsum, 0, sizeof(unsigned long long) * 4, s);
   if (e != cudaSuccess)
     return (int)e;
   DevMesh mm = *m;
   void *args[] = {&mm, &a, &cnt};
-  e = cudaLaunchCooperativeKernel((void *)k_sor32, dim3(w->grid), dim3(w->threads), args, w->smem, s);
+  e = cudaLaunchCooperativeKernel((const void *)k_sor32, dim3(w->grid), dim3(w->threads), args, w->smem, s);
   spiffe_note_launches(1);
   return (int)e;
 }

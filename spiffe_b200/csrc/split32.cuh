@@ -32,6 +32,8 @@
 #define S32_U_BR 16u   // Br interior update (iz <= cut1[ir], no FL_BR_ZERO)
 #define S32_U_BZ 32u   // Bz interior update (iz <= cut0[ir], no FL_BZ_ZERO)
 #define S32_U_METAL 64u // FL_IS_METAL
+#define S32_U_CLEAN 128u // no flag set on rows iz-1..iz+1 x columns ir..ir+1: the gather's metal
+                         // fix-ups (advance_particles.c:672-690, :730-735) cannot apply in cell (iz, ir)
 
 // particle status byte
 #define S32_ACTIVE 1u
