@@ -49,6 +49,7 @@ struct DevBeam64 {
 struct DevScreen {
   double z_position;
   int direction;
+  int cell; // floor((z_position - zmin)/dz): a crossing starts or ends in a cell range containing it
   int64_t capacity;
   double *col[SPIFFE_SCREEN_QUANS];
   double *rmin, *rmax, *zmin, *zmax;

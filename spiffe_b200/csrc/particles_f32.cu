@@ -465,7 +465,7 @@ __global__ void k_snapshot_last32(DevBeam32 b, DevCounts *cnt)
 // advance_particles (:131-339) and its screen loop (:362-434); with DEP the
 // pushed particle's current for the next step.
 template <bool DEP, bool DEF>
-__global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBeam32 b, Push32Params p, DevScreens scr,
+__global__ void __launch_bounds__(T, 3) k_push32(DevMesh m, DevFields32 f, DevBeam32 b, Push32Params p, DevScreens scr,
                                                DevCounts *cnt, int32_t *lost_list, S32Scales sc)
 {
   const long ip = (long)blockIdx.x * T + threadIdx.x;
@@ -525,7 +525,9 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
       }
     }
     float adjust = 1.f;
-    const double zd = m.zmin + ((double)iz + fz) * m.dz, z0d = m.zmin + ((double)iz0 + fz0) * m.dz;
+    // FP64 positions, formed only where a rare branch needs them
+    auto zd_of = [&]() { return m.zmin + ((double)iz + fz) * m.dz; };
+    auto z0d_of = [&]() { return m.zmin + ((double)iz0 + fz0) * m.dz; };
     // zmax = zmin + (nz-1) dz and rmax = (nr-1) dr (geometry.c:75-76)
     const bool above_zmin = iz >= 0, below_zmax = iz < nz - 1 || (iz == nz - 1 && fz == 0.f);
     const bool r_le_rmax = r_negative || irs < nr - 1 || (irs == nr - 1 && frs == 0.f);
@@ -536,7 +538,7 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
         atomic_add_ll(&cnt->new_active, 1LL);
         b.t0[ip] = p.time;
         b.r0[ip] = ((double)ir0 + fr0) * m.dr;
-        b.z0[ip] = z0d;
+        b.z0[ip] = z0d_of();
         const float dxi = ((float)(iz - iz0) + (fz - fz0));
         if (iz > 0 && loss_code32(m, fl, iz - 1, ir))
           adjust = fz / dxi;
@@ -546,7 +548,8 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
           adjust = 1.f;
       }
     }
-    if (p.z_forces_start > m.zmin && p.z_forces_start < m.zmax) {
+    if (p.zfs_on) {
+      const double zd = zd_of(), z0d = z0d_of();
       if (z0d < p.z_forces_start) {
         if (zd < p.z_forces_start)
           adjust = 0.f;
@@ -575,7 +578,7 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
       if (r > rmx) rmx = r;
       if (r < rmn) rmn = r;
     }
-    if (!p.forced) {
+    if (DEF || !p.forced) {
       // momentum kick with the old velocities (:270-287)
       float E[6];
       if (active)
@@ -596,7 +599,7 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
       const float pphi = rpp * ir_;
       const float ig = rsqrtf(pr * pr + pz * pz + pphi * pphi + 1.f);
       pr += p.dt * (pphi * pphi * C_F * ig * ir_);
-      if (zd <= p.tb_z_decel)
+      if (zd_of() <= p.tb_z_decel)
         pz += p.tb_z_force_dt;
       else {
         pz -= p.tb_z_force_dt;
@@ -633,7 +636,12 @@ __global__ void __launch_bounds__(T, 2) k_push32(DevMesh m, DevFields32 f, DevBe
       atomicOr(&cnt->error, SPIFFE_DEV_ERR_INDEX);
 
     // screen crossings (:362-434), in FP64
-    if (scr.n) {
+    // a crossing needs the screen's cell between the old and new cells
+    bool near_screen = false;
+    for (int is = 0; is < scr.n; is++)
+      near_screen |= min(iz0, iz) <= scr.s[is].cell && scr.s[is].cell <= max(iz0, iz);
+    if (near_screen) {
+      const double zd = zd_of(), z0d = z0d_of();
       const bool ref = p.screen_momentum == SPIFFE_SCREEN_REFERENCE;
       const double pz0s = ref ? cnt->last_pz0 : pz0, pr0s = ref ? cnt->last_pr0 : pr0;
       const double rpp0s = ref ? cnt->last_rpphi0 : rpp0;
@@ -1117,7 +1125,7 @@ extern "C" int s32_push(const DevMesh *m, const DevFields32 *f, const DevBeam32 
     const unsigned def_modes = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_LONGIT_INTERP | SPIFFE_FL_RADIAL_INTERP;
     const unsigned mode_bits = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_TE_FIELDS | SPIFFE_FL_LONGIT_INTERP |
                                SPIFFE_FL_RADIAL_INTERP | SPIFFE_FL_LONGIT_SMEAR | SPIFFE_FL_RADIAL_SMEAR;
-    bool def = (m->modes & mode_bits) == def_modes;
+    bool def = (m->modes & mode_bits) == def_modes && !p->forced;
     for (int k = 0; k < 6; k++)
       def = def && !m->turn_off[k];
     int32_t *ll = any ? w->lost_list : nullptr;

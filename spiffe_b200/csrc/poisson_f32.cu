@@ -312,14 +312,14 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
 // accumulators, publishes the second sum in *pub1 and releases the others
 // by storing the next generation (high 16 bits) with the first sum (low 48
 // bits) in *release.  The fence before the arrival releases the CTA's
-// earlier writes; the acquire of *release (or the fence after the last
-// arrival) makes every CTA's writes visible.  `gen` counts the barriers the
-// calling thread has passed.  Returns false (and raises the device error
-// bit) when the others do not arrive within the poll limit.
+// earlier writes (the caller synchronises the CTA first, so they precede
+// it); the acquire of *release (or the fence after the last arrival) makes
+// every CTA's writes visible.  `gen` counts the barriers the calling thread
+// has passed.  Returns false (and raises the device error bit) when the
+// others do not arrive within the poll limit.
 __device__ bool grid_sync_sum(const Sor32Args &s, unsigned long long v0, unsigned long long v1, unsigned &gen,
                               unsigned long long *t0, unsigned long long *t1, DevCounts *cnt, int *ok_sh)
 {
-  __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     gen = (gen + 1) & 0xffffu;
@@ -503,9 +503,13 @@ __device__ __forceinline__ float sweep4(const Sor32Args &s, float *D, const floa
 
 // One colour over D rows jlo..jhi (mesh row iz = iz_first + jd - 2; B/M row
 // jd - 1); |residual| summed over the own rows 2..nrow+1 only.
+// With xo, a slot of an exchanged row (the first two and the last two own
+// rows) also stores both colours of its four columns there, for the
+// neighbouring CTAs (the other colour was final after the previous sweep).
 template <bool UNDO>
 __device__ float sweep_rows(const DevMesh &m, const Sor32Args &s, float *D, const float *B, const uint8_t *M,
-                            const float *CR, const float *DR, int iz_first, int nrow, int jlo, int jhi, int c, float w)
+                            const float *CR, const float *DR, int iz_first, int nrow, int jlo, int jhi, int c, float w,
+                            float *xo = nullptr)
 {
   const int nz = m.nz, Q = s.H >> 2, NT = blockDim.x, tid = threadIdx.x;
   const int slots = (jhi - jlo + 1) * Q, jstep = NT / Q, qstep = NT - jstep * Q;
@@ -520,6 +524,25 @@ __device__ float sweep_rows(const DevMesh &m, const Sor32Args &s, float *D, cons
     const float r = sweep4<UNDO>(s, D, B, M, CR, DR, jd, uj, dj, jd - 1, p, q << 2, w);
     if (jd >= 2 && jd <= nrow + 1)
       acc += r;
+    if (xo) {
+      const int H = s.H;
+      // side 0: rows 2, 3 for the CTA above; side 1: rows nrow, nrow+1 for the one below
+      const bool s0 = jd <= 3, s1 = jd >= nrow;
+      if (s0 || s1) {
+        const float4 v0 = *reinterpret_cast<const float4 *>(D + (jd * 2) * H + 4 * q);
+        const float4 v1 = *reinterpret_cast<const float4 *>(D + (jd * 2 + 1) * H + 4 * q);
+        if (s0) {
+          float *x = xo + (jd - 2) * 2 * H + 4 * q;
+          __stcg(reinterpret_cast<float4 *>(x), v0);
+          __stcg(reinterpret_cast<float4 *>(x + H), v1);
+        }
+        if (s1) {
+          float *x = xo + 4 * H + (jd - nrow) * 2 * H + 4 * q;
+          __stcg(reinterpret_cast<float4 *>(x), v0);
+          __stcg(reinterpret_cast<float4 *>(x + H), v1);
+        }
+      }
+    }
     q += qstep;
     jd += jstep;
     if (q >= Q) {
@@ -641,6 +664,7 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
     }
   }
   unsigned gen = 0;
+  __syncthreads();
   if (G > 1) {
     if (!grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
       return;
@@ -668,12 +692,9 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
       // iterative refinement: Psi += d in FP64, r0 = rhs - A Psi in FP64 once
       // every band has folded its d in, and the sweeps go on from d = 0
       fold_d(s, P, D, M, iz_first, nrow);
-      if (G > 1) {
-        if (!grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
-          return;
-      } else {
-        __syncthreads();
-      }
+      __syncthreads();
+      if (G > 1 && !grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
+        return;
       double d0 = 0, q0 = 0;
       form_r0(m, s, B, iz_first - 1, nrow + 2, iz_first, iz_last, &d0, &q0);
       for (int t = tid; t < (R + 4) * 2 * H; t += NT)
@@ -684,29 +705,25 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
     const float w0 = s.omega[n0], w1 = two ? s.omega[n0 + 1] : 0.f;
     const float acc0 = sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, jlo0, jhi0, 0, w0);
     __syncthreads();
-    const float acc1 = two ? sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1) : 0.f;
-    __syncthreads();
-    if (G > 1) {
-      // own rows iz_first, iz_first+1 for the CTA above, iz_last-1, iz_last for the one below
-      float *xo = s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H + (size_t)b * 8 * H;
-      for (int t = tid; t < 8 * Q; t += NT) {
-        const int side = t / (4 * Q), r = t - side * 4 * Q; // r: (row, parity, k4) within the side
-        const int jd = (side == 0 ? 2 : nrow) + r / (2 * Q);
-        const float4 v = *reinterpret_cast<const float4 *>(D + jd * 2 * H + 4 * (r % (2 * Q)));
-        __stcg(reinterpret_cast<float4 *>(xo + side * 4 * H) + r, v);
-      }
-    }
+    // the colour-1 sweep also writes the exchanged rows for the neighbours
+    float *xo = G > 1 ? s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H + (size_t)b * 8 * H : nullptr;
+    const float acc1 =
+        two ? sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1, xo) : 0.f;
     block_sum2((double)acc0, red, 0);
     block_sum2((double)acc1, red, 1);
     __syncthreads();
-    if (tid == 0) {
-      double t = 0, t2 = 0;
-      for (int w = 0; w < (NT + 31) / 32; w++) {
-        t += red[w];
-        t2 += red[32 + w];
+    if (tid < 32) {
+      // fixed-order warp reduction of the per-warp partials
+      const int nw = (NT + 31) / 32;
+      double t = tid < nw ? red[tid] : 0.0, t2 = tid < nw ? red[32 + tid] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) {
+        t += __shfl_down_sync(0xffffffffu, t, o);
+        t2 += __shfl_down_sync(0xffffffffu, t2, o);
       }
-      p0_sh = t;
-      p1_sh = t2;
+      if (tid == 0) {
+        p0_sh = t;
+        p1_sh = t2;
+      }
     }
     double total0, total1;
     unsigned long long tf0 = 0, tf1 = 0;

@@ -694,6 +694,7 @@ static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, 
   p.QoMC_dt = (float)(in->QoMC * m.dt);
   p.stiff_inv = (float)(1 / in->stiffness);
   p.z_forces_start = o->z_forces_start;
+  p.zfs_on = o->z_forces_start > m.zmin && o->z_forces_start < m.zmax;
   p.forced = o->tb_electrons_per_macroparticle && (o->tb_z_force || o->tb_r_force);
   p.tb_z_force_dt = (float)(m.dt * o->tb_z_force);
   p.tb_r_force_dt = (float)(m.dt * o->tb_r_force);
@@ -1193,6 +1194,7 @@ extern "C" int spiffe_gpu_add_screen(spiffe_gpu_instance *in, double z_position,
   sc = DevScreen{};
   sc.z_position = z_position;
   sc.direction = direction;
+  sc.cell = (int)std::floor((z_position - in->mesh.zmin) / in->mesh.dz);
   sc.capacity = capacity;
   const size_t n = (size_t)capacity;
   for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)

@@ -115,6 +115,7 @@ struct Push32Params {
   double time;
   float dt, dt_dz, dt_dr, QoMC_dt, stiff_inv; // dt, dt/dz, dt/dr, QoMC dt, 1/stiffness
   double z_forces_start;
+  int zfs_on; // z_forces_start lies inside (zmin, zmax)
   int forced;
   float tb_z_force_dt, tb_r_force_dt;
   double tb_z_decel, tb_r_decel;
