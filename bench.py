@@ -142,21 +142,7 @@ class ClockSampler:
 def build_state(cfg):
     """Mesh flags from the product's define_geometry, the analytic field, the
     solenoid and the beam, as abi containers."""
-    from spiffe_b200 import abi, geometry
-
-    modes = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP | abi.FL_SPACE_CHARGE
-    f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(), modes=modes)
-    f.mesh.dt = cfg.dt
-    f["Ez"] = cfg.initial_ez(f.flags)
-    bz, br = cfg.solenoid()
-    f["BzImposed"] = bz
-    f["BrImposed"] = br
-    arrays = cfg.beam_arrays()
-    n = len(arrays["z"])
-    b = abi.Beam(int(n * 1.25))
-    b.set(n, **arrays)
-    b.npActive, b.nextParticleID, b.QoMC, b.stiffness = n, n + 1, QoMC, 1.0
-    return f, b
+    return cfg.state()
 
 
 def pinned_like(arr):

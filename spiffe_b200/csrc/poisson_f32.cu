@@ -13,12 +13,13 @@
 // in FP64.  Each CTA of a cooperative launch holds a band of mesh rows of d,
 // r0 and the node mask in shared memory for the whole solve (the FP32 mesh
 // of a 3000 x 820 gun is 20 MB, which the 148 SMs' shared memory holds), so
-// a half-sweep reads no global memory except the two neighbour rows that the
+// a round of half-sweeps reads no global memory except the halo rows that the
 // adjacent CTAs updated; the rows of each colour are stored as separate
-// contiguous halves so a warp's accesses are conflict-free.  The per-CTA
-// |residual| sums are added in 64-bit fixed point inside the grid barrier's
-// arrival atomic, so every CTA takes the same stop decision from an
-// order-independent total.  When the residual has fallen 2^8-fold the
+// contiguous halves so a warp's accesses are conflict-free.  A band carries
+// a halo deep enough for several half-sweeps per grid barrier (temporal
+// blocking).  The per-CTA |residual| sums of every half-sweep are added in
+// 64-bit fixed point with the barrier's arrival, so every CTA takes the
+// same stop decision from order-independent totals.  When the residual has fallen 2^8-fold the
 // correction is folded into Psi and the residual formed again in FP64
 // (iterative refinement), so FP32 rounding of d never limits convergence.
 #include "split32.cuh"
@@ -287,16 +288,16 @@ struct Sor32Args {
   double a_d, e_d, c4_d, e2c_d, dr2_inv;
   double accuracy;
   long long limit;
-  float *xbuf;                  // exchange rows [2][grid][2 sides][2 rows][2 parities][H]
-  unsigned long long *arrive;   // barrier arrivals (low byte) and the first fixed-point sum
-  unsigned long long *release;  // barrier generation (high 16 bits) and the first sum (low 48)
-  unsigned long long *acc1;     // the second fixed-point sum
-  unsigned long long *pub1;     // the second sum, published by the last CTA to arrive
+  float *xbuf;                  // exchange rows [2][grid][2 sides][depth rows][2 parities][H]
+  unsigned long long *count;    // barrier arrivals, monotonic over the launch
+  unsigned long long *slots;    // [3][SOR_SLOTS] fixed-point sums, one set per barrier in rotation
   double *dpart;                // [grid][2] |rhs| and |r0| partials
   PcState *st;
   long long *iters_out;
   int lo, hi, cols, H, rows_per; // H: half-row length, a multiple of 4
 };
+
+constexpr int SOR_SLOTS = 8; // sums carried by one barrier: one per half-sweep of a round, and sum |e d|
 
 __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p)
 {
@@ -305,61 +306,53 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
   return v;
 }
 
-// Bounded grid barrier that also sums two fixed-point values per CTA.  Each
-// CTA adds the second value to *acc1 and then (v0 << 8) | 1 to *arrive, so
-// the low byte of *arrive counts arrivals (at most 255 CTAs) and the rest
-// accumulates the first sum; the last CTA to arrive reads and clears both
-// accumulators, publishes the second sum in *pub1 and releases the others
-// by storing the next generation (high 16 bits) with the first sum (low 48
-// bits) in *release.  The fence before the arrival releases the CTA's
-// earlier writes (the caller synchronises the CTA first, so they precede
-// it); the acquire of *release (or the fence after the last arrival) makes
-// every CTA's writes visible.  `gen` counts the barriers the calling thread
-// has passed.  Returns false (and raises the device error bit) when the
-// others do not arrive within the poll limit.
-__device__ bool grid_sync_sum(const Sor32Args &s, unsigned long long v0, unsigned long long v1, unsigned &gen,
-                              unsigned long long *t0, unsigned long long *t1, DevCounts *cnt, int *ok_sh)
+__device__ __forceinline__ unsigned long long ld_relaxed64(const unsigned long long *p)
 {
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    gen = (gen + 1) & 0xffffu;
-    unsigned long long old, tot0 = 0, tot1 = 0;
-    const unsigned long long add = (v0 << 8) | 1ull;
-    if (v1)
-      asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(s.acc1), "l"(v1) : "memory");
-    asm volatile("fence.acq_rel.gpu;" ::: "memory");
-    asm volatile("atom.relaxed.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(s.arrive), "l"(add) : "memory");
-    if ((old & 0xffull) == gridDim.x - 1) {
-      asm volatile("fence.acq_rel.gpu;" ::: "memory");
-      tot0 = (old >> 8) + v0;
-      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(tot1) : "l"(s.acc1) : "memory");
-      const unsigned long long rel = ((unsigned long long)gen << 48) | (tot0 & 0xffffffffffffull);
-      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.acc1), "l"(0ull) : "memory");
-      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.pub1), "l"(tot1) : "memory");
-      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(s.arrive), "l"(0ull) : "memory");
-      asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(s.release), "l"(rel) : "memory");
-    } else {
-      unsigned long long polls = 0, v;
-      while (((v = ld_acquire64(s.release)) >> 48) != gen) {
-        if (++polls > (1ull << 24)) {
-          ok = 0;
-          atomicOr(&cnt->error, SPIFFE_DEV_ERR_BARRIER);
-          break;
-        }
-        if (polls > 256)
-          __nanosleep(20);
-      }
-      tot0 = v & 0xffffffffffffull;
-      asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(tot1) : "l"(s.pub1) : "memory");
-    }
-    if (t0)
-      *t0 = tot0;
-    if (t1)
-      *t1 = tot1;
-    *ok_sh = ok;
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Bounded grid barrier for thread 0 of every CTA (the caller synchronises
+// the CTA before and after).  Barrier number `gen` (counted by the caller
+// from 1) adds this CTA's NV fixed-point values to slot set gen % 3, then,
+// after a fence that releases the CTA's earlier writes, one arrival to the
+// monotonic counter; it is passed once the counter reaches grid * gen, and
+// the acquire of that read makes every CTA's writes and sums visible.  The
+// sums of barrier gen are read between barriers gen and gen + 1, so CTA 0
+// clears set (gen - 1) % 3 once past barrier gen, before its next arrival;
+// barrier gen + 2 adds into it only after passing gen + 1.  Returns false
+// (and raises the device error bit) when the others do not arrive within
+// the poll limit.
+template <int NV>
+__device__ bool grid_barrier(const Sor32Args &s, const unsigned long long *v, unsigned gen, DevCounts *cnt)
+{
+  if (NV > 0) {
+    unsigned long long *set = s.slots + (size_t)(gen % 3) * SOR_SLOTS;
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+      if (v[k])
+        asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(set + k), "l"(v[k]) : "memory");
   }
-  __syncthreads();
-  return *ok_sh != 0;
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
+  asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(s.count), "l"(1ull) : "memory");
+  const unsigned long long target = (unsigned long long)gridDim.x * gen;
+  unsigned long long polls = 0;
+  while (ld_acquire64(s.count) < target) {
+    if (++polls > (1ull << 24)) {
+      atomicOr(&cnt->error, SPIFFE_DEV_ERR_BARRIER);
+      return false;
+    }
+    if (polls > 64)
+      __nanosleep(20);
+  }
+  if (blockIdx.x == 0) {
+    unsigned long long *old = s.slots + (size_t)((gen + 2) % 3) * SOR_SLOTS;
+#pragma unroll
+    for (int k = 0; k < SOR_SLOTS; k++)
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(old + k), "l"(0ull) : "memory");
+  }
+  return true;
 }
 
 // Band of rows of CTA b: [start, start+n) of the update rows lo..hi.
@@ -371,9 +364,11 @@ __device__ __forceinline__ void band(int rows, int b, int G, int &start, int &n)
 }
 
 // r0 = rhs - A Psi (FP64, Psi read through L2) into B for the mesh rows
-// iz0 .. iz0+nb-1 (B row i = mesh row iz0+i) that the SOR updates; adds this
-// thread's share of sum |rhs| and sum |r0| over the band's own rows
-// [own_lo, own_hi] to *drive and *rsum.
+// iz0 .. iz0+nb-1 (B row i = mesh row iz0+i) that the SOR updates; a node
+// that the SOR does not update (metal, outside rows lo..hi, ir >= cols)
+// gets NaN, which marks it for the sweeps.  Adds this thread's share of
+// sum |rhs| and sum |r0| over the band's own rows [own_lo, own_hi] to
+// *drive and *rsum.
 __device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0, int nb, int own_lo, int own_hi,
                         double *drive, double *rsum)
 {
@@ -386,7 +381,7 @@ __device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0,
     const long dn = (iz == 0 && s.lo == 0) ? P : -P;
     for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
       const int p = t / H, k = t - p * H, ir = 2 * k + p;
-      float r0 = 0.f;
+      float r0 = __int_as_float(0x7fc00000); // quiet NaN: not updated
       if (upd && ir < cols) {
         const size_t j = node(iz, ir, P);
         const double rh = s.rhs ? s.rhs[j] : 0.0;
@@ -412,157 +407,140 @@ __device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0,
   *rsum += q;
 }
 
-// The SOR update of four consecutive nodes of one colour in one row (nodes
-// ir = 2(k0+i) + p): D row jd with neighbour rows uj, dj, B/M row jb.
-// Returns the sum of their |residual|.  With UNDO it instead restores the
-// values before that update: new = old(1-w) - w(nb - r0)/e, so
-// old = (new + w(nb - r0)/e)/(1-w) (w > 1 after the first half-sweep).
+// A thread's share of the sweeps: one column group -- the four nodes of
+// each colour half-row at half-row offset 4q, i.e. mesh columns 8q..8q+7 --
+// on a run of rows of the band, with the row coefficients of those columns
+// held in registers for the whole solve.
+struct Strip {
+  int q, g, ng;              // column group, row group, row groups in use
+  int off0, off1;            // offsets of the column group in the parity-0 and parity-1 half rows
+  float4 cr0, cr1, dr0, dr1; // c(ir) and d(ir) of the eight columns (the axis node: 4/dr^2 and 0)
+  float ex, iex;             // diagonal of column 8q and its inverse (e - 2c on the axis)
+};
+
+// The SOR update (or, with UNDO, its inverse) of one node: res = A d - r0
+// with the diagonal term, d -= w res / e; a node whose r0 is NaN is left
+// alone.  UNDO restores the value before the update from the value after
+// it: new = old (1-w) - w (nb - r0)/e, so old = (new + w (nb - r0)/e)/(1-w)
+// (w > 1 after the first half-sweep).
 template <bool UNDO>
-__device__ __forceinline__ float sweep4(const Sor32Args &s, float *D, const float *B, const uint8_t *M,
-                                        const float *CR, const float *DR, int jd, int uj, int dj, int jb, int p,
-                                        int k0, float w)
+__device__ __forceinline__ void sor_node(float &x, float a, float ud, float c, float r, float dl, float l, float b,
+                                         float e, float wie, float inv1w, float &acc)
 {
-  const int H = s.H;
-  const int rs = (jd * 2 + p) * H + k0, ro = (jd * 2 + (p ^ 1)) * H + k0, rb = (jb * 2 + p) * H + k0;
-  float4 sv = *reinterpret_cast<const float4 *>(D + rs);
-  const float4 uv = *reinterpret_cast<const float4 *>(D + (uj * 2 + p) * H + k0);
-  const float4 dv = *reinterpret_cast<const float4 *>(D + (dj * 2 + p) * H + k0);
-  const float4 ov = *reinterpret_cast<const float4 *>(D + ro);
-  const float4 bv = *reinterpret_cast<const float4 *>(B + rb);
-  const uchar4 mv = *reinterpret_cast<const uchar4 *>(M + rb);
-  const float4 cr = *reinterpret_cast<const float4 *>(CR + p * H + k0);
-  const float4 dr = *reinterpret_cast<const float4 *>(DR + p * H + k0);
-  // neighbours in r: the other colour's nodes ir-1 and ir+1
-  float l0, l1, l2, l3, r0, r1, r2, r3;
-  if (p == 0) {
-    l0 = k0 > 0 ? D[ro - 1] : 0.f;
-    l1 = ov.x;
-    l2 = ov.y;
-    l3 = ov.z;
-    r0 = ov.x;
-    r1 = ov.y;
-    r2 = ov.z;
-    r3 = ov.w;
-  } else {
-    l0 = ov.x;
-    l1 = ov.y;
-    l2 = ov.z;
-    l3 = ov.w;
-    r0 = ov.y;
-    r1 = ov.z;
-    r2 = ov.w;
-    r3 = D[ro + 4];
-  }
-  const float a = s.a, e = s.e, we = w * s.inv_e;
-  float acc = 0.f;
-  if (UNDO) {
-    const float inv1w = 1.f / (1.f - w);
-    if (mv.x) {
-      if (p == 0 && k0 == 0)
-        sv.x = (sv.x + w * s.inv_e2c * (a * (uv.x + dv.x) + s.c4 * r0 - bv.x)) * inv1w;
-      else
-        sv.x = (sv.x + we * (a * (uv.x + dv.x) + cr.x * r0 + dr.x * l0 - bv.x)) * inv1w;
-    }
-    if (mv.y)
-      sv.y = (sv.y + we * (a * (uv.y + dv.y) + cr.y * r1 + dr.y * l1 - bv.y)) * inv1w;
-    if (mv.z)
-      sv.z = (sv.z + we * (a * (uv.z + dv.z) + cr.z * r2 + dr.z * l2 - bv.z)) * inv1w;
-    if (mv.w)
-      sv.w = (sv.w + we * (a * (uv.w + dv.w) + cr.w * r3 + dr.w * l3 - bv.w)) * inv1w;
-  } else {
-    if (mv.x) {
-      float res;
-      if (p == 0 && k0 == 0) { // the axis node (poisson.c:386-387)
-        res = a * (uv.x + dv.x) + s.c4 * r0 + s.e2c * sv.x - bv.x;
-        sv.x -= w * s.inv_e2c * res;
-      } else {
-        res = a * (uv.x + dv.x) + cr.x * r0 + dr.x * l0 + e * sv.x - bv.x;
-        sv.x -= we * res;
-      }
-      acc += fabsf(res);
-    }
-    if (mv.y) {
-      const float res = a * (uv.y + dv.y) + cr.y * r1 + dr.y * l1 + e * sv.y - bv.y;
-      sv.y -= we * res;
-      acc += fabsf(res);
-    }
-    if (mv.z) {
-      const float res = a * (uv.z + dv.z) + cr.z * r2 + dr.z * l2 + e * sv.z - bv.z;
-      sv.z -= we * res;
-      acc += fabsf(res);
-    }
-    if (mv.w) {
-      const float res = a * (uv.w + dv.w) + cr.w * r3 + dr.w * l3 + e * sv.w - bv.w;
-      sv.w -= we * res;
+  const float nb = fmaf(a, ud, fmaf(c, r, fmaf(dl, l, -b))); // neighbours - r0
+  if (b == b) {
+    if (UNDO) {
+      x = fmaf(wie, nb, x) * inv1w;
+    } else {
+      const float res = fmaf(e, x, nb);
+      x = fmaf(-wie, res, x);
       acc += fabsf(res);
     }
   }
-  *reinterpret_cast<float4 *>(D + rs) = sv;
-  return acc;
 }
 
-// One colour over D rows jlo..jhi (mesh row iz = iz_first + jd - 2; B/M row
-// jd - 1); |residual| summed over the own rows 2..nrow+1 only.
-// With xo, a slot of an exchanged row (the first two and the last two own
-// rows) also stores both colours of its four columns there, for the
-// neighbouring CTAs (the other colour was final after the previous sweep).
-template <bool UNDO>
-__device__ float sweep_rows(const DevMesh &m, const Sor32Args &s, float *D, const float *B, const uint8_t *M,
-                            const float *CR, const float *DR, int iz_first, int nrow, int jlo, int jhi, int c, float w,
-                            float *xo = nullptr)
+// One row of one colour for a strip: D row j (mesh row iz), neighbour rows
+// uj, dj, B row j - 1; P is the parity of the row's nodes of this colour.
+// Returns the sum of |residual|.  With x0/x1 the row's new values of both
+// colours are also stored there for the neighbouring CTAs.
+template <int P, bool UNDO, bool DSUM>
+__device__ __forceinline__ float sor_row(const Sor32Args &s, const Strip &t, float *D, const float *B, int j, int uj,
+                                         int dj, float wie, float wiex, float inv1w, float *dsum, float *x0, float *x1)
 {
-  const int nz = m.nz, Q = s.H >> 2, NT = blockDim.x, tid = threadIdx.x;
-  const int slots = (jhi - jlo + 1) * Q, jstep = NT / Q, qstep = NT - jstep * Q;
-  int jd = jlo + tid / Q, q = tid - (tid / Q) * Q;
+  const int H2 = 2 * s.H, so = P ? t.off1 : t.off0, oo = P ? t.off0 : t.off1;
+  float *row = D + j * H2;
+  float4 sv = *reinterpret_cast<const float4 *>(row + so);
+  const float4 o = *reinterpret_cast<const float4 *>(row + oo);
+  // the fifth neighbour in r: node 8q-1 (parity 0; read but weighted 0 on
+  // the axis) or node 8q+8 (parity 1; beyond the mesh for the last group,
+  // whose node is not updated)
+  const float nbr = P ? row[oo + 4] : row[oo - 1];
+  const float4 u = *reinterpret_cast<const float4 *>(D + uj * H2 + so);
+  const float4 d = *reinterpret_cast<const float4 *>(D + dj * H2 + so);
+  const float4 b = *reinterpret_cast<const float4 *>(B + (j - 1) * H2 + so);
+  const float4 c = P ? t.cr1 : t.cr0, dl = P ? t.dr1 : t.dr0;
+  const float a = s.a, e = s.e;
   float acc = 0.f;
-  for (int t = tid; t < slots; t += NT) {
-    const int iz = iz_first + jd - 2;
-    const int p = (c + iz) & 1;
-    // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
-    const int uj = (iz == nz - 1 && s.hi == nz - 1) ? jd - 1 : jd + 1;
-    const int dj = (iz == 0 && s.lo == 0) ? jd + 1 : jd - 1;
-    const float r = sweep4<UNDO>(s, D, B, M, CR, DR, jd, uj, dj, jd - 1, p, q << 2, w);
-    if (jd >= 2 && jd <= nrow + 1)
-      acc += r;
-    if (xo) {
-      const int H = s.H;
-      // side 0: rows 2, 3 for the CTA above; side 1: rows nrow, nrow+1 for the one below
-      const bool s0 = jd <= 3, s1 = jd >= nrow;
-      if (s0 || s1) {
-        const float4 v0 = *reinterpret_cast<const float4 *>(D + (jd * 2) * H + 4 * q);
-        const float4 v1 = *reinterpret_cast<const float4 *>(D + (jd * 2 + 1) * H + 4 * q);
-        if (s0) {
-          float *x = xo + (jd - 2) * 2 * H + 4 * q;
-          __stcg(reinterpret_cast<float4 *>(x), v0);
-          __stcg(reinterpret_cast<float4 *>(x + H), v1);
-        }
-        if (s1) {
-          float *x = xo + 4 * H + (jd - nrow) * 2 * H + 4 * q;
-          __stcg(reinterpret_cast<float4 *>(x), v0);
-          __stcg(reinterpret_cast<float4 *>(x + H), v1);
-        }
-      }
-    }
-    q += qstep;
-    jd += jstep;
-    if (q >= Q) {
-      q -= Q;
-      jd++;
-    }
+  if (P == 0) {
+    sor_node<UNDO>(sv.x, a, u.x + d.x, c.x, o.x, dl.x, nbr, b.x, t.ex, wiex, inv1w, acc);
+    sor_node<UNDO>(sv.y, a, u.y + d.y, c.y, o.y, dl.y, o.x, b.y, e, wie, inv1w, acc);
+    sor_node<UNDO>(sv.z, a, u.z + d.z, c.z, o.z, dl.z, o.y, b.z, e, wie, inv1w, acc);
+    sor_node<UNDO>(sv.w, a, u.w + d.w, c.w, o.w, dl.w, o.z, b.w, e, wie, inv1w, acc);
+  } else {
+    sor_node<UNDO>(sv.x, a, u.x + d.x, c.x, o.y, dl.x, o.x, b.x, e, wie, inv1w, acc);
+    sor_node<UNDO>(sv.y, a, u.y + d.y, c.y, o.z, dl.y, o.y, b.y, e, wie, inv1w, acc);
+    sor_node<UNDO>(sv.z, a, u.z + d.z, c.z, o.w, dl.z, o.z, b.z, e, wie, inv1w, acc);
+    sor_node<UNDO>(sv.w, a, u.w + d.w, c.w, nbr, dl.w, o.w, b.w, e, wie, inv1w, acc);
+  }
+  *reinterpret_cast<float4 *>(row + so) = sv;
+  if (DSUM)
+    *dsum += fabsf(sv.x) + fabsf(sv.y) + fabsf(sv.z) + fabsf(sv.w);
+  if (x0) {
+    __stcg(reinterpret_cast<float4 *>(x0 + so), sv);
+    __stcg(reinterpret_cast<float4 *>(x0 + oo), o);
+  }
+  if (x1) {
+    __stcg(reinterpret_cast<float4 *>(x1 + so), sv);
+    __stcg(reinterpret_cast<float4 *>(x1 + oo), o);
   }
   return acc;
 }
 
-// Psi += d on the band's own updated nodes (FP64)
-__device__ void fold_d(const Sor32Args &s, int P, const float *D, const uint8_t *M, int iz_first, int nrow)
+// One colour c over D rows jlo..jhi (mesh row iz = iz_first + j - HD; B row
+// j - 1).  The rows are cut into runs of an even length, one per row group,
+// so every thread of a warp sees rows of the same parity.  Returns this
+// thread's sum of |residual| over the own rows HD..HD+nrow-1 and, with
+// DSUM, their sum of |d| in *dsum.  With xo, the first HD and the last HD
+// own rows also go to the exchange buffer (side 0: rows HD.., side 1: rows
+// nrow..).
+template <bool UNDO, int HD, bool DSUM = false>
+__device__ __forceinline__ float sweep_rows(const DevMesh &m, const Sor32Args &s, const Strip &t, float *D,
+                                            const float *B, int iz_first, int nrow, int jlo, int jhi, int c, float w,
+                                            float *xo = nullptr, float *dsum = nullptr)
+{
+  float acc = 0.f, dacc = 0.f;
+  if (t.g < t.ng) {
+    const int n = jhi - jlo + 1, per = 2 * ((n + 2 * t.ng - 1) / (2 * t.ng));
+    const int j0 = jlo + t.g * per, j1 = min(jhi, j0 + per - 1);
+    const float wie = w * s.inv_e, wiex = w * t.iex, inv1w = UNDO ? 1.f / (1.f - w) : 0.f;
+    const int nz = m.nz, H2 = 2 * s.H;
+    for (int j = j0; j <= j1; j++) {
+      const int iz = iz_first + j - HD;
+      // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
+      const int uj = (iz == nz - 1 && s.hi == nz - 1) ? j - 1 : j + 1;
+      const int dj = (iz == 0 && s.lo == 0) ? j + 1 : j - 1;
+      float *x0 = nullptr, *x1 = nullptr;
+      if (xo) {
+        if (j < 2 * HD)
+          x0 = xo + (j - HD) * H2;
+        if (j >= nrow)
+          x1 = xo + HD * H2 + (j - nrow) * H2;
+      }
+      float ds = 0.f;
+      const float r = ((c + iz) & 1) == 0 ? sor_row<0, UNDO, DSUM>(s, t, D, B, j, uj, dj, wie, wiex, inv1w, &ds, x0, x1)
+                                          : sor_row<1, UNDO, DSUM>(s, t, D, B, j, uj, dj, wie, wiex, inv1w, &ds, x0, x1);
+      if (j >= HD && j < HD + nrow) {
+        acc += r;
+        dacc += ds;
+      }
+    }
+  }
+  if (DSUM)
+    *dsum = dacc;
+  return acc;
+}
+
+// Psi += d on the band's own nodes (FP64); own rows are D rows hd ..
+// hd+nrow-1.  Nodes the SOR does not update keep d = 0.
+__device__ void fold_d(const Sor32Args &s, int P, const float *D, int iz_first, int nrow, int hd)
 {
   const int H = s.H, cols = s.cols;
-  for (int j = 2; j <= nrow + 1; j++) {
-    const int iz = iz_first + j - 2;
+  for (int j = hd; j < hd + nrow; j++) {
+    const int iz = iz_first + j - hd;
     for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
       const int p = t / H, k = t - p * H, ir = 2 * k + p;
       const float d = D[(j * 2 + p) * H + k];
-      if (ir < cols && M[((j - 1) * 2 + p) * H + k] && d != 0.f) {
+      if (ir < cols && d != 0.f) {
         const size_t i = node(iz, ir, P);
         __stcg(s.Psi + i, __ldcg(s.Psi + i) + (double)d);
       }
@@ -580,59 +558,74 @@ __device__ __forceinline__ double block_sum2(double v, double *red, int slot)
 }
 
 // solve_poisson_cyl (poisson.c:17-130) on the correction d of the warm
-// start.  Each round runs one half-sweep of each colour between two grid
-// barriers: a CTA's band carries two halo rows on each side, the colour-0
-// sweep also updates the nearer halo row (from exactly the inputs the
-// neighbour uses, so with the same result), and the colour-1 sweep then
-// needs nothing from the neighbours.  Both half-sweeps' |residual| sums
-// arrive with the barrier, so the reference's stop test runs after every
-// half-sweep; when it fires after colour 0, the colour-1 update of the
-// round is undone.
-constexpr int SOR_NT = 1024; // threads per CTA of the shared-memory kernel
+// start.  Each round runs HD half-sweeps (colours 0, 1, 0, ...) between two
+// grid barriers: a CTA's band carries HD halo rows on each side, sweep k of
+// the round also updates the HD-1-k nearest halo rows (from exactly the
+// inputs the neighbour uses, so with the same result), and the last sweep
+// needs nothing from the neighbours.  Every half-sweep's |residual| sum
+// arrives with the barrier, so the reference's stop test runs after every
+// half-sweep; when it fires before the last sweep of the round, the later
+// sweeps are undone in reverse order over the rows they updated, before
+// the neighbours' rows replace the halo.
+constexpr int SOR_NT = 768; // most threads per CTA of the shared-memory kernel (80 registers each)
 
+template <int HD>
 __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCounts *cnt)
 {
+  static_assert(HD % 2 == 0 && HD + 1 <= SOR_SLOTS, "rounds of an even number of half-sweeps");
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[64];
-  __shared__ int ok_sh, stop_sh, undo_sh, rebase_sh;
-  __shared__ double total_sh, thr_sh, quantum_sh, base_sh, p0_sh, p1_sh;
-  __shared__ unsigned long long t0_sh, t1_sh;
+  __shared__ float redf[HD + 1][32];
+  __shared__ int ok_sh, stop_sh, nundo_sh, rebase_sh;
+  __shared__ double total_sh, thr_sh, quantum_sh, base_sh;
   __shared__ long long result_sh;
   if (s.st && !s.st->do_solve)
     return;
   const int nz = m.nz, P = m.pitch, H = s.H, Q = s.H >> 2, cols = s.cols, R = s.rows_per;
   const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x, NT = blockDim.x;
+  const bool halo = G > 1;
   int start, nrow;
   band(s.hi - s.lo + 1, b, G, start, nrow);
   const int iz_first = s.lo + start;
-  // shared layout (32-bit offsets): D[(R+4)][2][H] d for mesh rows
-  // iz_first-2 .. iz_first+R+1 (D row iz - iz_first + 2), B[(R+2)][2][H] r0
-  // and M[(R+2)][2][H] node mask for rows iz_first-1 .. (B row iz -
-  // iz_first + 1), CR/DR[2][H] row coefficients; row j's nodes of parity p
-  // are the contiguous run (j*2+p)*H .. +H
+  // shared layout (32-bit words): D[(R+2HD)][2][H] d for mesh rows
+  // iz_first-HD .. iz_first+R+HD-1 (D row iz - iz_first + HD) and
+  // B[(R+2HD-2)][2][H] r0 (NaN where not updated) for rows iz_first-HD+1 ..
+  // (B row = D row - 1); row j's nodes of parity p are the contiguous run
+  // (j*2+p)*H .. +H
   float *D = (float *)smem;
-  float *B = D + (R + 4) * 2 * H;
-  float *CR = B + (R + 2) * 2 * H;
-  float *DR = CR + 2 * H;
-  uint8_t *M = (uint8_t *)(DR + 2 * H);
-  for (int t = tid; t < (R + 4) * 2 * H; t += NT)
+  float *B = D + (R + 2 * HD) * 2 * H;
+  for (int t = tid; t < (R + 2 * HD) * 2 * H; t += NT)
     D[t] = 0.f;
-  for (int t = tid; t < 2 * H; t += NT) {
-    const int p = t / H, k = t - p * H, ir = 2 * k + p;
-    CR[t] = ir < cols ? s.crow[ir] : 0.f;
-    DR[t] = ir < cols ? s.drow[ir] : 0.f;
-  }
-  for (int i = 0; i < nrow + 2; i++) {
-    const int iz = iz_first - 1 + i;
-    const bool upd = iz >= s.lo && iz <= s.hi;
-    for (int t = tid; t < 2 * H; t += NT) {
-      const int p = t / H, k = t - p * H, ir = 2 * k + p;
-      M[(i * 2 + p) * H + k] = upd && ir < cols && !(s.umask[node(iz, ir, P)] & S32_U_METAL) ? 1 : 0;
+  Strip st;
+  st.ng = NT / Q;
+  st.q = tid % Q;
+  st.g = tid / Q;
+  st.off0 = 4 * st.q;
+  st.off1 = H + 4 * st.q;
+  {
+    const float *cr = s.crow, *dr = s.drow;
+    float c0[4], c1[4], d0[4], d1[4];
+    for (int i = 0; i < 4; i++) {
+      const int ir0 = 8 * st.q + 2 * i, ir1 = ir0 + 1;
+      c0[i] = ir0 < cols ? cr[ir0] : 0.f;
+      d0[i] = ir0 < cols ? dr[ir0] : 0.f;
+      c1[i] = ir1 < cols ? cr[ir1] : 0.f;
+      d1[i] = ir1 < cols ? dr[ir1] : 0.f;
     }
+    if (st.q == 0) { // the axis node (poisson.c:386-387)
+      c0[0] = s.c4;
+      d0[0] = 0.f;
+    }
+    st.cr0 = make_float4(c0[0], c0[1], c0[2], c0[3]);
+    st.cr1 = make_float4(c1[0], c1[1], c1[2], c1[3]);
+    st.dr0 = make_float4(d0[0], d0[1], d0[2], d0[3]);
+    st.dr1 = make_float4(d1[0], d1[1], d1[2], d1[3]);
+    st.ex = st.q == 0 ? s.e2c : s.e;
+    st.iex = st.q == 0 ? s.inv_e2c : s.inv_e;
   }
   const int iz_last = iz_first + nrow - 1;
   double drive = 0, r0sum = 0;
-  form_r0(m, s, B, iz_first - 1, nrow + 2, iz_first, iz_last, &drive, &r0sum);
+  form_r0(m, s, B, iz_first - (HD - 1), nrow + 2 * (HD - 1), iz_first, iz_last, &drive, &r0sum);
   // rows outside lo..hi that the driving sum still covers (iz < nz)
   if (s.rhs) {
     const bool first = b == 0, last = b == G - 1;
@@ -649,156 +642,218 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
   block_sum2(drive, red, 0);
   block_sum2(r0sum, red, 1);
   __syncthreads();
+  unsigned gen = 0; // barriers passed (thread 0)
   if (tid == 0) {
     double t = 0, t2 = 0;
     for (int w = 0; w < (NT + 31) / 32; w++) {
       t += red[w];
       t2 += red[32 + w];
     }
-    if (G > 1) {
+    int ok = 1;
+    if (halo) {
       __stcg(s.dpart + 2 * b, t);
       __stcg(s.dpart + 2 * b + 1, t2);
-    } else {
-      thr_sh = s.accuracy * t;
-      base_sh = t2;
-    }
-  }
-  unsigned gen = 0;
-  __syncthreads();
-  if (G > 1) {
-    if (!grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
-      return;
-    if (tid == 0) {
-      double d = 0, qq = 0;
+      ok = grid_barrier<0>(s, nullptr, ++gen, cnt);
+      t = t2 = 0;
       for (int i = 0; i < G; i++) {
-        d += __ldcg(s.dpart + 2 * i);
-        qq += __ldcg(s.dpart + 2 * i + 1);
+        t += __ldcg(s.dpart + 2 * i);
+        t2 += __ldcg(s.dpart + 2 * i + 1);
       }
-      thr_sh = s.accuracy * d;
-      base_sh = qq;
     }
-  }
-  if (tid == 0) {
+    ok_sh = ok;
+    thr_sh = s.accuracy * t;
+    base_sh = t2;
     quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
     rebase_sh = 0;
     result_sh = -1;
     total_sh = 0;
   }
   __syncthreads();
-  // sweeps of the first colour cover the nearer halo rows when there are neighbours
-  const int jlo0 = G > 1 ? 1 : 2, jhi0 = G > 1 ? nrow + 2 : nrow + 1;
-  for (long long n0 = 0; n0 < s.limit; n0 += 2) {
-    if (rebase_sh) {
-      // iterative refinement: Psi += d in FP64, r0 = rhs - A Psi in FP64 once
-      // every band has folded its d in, and the sweeps go on from d = 0
-      fold_d(s, P, D, M, iz_first, nrow);
-      __syncthreads();
-      if (G > 1 && !grid_sync_sum(s, 0ull, 0ull, gen, nullptr, nullptr, cnt, &ok_sh))
-        return;
-      double d0 = 0, q0 = 0;
-      form_r0(m, s, B, iz_first - 1, nrow + 2, iz_first, iz_last, &d0, &q0);
-      for (int t = tid; t < (R + 4) * 2 * H; t += NT)
-        D[t] = 0.f;
-      __syncthreads();
-    }
-    const bool two = n0 + 1 < s.limit;
-    const float w0 = s.omega[n0], w1 = two ? s.omega[n0 + 1] : 0.f;
-    const float acc0 = sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, jlo0, jhi0, 0, w0);
-    __syncthreads();
-    // the colour-1 sweep also writes the exchanged rows for the neighbours
-    float *xo = G > 1 ? s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H + (size_t)b * 8 * H : nullptr;
-    const float acc1 =
-        two ? sweep_rows<false>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1, xo) : 0.f;
-    block_sum2((double)acc0, red, 0);
-    block_sum2((double)acc1, red, 1);
-    __syncthreads();
-    if (tid < 32) {
-      // fixed-order warp reduction of the per-warp partials
-      const int nw = (NT + 31) / 32;
-      double t = tid < nw ? red[tid] : 0.0, t2 = tid < nw ? red[32 + tid] : 0.0;
+  if (!ok_sh)
+    return;
+  const int nw = (NT + 31) / 32, Q2 = 2 * Q;
+  // the halo rows a thread fetches: element e = tid (+ NT) of the 2HD rows x
+  // 2Q float4s of the neighbours' exchanged rows (rows 0..HD-1 from the CTA
+  // before, HD..2HD-1 from the one after)
+  const int ne = 2 * HD * Q2;
+  const int e0r = tid / Q2, e0c = tid - e0r * Q2, e1r = (tid + NT) / Q2, e1c = tid + NT - e1r * Q2;
+  for (long long n0 = 0; n0 < s.limit; n0 += HD) {
+    const int keff = (int)(s.limit - n0 < HD ? s.limit - n0 : HD);
+    const bool last = n0 + HD >= s.limit;
+    // the last sweep of a round also writes the exchanged rows for the neighbours
+    float *xo = halo ? s.xbuf + (size_t)((n0 / HD) & 1) * G * 4 * HD * H + (size_t)b * 4 * HD * H : nullptr;
+#pragma unroll 1
+    for (int k = 0; k < HD; k++) {
+      float v = 0.f, ds = 0.f;
+      if (k < keff) {
+        const int ext = halo ? HD - 1 - k : 0;
+        if (k == HD - 1) // the last sweep also sums |d| over the own nodes it updates
+          v = sweep_rows<false, HD, true>(m, s, st, D, B, iz_first, nrow, HD, HD + nrow - 1, 1, s.omega[n0 + k], xo,
+                                          &ds);
+        else
+          v = sweep_rows<false, HD>(m, s, st, D, B, iz_first, nrow, HD - ext, HD + nrow - 1 + ext, k & 1,
+                                    s.omega[n0 + k]);
+      }
+      // fixed-order sums: per warp in FP32 here, across warps in FP64 by warp 0 below
       for (int o = 16; o > 0; o >>= 1) {
-        t += __shfl_down_sync(0xffffffffu, t, o);
-        t2 += __shfl_down_sync(0xffffffffu, t2, o);
+        v += __shfl_down_sync(0xffffffffu, v, o);
+        ds += __shfl_down_sync(0xffffffffu, ds, o);
       }
-      if (tid == 0) {
-        p0_sh = t;
-        p1_sh = t2;
+      if ((tid & 31) == 0) {
+        redf[k][tid >> 5] = v;
+        if (k == HD - 1)
+          redf[HD][tid >> 5] = ds;
+      }
+      __syncthreads();
+    }
+    double part[HD + 1]; // |residual| of each half-sweep, then |d| after the last
+    if (tid < 32) {
+#pragma unroll
+      for (int k = 0; k <= HD; k++) {
+        double v = tid < nw ? (double)redf[k][tid] : 0.0;
+        for (int o = 16; o > 0; o >>= 1)
+          v += __shfl_down_sync(0xffffffffu, v, o);
+        part[k] = v;
       }
     }
-    double total0, total1;
-    unsigned long long tf0 = 0, tf1 = 0;
-    if (G > 1) {
-      // this CTA's |residual| sums in quanta of 2^-30 of the larger of the
-      // refinement base and the stop threshold, capped at 2^40 quanta
-      unsigned long long q0 = 0, q1 = 0;
+    float4 pre0 = make_float4(0.f, 0.f, 0.f, 0.f), pre1 = pre0;
+    const float *xi = s.xbuf + (size_t)((n0 / HD) & 1) * G * 4 * HD * H;
+    if (halo) {
       if (tid == 0) {
-        const double x0 = p0_sh / quantum_sh, x1 = p1_sh / quantum_sh;
-        if (p0_sh != 0)
-          q0 = x0 >= 1099511627776.0 ? 1099511627776ull : ((unsigned long long)llrint(x0) | 1ull);
-        if (p1_sh != 0)
-          q1 = x1 >= 1099511627776.0 ? 1099511627776ull : ((unsigned long long)llrint(x1) | 1ull);
+        // this CTA's |residual| sums in quanta of 2^-30 of the larger of the
+        // refinement base and the stop threshold, capped at 2^40 quanta, and
+        // its |e| sum |d| in quanta 2^12 times larger, capped at 2^50
+        unsigned long long qv[HD + 1];
+#pragma unroll
+        for (int k = 0; k < HD; k++) {
+          const double x = part[k] / quantum_sh;
+          qv[k] = part[k] == 0 ? 0ull
+                               : (x >= 1099511627776.0 ? 1099511627776ull : ((unsigned long long)llrint(x) | 1ull));
+        }
+        const double xd = part[HD] * fabs(s.e_d) / (quantum_sh * 4096.0);
+        qv[HD] = xd >= 1125899906842624.0 ? 1125899906842624ull : (unsigned long long)llrint(xd);
+        ok_sh = grid_barrier<HD + 1>(s, qv, ++gen, cnt);
       }
-      if (!grid_sync_sum(s, q0, q1, gen, &t0_sh, &t1_sh, cnt, &ok_sh))
+      __syncthreads();
+      if (!ok_sh)
         return;
-      // the neighbours' rows into the halo rows
-      const float *xi = s.xbuf + (size_t)((n0 >> 1) & 1) * G * 8 * H;
-      for (int t = tid; t < 8 * Q; t += NT) {
-        const int side = t / (4 * Q), r = t - side * 4 * Q;
-        if (side == 0 && b > 0) {
-          const float4 v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)(b - 1) * 8 * H + 4 * H) + r);
-          *reinterpret_cast<float4 *>(D + (r / (2 * Q)) * 2 * H + 4 * (r % (2 * Q))) = v;
-        } else if (side == 1 && b < G - 1) {
-          const float4 v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)(b + 1) * 8 * H) + r);
-          *reinterpret_cast<float4 *>(D + (nrow + 2 + r / (2 * Q)) * 2 * H + 4 * (r % (2 * Q))) = v;
+      // the neighbours' rows, held in registers until the stop test has run
+      if (!last) {
+        if (tid < ne) {
+          const int nb_ = e0r < HD ? b - 1 : b + 1;
+          if (nb_ >= 0 && nb_ < G)
+            pre0 = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
+                                                           (e0r < HD ? 2 * HD * H : 0)) + (e0r % HD) * Q2 + e0c);
+        }
+        if (tid + NT < ne) {
+          const int nb_ = e1r < HD ? b - 1 : b + 1;
+          if (nb_ >= 0 && nb_ < G)
+            pre1 = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
+                                                           (e1r < HD ? 2 * HD * H : 0)) + (e1r % HD) * Q2 + e1c);
         }
       }
-      tf0 = t0_sh;
-      tf1 = t1_sh;
-      total0 = (double)tf0 * quantum_sh;
-      total1 = (double)tf1 * quantum_sh;
-    } else {
-      __syncthreads();
-      total0 = p0_sh;
-      total1 = p1_sh;
-      tf0 = total0 != 0;
-      tf1 = total1 != 0;
     }
     if (tid == 0) {
-      const bool stop0 = n0 > 0 && (total0 < thr_sh || tf0 == 0);
-      const bool stop1 = two && (total1 < thr_sh || tf1 == 0);
-      stop_sh = stop0 || stop1;
-      undo_sh = stop0 && two;
-      if (stop0) {
-        result_sh = n0;
-        total_sh = total0;
-      } else if (stop1) {
-        result_sh = n0 + 1;
-        total_sh = total1;
+      double tot[HD + 1];
+      unsigned long long tq[HD + 1];
+      const unsigned long long *set = s.slots + (size_t)(gen % 3) * SOR_SLOTS;
+#pragma unroll
+      for (int k = 0; k <= HD; k++) {
+        if (halo) {
+          tq[k] = ld_relaxed64(set + k);
+          tot[k] = (double)tq[k] * quantum_sh * (k == HD ? 4096.0 : 1.0);
+        } else {
+          tot[k] = k == HD ? part[k] * fabs(s.e_d) : part[k];
+          tq[k] = part[k] != 0;
+        }
+      }
+      // the first half-sweep of the round that meets the stop rule (unrolled
+      // selects keep the arrays in registers)
+      int ks = -1;
+      double tks = 0, tlast = 0;
+#pragma unroll
+      for (int k = 0; k < HD; k++) {
+        if (ks < 0 && k < keff && n0 + k > 0 && (tot[k] < thr_sh || tq[k] == 0)) {
+          ks = k;
+          tks = tot[k];
+        }
+        if (k == keff - 1)
+          tlast = tot[k];
+      }
+      stop_sh = ks >= 0;
+      rebase_sh = 0;
+      if (ks >= 0) {
+        nundo_sh = keff - 1 - ks;
+        result_sh = n0 + ks;
+        total_sh = tks;
       } else {
-        total_sh = two ? total1 : total0;
-        // Iterative refinement: once the residual has fallen 2^8-fold below
-        // the last FP64 residual (the base), fold d into Psi and form the
-        // residual again in FP64 before FP32 rounding of the growing d
-        // limits it.  The fixed-point quantum of the residual sums is 2^-30
-        // of the larger of the base and the stop threshold, so the stop test
-        // keeps its resolution as the base follows the residual down; a
-        // per-CTA sum is capped at 2^40 quanta (a barrier word holds 255).
-        rebase_sh = total_sh < base_sh * (1.0 / 256);
-        if (rebase_sh)
+        total_sh = tlast;
+        // Iterative refinement: fold d into Psi and form the residual again
+        // in FP64 once the residual has fallen 2^8-fold below the last FP64
+        // residual (the base), or to within 8x of the FP32 rounding noise of
+        // its own terms.  That noise is about 2^-21 |e| sum |d| (each
+        // node's residual cancels terms of size |e d| rounded to 2^-24), so
+        // the FP32 sweeps stall there when d has grown large.  The
+        // fixed-point quantum of the residual sums is 2^-30 of the larger of
+        // the base and the stop threshold, so the stop test keeps its
+        // resolution as the base follows the residual down.
+        if (!last && (total_sh < base_sh * (1.0 / 256) || total_sh < tot[HD] * (1.0 / 262144))) {
+          rebase_sh = 1;
           base_sh = total_sh;
+        }
         quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
       }
     }
     __syncthreads();
     if (stop_sh) {
-      if (undo_sh) {
-        sweep_rows<true>(m, s, D, B, M, CR, DR, iz_first, nrow, 2, nrow + 1, 1, w1);
+      for (int u = nundo_sh; u > 0; u--) {
+        const int k = keff - 1 - nundo_sh + u; // the latest sweep not yet undone
+        const int ext = halo ? HD - 1 - k : 0;
+        sweep_rows<true, HD>(m, s, st, D, B, iz_first, nrow, HD - ext, HD + nrow - 1 + ext, k & 1, s.omega[n0 + k]);
         __syncthreads();
       }
       break;
     }
+    if (rebase_sh) {
+      // Psi += d in FP64, then r0 = rhs - A Psi in FP64 once every band has
+      // folded its d in, and the sweeps go on from d = 0
+      fold_d(s, P, D, iz_first, nrow, HD);
+      __syncthreads();
+      if (halo) {
+        if (tid == 0)
+          ok_sh = grid_barrier<0>(s, nullptr, ++gen, cnt);
+        __syncthreads();
+        if (!ok_sh)
+          return;
+      }
+      double d0 = 0, q0 = 0;
+      form_r0(m, s, B, iz_first - (HD - 1), nrow + 2 * (HD - 1), iz_first, iz_last, &d0, &q0);
+      for (int t = tid; t < (R + 2 * HD) * 2 * H; t += NT)
+        D[t] = 0.f;
+      __syncthreads();
+      continue;
+    }
+    if (halo && !last) {
+      // halo rows 0..HD-1 from the CTA before, nrow+HD.. from the one after;
+      // the exchange rows hold both parities in D's row layout
+      for (int t = tid; t < ne; t += NT) {
+        const int r = t < NT ? e0r : (t < 2 * NT ? e1r : t / Q2), cc = t < NT ? e0c : (t < 2 * NT ? e1c : t % Q2);
+        const int nb_ = r < HD ? b - 1 : b + 1;
+        if (nb_ < 0 || nb_ >= G)
+          continue;
+        float4 v;
+        if (t < 2 * NT)
+          v = t < NT ? pre0 : pre1;
+        else
+          v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H + (r < HD ? 2 * HD * H : 0)) +
+                     (r % HD) * Q2 + cc);
+        const int row = r < HD ? r : nrow + r;
+        *reinterpret_cast<float4 *>(D + row * 2 * H + 4 * cc) = v;
+      }
+      __syncthreads();
+    }
   }
-  fold_d(s, P, D, M, iz_first, nrow);
+  fold_d(s, P, D, iz_first, nrow, HD);
   if (b == 0 && tid == 0) {
     const long long result = result_sh;
     if (s.iters_out)
@@ -886,17 +941,27 @@ __global__ void __launch_bounds__(BX *BY) k_imposed32(DevMesh m, DevFields32 f, 
   }
 }
 
-// shared bytes of a band of R rows: d with two halo rows a side, r0 and the
-// mask with one, the row coefficients
-size_t sor_smem(int R, int H)
+// shared bytes of a band of R rows: d with hd halo rows a side, r0 with hd - 1
+size_t sor_smem(int R, int H, int hd)
 {
-  return (size_t)(R + 4) * 2 * H * 4 + (size_t)(R + 2) * 2 * H * 4 + 2 * (size_t)2 * H * 4 + (size_t)(R + 2) * 2 * H;
+  const size_t row = (size_t)2 * H * 4;
+  return (R + 2 * hd) * row + (R + 2 * hd - 2) * row;
 }
 
-int sor_threads(int R, int H)
+// threads of a CTA: one per column group (H/4 of them) per row group, with
+// as many row groups as fit in SOR_NT threads and as runs of two rows need;
+// 0 when a half row has more than SOR_NT column groups
+int sor_threads(int R, int H, int hd)
 {
-  const int slots = (R + 2) * (H / 4);
-  return std::min(SOR_NT, std::max(128, (slots + 31) / 32 * 32));
+  const int Q = H / 4, groups = std::min(SOR_NT / std::max(Q, 1), (R + 2 * hd - 2 + 1) / 2);
+  if (Q > SOR_NT || groups < 1)
+    return 0;
+  return (groups * Q + 31) / 32 * 32;
+}
+
+const void *sor_kernel(int hd)
+{
+  return hd == 4 ? (const void *)k_sor32<4> : (const void *)k_sor32<2>;
 }
 
 } // namespace
@@ -930,26 +995,44 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
   const int rows = (m->right_bc == SPIFFE_DIRICHLET ? nz - 1 : nz - 2) - (m->left_bc == SPIFFE_DIRICHLET ? 0 : 1) + 1;
   const int cols = nr - 1, H = ((cols + 2) / 2 + 3) / 4 * 4; // half-row (one colour), a multiple of 4
   const size_t budget = (size_t)max_smem - 1024;
-  // one CTA when the mesh fits one SM (no grid barriers); otherwise bands of
-  // at least two rows (the halo exchange carries two rows) over all SMs
-  int G = 1;
-  if (sor_smem(rows, H) > budget || (size_t)rows * 2 * H > 65536) {
-    G = std::min(sms, rows / 2);
-    while (G < rows / 2 && sor_smem((rows + G - 1) / G, H) > budget)
-      G++;
-  }
+  // One CTA when the mesh fits one SM (no grid barriers); otherwise bands
+  // of at least `hd` rows (the halo exchange carries hd rows) over all SMs,
+  // with four half-sweeps per barrier where the deeper halo fits, else two
+  // (six measured slower on the 3000 x 820 gun: the extra halo rows cost
+  // more than the barriers they save).
+  int G = 0, hd = 4;
+  for (int h : {4, 2})
+    if (sor_smem(rows, H, h) <= budget && (size_t)rows * 2 * H <= 65536) {
+      G = 1;
+      hd = h;
+      break;
+    }
+  if (G == 0)
+    for (int h : {4, 2}) {
+      int g = std::min(sms, rows / h);
+      while (g < rows / h && sor_smem((rows + g - 1) / g, H, h) > budget)
+        g++;
+      if (g >= 1 && g <= sms && sor_smem((rows + g - 1) / g, H, h) <= budget) {
+        G = g;
+        hd = h;
+        break;
+      }
+    }
   cudaError_t e = cudaSuccess;
   int occ = 0;
-  const int R = (rows + G - 1) / G;
-  if (G < 1 || G > sms || G > 255 || sor_smem(R, H) > budget)
+  if (G < 1)
     return (int)cudaErrorInvalidConfiguration; // the mesh does not fit the shared-memory bands
+  const int R = (rows + G - 1) / G;
   w->grid = G;
+  w->depth = hd;
   w->rows_per = R;
-  w->smem = sor_smem(R, H);
-  w->threads = sor_threads(R, H);
-  e = cudaFuncSetAttribute(k_sor32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem);
+  w->smem = sor_smem(R, H, hd);
+  w->threads = sor_threads(R, H, hd);
+  if (w->threads < 1)
+    return (int)cudaErrorInvalidConfiguration; // a half row wider than one CTA's threads
+  e = cudaFuncSetAttribute(sor_kernel(hd), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sor32, w->threads, w->smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sor_kernel(hd), w->threads, w->smem);
   if (e == cudaSuccess && occ < 1)
     e = cudaErrorInvalidConfiguration;
   w->half = H;
@@ -968,10 +1051,9 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
     if (e == cudaSuccess) e = cudaMalloc(&w->st, sizeof(PcState));
     if (e == cudaSuccess) e = cudaMemsetAsync(w->st, 0, sizeof(PcState), s);
     if (e == cudaSuccess) e = cudaMalloc(&w->iters, sizeof(long long));
-    if (e == cudaSuccess) e = cudaMalloc(&w->bar, sizeof(unsigned) * 2);
-    if (e == cudaSuccess) e = cudaMalloc(&w->rsum, sizeof(unsigned long long) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&w->bar, sizeof(unsigned long long) * 48); // counter, sum slots
     if (e == cudaSuccess) e = cudaMalloc(&w->dpart, sizeof(double) * (size_t)sms * 2); // |rhs|, |r0| per CTA
-    if (e == cudaSuccess) e = cudaMalloc(&w->xbuf, sizeof(float) * (size_t)2 * sms * 8 * H); // exchange rows
+    if (e == cudaSuccess) e = cudaMalloc(&w->xbuf, sizeof(float) * (size_t)2 * sms * 16 * H); // exchange rows, 4 a side
     if (e == cudaSuccess) e = cudaMalloc(&w->part, sizeof(double) * parts);
     w->part_n = parts;
   }
@@ -988,7 +1070,7 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
 extern "C" void s32_poisson_free(Poisson32Work *w)
 {
   void *p[] = {w->Az, w->Ari, w->Aro, w->volume, w->crow, w->drow, w->scalars, w->qreal_fixed, w->st,
-               w->iters, w->bar, w->rsum, w->dpart, w->xbuf, w->part, w->omega};
+               w->iters, w->bar, w->dpart, w->xbuf, w->part, w->omega};
   for (void *q : p)
     cudaFree(q);
   *w = Poisson32Work();
@@ -1047,10 +1129,8 @@ extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const do
   a.accuracy = accuracy;
   a.limit = limit;
   a.xbuf = w->xbuf;
-  a.arrive = w->rsum;
-  a.release = w->rsum + 1;
-  a.acc1 = w->rsum + 2;
-  a.pub1 = w->rsum + 3;
+  a.count = w->bar;
+  a.slots = w->bar + 16; // another 128-byte line than the polled counter
   a.dpart = w->dpart;
   a.st = st;
   a.iters_out = w->iters;
@@ -1059,14 +1139,12 @@ extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const do
   a.cols = m->nr - 1;
   a.H = w->half;
   a.rows_per = w->rows_per;
-  cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(unsigned) * 2, s);
-  if (e == cudaSuccess)
-    e = cudaMemsetAsync(w->rsum, 0, sizeof(unsigned long long) * 4, s);
+  cudaError_t e = cudaMemsetAsync(w->bar, 0, sizeof(unsigned long long) * 48, s);
   if (e != cudaSuccess)
     return (int)e;
   DevMesh mm = *m;
   void *args[] = {&mm, &a, &cnt};
-  e = cudaLaunchCooperativeKernel((const void *)k_sor32, dim3(w->grid), dim3(w->threads), args, w->smem, s);
+  e = cudaLaunchCooperativeKernel(sor_kernel(w->depth), dim3(w->grid), dim3(w->threads), args, w->smem, s);
   spiffe_note_launches(1);
   return (int)e;
 }

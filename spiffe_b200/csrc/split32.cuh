@@ -165,10 +165,9 @@ struct Poisson32Work {
   long long omega_n = 0;
   float *crow = nullptr, *drow = nullptr;
   float *xbuf = nullptr;
-  unsigned *bar = nullptr;            // [0] count [1] generation
-  unsigned long long *rsum = nullptr; // fixed-point |residual| sums, double-buffered
-  double *dpart = nullptr;            // per-CTA driving partials
-  int grid = 0, threads = 0;
+  unsigned long long *bar = nullptr; // [0] barrier counter, [16..39] fixed-point sum slots
+  double *dpart = nullptr;           // per-CTA driving partials
+  int grid = 0, threads = 0, depth = 2; // depth: halo rows a side = half-sweeps per barrier
   size_t smem = 0;
   int rows_per = 0, half = 0; // rows of the widest CTA band; half-row length (nodes of one colour)
 };

@@ -235,6 +235,25 @@ class Gun16Config:
     def screen_z(self):
         return self.length - self.dz
 
+    def state(self, capacity_factor=1.25):
+        """Fields (flags and PsiImposed from the product's define_geometry,
+        the analytic field, the solenoid) and the beam, as abi containers."""
+        from . import abi, geometry
+
+        modes = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP | abi.FL_SPACE_CHARGE
+        f = geometry.fields_for(self.nz, self.nr, self.zmin, self.zmax, self.rmax, self.geo_text(), modes=modes)
+        f.mesh.dt = self.dt
+        f["Ez"] = self.initial_ez(f.flags)
+        bz, br = self.solenoid()
+        f["BzImposed"] = bz
+        f["BrImposed"] = br
+        arrays = self.beam_arrays()
+        n = len(arrays["z"])
+        b = abi.Beam(int(n * capacity_factor))
+        b.set(n, **arrays)
+        b.npActive, b.nextParticleID, b.QoMC, b.stiffness = n, n + 1, -E_MKS / (9.1093837015e-31 * C_MKS), 1.0
+        return f, b
+
     def poisson(self):
         from . import abi
 

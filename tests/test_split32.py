@@ -177,6 +177,33 @@ def test_sor_within_tolerance(oracle):
     assert rel_l2(out["Psi"], ref["Psi"]) <= SOR_TOL
 
 
+@pytest.mark.parametrize("accuracy", [1e-2, 5e-3, 2e-3, 1e-3])
+def test_sor_multi_cta_stop_and_undo(oracle, accuracy):
+    """A pillbox on a 601 x 321 mesh spreads the solve over every SM, with
+    several half-sweeps per grid barrier.  The stop rule fires inside a round
+    for some of these accuracies, and the later half-sweeps of that round are
+    undone: Psi must equal the oracle's after exactly as many half-sweeps as
+    the device reports, and the stop index must agree with the oracle's."""
+    cfg = workloads.PillboxConfig(nz=601, nr=321)
+    f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(), modes=MODES)
+    f.mesh.dt = cfg.dt
+    z = np.arange(cfg.nz)[:, None] * cfg.dz
+    r = np.arange(cfg.nr)[None, :] * cfg.dr
+    q = np.zeros(f.shape)
+    q[: cfg.nz, : cfg.nr] = 1e6 * np.exp(-((z - 0.013) ** 2 + r ** 2) / (2 * 0.003 ** 2))
+    f["Q"] = q
+    f["Psi"] = np.zeros(f.shape)
+    g = split(f)
+    n_g = g.solve_poisson(0, accuracy, 5000)
+    out = g.fields(f)
+    ref = f.copy()
+    n_o, _, _ = oracle.solve_poisson(ref, ref["Psi"], ref["Q"], accuracy, 5000)
+    assert n_o > 0 and abs(n_g - n_o) <= 2, (n_g, n_o)
+    same = f.copy()
+    oracle.solve_poisson(same, same["Psi"], same["Q"], 1e-300, n_g + 1)
+    assert rel_l2(out["Psi"], same["Psi"]) <= SOR_TOL
+
+
 def test_imposed_field_within_tolerance():
     fx = load("dcgun_poisson")
     f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
