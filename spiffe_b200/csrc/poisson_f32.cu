@@ -374,6 +374,7 @@ __device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0,
 {
   const int nz = m.nz, P = m.pitch, H = s.H, cols = s.cols;
   double d = 0, q = 0;
+#pragma unroll 4
   for (int i = 0; i < nb; i++) {
     const int iz = iz0 + i;
     const bool upd = iz >= s.lo && iz <= s.hi, own = iz >= own_lo && iz <= own_hi;
@@ -392,9 +393,11 @@ __device__ void form_r0(const DevMesh &m, const Sor32Args &s, float *B, int iz0,
           double ap;
           if (ir == 0)
             ap = s.a_d * lr + s.c4_d * __ldcg(s.Psi + j + 1) + s.e2c_d * psi;
-          else
-            ap = s.a_d * lr + s.dr2_inv * (1 + 1. / (2 * ir)) * __ldcg(s.Psi + j + 1) +
-                 s.dr2_inv * (1 - 1. / (2 * ir)) * __ldcg(s.Psi + j - 1) + s.e_d * psi;
+          else {
+            const double h = 0.5 / ir; // = 1/(2 ir), correctly rounded either way
+            ap = s.a_d * lr + s.dr2_inv * (1 + h) * __ldcg(s.Psi + j + 1) + s.dr2_inv * (1 - h) * __ldcg(s.Psi + j - 1) +
+                 s.e_d * psi;
+          }
           r0 = (float)(rh - ap);
           if (own)
             q += fabs(rh - ap);
@@ -441,22 +444,27 @@ __device__ __forceinline__ void sor_node(float &x, float a, float ud, float c, f
 
 // One row of one colour for a strip: D row j (mesh row iz), neighbour rows
 // uj, dj, B row j - 1; P is the parity of the row's nodes of this colour.
+// With LOAD_OD the other colour of the row (o) and the row below (d) are
+// loaded here, otherwise the caller passes them; u returns the row above.
 // Returns the sum of |residual|.  With x0/x1 the row's new values of both
 // colours are also stored there for the neighbouring CTAs.
-template <int P, bool UNDO, bool DSUM>
+template <int P, bool UNDO, bool DSUM, bool LOAD_OD>
 __device__ __forceinline__ float sor_row(const Sor32Args &s, const Strip &t, float *D, const float *B, int j, int uj,
-                                         int dj, float wie, float wiex, float inv1w, float *dsum, float *x0, float *x1)
+                                         int dj, float4 &o, float4 &d, float4 &u, float wie, float wiex, float inv1w,
+                                         float *dsum, float *x0, float *x1)
 {
   const int H2 = 2 * s.H, so = P ? t.off1 : t.off0, oo = P ? t.off0 : t.off1;
   float *row = D + j * H2;
   float4 sv = *reinterpret_cast<const float4 *>(row + so);
-  const float4 o = *reinterpret_cast<const float4 *>(row + oo);
+  if (LOAD_OD) {
+    o = *reinterpret_cast<const float4 *>(row + oo);
+    d = *reinterpret_cast<const float4 *>(D + dj * H2 + so);
+  }
   // the fifth neighbour in r: node 8q-1 (parity 0; read but weighted 0 on
   // the axis) or node 8q+8 (parity 1; beyond the mesh for the last group,
   // whose node is not updated)
   const float nbr = P ? row[oo + 4] : row[oo - 1];
-  const float4 u = *reinterpret_cast<const float4 *>(D + uj * H2 + so);
-  const float4 d = *reinterpret_cast<const float4 *>(D + dj * H2 + so);
+  u = *reinterpret_cast<const float4 *>(D + uj * H2 + so);
   const float4 b = *reinterpret_cast<const float4 *>(B + (j - 1) * H2 + so);
   const float4 c = P ? t.cr1 : t.cr0, dl = P ? t.dr1 : t.dr0;
   const float a = s.a, e = s.e;
@@ -486,10 +494,72 @@ __device__ __forceinline__ float sor_row(const Sor32Args &s, const Strip &t, flo
   return acc;
 }
 
+// Rows j0..j1 of a strip in pairs, the first of parity P0 (rows alternate
+// parity).  The second row of a pair takes its other colour from the first
+// row's row above and its row below from the first row's other colour (the
+// sweep changes neither), except where a Dirichlet end row mirrors its
+// neighbour.  Adds |residual| and, with DSUM, |d| over own rows to acc, dacc.
+template <int P0, bool UNDO, int HD, bool DSUM>
+__device__ __forceinline__ void strip_rows(const DevMesh &m, const Sor32Args &s, const Strip &t, float *D,
+                                           const float *B, int iz_first, int nrow, int j0, int j1, float wie, float wiex,
+                                           float inv1w, float *xo, float &acc, float &dacc)
+{
+  const int nz = m.nz, H2 = 2 * s.H;
+  const bool lo0 = s.lo == 0, hin = s.hi == nz - 1;
+  for (int j = j0; j <= j1; j += 2) {
+    float4 oA, dA, uA;
+    int ujA;
+    {
+      const int iz = iz_first + j - HD;
+      // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
+      ujA = (iz == nz - 1 && hin) ? j - 1 : j + 1;
+      const int dj = (iz == 0 && lo0) ? j + 1 : j - 1;
+      float *x0 = nullptr, *x1 = nullptr;
+      if (xo) {
+        if (j < 2 * HD)
+          x0 = xo + (j - HD) * H2;
+        if (j >= nrow)
+          x1 = xo + HD * H2 + (j - nrow) * H2;
+      }
+      float ds = 0.f;
+      const float r = sor_row<P0, UNDO, DSUM, true>(s, t, D, B, j, ujA, dj, oA, dA, uA, wie, wiex, inv1w, &ds, x0, x1);
+      if (j >= HD && j < HD + nrow) {
+        acc += r;
+        dacc += ds;
+      }
+    }
+    const int jj = j + 1;
+    if (jj <= j1) {
+      const int iz = iz_first + jj - HD;
+      const int uj = (iz == nz - 1 && hin) ? jj - 1 : jj + 1;
+      const int dj = (iz == 0 && lo0) ? jj + 1 : jj - 1;
+      constexpr int P1 = P0 ^ 1;
+      float4 o = uA, d = oA, u;
+      if (ujA != jj) // the first row mirrored: its row above was not this row
+        o = *reinterpret_cast<const float4 *>(D + jj * H2 + (P1 ? t.off0 : t.off1));
+      if (dj != j) // this row mirrors: its row below is the row above
+        d = *reinterpret_cast<const float4 *>(D + dj * H2 + (P1 ? t.off1 : t.off0));
+      float *x0 = nullptr, *x1 = nullptr;
+      if (xo) {
+        if (jj < 2 * HD)
+          x0 = xo + (jj - HD) * H2;
+        if (jj >= nrow)
+          x1 = xo + HD * H2 + (jj - nrow) * H2;
+      }
+      float ds = 0.f;
+      const float r = sor_row<P1, UNDO, DSUM, false>(s, t, D, B, jj, uj, dj, o, d, u, wie, wiex, inv1w, &ds, x0, x1);
+      if (jj >= HD && jj < HD + nrow) {
+        acc += r;
+        dacc += ds;
+      }
+    }
+  }
+}
+
 // One colour c over D rows jlo..jhi (mesh row iz = iz_first + j - HD; B row
 // j - 1).  The rows are cut into runs of an even length, one per row group,
-// so every thread of a warp sees rows of the same parity.  Returns this
-// thread's sum of |residual| over the own rows HD..HD+nrow-1 and, with
+// so every thread of a warp starts on a row of the same parity.  Returns
+// this thread's sum of |residual| over the own rows HD..HD+nrow-1 and, with
 // DSUM, their sum of |d| in *dsum.  With xo, the first HD and the last HD
 // own rows also go to the exchange buffer (side 0: rows HD.., side 1: rows
 // nrow..).
@@ -503,27 +573,10 @@ __device__ __forceinline__ float sweep_rows(const DevMesh &m, const Sor32Args &s
     const int n = jhi - jlo + 1, per = 2 * ((n + 2 * t.ng - 1) / (2 * t.ng));
     const int j0 = jlo + t.g * per, j1 = min(jhi, j0 + per - 1);
     const float wie = w * s.inv_e, wiex = w * t.iex, inv1w = UNDO ? 1.f / (1.f - w) : 0.f;
-    const int nz = m.nz, H2 = 2 * s.H;
-    for (int j = j0; j <= j1; j++) {
-      const int iz = iz_first + j - HD;
-      // Dirichlet end rows mirror their only neighbour (poisson.c:369-375, :404-410)
-      const int uj = (iz == nz - 1 && s.hi == nz - 1) ? j - 1 : j + 1;
-      const int dj = (iz == 0 && s.lo == 0) ? j + 1 : j - 1;
-      float *x0 = nullptr, *x1 = nullptr;
-      if (xo) {
-        if (j < 2 * HD)
-          x0 = xo + (j - HD) * H2;
-        if (j >= nrow)
-          x1 = xo + HD * H2 + (j - nrow) * H2;
-      }
-      float ds = 0.f;
-      const float r = ((c + iz) & 1) == 0 ? sor_row<0, UNDO, DSUM>(s, t, D, B, j, uj, dj, wie, wiex, inv1w, &ds, x0, x1)
-                                          : sor_row<1, UNDO, DSUM>(s, t, D, B, j, uj, dj, wie, wiex, inv1w, &ds, x0, x1);
-      if (j >= HD && j < HD + nrow) {
-        acc += r;
-        dacc += ds;
-      }
-    }
+    if (((c + iz_first + j0 - HD) & 1) == 0)
+      strip_rows<0, UNDO, HD, DSUM>(m, s, t, D, B, iz_first, nrow, j0, j1, wie, wiex, inv1w, xo, acc, dacc);
+    else
+      strip_rows<1, UNDO, HD, DSUM>(m, s, t, D, B, iz_first, nrow, j0, j1, wie, wiex, inv1w, xo, acc, dacc);
   }
   if (DSUM)
     *dsum = dacc;
@@ -531,19 +584,27 @@ __device__ __forceinline__ float sweep_rows(const DevMesh &m, const Sor32Args &s
 }
 
 // Psi += d on the band's own nodes (FP64); own rows are D rows hd ..
-// hd+nrow-1.  Nodes the SOR does not update keep d = 0.
+// hd+nrow-1.  Nodes the SOR does not update keep d = 0.  Four rows' loads
+// are issued before their stores.
 __device__ void fold_d(const Sor32Args &s, int P, const float *D, int iz_first, int nrow, int hd)
 {
   const int H = s.H, cols = s.cols;
-  for (int j = hd; j < hd + nrow; j++) {
-    const int iz = iz_first + j - hd;
-    for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
-      const int p = t / H, k = t - p * H, ir = 2 * k + p;
-      const float d = D[(j * 2 + p) * H + k];
-      if (ir < cols && d != 0.f) {
-        const size_t i = node(iz, ir, P);
-        __stcg(s.Psi + i, __ldcg(s.Psi + i) + (double)d);
+  for (int t = threadIdx.x; t < 2 * H; t += blockDim.x) {
+    const int p = t / H, k = t - p * H, ir = 2 * k + p;
+    if (ir >= cols)
+      continue;
+    for (int j = hd; j < hd + nrow; j += 4) {
+      double v[4];
+      float dd[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        dd[u] = j + u < hd + nrow ? D[((j + u) * 2 + p) * H + k] : 0.f;
+        v[u] = dd[u] != 0.f ? __ldcg(s.Psi + node(iz_first + j + u - hd, ir, P)) : 0.0;
       }
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        if (dd[u] != 0.f)
+          __stcg(s.Psi + node(iz_first + j + u - hd, ir, P), v[u] + (double)dd[u]);
     }
   }
 }
@@ -576,6 +637,7 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[64];
   __shared__ float redf[HD + 1][32];
+  __shared__ float om_sh[2][HD]; // Chebyshev factors of this round and the next
   __shared__ int ok_sh, stop_sh, nundo_sh, rebase_sh;
   __shared__ double total_sh, thr_sh, quantum_sh, base_sh;
   __shared__ long long result_sh;
@@ -626,17 +688,17 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
   const int iz_last = iz_first + nrow - 1;
   double drive = 0, r0sum = 0;
   form_r0(m, s, B, iz_first - (HD - 1), nrow + 2 * (HD - 1), iz_first, iz_last, &drive, &r0sum);
-  // rows outside lo..hi that the driving sum still covers (iz < nz)
+  // rows outside lo..hi that the driving sum still covers (iz < nz): the
+  // first CTA takes those below lo, the last those above hi
   if (s.rhs) {
-    const bool first = b == 0, last = b == G - 1;
-    for (int iz = 0; iz < nz; iz++) {
-      if (iz >= s.lo && iz <= s.hi)
-        continue;
-      if ((iz < s.lo && !first) || (iz > s.hi && !last))
-        continue;
-      for (int ir = tid; ir < cols; ir += NT)
-        drive += fabs(s.rhs[node(iz, ir, P)]);
-    }
+    if (b == 0)
+      for (int iz = 0; iz < s.lo; iz++)
+        for (int ir = tid; ir < cols; ir += NT)
+          drive += fabs(s.rhs[node(iz, ir, P)]);
+    if (b == G - 1)
+      for (int iz = s.hi + 1; iz < nz; iz++)
+        for (int ir = tid; ir < cols; ir += NT)
+          drive += fabs(s.rhs[node(iz, ir, P)]);
   }
   // fixed-order block sums of the |rhs| and |r0| partials
   block_sum2(drive, red, 0);
@@ -669,41 +731,58 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
     total_sh = 0;
   }
   __syncthreads();
+  if (tid < HD)
+    om_sh[0][tid] = tid < s.limit ? s.omega[tid] : 0.f;
+  __syncthreads();
   if (!ok_sh)
     return;
   const int nw = (NT + 31) / 32, Q2 = 2 * Q;
-  // the halo rows a thread fetches: element e = tid (+ NT) of the 2HD rows x
-  // 2Q float4s of the neighbours' exchanged rows (rows 0..HD-1 from the CTA
-  // before, HD..2HD-1 from the one after)
+  // the halo rows a thread fetches: elements tid + u NT (u < PRE) of the 2HD
+  // rows x 2Q float4s of the neighbours' exchanged rows (rows 0..HD-1 from
+  // the CTA before, HD..2HD-1 from the one after), as row and column
+  constexpr int PRE = 3;
   const int ne = 2 * HD * Q2;
-  const int e0r = tid / Q2, e0c = tid - e0r * Q2, e1r = (tid + NT) / Q2, e1c = tid + NT - e1r * Q2;
+  int er[PRE], ec[PRE];
+#pragma unroll
+  for (int u = 0; u < PRE; u++) {
+    er[u] = (tid + u * NT) / Q2;
+    ec[u] = tid + u * NT - er[u] * Q2;
+  }
   for (long long n0 = 0; n0 < s.limit; n0 += HD) {
     const int keff = (int)(s.limit - n0 < HD ? s.limit - n0 : HD);
     const bool last = n0 + HD >= s.limit;
     // the last sweep of a round also writes the exchanged rows for the neighbours
     float *xo = halo ? s.xbuf + (size_t)((n0 / HD) & 1) * G * 4 * HD * H + (size_t)b * 4 * HD * H : nullptr;
+    const int rb = (int)((n0 / HD) & 1);
+    // the next round's factors load while this one sweeps
+    const float om_next = tid < HD && n0 + HD + tid < s.limit ? __ldg(s.omega + n0 + HD + tid) : 0.f;
 #pragma unroll 1
     for (int k = 0; k < HD; k++) {
-      float v = 0.f, ds = 0.f;
+      float v = 0.f;
       if (k < keff) {
         const int ext = halo ? HD - 1 - k : 0;
-        if (k == HD - 1) // the last sweep also sums |d| over the own nodes it updates
-          v = sweep_rows<false, HD, true>(m, s, st, D, B, iz_first, nrow, HD, HD + nrow - 1, 1, s.omega[n0 + k], xo,
+        if (k == HD - 1) { // the last sweep also sums |d| over the own nodes it updates
+          float ds = 0.f;
+          v = sweep_rows<false, HD, true>(m, s, st, D, B, iz_first, nrow, HD, HD + nrow - 1, 1, om_sh[rb][k], xo,
                                           &ds);
-        else
+          for (int o = 16; o > 0; o >>= 1)
+            ds += __shfl_down_sync(0xffffffffu, ds, o);
+          if ((tid & 31) == 0)
+            redf[HD][tid >> 5] = ds;
+        } else {
           v = sweep_rows<false, HD>(m, s, st, D, B, iz_first, nrow, HD - ext, HD + nrow - 1 + ext, k & 1,
-                                    s.omega[n0 + k]);
+                                    om_sh[rb][k]);
+        }
+      } else if (k == HD - 1 && (tid & 31) == 0) {
+        redf[HD][tid >> 5] = 0.f;
       }
       // fixed-order sums: per warp in FP32 here, across warps in FP64 by warp 0 below
-      for (int o = 16; o > 0; o >>= 1) {
+      for (int o = 16; o > 0; o >>= 1)
         v += __shfl_down_sync(0xffffffffu, v, o);
-        ds += __shfl_down_sync(0xffffffffu, ds, o);
-      }
-      if ((tid & 31) == 0) {
+      if ((tid & 31) == 0)
         redf[k][tid >> 5] = v;
-        if (k == HD - 1)
-          redf[HD][tid >> 5] = ds;
-      }
+      if (k == HD - 1 && tid < HD)
+        om_sh[rb ^ 1][tid] = om_next;
       __syncthreads();
     }
     double part[HD + 1]; // |residual| of each half-sweep, then |d| after the last
@@ -716,7 +795,10 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
         part[k] = v;
       }
     }
-    float4 pre0 = make_float4(0.f, 0.f, 0.f, 0.f), pre1 = pre0;
+    float4 pre[PRE];
+#pragma unroll
+    for (int u = 0; u < PRE; u++)
+      pre[u] = make_float4(0.f, 0.f, 0.f, 0.f);
     const float *xi = s.xbuf + (size_t)((n0 / HD) & 1) * G * 4 * HD * H;
     if (halo) {
       if (tid == 0) {
@@ -739,17 +821,13 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
         return;
       // the neighbours' rows, held in registers until the stop test has run
       if (!last) {
-        if (tid < ne) {
-          const int nb_ = e0r < HD ? b - 1 : b + 1;
-          if (nb_ >= 0 && nb_ < G)
-            pre0 = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
-                                                           (e0r < HD ? 2 * HD * H : 0)) + (e0r % HD) * Q2 + e0c);
-        }
-        if (tid + NT < ne) {
-          const int nb_ = e1r < HD ? b - 1 : b + 1;
-          if (nb_ >= 0 && nb_ < G)
-            pre1 = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
-                                                           (e1r < HD ? 2 * HD * H : 0)) + (e1r % HD) * Q2 + e1c);
+#pragma unroll
+        for (int u = 0; u < PRE; u++) {
+          const int nb_ = er[u] < HD ? b - 1 : b + 1;
+          if (tid + u * NT < ne && nb_ >= 0 && nb_ < G)
+            pre[u] = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
+                                                             (er[u] < HD ? 2 * HD * H : 0)) +
+                            (er[u] < HD ? er[u] : er[u] - HD) * Q2 + ec[u]);
         }
       }
     }
@@ -809,7 +887,7 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
       for (int u = nundo_sh; u > 0; u--) {
         const int k = keff - 1 - nundo_sh + u; // the latest sweep not yet undone
         const int ext = halo ? HD - 1 - k : 0;
-        sweep_rows<true, HD>(m, s, st, D, B, iz_first, nrow, HD - ext, HD + nrow - 1 + ext, k & 1, s.omega[n0 + k]);
+        sweep_rows<true, HD>(m, s, st, D, B, iz_first, nrow, HD - ext, HD + nrow - 1 + ext, k & 1, om_sh[rb][k]);
         __syncthreads();
       }
       break;
@@ -836,19 +914,20 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
     if (halo && !last) {
       // halo rows 0..HD-1 from the CTA before, nrow+HD.. from the one after;
       // the exchange rows hold both parities in D's row layout
-      for (int t = tid; t < ne; t += NT) {
-        const int r = t < NT ? e0r : (t < 2 * NT ? e1r : t / Q2), cc = t < NT ? e0c : (t < 2 * NT ? e1c : t % Q2);
+#pragma unroll
+      for (int u = 0; u < PRE; u++) {
+        const int nb_ = er[u] < HD ? b - 1 : b + 1;
+        if (tid + u * NT < ne && nb_ >= 0 && nb_ < G)
+          *reinterpret_cast<float4 *>(D + (er[u] < HD ? er[u] : nrow + er[u]) * 2 * H + 4 * ec[u]) = pre[u];
+      }
+      for (int t = tid + PRE * NT; t < ne; t += NT) { // wide meshes: the rest directly
+        const int r = t / Q2, cc = t - r * Q2;
         const int nb_ = r < HD ? b - 1 : b + 1;
         if (nb_ < 0 || nb_ >= G)
           continue;
-        float4 v;
-        if (t < 2 * NT)
-          v = t < NT ? pre0 : pre1;
-        else
-          v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H + (r < HD ? 2 * HD * H : 0)) +
-                     (r % HD) * Q2 + cc);
-        const int row = r < HD ? r : nrow + r;
-        *reinterpret_cast<float4 *>(D + row * 2 * H + 4 * cc) = v;
+        const float4 v = __ldcg(reinterpret_cast<const float4 *>(xi + (size_t)nb_ * 4 * HD * H +
+                                                                 (r < HD ? 2 * HD * H : 0)) + (r < HD ? r : r - HD) * Q2 + cc);
+        *reinterpret_cast<float4 *>(D + (r < HD ? r : nrow + r) * 2 * H + 4 * cc) = v;
       }
       __syncthreads();
     }
