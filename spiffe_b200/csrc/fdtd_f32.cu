@@ -23,7 +23,24 @@ struct Coef32 {
   const float *cpd, *cmd, *bzf;
   float fEr, topf, fEphi_dz, fEphi_dr, dt_dz, dt_dr, kJ;
   int zero_j;
+  int reset_box; // this B kernel is the step's last: empty the current box
 };
+
+// rows [lo, hi] of the current box (lo > hi: no current anywhere)
+__device__ __forceinline__ void jbox_rows(const int *jbox, int P, int &lo, int &hi)
+{
+  const int a = jbox[0], b = jbox[1];
+  lo = a <= b ? a / P : 1;
+  hi = a <= b ? b / P : 0;
+}
+
+__device__ __forceinline__ void jbox_reset(int *jbox)
+{
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
+    jbox[0] = 0x7fffffff;
+    jbox[1] = -1;
+  }
+}
 
 __global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coef32 c)
 {
@@ -34,9 +51,13 @@ __global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coe
   const size_t i = node(iz, ir, P);
   const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
   const bool ez_row = ir < nr && iz >= 1 && iz <= nz - 1, er_row = iz <= nz - 1;
-  // every load before any store, so no store can order the loads behind it
+  // every load before any store, so no store can order the loads behind it;
+  // J is read (and cleared) only on the rows a deposit touched
+  int jlo, jhi;
+  jbox_rows(f.jbox, P, jlo, jhi);
+  const bool jrow = iz >= jlo && iz <= jhi;
   const uint8_t u = f.umask[i];
-  const long long jz = f.Jz[i], jr = f.Jr[i];
+  const long long jz = jrow ? f.Jz[i] : 0, jr = jrow ? f.Jr[i] : 0;
   const float ez = ez_row ? f.Ez[i] : 0.f, er = er_row ? f.Er[i] : 0.f;
   const float b0 = f.Bphi[i];
   const float b1 = ez_row && ir < nr - 1 ? f.Bphi[i + 1] : 0.f;
@@ -72,7 +93,7 @@ __global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coe
       f.Er[i] = 0.f;
     }
   }
-  if (c.zero_j) {
+  if (c.zero_j && jrow) {
     f.Jz[i] = 0;
     f.Jr[i] = 0;
   }
@@ -82,11 +103,13 @@ __global__ void __launch_bounds__(BX *BY) k_tm_b32(DevMesh m, DevFields32 f, Coe
 {
   const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
   const int nz = m.nz, nr = m.nr, P = m.pitch;
+  if (c.reset_box)
+    jbox_reset(f.jbox);
   if (ir > nr || iz < 1 || iz > nz - 1)
     return;
   const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
   const size_t i = node(iz, ir, P);
-  float b = f.Bphi[i], b2 = f.Bphi2[i];
+  float b = f.Bphi[i], b2;
   if (ir >= 1 && ir <= nr - 2) {
     const uint8_t u = f.umask[i];
     const float ez = f.Ez[i], ezm = f.Ez[i - 1], er = f.Er[i], erm = f.Er[i - P];
@@ -96,6 +119,8 @@ __global__ void __launch_bounds__(BX *BY) k_tm_b32(DevMesh m, DevFields32 f, Coe
       b += dB;
       f.Bphi2[i] = b2;
       f.Bphi[i] = b;
+    } else {
+      b2 = f.Bphi2[i]; // the old half-step value is read only where it is kept
     }
     if (ir == 1) {
       f.Bphi[node(iz, 0, P)] = -b;
@@ -126,6 +151,7 @@ __global__ void __launch_bounds__(BX *BY) k_tm_b32(DevMesh m, DevFields32 f, Coe
     }
   } else if (ir == nr) {
     // column nr is never updated; the end rows still copy it
+    b2 = f.Bphi2[i];
     if (iz == 1) {
       f.Bphi[node(0, nr, P)] = leftN ? b : -b;
       f.Bphi2[node(0, nr, P)] = leftN ? b2 : -b2;
@@ -145,8 +171,11 @@ __global__ void __launch_bounds__(BX *BY) k_te_e32(DevMesh m, DevFields32 f, Coe
   if (ir > nr || iz > nz)
     return;
   const size_t i = node(iz, ir, P);
-  const long long jphi = f.Jphi[i];
-  if (c.zero_j)
+  int jlo, jhi;
+  jbox_rows(f.jbox, P, jlo, jhi);
+  const bool jrow = iz >= jlo && iz <= jhi;
+  const long long jphi = jrow ? f.Jphi[i] : 0;
+  if (c.zero_j && jrow)
     f.Jphi[i] = 0;
   const bool zero = ir == 0 || (m.right_bc == SPIFFE_NEUMANN && iz == nz - 1) ||
                     (m.left_bc == SPIFFE_NEUMANN && iz == 0) || (m.upper_bc == SPIFFE_NEUMANN && ir == nr - 1);
@@ -163,6 +192,8 @@ __global__ void __launch_bounds__(BX *BY) k_te_b32(DevMesh m, DevFields32 f, Coe
 {
   const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
   const int nz = m.nz, nr = m.nr, P = m.pitch;
+  if (c.reset_box)
+    jbox_reset(f.jbox);
   if (ir > nr || iz > nz)
     return;
   const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
@@ -257,16 +288,23 @@ __global__ void k_from_fixed(int nz, int nr, int P, const long long *src, double
   dst[node(iz, ir, nr + 1)] = (double)src[node(iz, ir, P)] * q;
 }
 
-__global__ void k_antenna32(long long *J, int P, int direction, long istart, long iend, long iposition, long long v)
+__global__ void k_antenna32(long long *J, int *jbox, int P, int direction, long istart, long iend, long iposition,
+                            long long v)
 {
   const long i = istart + (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i > iend)
     return;
   // antenna.c:398-415
-  if (direction == 1)
-    J[node((int)iposition, (int)i, P)] += v;
-  else
-    J[node((int)i, (int)iposition, P)] += v;
+  const int nd = direction == 1 ? (int)node((int)iposition, (int)i, P) : (int)node((int)i, (int)iposition, P);
+  J[nd] += v;
+  atomicMin(jbox, nd);
+  atomicMax(jbox + 1, nd);
+}
+
+__global__ void k_jbox_set(int *jbox, int lo, int hi)
+{
+  jbox[0] = lo;
+  jbox[1] = hi;
 }
 
 // a >>= shift with rounding to nearest: values in old quanta to quanta 2^shift times larger
@@ -373,11 +411,13 @@ extern "C" int s32_fdtd_step(const DevMesh *m, const DevFields32 *f, const Fdtd3
            (float)(dt / m->dz), (float)(dt / m->dr), kJ, zero_j};
   const dim3 block(BX, BY), grid = grid_for(m, m->nr + 1);
   if (m->modes & SPIFFE_FL_TM_FIELDS) {
+    c.reset_box = zero_j && !(m->modes & SPIFFE_FL_TE_FIELDS);
     k_tm_e32<<<grid, block, 0, s>>>(*m, *f, c);
     k_tm_b32<<<grid, block, 0, s>>>(*m, *f, c);
     spiffe_note_launches(2);
   }
   if (m->modes & SPIFFE_FL_TE_FIELDS) {
+    c.reset_box = zero_j;
     k_te_e32<<<grid, block, 0, s>>>(*m, *f, c);
     k_te_b32<<<grid, block, 0, s>>>(*m, *f, c);
     spiffe_note_launches(2);
@@ -427,14 +467,21 @@ extern "C" int s32_from_fixed(const DevMesh *m, const long long *src, double *d_
   return (int)cudaGetLastError();
 }
 
-extern "C" int s32_antenna(long long *J, int pitch, int direction, long istart, long iend, long iposition,
-                           double value, double qJ, cudaStream_t s)
+extern "C" int s32_antenna(long long *J, int *jbox, int pitch, int direction, long istart, long iend,
+                           long iposition, double value, double qJ, cudaStream_t s)
 {
   if (iend < istart)
     return 0;
   const long n = iend - istart + 1;
-  k_antenna32<<<blocks_for(n, 128), 128, 0, s>>>(J, pitch, direction, istart, iend, iposition,
+  k_antenna32<<<blocks_for(n, 128), 128, 0, s>>>(J, jbox, pitch, direction, istart, iend, iposition,
                                                   (long long)std::llround(value / qJ));
+  spiffe_note_launches(1);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int s32_jbox_set(int *jbox, int lo, int hi, cudaStream_t s)
+{
+  k_jbox_set<<<1, 1, 0, s>>>(jbox, lo, hi);
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

@@ -383,6 +383,7 @@ __device__ void deposit_particle(const DevMesh &m, const DevFields32 &f, bool on
   const bool lsm = !DEF && (m.modes & SPIFFE_FL_LONGIT_SMEAR), rsm = !DEF && (m.modes & SPIFFE_FL_RADIAL_SMEAR);
   const bool tm = DEF || (m.modes & SPIFFE_FL_TM_FIELDS), te = !DEF && (m.modes & SPIFFE_FL_TE_FIELDS);
   Contrib32 c;
+  unsigned lo = 0xffffffffu, hi = 0u; // node indices this lane adds to
   for (int comp = 0; comp < 3; comp++) {
     if ((comp < 2 && !tm) || (comp == 2 && !te))
       continue;
@@ -397,7 +398,21 @@ __device__ void deposit_particle(const DevMesh &m, const DevFields32 &f, bool on
       if ((k == 1 && !lsm) || (k == 2 && !rsm) || (k == 3 && !(lsm && rsm)))
         continue;
       warp_add(J, c.node[k], c.node[k] >= 0 ? c.q[k] : 0);
+      if (c.node[k] >= 0) {
+        lo = min(lo, (unsigned)c.node[k]);
+        hi = max(hi, (unsigned)c.node[k]);
+      }
     }
+  }
+  // widen the box of nodes holding current (the FDTD reads and clears only
+  // its rows); a warp skips the atomics when the box already covers it
+  lo = __reduce_min_sync(0xffffffffu, lo);
+  hi = __reduce_max_sync(0xffffffffu, hi);
+  if ((threadIdx.x & 31) == 0 && lo <= hi) {
+    if ((int)lo < f.jbox[0])
+      atomicMin(f.jbox, (int)lo);
+    if ((int)hi > f.jbox[1])
+      atomicMax(f.jbox + 1, (int)hi);
   }
 }
 

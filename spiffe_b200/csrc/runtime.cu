@@ -418,6 +418,8 @@ static int s32_create(spiffe_gpu_instance *in, const int16_t *flags)
   RC_TRY(s32_alloc_z(&S.f.PsiImposed, n, s));
   RC_TRY(s32_alloc_z(&S.f.Q, n, s));
   RC_TRY(s32_alloc_z(&S.f.Qp, n, s));
+  CUDA_TRY(cudaMalloc(&S.f.jbox, 2 * sizeof(int)));
+  RC_TRY(s32_jbox_set(S.f.jbox, 0x7fffffff, -1, s));
   RC_TRY(s32_beam_alloc(&S.b, in->capacity));
   RC_TRY(s32_particles_work(&S.pw, in->capacity));
   RC_TRY(s32_fdtd_tables(&in->dm, in->h_flags.data(), &S.fdtd, S.umask, s));
@@ -432,7 +434,7 @@ static void s32_destroy(spiffe_gpu_instance *in)
   S32State &S = *in->s32;
   void *p[] = {S.f.Ez, S.f.Er, S.f.Bphi, S.f.Bphi2, S.f.Ephi, S.f.Br, S.f.Br2, S.f.Bz, S.f.Bz2,
                S.f.EzImposed, S.f.ErImposed, S.f.BzImposed, S.f.BrImposed, S.f.Jz, S.f.Jr, S.f.Jphi,
-               S.f.Psi, S.f.PsiImposed, S.f.Q, S.f.Qp, S.umask, S.staging};
+               S.f.Psi, S.f.PsiImposed, S.f.Q, S.f.Qp, S.f.jbox, S.umask, S.staging};
   for (void *q : p)
     cudaFree(q);
   s32_beam_free(&S.b);
@@ -514,6 +516,8 @@ static int s32_upload_fields(spiffe_gpu_instance *in, const spiffe_field_set *h)
   S32_FLOAT_FIELDS(UPF)
   S32_F64_FIELDS(UPD)
   S32_FIXED_FIELDS(UPJ)
+  if (h->Jz || h->Jr || h->Jphi) // uploaded current may be anywhere
+    RC_TRY(s32_jbox_set(S.f.jbox, 0, 0x7ffffffe, s));
 #undef UPF
 #undef UPD
 #undef UPJ
@@ -597,6 +601,7 @@ static int s32_upload_beam(spiffe_gpu_instance *in, const spiffe_beam_set *h)
   in->QoMC = h->QoMC;
   in->stiffness = h->stiffness;
   S.j_state = S32_J_UNKNOWN;
+  S.since_sort = S.sort_interval; // an uploaded beam is sorted on the next step
   return 0;
 }
 
@@ -652,6 +657,7 @@ static int s32_zero_j(spiffe_gpu_instance *in)
   for (long long *a : J)
     if (a)
       CUDA_TRY(cudaMemsetAsync(a, 0, bytes, in->stream));
+  RC_TRY(s32_jbox_set(S.f.jbox, 0x7fffffff, -1, in->stream));
   S.j_state = S32_J_ZERO;
   return 0;
 }
@@ -1657,7 +1663,7 @@ static int antennas(spiffe_gpu_instance *in, double time)
     if (in->s32) {
       const DevFields32 &F = in->s32->f;
       long long *arr = a.direction == 0 ? F.Jz : (a.direction == 1 ? F.Jr : F.Jphi);
-      rc = s32_antenna(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->s32->sc.qJ, in->stream);
+      rc = s32_antenna(arr, F.jbox, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->s32->sc.qJ, in->stream);
     } else {
       double *arr = a.direction == 0 ? in->f.Jz : (a.direction == 1 ? in->f.Jr : in->f.Jphi);
       rc = spiffe_antenna64(arr, in->dm.pitch, a.direction, a.istart, a.iend, a.iposition, J, in->stream);
@@ -1737,15 +1743,18 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
       RC_TRY(spiffe_gpu_advance_field_solutions(in));
       RC_TRY(spiffe_gpu_advance_particles(in, &in->push));
     } else {
-      RC_TRY(s32_fdtd(in, 1)); // reads J and leaves it zero
-      RC_TRY(s32_push_step(in, &in->push, in->space_charge)); // deposits J for the next step
-      if (!in->space_charge)
-        S->j_state = S32_J_ZERO;
-      if (S->sort_interval > 0 && ++S->since_sort >= S->sort_interval) {
+      // particles by cell before the push, every sort_interval steps and on
+      // the first step after an upload
+      if (S->sort_interval > 0 && S->since_sort >= S->sort_interval) {
         S->since_sort = 0;
         PhaseScope ps(in, PH_PUSH);
         RC_TRY(s32_sort(&in->dm, &S->b, in->cnt, in->np_upper, &S->pw, in->stream));
       }
+      RC_TRY(s32_fdtd(in, 1)); // reads J and leaves it zero
+      RC_TRY(s32_push_step(in, &in->push, in->space_charge)); // deposits J for the next step
+      if (!in->space_charge)
+        S->j_state = S32_J_ZERO;
+      S->since_sort++;
     }
     RC_TRY(set_current_density(in));
     m.time_step++;
@@ -1829,7 +1838,7 @@ extern "C" int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *in, int64_t n)
     return fail(SPIFFE_ERR_INVALID, "bad argument");
   if (in->s32) {
     in->s32->sort_interval = n;
-    in->s32->since_sort = 0;
+    in->s32->since_sort = n; // the next step sorts
   }
   return 0;
 }

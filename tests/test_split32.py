@@ -101,6 +101,27 @@ def test_deposit_within_tolerance():
         assert rel_l2(out[n], fx[n]) <= FIELD_TOL, n
 
 
+def test_current_box_covers_the_deposit():
+    """The split form's FDTD reads (and clears) J only on the rows a deposit
+    touched.  A field step after a deposit must equal the same step from the
+    same current uploaded explicitly, which marks every row."""
+    fx = load("pillbox_push")
+    f, b = push_fixture_state(fx)
+    g = split(f)
+    g.upload_beam(b)
+    g.zero_currents()
+    g.deposit()
+    dep = g.fields(f)
+    assert np.count_nonzero(dep["Jz"]) > 0
+    g.advance_fields()
+    tracked = g.fields(f)
+    h = split(dep)
+    h.advance_fields()
+    full = h.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Jz", "Jr"):
+        assert np.array_equal(tracked[n], full[n]), n
+
+
 def test_push_within_tolerance(oracle):
     fx = load("pillbox_push")
     f, b = push_fixture_state(fx)
