@@ -63,7 +63,7 @@ def parse():
     p.add_argument("--precision", default="split32", choices=["split32", "f64"],
                    help="split32: FP32 fields/push, split positions, fixed-point current (the form the metric is "
                         "quoted on); f64: the plain FP64 drop-in")
-    p.add_argument("--f64-steps", type=int, default=100,
+    p.add_argument("--f64-steps", type=int, default=200,
                    help="steps of the plain FP64 form timed on the same state for comparison (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling captures)")

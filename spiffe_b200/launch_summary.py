@@ -3,7 +3,7 @@
 Input: the CSV that `ncu --metrics gpu__time_duration.sum --csv --log-file X`
 writes.  Output: a markdown table, one row per kernel name, sorted by time.
 
-    python profiles/summarize_launches.py launches.csv [--top N]
+    python -m spiffe_b200.launch_summary launches.csv [--top N]
 """
 import argparse
 import csv
