@@ -68,6 +68,15 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling captures)")
     p.add_argument("--cpu-steps", type=int, default=20, help="reference steps timed for the CPU baseline")
+    p.add_argument("--workload", default="gun16", choices=["gun16", "scan", "serve"],
+                   help="gun16: the benchmark (config 2); scan: a sample of the batched scan (config 4) run together; "
+                        "serve: a sample of the request stream (config 5) at several arrival rates")
+    p.add_argument("--instances", type=int, default=64, help="scan: instances drawn from the scan distribution")
+    p.add_argument("--scan-steps", type=int, default=500, help="scan/serve: integration steps per instance")
+    p.add_argument("--workers", type=int, default=4, help="scan/serve: host threads driving instances")
+    p.add_argument("--requests", type=int, default=48, help="serve: requests per arrival rate")
+    p.add_argument("--rates", default="5,10,20", help="serve: arrival rates in requests/s")
+    p.add_argument("--budget-gb", type=float, default=150.0, help="serve: device-memory admission budget")
     p.add_argument("--scale", type=int, default=1,
                    help="coarsen the mesh by this factor and the beam by its square (small profiling cases)")
     return p.parse_args()
@@ -449,10 +458,86 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def scan_arm(args):
+    """A sample of the batched scan: --instances drawn from its distribution,
+    --scan-steps each, advanced together by the native scheduler on
+    --workers threads, then the same instances one at a time."""
+    import torch
+
+    from spiffe_b200 import serve
+
+    torch.cuda.set_device(0)
+    serve.run_scan(serve.draw_requests(2, steps=5, size_scale=0.25, particle_scale=0.02), workers=2)  # warm-up
+    reqs = serve.draw_requests(args.instances, steps=args.scan_steps)
+    clocks = ClockSampler(0)
+    clocks.start()
+    res, done, build_s = serve.run_scan(reqs, workers=args.workers, chunk=20)
+    clk = clocks.stop()
+    seq, seq_done, _ = serve.run_scan(reqs, workers=1, chunk=0)
+    wall = max(done) / 1e3
+    ps = sum(r["particle_steps"] for r in res)
+    cu = sum(r["cell_updates"] for r in res)
+    assert [r["moments"] for r in res] == [r["moments"] for r in seq], "a result changed in the mix"
+    line = {"metric": "particle-steps/s & cell-updates/s of a batched scan (config 4 sample)", "value": round(ps / wall, 1),
+            "unit": UNIT, "n_gpus": 1, "steps": args.scan_steps, "warmup": 0, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d scan instances (pillbox or 1.6-cell gun, 80x120..400x1500 nodes, "
+                                   "10k..500k macroparticles, seeds 1234 / 987654321+i), %d steps each"
+                                   % (args.instances, args.scan_steps),
+                       "form": "split precision", "workers": args.workers, "chunk": 20},
+            "cell_updates_per_s": round(cu / wall, 1), "wall_s": round(wall, 3), "build_s": round(build_s, 3),
+            "completion_ms": {"p50": round(statistics.median(done), 1),
+                              "p99": round(sorted(done)[max(0, math.ceil(0.99 * len(done)) - 1)], 1)},
+            "one_at_a_time": {"wall_s": round(max(seq_done) / 1e3, 3),
+                              "value": round(ps / (max(seq_done) / 1e3), 1)},
+            "results_identical_alone_and_in_the_mix": True, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def serve_arm(args):
+    """A sample of the request stream: --requests per rate from the scan
+    distribution, --scan-steps each, Poisson arrivals, admission within
+    --budget-gb of device memory, --workers concurrent requests."""
+    import torch
+
+    from spiffe_b200 import serve
+
+    torch.cuda.set_device(0)
+    serve.run_scan(serve.draw_requests(2, steps=5, size_scale=0.25, particle_scale=0.02), workers=2)  # warm-up
+    rates = [float(x) for x in args.rates.split(",") if x]
+    out = {}
+    for k, rate in enumerate(rates):
+        reqs = serve.draw_requests(args.requests, steps=args.scan_steps, seed=1234 + k)
+        srv = serve.Server(args.budget_gb * 1e9, workers=args.workers)
+        rows = srv.serve(reqs, rate=rate, seed=4321 + k)
+        lat = [r["latency"] for r in rows]
+        errs = [r["error"] for r in rows if r["error"]]
+        span = max(r["end"] for r in rows)
+        out["%g" % rate] = {"p50_s": round(serve.percentile(lat, 50), 4), "p99_s": round(serve.percentile(lat, 99), 4),
+                            "served_per_s": round(len(rows) / span, 2), "errors": len(errs),
+                            "peak_budget_gb": round(rows[0]["peak_in_use"] / 1e9, 3),
+                            "particle_steps_per_s": round(sum(r["result"]["particle_steps"] for r in rows
+                                                              if r["result"]) / span, 1)}
+    worst = max(out.values(), key=lambda v: v["p99_s"])
+    line = {"metric": "request latency p50/p99 under Poisson arrivals (config 5 sample)", "value": worst["p99_s"],
+            "unit": "s (p99, highest rate)", "n_gpus": 1, "steps": args.scan_steps, "warmup": 0,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "%d requests per rate from the scan distribution, %d steps each, Poisson "
+                                   "arrivals, %.0f GB admission budget" % (args.requests, args.scan_steps,
+                                                                          args.budget_gb),
+                       "form": "split precision", "workers": args.workers},
+            "rates": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "scan":
+        scan_arm(args)
+    elif args.workload == "serve":
+        serve_arm(args)
     else:
         gpu_arm(args)
 

@@ -143,6 +143,18 @@ int64_t spiffe_gpu_launch_count(void);
  * beam upload; this keeps the gather and the deposition of neighbouring
  * threads on the same nodes.  No effect on the FP64 form. */
 int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *inst, int64_t n);
+/* Batched execution (no counterpart in the reference, which runs one problem
+ * per process): advances n independent instances concurrently, instance i by
+ * steps[i] steps of spiffe_gpu_run_steps, on `workers` host threads.  Each
+ * instance keeps its own stream, so kernels of different instances overlap
+ * on the device; an instance is advanced `chunk` steps at a time (<= 0: all
+ * at once) by one thread at a time, the instances served round-robin.
+ * done_ms[i] (may be null) receives the milliseconds from the call to the
+ * completion of instance i.  Returns 0 or the first error; on an error the
+ * other instances stop after their current chunk.  The instances must not be
+ * used by other threads during the call. */
+int spiffe_gpu_batch_run(spiffe_gpu_instance *const *inst, int32_t n, const int64_t *steps, int32_t workers,
+                         int64_t chunk, double *done_ms);
 /* Work done so far: out[0] particle-steps (active particles summed over
  * pushes), out[1] SOR half-sweeps, out[2] SOR solves, out[3] FDTD steps. */
 int spiffe_gpu_work_counters(spiffe_gpu_instance *inst, int64_t *out);

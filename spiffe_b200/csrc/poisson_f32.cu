@@ -1073,7 +1073,14 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
   cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const int rows = (m->right_bc == SPIFFE_DIRICHLET ? nz - 1 : nz - 2) - (m->left_bc == SPIFFE_DIRICHLET ? 0 : 1) + 1;
   const int cols = nr - 1, H = ((cols + 2) / 2 + 3) / 4 * 4; // half-row (one colour), a multiple of 4
-  const size_t budget = (size_t)max_smem - 1024;
+  // dynamic shared memory a CTA of depth h may use: the opt-in limit less
+  // the kernel's own static shared memory
+  auto budget_of = [&](int h) -> size_t {
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, sor_kernel(h)) != cudaSuccess)
+      return 0;
+    return (size_t)max_smem > fa.sharedSizeBytes ? (size_t)max_smem - fa.sharedSizeBytes : 0;
+  };
   // One CTA when the mesh fits one SM (no grid barriers); otherwise bands
   // of at least `hd` rows (the halo exchange carries hd rows) over all SMs,
   // with four half-sweeps per barrier where the deeper halo fits, else two
@@ -1081,13 +1088,14 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
   // more than the barriers they save).
   int G = 0, hd = 4;
   for (int h : {4, 2})
-    if (sor_smem(rows, H, h) <= budget && (size_t)rows * 2 * H <= 65536) {
+    if (sor_smem(rows, H, h) <= budget_of(h) && (size_t)rows * 2 * H <= 65536) {
       G = 1;
       hd = h;
       break;
     }
   if (G == 0)
     for (int h : {4, 2}) {
+      const size_t budget = budget_of(h);
       int g = std::min(sms, rows / h);
       while (g < rows / h && sor_smem((rows + g - 1) / g, H, h) > budget)
         g++;
@@ -1109,7 +1117,10 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
   w->threads = sor_threads(R, H, hd);
   if (w->threads < 1)
     return (int)cudaErrorInvalidConfiguration; // a half row wider than one CTA's threads
-  e = cudaFuncSetAttribute(sor_kernel(hd), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)w->smem);
+  // the attribute is process-wide: set it to the kernel's limit (the same
+  // value for every instance), not to this instance's band, so that setting
+  // up another instance cannot lower it under this one's launch
+  e = cudaFuncSetAttribute(sor_kernel(hd), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)budget_of(hd));
   if (e == cudaSuccess)
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sor_kernel(hd), w->threads, w->smem);
   if (e == cudaSuccess && occ < 1)

@@ -77,6 +77,8 @@ def load():
         "spiffe_gpu_phase_times": ([H, P(C.c_double), P(C.c_int64)], C.c_int),
         "spiffe_gpu_launch_count": ([], C.c_int64),
         "spiffe_gpu_work_counters": ([H, P(C.c_int64)], C.c_int),
+        "spiffe_gpu_set_sort_interval": ([H, C.c_int64], C.c_int),
+        "spiffe_gpu_batch_run": ([P(H), C.c_int32, P(C.c_int64), C.c_int32, C.c_int64, P(C.c_double)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -93,6 +95,19 @@ def select_device(device):
 
 def launch_count():
     return load().spiffe_gpu_launch_count()
+
+
+def batch_run(instances, steps, workers=8, chunk=20):
+    """Advances the instances concurrently (spiffe_gpu_batch_run): instance i
+    by steps[i] integration steps, on `workers` host threads, `chunk` steps
+    at a time.  Returns the milliseconds from the call to each instance's
+    completion."""
+    n = len(instances)
+    hs = (H * max(n, 1))(*[g.h for g in instances])
+    st = (C.c_int64 * max(n, 1))(*[int(k) for k in steps])
+    done = (C.c_double * max(n, 1))()
+    _check(load().spiffe_gpu_batch_run(hs, n, st, int(workers), int(chunk), done))
+    return [done[i] for i in range(n)]
 
 
 def _check(rc):

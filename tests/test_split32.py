@@ -116,6 +116,8 @@ def test_current_box_covers_the_deposit():
     g.advance_fields()
     tracked = g.fields(f)
     h = split(dep)
+    h.upload_beam(b)  # the same charge bound, so the same fixed-point current quantum
+    h.upload_fields(dep)
     h.advance_fields()
     full = h.fields(f)
     for n in ("Ez", "Er", "Bphi", "Jz", "Jr"):
