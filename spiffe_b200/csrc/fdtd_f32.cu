@@ -27,11 +27,10 @@ struct Coef32 {
 };
 
 // rows [lo, hi] of the current box (lo > hi: no current anywhere)
-__device__ __forceinline__ void jbox_rows(const int *jbox, int P, int &lo, int &hi)
+__device__ __forceinline__ void jbox_rows(const int *jbox, int &lo, int &hi)
 {
-  const int a = jbox[0], b = jbox[1];
-  lo = a <= b ? a / P : 1;
-  hi = a <= b ? b / P : 0;
+  lo = jbox[0];
+  hi = jbox[1];
 }
 
 __device__ __forceinline__ void jbox_reset(int *jbox)
@@ -54,7 +53,7 @@ __global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coe
   // every load before any store, so no store can order the loads behind it;
   // J is read (and cleared) only on the rows a deposit touched
   int jlo, jhi;
-  jbox_rows(f.jbox, P, jlo, jhi);
+  jbox_rows(f.jbox, jlo, jhi);
   const bool jrow = iz >= jlo && iz <= jhi;
   const uint8_t u = f.umask[i];
   const long long jz = jrow ? f.Jz[i] : 0, jr = jrow ? f.Jr[i] : 0;
@@ -172,7 +171,7 @@ __global__ void __launch_bounds__(BX *BY) k_te_e32(DevMesh m, DevFields32 f, Coe
     return;
   const size_t i = node(iz, ir, P);
   int jlo, jhi;
-  jbox_rows(f.jbox, P, jlo, jhi);
+  jbox_rows(f.jbox, jlo, jhi);
   const bool jrow = iz >= jlo && iz <= jhi;
   const long long jphi = jrow ? f.Jphi[i] : 0;
   if (c.zero_j && jrow)
@@ -297,8 +296,8 @@ __global__ void k_antenna32(long long *J, int *jbox, int P, int direction, long 
   // antenna.c:398-415
   const int nd = direction == 1 ? (int)node((int)iposition, (int)i, P) : (int)node((int)i, (int)iposition, P);
   J[nd] += v;
-  atomicMin(jbox, nd);
-  atomicMax(jbox + 1, nd);
+  atomicMin(jbox, nd / P);
+  atomicMax(jbox + 1, nd / P);
 }
 
 __global__ void k_jbox_set(int *jbox, int lo, int hi)

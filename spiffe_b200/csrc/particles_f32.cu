@@ -404,15 +404,16 @@ __device__ void deposit_particle(const DevMesh &m, const DevFields32 &f, bool on
       }
     }
   }
-  // widen the box of nodes holding current (the FDTD reads and clears only
-  // its rows); a warp skips the atomics when the box already covers it
+  // widen the box of rows holding current (the FDTD reads and clears only
+  // those rows); a warp skips the atomics when the box already covers it
   lo = __reduce_min_sync(0xffffffffu, lo);
   hi = __reduce_max_sync(0xffffffffu, hi);
   if ((threadIdx.x & 31) == 0 && lo <= hi) {
-    if ((int)lo < f.jbox[0])
-      atomicMin(f.jbox, (int)lo);
-    if ((int)hi > f.jbox[1])
-      atomicMax(f.jbox + 1, (int)hi);
+    const int rlo = (int)(lo / (unsigned)m.pitch), rhi = (int)(hi / (unsigned)m.pitch);
+    if (rlo < f.jbox[0])
+      atomicMin(f.jbox, rlo);
+    if (rhi > f.jbox[1])
+      atomicMax(f.jbox + 1, rhi);
   }
 }
 

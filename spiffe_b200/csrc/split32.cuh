@@ -48,9 +48,9 @@ struct DevFields32 {
   long long *Jz, *Jr, *Jphi; // fixed point, quantum S32Scales::qJ
   double *Psi, *PsiImposed, *Q;
   long long *Qp; // particle charge per node (fixed point, quantum qQ) of the last correction
-  // The node indices iz*P+ir that may hold nonzero current: [0] lowest,
-  // [1] highest (empty when [0] > [1]).  Every deposit widens it; the FDTD
-  // step that zeroes J reads and clears only those rows, then empties it.
+  // The rows that may hold nonzero current: [0] lowest, [1] highest (empty
+  // when [0] > [1]).  Every deposit widens it; the FDTD step that zeroes J
+  // reads and clears only those rows, then empties it.
   int *jbox;
 };
 
@@ -95,7 +95,7 @@ extern "C" int s32_fdtd_tables(const DevMesh *m, const int16_t *host_flags, Fdtd
 extern "C" void s32_fdtd_tables_free(Fdtd32Tables *t);
 extern "C" int s32_fdtd_step(const DevMesh *m, const DevFields32 *f, const Fdtd32Tables *t, float kJ, int zero_j,
                              cudaStream_t s);
-// jbox = [lo, hi] (node indices; lo > hi: empty)
+// jbox = [lo, hi] (rows; lo > hi: empty)
 extern "C" int s32_jbox_set(int *jbox, int lo, int hi, cudaStream_t s);
 // FP64 host array (pitch nr+1) <-> FP32 device array (pitch P) through a device staging buffer
 extern "C" int s32_to_f32(const DevMesh *m, const double *d_staging, float *dst, cudaStream_t s);
