@@ -200,27 +200,36 @@ def test_sor_within_tolerance(oracle):
     assert rel_l2(out["Psi"], ref["Psi"]) <= SOR_TOL
 
 
-@pytest.mark.parametrize("accuracy", [1e-2, 5e-3, 2e-3, 1e-3])
-def test_sor_multi_cta_stop_and_undo(oracle, accuracy):
-    """A pillbox on a 601 x 321 mesh spreads the solve over every SM, with
-    several half-sweeps per grid barrier.  The stop rule fires inside a round
-    for some of these accuracies, and the later half-sweeps of that round are
-    undone: Psi must equal the oracle's after exactly as many half-sweeps as
-    the device reports, and the stop index must agree with the oracle's."""
-    cfg = workloads.PillboxConfig(nz=601, nr=321)
+@pytest.mark.parametrize("case", [("pillbox", 601, 321, a) for a in (1e-2, 5e-3, 2e-3, 1e-3)] +
+                         [("gun", 1400, 200, a) for a in (6e-3, 2e-2, 7e-3, 3e-2)])
+def test_sor_multi_cta_stop_and_undo(oracle, case):
+    """Meshes that spread the solve over every SM, with four half-sweeps per
+    grid barrier: a 601 x 321 pillbox (bands of 4-5 rows) and a 1400 x 200
+    gun (bands of 9-10 rows).  For these accuracies the stop rule fires at
+    each of the four positions in a round and the round's later half-sweeps
+    are undone.  Psi must equal the oracle's after exactly as many
+    half-sweeps as the device reports, and the stop index must agree with
+    the oracle's."""
+    kind, nz, nr, accuracy = case
+    if kind == "pillbox":
+        cfg = workloads.PillboxConfig(nz=nz, nr=nr)
+        zc, sig = 0.013, 0.003
+    else:
+        cfg = workloads.Gun16Config(nz=nz, nr=nr)
+        zc, sig = 0.05, 0.004
     f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(), modes=MODES)
     f.mesh.dt = cfg.dt
     z = np.arange(cfg.nz)[:, None] * cfg.dz
     r = np.arange(cfg.nr)[None, :] * cfg.dr
     q = np.zeros(f.shape)
-    q[: cfg.nz, : cfg.nr] = 1e6 * np.exp(-((z - 0.013) ** 2 + r ** 2) / (2 * 0.003 ** 2))
+    q[: cfg.nz, : cfg.nr] = 1e6 * np.exp(-((z - zc) ** 2 + r ** 2) / (2 * sig ** 2))
     f["Q"] = q
     f["Psi"] = np.zeros(f.shape)
     g = split(f)
-    n_g = g.solve_poisson(0, accuracy, 5000)
+    n_g = g.solve_poisson(0, accuracy, 20000)
     out = g.fields(f)
     ref = f.copy()
-    n_o, _, _ = oracle.solve_poisson(ref, ref["Psi"], ref["Q"], accuracy, 5000)
+    n_o, _, _ = oracle.solve_poisson(ref, ref["Psi"], ref["Q"], accuracy, 20000)
     assert n_o > 0 and abs(n_g - n_o) <= 2, (n_g, n_o)
     same = f.copy()
     oracle.solve_poisson(same, same["Psi"], same["Q"], 1e-300, n_g + 1)
