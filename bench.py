@@ -68,9 +68,10 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true", help="skip the end-to-end run (profiling captures)")
     p.add_argument("--cpu-steps", type=int, default=20, help="reference steps timed for the CPU baseline")
-    p.add_argument("--workload", default="gun16", choices=["gun16", "scan", "serve"],
-                   help="gun16: the benchmark (config 2); scan: a sample of the batched scan (config 4) run together; "
-                        "serve: a sample of the request stream (config 5) at several arrival rates")
+    p.add_argument("--workload", default="gun16", choices=["gun16", "dcgun", "scan", "serve"],
+                   help="gun16: the benchmark (config 2); dcgun: the DC gun (config 3), both forms; scan: a sample "
+                        "of the batched scan (config 4) run together; serve: a sample of the request stream "
+                        "(config 5) at several arrival rates")
     p.add_argument("--instances", type=int, default=64, help="scan: instances drawn from the scan distribution")
     p.add_argument("--scan-steps", type=int, default=500, help="scan/serve: integration steps per instance")
     p.add_argument("--workers", type=int, default=4, help="scan/serve: host threads driving instances")
@@ -458,6 +459,66 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def dcgun_arm(args):
+    """The DC gun (1501 x 1001 nodes, 4M particles, a Poisson correction
+    every step): --steps timed steps of the split form and half as many of
+    the FP64 form, on the same state after --warmup steps each."""
+    import torch
+
+    from spiffe_b200 import abi, gpu, workloads
+
+    torch.cuda.set_device(0)
+    cfg = workloads.DcGunConfig()
+    f, b = cfg.state()
+    push = abi.push_options(compaction=abi.COMPACT_SWAP, screen_momentum=abi.SCREEN_PARTICLE)
+    nodes = (cfg.nz + 1) * (cfg.nr + 1)
+    legs = {}
+    clk = None
+    for name, prec, K in (("split32", gpu.PRECISION_SPLIT32, args.steps),
+                          ("f64", gpu.PRECISION_F64, max(args.steps // 2, 3))):
+        g = gpu.GpuInstance(f, capacity=b.capacity, precision=prec)
+        g.upload_beam(b)
+        g.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
+        g.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
+        g.run_begin()
+        g.run_steps(args.warmup)
+        g.synchronize()
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(0)
+        g.set_profiling(True)
+        w0 = g.work_counters()
+        torch.cuda.synchronize()
+        clocks.start()
+        ev0.record(stream)
+        g.run_steps(K)
+        ev1.record(stream)
+        ev1.synchronize()
+        c = clocks.stop()
+        clk = clk or c
+        ms = ev0.elapsed_time(ev1)
+        w1 = g.work_counters()
+        phases = g.phase_times()
+        np_end, _ = g.counts()
+        g.close()
+        ps = w1["particle_steps"] - w0["particle_steps"]
+        legs[name] = {"steps": K, "ms_per_step": round(ms / K, 4), "particle_steps_per_s": round(ps / (ms / 1e3), 1),
+                      "cell_updates_per_s": round(nodes * K / (ms / 1e3), 1),
+                      "sor_halfsweeps_per_step": round((w1["sor_halfsweeps"] - w0["sor_halfsweeps"]) / K, 1),
+                      "particles_end": np_end,
+                      "phases_ms_per_step": {k: round(v[0] / K, 4) for k, v in phases.items() if v[1]}}
+    line = {"metric": "particle-steps/s & cell-updates/s of the DC gun (config 3)",
+            "value": legs["split32"]["particle_steps_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": legs["split32"]["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "DC gun, 1501x1001 nodes at 20um, 300 kV gap of 10 mm, 4,000,000 macroparticles "
+                                   "(0.5 nC, 100 ps flat top, already emitted), Poisson correction every step",
+                       "form": "split precision; plain FP64 leg on the same state"},
+            "cell_updates_per_s": legs["split32"]["cell_updates_per_s"], "legs": legs,
+            "split_over_f64": round(legs["f64"]["ms_per_step"] / legs["split32"]["ms_per_step"], 3), "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def scan_arm(args):
     """A sample of the batched scan: --instances drawn from its distribution,
     --scan-steps each, advanced together by the native scheduler on
@@ -534,6 +595,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         reference_arm(args)
+    elif args.workload == "dcgun":
+        dcgun_arm(args)
     elif args.workload == "scan":
         scan_arm(args)
     elif args.workload == "serve":

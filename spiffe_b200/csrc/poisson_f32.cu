@@ -868,14 +868,16 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
         total_sh = tlast;
         // Iterative refinement: fold d into Psi and form the residual again
         // in FP64 once the residual has fallen 2^8-fold below the last FP64
-        // residual (the base), or to within 8x of the FP32 rounding noise of
-        // its own terms.  That noise is about 2^-21 |e| sum |d| (each
-        // node's residual cancels terms of size |e d| rounded to 2^-24), so
-        // the FP32 sweeps stall there when d has grown large.  The
-        // fixed-point quantum of the residual sums is 2^-30 of the larger of
-        // the base and the stop threshold, so the stop test keeps its
-        // resolution as the base follows the residual down.
-        if (!last && (total_sh < base_sh * (1.0 / 256) || total_sh < tot[HD] * (1.0 / 262144))) {
+        // residual (the base), or to within 2^11 of the FP32 rounding noise
+        // of its own terms.  That noise is about 2^-21 |e| sum |d| (each
+        // node's residual cancels terms of size |e d| rounded to 2^-24);
+        // near it the FP32 residual sums lag the true ones and delay the
+        // stop rule (by up to 6 % of the half-sweeps on a 1400 x 200 gun mesh
+        // with a trigger 2^3 above the noise; within 2 half-sweeps of the
+        // FP64 count at 2^11).  The fixed-point quantum of the residual sums
+        // is 2^-30 of the larger of the base and the stop threshold, so the
+        // stop test keeps its resolution as the base follows the residual down.
+        if (!last && (total_sh < base_sh * (1.0 / 256) || total_sh < tot[HD] * (1.0 / 1024))) {
           rebase_sh = 1;
           base_sh = total_sh;
         }

@@ -258,3 +258,76 @@ class Gun16Config:
         from . import abi
 
         return abi.poisson_options(step_interval=self.step_interval, accuracy=1e-6, maximum_iterations=1000)
+
+
+class DcGunConfig:
+    """The DC gun workload: cathode plane at z=0 (0 V), anode plate at z=10 mm
+    with a 3 mm hole at 300 kV, an outer wall of radius 20 mm whose potential
+    ramps between them, drift to z=30 mm (dc_gun_geo); mesh dr=dz=20 um (1501
+    x 1001 nodes), dt = 0.5 x Courant.  Field: the imposed field of the
+    electrodes' Laplace solve, which the integration's start computes
+    (compute_imposed_Efield).  Beam: 0.5 nC as 4,000,000 macroparticles from a
+    2 mm disk (inside the anode hole), emitted from rest uniformly over a
+    100 ps flat top and already emitted: a particle emitted tau before t=0
+    sits where uniform acceleration by the gap field (V/gap) carries it, or,
+    past the anode, drifts with the gap's full energy.  Poisson correction
+    every step (accuracy 1e-6, at most 1000 iterations)."""
+
+    def __init__(self, nz=1501, nr=1001, length=0.030, radius=0.020, gap=0.010, voltage=300e3,
+                 n_macro=4_000_000, charge=0.5e-9, flat_top=100e-12, cathode_radius=2e-3, seed=2024):
+        self.nz, self.nr, self.length, self.radius = nz, nr, length, radius
+        self.zmin, self.zmax, self.rmax = 0.0, length, radius
+        self.dz = length / (nz - 1)
+        self.dr = radius / (nr - 1)
+        self.dt = 0.5 * min(self.dz, self.dr) / C_MKS / math.sqrt(2.0)
+        self.gap, self.voltage = gap, voltage
+        self.n_macro, self.charge, self.flat_top = n_macro, charge, flat_top
+        self.cathode_radius, self.seed = cathode_radius, seed
+
+    def geo_text(self):
+        return dc_gun_geo(cathode_radius=self.cathode_radius, gap=self.gap, wall=self.radius, length=self.length,
+                          voltage=self.voltage)
+
+    def beam_arrays(self):
+        rng = np.random.default_rng(self.seed)
+        n = self.n_macro
+        tau = rng.uniform(0.0, self.flat_top, n)
+        kappa = E_MKS * (self.voltage / self.gap) / (9.1093837015e-31 * C_MKS)
+        g_gap = 1 + E_MKS * self.voltage / (9.1093837015e-31 * C_MKS ** 2)  # gamma at the anode
+        p_gap = math.sqrt(g_gap ** 2 - 1)
+        tau_gap = p_gap / kappa  # time to cross the gap
+        pz = np.minimum(kappa * tau, p_gap)
+        gamma = np.sqrt(1 + pz ** 2)
+        z = np.where(tau < tau_gap, C_MKS / kappa * (gamma - 1),
+                     self.gap + C_MKS * p_gap / g_gap * (tau - tau_gap)) + 1e-9
+        r = self.cathode_radius * np.sqrt(rng.uniform(0, 1, n))
+        vz = C_MKS * pz / gamma
+        zeros = np.zeros(n)
+        return dict(z=z, r=r, pz=pz, pr=zeros, r_pphi=zeros, vz=vz, vr=zeros, vphi=zeros,
+                    Q=np.full(n, -self.charge / n), r0=r.copy(), z0=np.zeros(n), t0=-tau, rmin=r.copy(),
+                    rmax=r.copy(), zmin=np.zeros(n), zmax=z.copy(), particleID=np.arange(1, n + 1, dtype=np.int32),
+                    generation=np.zeros(n, np.int16), status=np.ones(n, np.uint64))
+
+    def screen_z(self):
+        return self.length - self.dz
+
+    def state(self, capacity_factor=1.25):
+        """Fields (flags and electrode potentials from the product's
+        define_geometry, no initial field) and the beam, as abi containers."""
+        from . import abi, geometry
+
+        modes = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP | abi.FL_SPACE_CHARGE
+        f = geometry.fields_for(self.nz, self.nr, self.zmin, self.zmax, self.rmax, self.geo_text(), modes=modes)
+        f.mesh.dt = self.dt
+        arrays = self.beam_arrays()
+        n = len(arrays["z"])
+        b = abi.Beam(int(n * capacity_factor))
+        b.set(n, **arrays)
+        b.npActive, b.nextParticleID, b.QoMC, b.stiffness = n, n + 1, -E_MKS / (9.1093837015e-31 * C_MKS), 1.0
+        return f, b
+
+    def poisson(self):
+        from . import abi
+
+        return abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+

