@@ -116,6 +116,13 @@ int spiffe_gpu_add_antenna(spiffe_gpu_instance *inst, int32_t direction, int64_t
                            int64_t iposition, double current, double frequency, double phase, const double *t,
                            const double *W, int64_t n_points);
 
+/* define_test_beam (test_beam.c:17-56): emission of test particles by the
+ * device integration loop.  NULL or electrons_per_macroparticle 0 removes it.
+ * The reference gives each test particle only a position, momenta, velocities
+ * and a charge (test_beam.c:91-103); the other values are those of a zeroed
+ * slot (particle ID 0, extrema 0, inactive until its first push). */
+int spiffe_gpu_set_test_beam(spiffe_gpu_instance *inst, const spiffe_test_beam_options *opt);
+
 /* perform_integration (integrate.c:24-194) on the device: configure, the
  * setup before the loop (:125-133), then any number of loop steps. */
 int spiffe_gpu_configure_run(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_push_options *push,

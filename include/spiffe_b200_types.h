@@ -87,6 +87,7 @@ typedef struct spiffe_beam_set {
 } spiffe_beam_set;
 
 /* Screen crossing records (SCREEN, spiffe.h:341-352; columns of screens.c:18). */
+#define SPIFFE_MAX_SCREENS 8 /* screens one instance records */
 #define SPIFFE_SCREEN_QUANS 8 /* r, pz, pr, pphi, t, q, r0, t0 */
 typedef struct spiffe_screen_set {
   double z_position;
@@ -138,6 +139,19 @@ typedef struct spiffe_poisson_options {
   int32_t verbosity;
   int32_t guess_code; /* 0 none, 1 line-charge, 2 point-charge, 3 zero */
 } spiffe_poisson_options;
+
+/* define_test_beam command (test_beam.nl, defaults test_beam.c:24-27): one
+ * macroparticle of electrons_per_macroparticle electrons is added every step
+ * from int((start_time-t0)/dt) to int((stop_time-t0)/dt) at (initial_z,
+ * initial_r) with the given momenta (emit_test_particles, test_beam.c:57-104).
+ * The forced acceleration (z_force, r_force and the deceleration starts) is
+ * part of spiffe_push_options. */
+typedef struct spiffe_test_beam_options {
+  double start_time, stop_time;
+  double initial_z, initial_r;
+  double initial_pz, initial_pr, initial_rpphi;
+  double electrons_per_macroparticle;
+} spiffe_test_beam_options;
 
 /* define_cathode command (cathode.nl:8-40, defaults cathode.c:32-40).  A
  * time profile, when given, is n_profile (t, factor) pairs in increasing t. */

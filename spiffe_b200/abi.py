@@ -138,6 +138,21 @@ class CathodeOptions(C.Structure):
         ("profile_t", D), ("profile_A", D)]
 
 
+class TestBeamOptions(C.Structure):
+    _fields_ = [
+        ("start_time", C.c_double), ("stop_time", C.c_double),
+        ("initial_z", C.c_double), ("initial_r", C.c_double),
+        ("initial_pz", C.c_double), ("initial_pr", C.c_double), ("initial_rpphi", C.c_double),
+        ("electrons_per_macroparticle", C.c_double)]
+
+
+class SolenoidOptions(C.Structure):
+    _fields_ = [
+        ("radius", C.c_double), ("evaluation_radius_limit", C.c_double), ("z_start", C.c_double),
+        ("z_end", C.c_double), ("current", C.c_double), ("Bz_peak", C.c_double),
+        ("turns", C.c_int64), ("symmetry", C.c_int32), ("bucking", C.c_int32), ("z_buck", C.c_double)]
+
+
 def _dptr(a):
     return a.ctypes.data_as(D) if a is not None else None
 

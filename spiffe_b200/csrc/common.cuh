@@ -13,8 +13,6 @@
 #include "../../include/spiffe_b200_constants.h"
 #include "../../include/spiffe_b200_types.h"
 
-#define SPIFFE_MAX_SCREENS 8
-
 // Per-instance scalars every kernel needs (the FIELDS scalars of spiffe.h).
 struct DevMesh {
   int nz, nr, pitch;

@@ -29,6 +29,35 @@ __global__ void __launch_bounds__(T) k_births(DevMesh m, DevFields<double> f, De
   }
   const long long ip = np + k;
   const double c = SPIFFE_C_MKS;
+  if (p.mode == SPIFFE_BIRTH_TEST) {
+    // test_beam.c:91-103 sets position, momenta, velocities and charge only;
+    // every other per-particle value is what a fresh (zeroed) slot holds, and
+    // the push activates the particle (advance_particles.c:165-187)
+    const double r = p.inner_radius, pz = p.pz0, pr = p.pr0, r_pphi = p.rpphi0;
+    double gamma, vphi;
+    if (r) {
+      gamma = sqrt(pz * pz + pr * pr + (r_pphi / r) * (r_pphi / r) + 1);
+      vphi = c * r_pphi / r / gamma;
+    } else {
+      gamma = sqrt(pz * pz + pr * pr + 1);
+      vphi = 0;
+    }
+    b.z[ip] = p.z_position;
+    b.r[ip] = r;
+    b.pz[ip] = pz;
+    b.pr[ip] = pr;
+    b.r_pphi[ip] = r_pphi;
+    b.vz[ip] = c * pz / gamma;
+    b.vr[ip] = c * pr / gamma;
+    b.vphi[ip] = vphi;
+    b.Q[ip] = p.Q;
+    b.z0[ip] = b.r0[ip] = b.t0[ip] = 0;
+    b.rmin[ip] = b.rmax[ip] = b.zmin[ip] = b.zmax[ip] = 0;
+    b.particleID[ip] = 0;
+    b.generation[ip] = 0;
+    b.status[ip] = 0;
+    return;
+  }
   double r, dte = 0;
   if (p.mode == 1) {
     int bin = 0;
@@ -95,11 +124,13 @@ __global__ void __launch_bounds__(T) k_births(DevMesh m, DevFields<double> f, De
   b.status[ip] = SPIFFE_PART_ACTIVE;
 }
 
-__global__ void k_births_commit(long long total, long long capacity, DevCounts *cnt)
+__global__ void k_births_commit(long long total, long long capacity, int test, DevCounts *cnt)
 {
   if (cnt->np + total > capacity)
     return;
   cnt->np += total;
+  if (test) // inactive and without an ID, test_beam.c:104
+    return;
   cnt->npActive += total;
   cnt->nextParticleID += total;
 }
@@ -125,7 +156,7 @@ extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, con
     return 0;
   k_births<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt);
   spiffe_note_launches(1);
-  k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, cnt);
+  k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode == SPIFFE_BIRTH_TEST, cnt);
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

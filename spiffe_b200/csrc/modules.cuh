@@ -74,6 +74,11 @@ struct BirthBin {
   long long start, count;
   double area, rmin;
 };
+// mode 0: uniform in r^2 from the generator; 1: per-bin counts (distribution
+// correction); 2: discrete radii; 3: test-beam particle (emit_test_particles,
+// test_beam.c:57-104) at (z_position, inner_radius) with momenta pz0, pr0,
+// rpphi0, inactive until the push activates it.
+#define SPIFFE_BIRTH_TEST 3
 struct BirthParams {
   long long total;
   uint64_t key, counter_base;
@@ -81,6 +86,7 @@ struct BirthParams {
   int spread;
   double z_position, inner_radius, outer_radius, inner_r2, dr2;
   double initial_vz, initial_omega, Q, time, dt, QoMC, stiffness;
+  double pz0, pr0, rpphi0;
   const BirthBin *bins;
   int n_bins;
 };

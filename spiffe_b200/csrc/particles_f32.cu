@@ -863,7 +863,37 @@ __global__ void __launch_bounds__(T) k_births32(DevMesh m, DevFields32 f, DevBea
     atomicOr(&cnt->error, SPIFFE_DEV_ERR_CAPACITY);
   int iz = 0, ir = 0;
   float fz = 0, fr = 0, bz = 0, br = 0, bphi = 0, qs = 0;
-  if (on) {
+  const bool test = p.mode == SPIFFE_BIRTH_TEST;
+  if (on && test) {
+    // test_beam.c:91-103: position, momenta and charge; the rest as a fresh
+    // slot holds it, inactive until the push activates it (no deposit)
+    const long long ip = np + k;
+    const double xz = (p.z_position - m.zmin) / m.dz, xr = p.inner_radius / m.dr;
+    iz = (int)floor(xz);
+    fz = (float)(xz - iz);
+    if (fz >= 1.f) {
+      fz = 0.f;
+      iz++;
+    }
+    ir = (int)floor(xr);
+    fr = (float)(xr - ir);
+    if (fr >= 1.f) {
+      fr = 0.f;
+      ir++;
+    }
+    b.cell[ip] = s32_cell(iz, ir);
+    b.fz[ip] = fz;
+    b.fr[ip] = fr;
+    b.pz[ip] = (float)p.pz0;
+    b.pr[ip] = (float)p.pr0;
+    b.rpphi[ip] = (float)p.rpphi0;
+    b.Q[ip] = (float)p.Q;
+    b.status[ip] = 0;
+    b.rmin[ip] = b.zmin[ip] = b.rmax[ip] = b.zmax[ip] = 0;
+    b.z0[ip] = b.r0[ip] = b.t0[ip] = 0;
+    b.particleID[ip] = 0;
+    b.generation[ip] = 0;
+  } else if (on) {
     const long long ip = np + k;
     const double c = SPIFFE_C_MKS;
     double r, dte = 0;
@@ -942,14 +972,16 @@ __global__ void __launch_bounds__(T) k_births32(DevMesh m, DevFields32 f, DevBea
     qs = b.Q[ip] * sc.s_charge;
   }
   if (deposit)
-    deposit_particle<false>(m, f, on, iz, fz, ir, fr, bz, br, bphi, qs);
+    deposit_particle<false>(m, f, on && !test, iz, fz, ir, fr, bz, br, bphi, qs);
 }
 
-__global__ void k_births_commit32(long long total, long long capacity, DevCounts *cnt)
+__global__ void k_births_commit32(long long total, long long capacity, int test, DevCounts *cnt)
 {
   if (cnt->np + total > capacity)
     return;
   cnt->np += total;
+  if (test) // inactive and without an ID, test_beam.c:104
+    return;
   cnt->npActive += total;
   cnt->nextParticleID += total;
 }
@@ -1195,7 +1227,7 @@ extern "C" int s32_births(const DevMesh *m, const DevFields32 *f, const DevBeam3
   if (p->total <= 0)
     return 0;
   k_births32<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt, *sc, deposit);
-  k_births_commit32<<<1, 1, 0, s>>>(p->total, b->capacity, cnt);
+  k_births_commit32<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode == SPIFFE_BIRTH_TEST, cnt);
   spiffe_note_launches(2);
   return (int)cudaGetLastError();
 }

@@ -109,6 +109,12 @@ struct HostCathode {
   std::vector<double> area, rmin;
 };
 
+// The test beam (TEST_BEAM_DEFN, spiffe.h); start_step -1 until the first step.
+struct HostTestBeam {
+  spiffe_test_beam_options o{};
+  long long start_step = -1, stop_step = -1;
+};
+
 struct HostAntenna {
   int direction;
   long istart, iend, iposition;
@@ -168,6 +174,7 @@ struct spiffe_gpu_instance {
   std::vector<HostCathode> cathodes;
   uint64_t rng_key = 0, rng_counter = 0;
   std::vector<HostAntenna> antennas;
+  HostTestBeam test_beam;
   double QoMC = 0, stiffness = 1;
   BirthBin *d_bins = nullptr, *h_bins = nullptr;
   size_t bins_n = 0;
@@ -1270,12 +1277,13 @@ extern "C" int spiffe_gpu_clear_screens(spiffe_gpu_instance *in)
 
 // ---------------------------------------------------------------- cathodes
 
-// process_cathode_definition, cathode.c:21-237.
-extern "C" int spiffe_gpu_add_cathode(spiffe_gpu_instance *in, const spiffe_cathode_options *o)
+// The checks of process_cathode_definition (cathode.c:43-81) that concern
+// the options the device loop uses.
+extern "C" int spiffe_cathode_check(const spiffe_mesh *mesh, const spiffe_cathode_options *o)
 {
-  if (!in || !o)
+  if (!mesh || !o)
     return fail(SPIFFE_ERR_INVALID, "null argument");
-  const spiffe_mesh &m = in->mesh;
+  const spiffe_mesh &m = *mesh;
   if (o->z_position < m.zmin || o->z_position > m.zmax)
     return fail(SPIFFE_ERR_INVALID, "cathode is outside of simulation region");
   if (o->inner_radius > o->outer_radius)
@@ -1309,6 +1317,16 @@ extern "C" int spiffe_gpu_add_cathode(spiffe_gpu_instance *in, const spiffe_cath
       if (o->profile_t[i - 1] >= o->profile_t[i])
         return fail(SPIFFE_ERR_INVALID, "profile data is not ordered by increasing time values");
   }
+  return 0;
+}
+
+// process_cathode_definition, cathode.c:21-237.
+extern "C" int spiffe_gpu_add_cathode(spiffe_gpu_instance *in, const spiffe_cathode_options *o)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const spiffe_mesh &m = in->mesh;
+  RC_TRY(spiffe_cathode_check(&m, o));
   long n = 1;
   if (o->field_emission) {
     if (o->inner_radius != 0)
@@ -1561,6 +1579,73 @@ static int emit(spiffe_gpu_instance *in)
   return 0;
 }
 
+// emit_test_particles, test_beam.c:57-104
+static int emit_test(spiffe_gpu_instance *in)
+{
+  HostTestBeam &t = in->test_beam;
+  if (t.o.electrons_per_macroparticle == 0)
+    return 0;
+  PhaseScope ps(in, PH_EMIT);
+  const spiffe_mesh &m = in->mesh;
+  if (t.start_step == -1) {
+    if (m.dt <= 0)
+      return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (emit_test_particles)");
+    t.start_step = (long long)((t.o.start_time - m.start_time) / m.dt);
+    t.stop_step = (long long)((t.o.stop_time - m.start_time) / m.dt);
+    in->QoMC = -SPIFFE_E_MKS / (SPIFFE_ME_MKS * SPIFFE_C_MKS);
+  }
+  if (!(t.start_step <= m.time_step && t.stop_step >= m.time_step))
+    return 0;
+  if (in->np_upper + 1 > in->capacity) {
+    RC_TRY(read_counts(in));
+    RC_TRY(grow_beam(in, in->h_cnt->np + 1));
+  }
+  BirthParams p{};
+  p.total = 1;
+  p.mode = SPIFFE_BIRTH_TEST;
+  p.z_position = t.o.initial_z;
+  p.inner_radius = t.o.initial_r;
+  p.pz0 = t.o.initial_pz;
+  p.pr0 = t.o.initial_pr;
+  p.rpphi0 = t.o.initial_rpphi;
+  p.Q = -SPIFFE_E_MKS * t.o.electrons_per_macroparticle;
+  p.time = m.time;
+  p.dt = m.dt;
+  int rc;
+  if (in->s32) {
+    S32State &S = *in->s32;
+    RC_TRY(s32_cover_charge(in, std::fabs(p.Q)));
+    rc = s32_births(&in->dm, &S.f, &S.b, &p, in->cnt, &S.sc, 0, in->stream);
+  } else {
+    rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+  }
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "test-beam launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  in->np_upper += 1;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_test_beam(spiffe_gpu_instance *in, const spiffe_test_beam_options *o)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  in->test_beam = HostTestBeam{};
+  if (!o || o->electrons_per_macroparticle == 0)
+    return 0;
+  const spiffe_mesh &m = in->mesh;
+  // test_beam.c:32-41
+  if (o->initial_z < m.zmin || o->initial_z > m.zmax)
+    return fail(SPIFFE_ERR_INVALID, "test beam initial_z is outside of simulation region");
+  if (o->initial_r < 0 || o->initial_r > m.rmax)
+    return fail(SPIFFE_ERR_INVALID, "test beam initial_r is outside of simulation region");
+  if (o->start_time >= o->stop_time)
+    return fail(SPIFFE_ERR_INVALID, "start_time >= stop_time for test beam");
+  if (o->electrons_per_macroparticle < 0)
+    return fail(SPIFFE_ERR_INVALID, "electrons_per_macroparticle <= 0 for test beam");
+  in->test_beam.o = *o;
+  return 0;
+}
+
 // set_current_density, cathode.c:673-715
 static int set_current_density(spiffe_gpu_instance *in)
 {
@@ -1721,6 +1806,7 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
       RC_TRY(imposed_efield(in, &in->pc, 0));
     m.time = m.time_step * m.dt + m.start_time;
     RC_TRY(emit(in));
+    RC_TRY(emit_test(in));
     S32State *S = in->s32;
     if (!S) {
       RC_TRY(spiffe_gpu_zero_current_arrays(in));

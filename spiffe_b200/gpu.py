@@ -79,6 +79,17 @@ def load():
         "spiffe_gpu_work_counters": ([H, P(C.c_int64)], C.c_int),
         "spiffe_gpu_set_sort_interval": ([H, C.c_int64], C.c_int),
         "spiffe_gpu_batch_run": ([P(H), C.c_int32, P(C.c_int64), C.c_int32, C.c_int64, P(C.c_double)], C.c_int),
+        "spiffe_gpu_set_test_beam": ([H, P(abi.TestBeamOptions)], C.c_int),
+        "spiffe_session_create": ([C.c_int32, C.c_char_p, P(H)], C.c_int),
+        "spiffe_session_destroy": ([H], C.c_int),
+        "spiffe_session_execute": ([H, C.c_char_p], C.c_int),
+        "spiffe_session_run_file": ([H, C.c_char_p], C.c_int),
+        "spiffe_session_set": ([H, C.c_char_p, C.c_double], C.c_int),
+        "spiffe_session_mesh": ([H, M], C.c_int),
+        "spiffe_session_fields": ([H, F], C.c_int),
+        "spiffe_session_instance": ([H, P(H)], C.c_int),
+        "spiffe_session_steps": ([H], C.c_int64),
+        "spiffe_solenoid_add": ([M, P(abi.SolenoidOptions), P(C.c_double), P(C.c_double), P(C.c_double)], C.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -131,10 +142,22 @@ class GpuInstance:
         self.h = h
         self.upload_fields(fields)
 
+    @classmethod
+    def attach(cls, handle, precision):
+        """A view of an instance another owner (a session) created and destroys."""
+        g = cls.__new__(cls)
+        g.lib = load()
+        g.precision = precision
+        g.h = handle
+        g.borrowed = True
+        g.mesh = g.get_mesh()
+        g.shape = (g.mesh.nz + 1, g.mesh.nr + 1)
+        return g
+
     def close(self):
-        if getattr(self, "h", None):
+        if getattr(self, "h", None) and not getattr(self, "borrowed", False):
             self.lib.spiffe_gpu_destroy(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -221,6 +244,10 @@ class GpuInstance:
 
     def add_cathode(self, opts):
         _check(self.lib.spiffe_gpu_add_cathode(self.h, C.byref(opts)))
+
+    def set_test_beam(self, opts):
+        """define_test_beam's emission (abi.TestBeamOptions, or None to remove it)."""
+        _check(self.lib.spiffe_gpu_set_test_beam(self.h, C.byref(opts) if opts is not None else None))
 
     def add_antenna(self, direction, istart, iend, iposition, current, frequency, phase, t, W):
         t = np.ascontiguousarray(t, np.float64)

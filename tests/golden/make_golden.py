@@ -7,7 +7,8 @@ synthetic inputs (spiffe_b200.workloads).  Inputs and outputs are stored
 together so the oracle and the CUDA path can be checked without the
 reference present.  Run from the repository root:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          # every fixture
+    python tests/golden/make_golden.py decks    # the input-deck fixtures only
 """
 import os
 import sys
@@ -160,5 +161,57 @@ def main():
     save("dcgun_geometry", flags=flags2, PsiImposed=psi_imp0, geo=np.array(geo), **mesh_arrays(mesh2))
 
 
+# Input decks run through the reference's own command processors and
+# perform_integration (spiffe.c:213-308), for the command session.  The DC
+# gun deck exercises the imposed-field ramp, a ring-coil solenoid, constant
+# fields, a cathode with distribution correction, a screen and periodic
+# Poisson correction; the test-beam deck exercises define_test_beam's
+# emission and forced acceleration.  One screen each: the reference gives
+# buffers to the first screen only (advance_particles.c:343-359 clears its
+# allocation flag inside the screen loop), so a second screen that records a
+# crossing writes through a null pointer.
+DECK_DCGUN = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02, boundary="dc.geo" &end
+&define_solenoid radius=0.025, z_start=0.012, z_end=0.02, turns=4, current=1000, Bz_peak=0.03 &end
+&set_constant_fields Br=1e-4 &end
+&define_cathode z_position=1e-6, outer_radius=0.002, current_density=2e6, start_time=0, stop_time=40e-12,
+    number_per_step=10, initial_pz=1e-6, distribution_correction_interval=1 &end
+&define_screen filename="deck.sc1", z_position=0.012, direction="forward" &end
+&poisson_correction step_interval=4, accuracy=1e-4, error_charge_threshold=1e-15 &end
+&integrate dt_integration=4e-13, start_time=0, finish_time=300e-12, space_charge=1, imposed_Efield_ramp_time=20e-12 &end
+"""
+
+DECK_TESTBEAM = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02, boundary="dc.geo" &end
+&define_test_beam start_time=0, stop_time=30e-12, initial_z=0.0005, initial_r=0.0012, initial_pz=0.02,
+    initial_pr=0.001, initial_rpphi=1e-7, electrons_per_macroparticle=2e5, z_force=5e9, r_force=1e8,
+    z_start_deceleration=0.02, r_start_deceleration=0.003 &end
+&define_screen filename="tb.sc1", z_position=0.012, direction="forward" &end
+&poisson_correction step_interval=4, accuracy=1e-4, error_charge_threshold=1e-15 &end
+&integrate dt_integration=4e-13, start_time=0, finish_time=200e-12, space_charge=1 &end
+"""
+
+
+def decks():
+    geo = str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"])
+    for name, deck, screens in (("deck_dcgun", DECK_DCGUN, 1), ("deck_testbeam", DECK_TESTBEAM, 1)):
+        d = tempfile.mkdtemp()
+        with open(os.path.join(d, "dc.geo"), "w") as f:
+            f.write(geo)
+        cmds = [b.strip() + " &end" for b in deck.split("&end") if b.strip()]
+        prog = [("command", c) for c in cmds] + [("mesh",), ("get_beam",)]
+        prog += [("screen", i) for i in range(screens)]
+        prog += [("get_field", n) for n in ("Ez", "Er", "Bphi", "Psi")]
+        res = pyoracle.run_reference(prog, cwd=d, capacity=20000)
+        mesh, rb, scr, fields = res[0], res[1], res[2:2 + screens], res[2 + screens:]
+        out = dict(deck=np.array(deck), geo=np.array(geo), time=mesh["time"], **beam_out(rb))
+        for i, rs in enumerate(scr):
+            out.update({f"screen{i}_{k}": v for k, v in rs.items()})
+        out.update(dict(zip(("Ez", "Er", "Bphi", "Psi"), fields)))
+        save(name, **out)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["decks"]:
+        decks()
+    else:
+        main()
+        decks()
