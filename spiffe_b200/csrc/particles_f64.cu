@@ -653,14 +653,22 @@ __device__ void contrib_jphi(const DevMesh &m, double z, double r, double v, dou
 }
 
 // component: 0 Jz, 1 Jr, 2 Jphi.  keys/vals != nullptr selects the ordered
-// mode: slot 4*ip+k receives contribution k (key = node, or INT_MAX).
+// mode: slot 4*ip+k receives contribution k (key = node, or INT_MAX) for
+// every ip below the host's bound n_slots, so slots past the live np (after
+// losses) hold padding rather than an earlier step's contributions.
 __global__ void __launch_bounds__(T) k_deposit(DevMesh m, DevFields<double> f, DevBeam64 b, const DevCounts *cnt,
-                                                int component, int *keys, double *vals)
+                                                int component, int *keys, double *vals, long long n_slots)
 {
   const long ip = (long)blockIdx.x * T + threadIdx.x;
   const long np = (long)cnt->np;
-  if (ip >= np)
+  if (ip >= np) {
+    if (keys && ip < n_slots)
+      for (int k = 0; k < 4; k++) {
+        keys[4 * ip + k] = 0x7fffffff;
+        vals[4 * ip + k] = 0.0;
+      }
     return;
+  }
   Contrib c;
   c.n = 0;
   if (b.status[ip] & SPIFFE_PART_ACTIVE) {
@@ -859,12 +867,12 @@ extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, co
     if (comp == 2 && !(m->modes & SPIFFE_FL_TE_FIELDS))
       continue;
     if (!ordered) {
-      k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, nullptr, nullptr);
+      k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, nullptr, nullptr, 0);
       spiffe_note_launches(1);
       continue;
     }
     const int n = (int)(4 * np_bound);
-    k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, w->keys, w->vals);
+    k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, w->keys, w->vals, np_bound);
     spiffe_note_launches(1);
     // stable LSD radix sort keeps particle order inside each node's run;
     // the INT_MAX pad key sorts last within the 31-bit key space

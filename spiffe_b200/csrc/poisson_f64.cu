@@ -181,9 +181,27 @@ __global__ void k_finish_sum(const double *part, int n, int stride, double *out)
     *out = sh[0];
 }
 
-// error-charge threshold test (:258-265)
-__global__ void k_pc_decide(PcState *st, double threshold)
+// error-charge threshold test (:258-265).  The reference sums Qerror
+// serially, iz outer and ir inner (:245-248); the device's tree sum of the
+// same values differs from it by at most 2 gamma_(n-1) sum|Q| (n terms,
+// gamma_k = k u / (1 - k u), u = 2^-53).  When |Qerror| is farther than that
+// from a positive threshold the decision is the reference's; otherwise (an
+// error charge at the level of rounding noise, as with no particles left)
+// this thread redoes the sum in the reference's order.
+__global__ void k_pc_decide(PcState *st, double threshold, const double *Q, int nz, int nr, int P,
+                            const double *abs_sum)
 {
+  if (threshold > 0 && abs_sum) {
+    const double n = (double)nz * (double)nr, u = 1.1102230246251565e-16;
+    const double margin = 2.0 * (n * u / (1.0 - n * u)) * *abs_sum * 1.0001 + 1e-300;
+    if (fabs(fabs(st->Qerror) - threshold) <= margin) {
+      double q = 0;
+      for (int iz = 0; iz < nz; iz++)
+        for (int ir = 0; ir < nr; ir++)
+          q += Q[node(iz, ir, P)];
+      st->Qerror = q;
+    }
+  }
   const double Qerror = st->Qerror, Qreal = st->Qreal;
   int skip = (threshold > 0 && fabs(Qerror) < threshold) ||
              (threshold < 0 && (Qreal == 0 || fabs(Qerror / Qreal) < fabs(threshold)));
@@ -646,9 +664,13 @@ extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<dou
     cudaMemsetAsync(w->scalars + 2, 0, sizeof(double), s);
   }
   sum_region(f->Q, m->nz, m->nr, m->pitch, 0, w, w->scalars + 3, s);
+  const bool bound = o->error_charge_threshold > 0;
+  if (bound)
+    sum_region(f->Q, m->nz, m->nr, m->pitch, 1, w, w->scalars + 5, s);
   k_set_state<<<1, 1, 0, s>>>(w->st, w->scalars, w->scalars + 2, w->scalars + 3, o->space_charge);
   spiffe_note_launches(1);
-  k_pc_decide<<<1, 1, 0, s>>>(w->st, o->error_charge_threshold);
+  k_pc_decide<<<1, 1, 0, s>>>(w->st, o->error_charge_threshold, f->Q, m->nz, m->nr, m->pitch,
+                              bound ? w->scalars + 5 : nullptr);
   spiffe_note_launches(1);
   k_scale_rhs<<<grid, block, 0, s>>>(*m, *f, w->volume, w->st);
   spiffe_note_launches(1);
