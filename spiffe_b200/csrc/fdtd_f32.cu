@@ -41,19 +41,19 @@ __device__ __forceinline__ void jbox_reset(int *jbox)
   }
 }
 
-__global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coef32 c)
+// ---- TM update, one node at a time: the boundary rows and columns
+// (copies to the axis, the top and the end rows) and the cells next to them.
+
+// Ez and Er of node (iz, ir), 0 <= iz <= nz, 0 <= ir <= nr; J rows jlo..jhi
+__device__ __forceinline__ void tm_e_node(const DevMesh &m, const DevFields32 &f, const Coef32 &c, int iz, int ir,
+                                          int jlo, int jhi)
 {
-  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
   const int nz = m.nz, nr = m.nr, P = m.pitch;
-  if (ir > nr || iz > nz)
-    return;
   const size_t i = node(iz, ir, P);
   const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
   const bool ez_row = ir < nr && iz >= 1 && iz <= nz - 1, er_row = iz <= nz - 1;
   // every load before any store, so no store can order the loads behind it;
   // J is read (and cleared) only on the rows a deposit touched
-  int jlo, jhi;
-  jbox_rows(f.jbox, jlo, jhi);
   const bool jrow = iz >= jlo && iz <= jhi;
   const uint8_t u = f.umask[i];
   const long long jz = jrow ? f.Jz[i] : 0, jr = jrow ? f.Jr[i] : 0;
@@ -98,14 +98,10 @@ __global__ void __launch_bounds__(BX *BY) k_tm_e32(DevMesh m, DevFields32 f, Coe
   }
 }
 
-__global__ void __launch_bounds__(BX *BY) k_tm_b32(DevMesh m, DevFields32 f, Coef32 c)
+// Bphi and Bphi2 of node (iz, ir), 1 <= iz <= nz-1, 0 <= ir <= nr
+__device__ __forceinline__ void tm_b_node(const DevMesh &m, const DevFields32 &f, const Coef32 &c, int iz, int ir)
 {
-  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
   const int nz = m.nz, nr = m.nr, P = m.pitch;
-  if (c.reset_box)
-    jbox_reset(f.jbox);
-  if (ir > nr || iz < 1 || iz > nz - 1)
-    return;
   const bool leftN = m.left_bc == SPIFFE_NEUMANN, rightN = m.right_bc == SPIFFE_NEUMANN;
   const size_t i = node(iz, ir, P);
   float b = f.Bphi[i], b2;
@@ -159,6 +155,208 @@ __global__ void __launch_bounds__(BX *BY) k_tm_b32(DevMesh m, DevFields32 f, Coe
       f.Bphi[node(nz, nr, P)] = rightN ? b : -b;
       f.Bphi2[node(nz, nr, P)] = rightN ? b2 : -b2;
     }
+  }
+}
+
+// ---- TM update, four columns per thread.  The launch has two kinds of
+// blocks.  Interior tiles: a warp covers 32 groups of four consecutive
+// columns of one row in 2 <= iz <= nz-2, every node of which is an ordinary
+// interior node (no boundary copy); 16-byte loads and stores move four nodes
+// at a time (rows start on 128-byte boundaries), every load is issued before
+// the one shuffle that passes the neighbour column between lanes, so a thread
+// waits for memory once.  Boundary blocks: one node per thread, with the
+// per-node code above, over the rows and columns the tiles leave out.
+constexpr int VX = 32, VY = 8, VW = 4; // lanes per row segment, rows per tile, columns per group
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+
+// Work split of one TM kernel.  Groups g = 1..G cover columns 4..4G+3; the
+// boundary columns are 0..left-1 and right..nr; rows 2..nz-2 are interior.
+struct TmSplit {
+  int G, tiles_x, tiles, left, right, W; // W: boundary nodes per interior row
+  int nrows_b;                           // boundary rows (E: outside 2..nz-2; B: rows 1 and nz-1)
+  long long nb;                          // boundary nodes in all
+};
+
+__host__ __device__ inline TmSplit tm_split(int nz, int nr, bool b_kernel)
+{
+  TmSplit t;
+  const int last = b_kernel ? nr - 3 : nr - 2; // last column a group may reach
+  t.G = last >= 7 ? (last - 3) / VW : 0;
+  const int ni = nz - 3 > 0 ? nz - 3 : 0; // interior rows 2..nz-2
+  t.tiles_x = (t.G + VX - 1) / VX;
+  t.tiles = t.G > 0 ? t.tiles_x * ((ni + VY - 1) / VY) : 0;
+  t.left = nr + 1 < VW ? nr + 1 : VW;
+  t.right = t.G > 0 ? VW * t.G + VW : t.left;
+  t.W = t.left + (nr + 1 - t.right);
+  if (t.G == 0) // rows are boundary throughout
+    t.W = nr + 1;
+  if (b_kernel)
+    t.nrows_b = nz >= 3 ? 2 : (nz == 2 ? 1 : 0);
+  else
+    t.nrows_b = (nz + 1) - ni;
+  t.nb = (long long)t.nrows_b * (nr + 1) + (long long)ni * t.W;
+  return t;
+}
+
+// boundary node k of the split -> (iz, ir)
+__device__ __forceinline__ void tm_boundary_node(const TmSplit &t, int nz, int nr, bool b_kernel, long long k, int &iz,
+                                                 int &ir)
+{
+  const long long nrow = (long long)t.nrows_b * (nr + 1);
+  if (k < nrow) {
+    const int r = (int)(k / (nr + 1));
+    ir = (int)(k % (nr + 1));
+    if (b_kernel)
+      iz = r == 0 ? 1 : nz - 1;
+    else
+      iz = r < 2 ? r : nz - (t.nrows_b - 1 - r);
+  } else {
+    k -= nrow;
+    iz = 2 + (int)(k / t.W);
+    const int c = (int)(k % t.W);
+    ir = t.G == 0 ? c : (c < t.left ? c : t.right + (c - t.left));
+  }
+}
+
+__global__ void __launch_bounds__(VX *VY) k_tm_e32(DevMesh m, DevFields32 f, Coef32 c, TmSplit t)
+{
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  int jlo, jhi;
+  jbox_rows(f.jbox, jlo, jhi);
+  if ((int)blockIdx.x >= t.tiles) {
+    const long long k = (long long)(blockIdx.x - t.tiles) * (VX * VY) + threadIdx.y * VX + threadIdx.x;
+    if (k < t.nb) {
+      int iz, ir;
+      tm_boundary_node(t, nz, nr, false, k, iz, ir);
+      tm_e_node(m, f, c, iz, ir, jlo, jhi);
+    }
+    return;
+  }
+  const int tx = blockIdx.x % t.tiles_x, ty = blockIdx.x / t.tiles_x;
+  const int g = 1 + tx * VX + threadIdx.x, iz = 2 + ty * VY + threadIdx.y;
+  if (iz > nz - 2) // whole warps: a warp is one row segment
+    return;
+  const int ir0 = g * VW;
+  const bool mine = g <= t.G, in_row = ir0 <= nr;
+  const size_t i = node(iz, ir0, P);
+  const bool jrow = iz >= jlo && iz <= jhi;
+  // every load first; the next group's first Bphi comes from the next lane
+  float4 b0 = make_float4(0.f, 0.f, 0.f, 0.f), ez = b0, er = b0, bP = b0, cp = b0, cm = b0;
+  uchar4 u = make_uchar4(0, 0, 0, 0);
+  longlong2 z01 = make_longlong2(0, 0), z23 = z01, r01 = z01, r23 = z01;
+  float bnext = 0.f;
+  if (in_row)
+    b0 = ldg4(f.Bphi + i);
+  if (mine) {
+    u = __ldg(reinterpret_cast<const uchar4 *>(f.umask + i));
+    ez = ld4(f.Ez + i);
+    er = ld4(f.Er + i);
+    bP = ldg4(f.Bphi + i + P);
+    cp = ldg4(c.cpd + ir0);
+    cm = ldg4(c.cmd + ir0);
+    if (jrow) {
+      z01 = *reinterpret_cast<const longlong2 *>(f.Jz + i);
+      z23 = *reinterpret_cast<const longlong2 *>(f.Jz + i + 2);
+      r01 = *reinterpret_cast<const longlong2 *>(f.Jr + i);
+      r23 = *reinterpret_cast<const longlong2 *>(f.Jr + i + 2);
+    }
+    if (threadIdx.x == VX - 1)
+      bnext = __ldg(f.Bphi + i + VW); // ir0 + 4 <= nr - 1: inside the row
+  }
+  const float bsh = __shfl_down_sync(0xffffffffu, b0.x, 1);
+  if (!mine)
+    return;
+  if (threadIdx.x != VX - 1)
+    bnext = bsh;
+  const float jz0 = (float)z01.x, jz1 = (float)z01.y, jz2 = (float)z23.x, jz3 = (float)z23.y;
+  const float jr0 = (float)r01.x, jr1 = (float)r01.y, jr2 = (float)r23.x, jr3 = (float)r23.y;
+  // integrate.c:323-344 and :362-368 on four interior nodes
+  if (u.x & S32_U_EZ) ez.x += c.kJ * jz0 + (cp.x * b0.y - cm.x * b0.x);
+  if (u.y & S32_U_EZ) ez.y += c.kJ * jz1 + (cp.y * b0.z - cm.y * b0.y);
+  if (u.z & S32_U_EZ) ez.z += c.kJ * jz2 + (cp.z * b0.w - cm.z * b0.z);
+  if (u.w & S32_U_EZ) ez.w += c.kJ * jz3 + (cp.w * bnext - cm.w * b0.w);
+  if (u.x & S32_U_ER) er.x += c.kJ * jr0 - c.fEr * (bP.x - b0.x);
+  if (u.y & S32_U_ER) er.y += c.kJ * jr1 - c.fEr * (bP.y - b0.y);
+  if (u.z & S32_U_ER) er.z += c.kJ * jr2 - c.fEr * (bP.z - b0.z);
+  if (u.w & S32_U_ER) er.w += c.kJ * jr3 - c.fEr * (bP.w - b0.w);
+  st4(f.Ez + i, ez);
+  st4(f.Er + i, er);
+  if (c.zero_j && jrow) {
+    const longlong2 zero = make_longlong2(0, 0);
+    *reinterpret_cast<longlong2 *>(f.Jz + i) = zero;
+    *reinterpret_cast<longlong2 *>(f.Jz + i + 2) = zero;
+    *reinterpret_cast<longlong2 *>(f.Jr + i) = zero;
+    *reinterpret_cast<longlong2 *>(f.Jr + i + 2) = zero;
+  }
+}
+
+__global__ void __launch_bounds__(VX *VY) k_tm_b32(DevMesh m, DevFields32 f, Coef32 c, TmSplit t)
+{
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  if (c.reset_box)
+    jbox_reset(f.jbox);
+  if ((int)blockIdx.x >= t.tiles) {
+    const long long k = (long long)(blockIdx.x - t.tiles) * (VX * VY) + threadIdx.y * VX + threadIdx.x;
+    if (k < t.nb) {
+      int iz, ir;
+      tm_boundary_node(t, nz, nr, true, k, iz, ir);
+      tm_b_node(m, f, c, iz, ir);
+    }
+    return;
+  }
+  const int tx = blockIdx.x % t.tiles_x, ty = blockIdx.x / t.tiles_x;
+  const int g = 1 + tx * VX + threadIdx.x, iz = 2 + ty * VY + threadIdx.y;
+  if (iz > nz - 2) // whole warps
+    return;
+  const int ir0 = g * VW;
+  const bool mine = g <= t.G, in_row = ir0 <= nr;
+  const size_t i = node(iz, ir0, P);
+  // every load first; the previous group's last Ez comes from the previous lane
+  float4 ez = make_float4(0.f, 0.f, 0.f, 0.f), er = ez, erm = ez, b = ez;
+  uchar4 u = make_uchar4(0, 0, 0, 0);
+  float eprev = 0.f;
+  if (in_row)
+    ez = ldg4(f.Ez + i);
+  if (mine) {
+    u = __ldg(reinterpret_cast<const uchar4 *>(f.umask + i));
+    er = ldg4(f.Er + i);
+    erm = ldg4(f.Er + i - P);
+    b = ld4(f.Bphi + i);
+    if (threadIdx.x == 0)
+      eprev = __ldg(f.Ez + i - 1); // ir0 - 1 >= 3: inside the row
+  }
+  const float esh = __shfl_up_sync(0xffffffffu, ez.w, 1);
+  if (!mine)
+    return;
+  if (threadIdx.x != 0)
+    eprev = esh;
+  // integrate.c:391-394 on four interior nodes
+  const float dBx = c.dt_dr * (ez.x - eprev) - c.dt_dz * (er.x - erm.x);
+  const float dBy = c.dt_dr * (ez.y - ez.x) - c.dt_dz * (er.y - erm.y);
+  const float dBz = c.dt_dr * (ez.z - ez.y) - c.dt_dz * (er.z - erm.z);
+  const float dBw = c.dt_dr * (ez.w - ez.z) - c.dt_dz * (er.w - erm.w);
+  const bool ux = u.x & S32_U_BPHI, uy = u.y & S32_U_BPHI, uz = u.z & S32_U_BPHI, uw = u.w & S32_U_BPHI;
+  float4 b2;
+  b2.x = b.x + 0.5f * dBx;
+  b2.y = b.y + 0.5f * dBy;
+  b2.z = b.z + 0.5f * dBz;
+  b2.w = b.w + 0.5f * dBw;
+  if (ux && uy && uz && uw) {
+    b.x += dBx;
+    b.y += dBy;
+    b.z += dBz;
+    b.w += dBw;
+    st4(f.Bphi2 + i, b2);
+    st4(f.Bphi + i, b);
+  } else {
+    // a node that is not updated keeps both of its values (next to metal)
+    if (ux) { f.Bphi2[i] = b2.x; f.Bphi[i] = b.x + dBx; }
+    if (uy) { f.Bphi2[i + 1] = b2.y; f.Bphi[i + 1] = b.y + dBy; }
+    if (uz) { f.Bphi2[i + 2] = b2.z; f.Bphi[i + 2] = b.z + dBz; }
+    if (uw) { f.Bphi2[i + 3] = b2.w; f.Bphi[i + 3] = b.w + dBw; }
   }
 }
 
@@ -411,8 +609,11 @@ extern "C" int s32_fdtd_step(const DevMesh *m, const DevFields32 *f, const Fdtd3
   const dim3 block(BX, BY), grid = grid_for(m, m->nr + 1);
   if (m->modes & SPIFFE_FL_TM_FIELDS) {
     c.reset_box = zero_j && !(m->modes & SPIFFE_FL_TE_FIELDS);
-    k_tm_e32<<<grid, block, 0, s>>>(*m, *f, c);
-    k_tm_b32<<<grid, block, 0, s>>>(*m, *f, c);
+    const TmSplit te = tm_split(m->nz, m->nr, false), tb = tm_split(m->nz, m->nr, true);
+    const int per = VX * VY;
+    const dim3 vblock(VX, VY);
+    k_tm_e32<<<te.tiles + (unsigned)((te.nb + per - 1) / per), vblock, 0, s>>>(*m, *f, c, te);
+    k_tm_b32<<<tb.tiles + (unsigned)((tb.nb + per - 1) / per), vblock, 0, s>>>(*m, *f, c, tb);
     spiffe_note_launches(2);
   }
   if (m->modes & SPIFFE_FL_TE_FIELDS) {
