@@ -165,7 +165,8 @@ __device__ __forceinline__ void tm_b_node(const DevMesh &m, const DevFields32 &f
 // at a time (rows start on 128-byte boundaries), every load is issued before
 // the one shuffle that passes the neighbour column between lanes, so a thread
 // waits for memory once.  Boundary blocks: one node per thread, with the
-// per-node code above, over the rows and columns the tiles leave out.
+// per-node code above, over the rows and columns the tiles leave out; they
+// take the first block indices, so they run beside the tiles.
 constexpr int VX = 32, VY = 8, VW = 4; // lanes per row segment, rows per tile, columns per group
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -226,8 +227,10 @@ __global__ void __launch_bounds__(VX *VY) k_tm_e32(DevMesh m, DevFields32 f, Coe
   const int nz = m.nz, nr = m.nr, P = m.pitch;
   int jlo, jhi;
   jbox_rows(f.jbox, jlo, jhi);
-  if ((int)blockIdx.x >= t.tiles) {
-    const long long k = (long long)(blockIdx.x - t.tiles) * (VX * VY) + threadIdx.y * VX + threadIdx.x;
+  // the boundary blocks come first, so they run beside the tiles, not after them
+  const int nbb = (int)((t.nb + VX * VY - 1) / (VX * VY));
+  if ((int)blockIdx.x < nbb) {
+    const long long k = (long long)blockIdx.x * (VX * VY) + threadIdx.y * VX + threadIdx.x;
     if (k < t.nb) {
       int iz, ir;
       tm_boundary_node(t, nz, nr, false, k, iz, ir);
@@ -235,7 +238,8 @@ __global__ void __launch_bounds__(VX *VY) k_tm_e32(DevMesh m, DevFields32 f, Coe
     }
     return;
   }
-  const int tx = blockIdx.x % t.tiles_x, ty = blockIdx.x / t.tiles_x;
+  const int tile = blockIdx.x - nbb;
+  const int tx = tile % t.tiles_x, ty = tile / t.tiles_x;
   const int g = 1 + tx * VX + threadIdx.x, iz = 2 + ty * VY + threadIdx.y;
   if (iz > nz - 2) // whole warps: a warp is one row segment
     return;
@@ -298,8 +302,9 @@ __global__ void __launch_bounds__(VX *VY) k_tm_b32(DevMesh m, DevFields32 f, Coe
   const int nz = m.nz, nr = m.nr, P = m.pitch;
   if (c.reset_box)
     jbox_reset(f.jbox);
-  if ((int)blockIdx.x >= t.tiles) {
-    const long long k = (long long)(blockIdx.x - t.tiles) * (VX * VY) + threadIdx.y * VX + threadIdx.x;
+  const int nbb = (int)((t.nb + VX * VY - 1) / (VX * VY));
+  if ((int)blockIdx.x < nbb) {
+    const long long k = (long long)blockIdx.x * (VX * VY) + threadIdx.y * VX + threadIdx.x;
     if (k < t.nb) {
       int iz, ir;
       tm_boundary_node(t, nz, nr, true, k, iz, ir);
@@ -307,7 +312,8 @@ __global__ void __launch_bounds__(VX *VY) k_tm_b32(DevMesh m, DevFields32 f, Coe
     }
     return;
   }
-  const int tx = blockIdx.x % t.tiles_x, ty = blockIdx.x / t.tiles_x;
+  const int tile = blockIdx.x - nbb;
+  const int tx = tile % t.tiles_x, ty = tile / t.tiles_x;
   const int g = 1 + tx * VX + threadIdx.x, iz = 2 + ty * VY + threadIdx.y;
   if (iz > nz - 2) // whole warps
     return;
