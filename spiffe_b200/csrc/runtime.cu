@@ -142,6 +142,8 @@ struct S32State {
   long long sort_interval = 20, since_sort = 0;
   double *staging = nullptr; // device FP64 staging for host transfers
   size_t staging_n = 0;
+  float *tm_slab = nullptr; // Ez, Er, Bphi, Bphi2 in one allocation
+  bool l2_window = false;   // the stream holds an L2 persisting window over tm_slab
 };
 
 struct spiffe_gpu_instance {
@@ -392,6 +394,38 @@ template <typename T> static int s32_alloc_z(T **p, size_t n, cudaStream_t s)
   return 0;
 }
 
+// Marks [base, base+bytes) persisting in L2 for this instance's stream: the
+// FDTD reads and writes the TM fields every step and the push gathers from
+// them, while the particle stream between two steps (tens of MB) would
+// otherwise evict them.  The set-aside is the smaller of the device's maximum
+// and the window; it belongs to this process's context.  Without support the
+// call does nothing.
+static int s32_l2_window(spiffe_gpu_instance *in, const void *base, size_t bytes)
+{
+  int dev = 0, max_persist = 0, max_window = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev));
+  CUDA_TRY(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev));
+  if (max_persist <= 0 || max_window <= 0)
+    return 0;
+  const size_t win = bytes < (size_t)max_window ? bytes : (size_t)max_window;
+  size_t cur = 0;
+  CUDA_TRY(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+  const size_t want = win < (size_t)max_persist ? win : (size_t)max_persist;
+  if (want > cur)
+    CUDA_TRY(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+  CUDA_TRY(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+  cudaStreamAttrValue a{};
+  a.accessPolicyWindow.base_ptr = const_cast<void *>(base);
+  a.accessPolicyWindow.num_bytes = win;
+  a.accessPolicyWindow.hitRatio = cur >= win ? 1.0f : (float)cur / (float)win;
+  a.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  a.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  CUDA_TRY(cudaStreamSetAttribute(in->stream, cudaStreamAttributeAccessPolicyWindow, &a));
+  in->s32->l2_window = true;
+  return 0;
+}
+
 static int s32_create(spiffe_gpu_instance *in, const int16_t *flags)
 {
   in->s32 = new S32State();
@@ -407,11 +441,18 @@ static int s32_create(spiffe_gpu_instance *in, const int16_t *flags)
   S.f.flags = in->d_flags;
   S.f.umask = S.umask;
   if (in->mesh.modes & SPIFFE_FL_TM_FIELDS) {
-    float **tm[] = {&S.f.Ez, &S.f.Er, &S.f.Bphi, &S.f.Bphi2};
-    for (float **p : tm)
-      RC_TRY(s32_alloc_f(p, n, s));
+    // Ez, Er, Bphi, Bphi2 in one block, so one L2 access window can cover them
+    RC_TRY(s32_alloc_f(&S.tm_slab, 4 * n, s));
+    S.f.Ez = S.tm_slab;
+    S.f.Er = S.tm_slab + n;
+    S.f.Bphi = S.tm_slab + 2 * n;
+    S.f.Bphi2 = S.tm_slab + 3 * n;
     RC_TRY(s32_alloc_z(&S.f.Jz, n, s));
     RC_TRY(s32_alloc_z(&S.f.Jr, n, s));
+    // large problems only: windows of many small instances would compete
+    // for one set-aside (a batch's instances are small)
+    if (4 * n * sizeof(float) >= ((size_t)32 << 20))
+      RC_TRY(s32_l2_window(in, S.tm_slab, 4 * n * sizeof(float)));
   }
   if (in->mesh.modes & SPIFFE_FL_TE_FIELDS) {
     float **te[] = {&S.f.Ephi, &S.f.Br, &S.f.Br2, &S.f.Bz, &S.f.Bz2};
@@ -439,7 +480,13 @@ static int s32_create(spiffe_gpu_instance *in, const int16_t *flags)
 static void s32_destroy(spiffe_gpu_instance *in)
 {
   S32State &S = *in->s32;
-  void *p[] = {S.f.Ez, S.f.Er, S.f.Bphi, S.f.Bphi2, S.f.Ephi, S.f.Br, S.f.Br2, S.f.Bz, S.f.Bz2,
+  if (S.l2_window) {
+    cudaStreamAttrValue a{};
+    a.accessPolicyWindow.num_bytes = 0; // no window: release the persisting lines
+    cudaStreamSetAttribute(in->stream, cudaStreamAttributeAccessPolicyWindow, &a);
+    cudaCtxResetPersistingL2Cache();
+  }
+  void *p[] = {S.tm_slab, S.f.Ephi, S.f.Br, S.f.Br2, S.f.Bz, S.f.Bz2,
                S.f.EzImposed, S.f.ErImposed, S.f.BzImposed, S.f.BrImposed, S.f.Jz, S.f.Jr, S.f.Jphi,
                S.f.Psi, S.f.PsiImposed, S.f.Q, S.f.Qp, S.f.jbox, S.umask, S.staging};
   for (void *q : p)
