@@ -208,17 +208,24 @@ def scaled_config(scale):
 
 def e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist):
     """The same K steps end to end through the public API from pinned host
-    buffers: state upload, K single-step calls each reading the particle
-    count back, state download.  Returns (ms, particle-steps, state bytes)."""
+    buffers: state upload, K single-step calls each followed by a read-back of
+    that step's particle count into pinned memory (queued, no per-step stall),
+    state download.  Returns (ms, particle-steps, state bytes)."""
+    import numpy as np
     import torch
 
     from spiffe_b200 import gpu
 
+    # pinned copies: the caller's post-warm-up state stays as it is
+    host_f, host_b = host_f.copy(), host_b.copy()
     pin = {}
     for k, v in host_f.a.items():
         host_f.a[k], pin[k] = pinned_like(v)
     for k, v in host_b.a.items():
         host_b.a[k], pin["b" + k] = pinned_like(v)
+    counts = pinned_like(np.zeros((K, 2), np.int64))
+    pin["counts"] = counts[1]
+    counts = counts[0]
     g2 = gpu.GpuInstance(f, capacity=b.capacity, precision=prec)
     g2.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
     g2.configure_run(space_charge=1, push=push, poisson=cfg.poisson())
@@ -234,15 +241,17 @@ def e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist):
     g2.upload_fields(host_f)
     g2.upload_beam(host_b)
     wb0 = g2.work_counters()
-    for _ in range(K):
+    for k in range(K):
         g2.run_steps(1)
-        g2.counts()
+        g2.counts_async(counts[k])  # this step's particle count, read back without a stall
+    g2.synchronize()
     wb1 = g2.work_counters()
     g2.download_beam(host_b)
     g2.download_fields(host_f)
     e1.record(stream2)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    assert tuple(counts[-1]) == g2.counts(), "per-step count read back"
     g2.close()
     return ms, wb1["particle_steps"] - wb0["particle_steps"], state_bytes
 
@@ -310,6 +319,13 @@ def gpu_arm(args):
     np_end, _ = g.counts()
     g.close()
 
+    # --- end to end through the public API from pinned host buffers, right
+    # after the timed run (before the FP64 comparison, whose FP64-heavy
+    # instance would otherwise precede it)
+    e2e_ms, e2e_psteps, state_bytes = 0.0, 0, 0
+    if not args.no_e2e:
+        e2e_ms, e2e_psteps, state_bytes = e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist)
+
     f64_form = None
     if prec == gpu.PRECISION_SPLIT32 and args.f64_steps > 0:
         # the plain FP64 drop-in on the same post-warm-up state, same GPU, same run
@@ -336,11 +352,6 @@ def gpu_arm(args):
                     "how": "plain FP64 drop-in on the same post-warm-up state and GPU, right after the split-form "
                            "run; its K steps hold the same share of Poisson corrections (one per 20 steps)"}
         g3.close()
-    # --- end to end through the public API from pinned host buffers
-    e2e_ms, e2e_psteps, state_bytes = 0.0, 0, 0
-    if not args.no_e2e:
-        e2e_ms, e2e_psteps, state_bytes = e2e_phase(f, host_f, host_b, b, cfg, push, mesh_w, prec, K, dist)
-
     # --- totals over ranks (max time, summed work)
     if dist:
         t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
@@ -407,8 +418,8 @@ def gpu_arm(args):
         "clocks": clk,
         "e2e": None if args.no_e2e else {"value": round(e2e_all / (e2e_ms / 1e3), 1), "unit": UNIT,
                 "h2d_bytes_per_step": int(state_bytes / K), "d2h_bytes_per_step": int((state_bytes + 8 * K) / K),
-                "how": "public API from pinned host buffers: state upload, K single-step calls each reading the "
-                       "particle count back, state download"},
+                "how": "public API from pinned host buffers: state upload, K single-step calls each followed by a "
+                       "queued read-back of that step's particle count into pinned memory, state download"},
     }
     if f64_form:
         f64_form["split_over_f64"] = round(value / f64_form["value"], 3) if f64_form["value"] else None

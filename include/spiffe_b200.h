@@ -133,6 +133,12 @@ int spiffe_gpu_run_steps(spiffe_gpu_instance *inst, int64_t n_steps);
 /* Waits for queued work and reports device-side errors. */
 int spiffe_gpu_synchronize(spiffe_gpu_instance *inst);
 int spiffe_gpu_counts(spiffe_gpu_instance *inst, int64_t *np, int64_t *np_active);
+/* No counterpart in the reference.  Enqueues a copy of (np, npActive) into
+ * out[0..1] behind the work queued so far, without waiting: a host loop can
+ * read every step's particle count and synchronise once at the end.  `out`
+ * should be page-locked host memory (pageable memory makes the copy wait);
+ * the values are valid after spiffe_gpu_synchronize. */
+int spiffe_gpu_counts_async(spiffe_gpu_instance *inst, int64_t *out);
 
 /* Measurement (no counterpart in the reference, which has no timers): the device used by instances created afterwards on
  * this thread; the instance's CUDA stream (a cudaStream_t); per-phase device

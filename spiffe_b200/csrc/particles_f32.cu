@@ -481,7 +481,7 @@ __global__ void k_snapshot_last32(DevBeam32 b, DevCounts *cnt)
 // advance_particles (:131-339) and its screen loop (:362-434); with DEP the
 // pushed particle's current for the next step.
 template <bool DEP, bool DEF>
-__global__ void __launch_bounds__(T, 3) k_push32(DevMesh m, DevFields32 f, DevBeam32 b, Push32Params p, DevScreens scr,
+__global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBeam32 b, Push32Params p, DevScreens scr,
                                                DevCounts *cnt, int32_t *lost_list, S32Scales sc)
 {
   const long ip = (long)blockIdx.x * T + threadIdx.x;

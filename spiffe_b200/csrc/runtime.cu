@@ -11,6 +11,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1912,6 +1913,15 @@ extern "C" int spiffe_gpu_counts(spiffe_gpu_instance *in, int64_t *np, int64_t *
     *np = in->h_cnt->np;
   if (np_active)
     *np_active = in->h_cnt->npActive;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_counts_async(spiffe_gpu_instance *in, int64_t *out)
+{
+  if (!in || !out)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  static_assert(offsetof(DevCounts, npActive) == offsetof(DevCounts, np) + sizeof(long long), "np, npActive adjacent");
+  CUDA_TRY(cudaMemcpyAsync(out, &in->cnt->np, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, in->stream));
   return 0;
 }
 

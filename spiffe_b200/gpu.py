@@ -71,6 +71,7 @@ def load():
         "spiffe_gpu_run_steps": ([H, C.c_int64], C.c_int),
         "spiffe_gpu_synchronize": ([H], C.c_int),
         "spiffe_gpu_counts": ([H, P(C.c_int64), P(C.c_int64)], C.c_int),
+        "spiffe_gpu_counts_async": ([H, C.c_void_p], C.c_int),
         "spiffe_gpu_select_device": ([C.c_int32], C.c_int),
         "spiffe_gpu_stream": ([H, P(C.c_void_p)], C.c_int),
         "spiffe_gpu_set_profiling": ([H, C.c_int32], C.c_int),
@@ -294,6 +295,12 @@ class GpuInstance:
         out = (C.c_int64 * 4)()
         _check(self.lib.spiffe_gpu_work_counters(self.h, out))
         return dict(particle_steps=out[0], sor_halfsweeps=out[1], sor_solves=out[2], fdtd_steps=out[3])
+
+    def counts_async(self, out):
+        """Enqueues a copy of (np, npActive) into out[0:2] (an int64 numpy
+        array, best page-locked) without waiting; valid after synchronize()."""
+        assert out.dtype == np.int64 and out.size >= 2 and out.flags["C_CONTIGUOUS"]
+        _check(self.lib.spiffe_gpu_counts_async(self.h, out.ctypes.data))
 
     def counts(self):
         a, b = C.c_int64(), C.c_int64()

@@ -225,3 +225,33 @@ def test_device_errors_are_reported():
         g.solve_poisson(0, -1.0, 10)  # accuracy <= 0 is rejected as the reference does (poisson.c:27)
     with pytest.raises(gpu.SpiffeGpuError):
         g.add_screen(0.01, direction=2)
+
+
+def test_counts_async_matches_counts():
+    """The queued count read returns what the synchronous one does, step by step."""
+    fx = load("pillbox_loop")
+    cfg = workloads.PillboxConfig()
+    f = fields_from(fx, modes=MODES | abi.FL_SPACE_CHARGE, dt=float(fx["dt"]))
+    f["Ez"] = fx["Ez0"]
+    g = gpu.GpuInstance(f, capacity=40000)
+    g.add_cathode(cfg.cathode_options())
+    g.configure_run(space_charge=1, push=abi.push_options())
+    g.run_begin()
+    g.run_steps(120)  # emission starts near step 70
+    out = np.zeros((30, 2), np.int64)
+    seen = []
+    for k in range(30):
+        g.run_steps(1)
+        g.counts_async(out[k])
+    g.synchronize()
+    g2 = gpu.GpuInstance(f, capacity=40000)
+    g2.add_cathode(cfg.cathode_options())
+    g2.configure_run(space_charge=1, push=abi.push_options())
+    g2.run_begin()
+    g2.run_steps(120)
+    for k in range(30):
+        g2.run_steps(1)
+        seen.append(g2.counts())
+    assert [tuple(r) for r in out] == seen and seen[-1][0] > 0
+    g.close()
+    g2.close()
