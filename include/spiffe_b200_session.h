@@ -16,9 +16,10 @@
  *   define_test_beam (test_beam.c:17), poisson_correction
  *   (poisson_correction.c:31), load_fields (load_fields.c:20),
  *   define_field_saving (field_saving.c:16; time_interval saving),
+ *   define_snapshots (snapshots.c:16), define_field_output (field_output.c:16),
  *   integrate (integrate.c:24), trace (obsolete, as spiffe), stop.
  * Accepted with a warning and no output (diagnostic files only):
- *   define_field_sampling, define_snapshots, define_field_output, and the
+ *   define_field_sampling, and the
  *   output-file variables boundary_output, urmel_boundary_output,
  *   discrete_boundary_output, interior_points, emission_log, field_output,
  *   status_output, lost_particles.
@@ -28,8 +29,8 @@
  * (current smoothing and filtering, test charges, thermal velocities, Halton
  * sequences, field saving on an Ez trigger).
  *
- * Outputs: screens and field saves are SDDS1 binary files with the
- * reference's columns and parameters.  A screen page holds the crossings of
+ * Outputs: screens, field saves, beam snapshots and field output are SDDS1
+ * binary files with the reference's columns and parameters.  A screen page holds the crossings of
  * one run segment (the steps between two host synchronisations, at most
  * the session's flush interval) instead of one time step.
  */

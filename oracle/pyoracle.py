@@ -201,6 +201,10 @@ def _ref_lib():
     lib.ref_screen_count.restype = C.c_int64
     lib.ref_screen_column.argtypes = [C.c_long, C.c_char_p, P(C.c_double)]
     lib.ref_screen_column.restype = C.c_int64
+    lib.ref_table_column.argtypes = [C.c_long, C.c_char_p, P(C.c_double)]
+    lib.ref_table_column.restype = C.c_int64
+    lib.ref_table_pages.argtypes = [C.c_long]
+    lib.ref_table_pages.restype = C.c_int64
     lib.ref_kinetic_energy.restype = C.c_double
     lib.ref_field_energy.argtypes = [P(C.c_double)]
     lib.ref_time_step.restype = C.c_int64
@@ -299,6 +303,17 @@ def _child(program, capacity, cwd):
                 a = np.zeros(max(n, 0))
                 lib.ref_screen_column(args[0], col.encode(), a.ctypes.data_as(P(C.c_double)))
                 d[col] = a
+            out.append(d)
+        elif kind == "table":
+            # ("table", which, [columns]): which 0 beam snapshots, 1 field output
+            which, cols = args
+            d = {"pages": lib.ref_table_pages(which)}
+            for col in cols:
+                n = lib.ref_table_column(which, col.encode(), None)
+                a = np.zeros(max(n, 0))
+                if n > 0:
+                    lib.ref_table_column(which, col.encode(), a.ctypes.data_as(P(C.c_double)))
+                d[col] = a if n >= 0 else None
             out.append(d)
         elif kind == "kinetic_energy":
             out.append(lib.ref_kinetic_energy())

@@ -96,7 +96,11 @@ int ref_command(const char *text)
   else if (strcmp(nl.group_name, "define_antenna") == 0) {
     process_antenna_definition(&antenna, n_antennae, &EM, &nl);
     n_antennae++;
-  } else if (strcmp(nl.group_name, "define_test_beam") == 0)
+  } else if (strcmp(nl.group_name, "define_snapshots") == 0)
+    process_snapshot_definition(&snapshot_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "define_field_output") == 0)
+    process_field_output_definition(&field_output_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "define_test_beam") == 0)
     process_testbeam_definition(&test_beam_defn, &EM, &nl);
   else if (strcmp(nl.group_name, "integrate") == 0)
     perform_integration(&EM, &beam, cathode, cathodes, &test_beam_defn, antenna, n_antennae, &resistor_defns,
@@ -397,6 +401,25 @@ void ref_step(long space_charge, double z_forces_start)
     fprintf(stderr, "ref_driver: particle capacity exceeded\n");
     exit(3);
   }
+}
+
+/* -------------------------------------------- snapshots and field output */
+
+/* every row written to the beam-snapshot table (which 0) or the field-output
+ * table (which 1), all pages in order; returns the row count, -1 for an
+ * unknown column */
+int64_t ref_table_column(long which, const char *column, double *out)
+{
+  double *v;
+  int64_t n = shim_sdds_column(which == 0 ? &snapshot_defn.table : &field_output_defn.SDDSout, column, &v);
+  if (n > 0 && v && out)
+    memcpy(out, v, sizeof(double) * (size_t)n);
+  return v ? n : -1;
+}
+
+int64_t ref_table_pages(long which)
+{
+  return (which == 0 ? &snapshot_defn.table : &field_output_defn.SDDSout)->pages;
 }
 
 /* --------------------------------------------------------------- screens */

@@ -28,6 +28,7 @@
 #define SDDS_SET_BY_INDEX 1
 #define SDDS_SET_BY_NAME 2
 #define SDDS_PASS_BY_VALUE 4
+#define SDDS_BY_INDEX SDDS_SET_BY_INDEX
 #define SDDS_PASS_BY_REFERENCE 8
 
 #define SDDS_EXIT_PrintErrors 1
@@ -67,6 +68,8 @@ int32_t SDDS_SaveLayout(SDDS_DATASET *t);
 int32_t SDDS_StartPage(SDDS_DATASET *t, int64_t expected_n_rows);
 int32_t SDDS_StartTable(SDDS_DATASET *t, int64_t expected_n_rows);
 int32_t SDDS_SetRowValues(SDDS_DATASET *t, int32_t mode, int64_t row, ...);
+int32_t SDDS_GetColumnIndex(SDDS_DATASET *t, char *name);
+int32_t SDDS_NumberOfErrors(void);
 int32_t SDDS_SetColumn(SDDS_DATASET *t, int32_t mode, void *data, int64_t rows, ...);
 int32_t SDDS_SetParameters(SDDS_DATASET *t, int32_t mode, ...);
 int32_t SDDS_WritePage(SDDS_DATASET *t);

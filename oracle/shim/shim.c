@@ -515,15 +515,17 @@ static int col_index(SDDS_DATASET *t, const char *name)
   return -1;
 }
 
+/* grows every column to hold `rows`; only the new slots are cleared (rows of
+ * the page being assembled, beyond n_rows, may already hold values) */
 static void ensure_rows(SDDS_DATASET *t, int64_t rows)
 {
   int i;
+  const int64_t old = t->max_rows;
   if (rows <= t->max_rows)
     return;
   while (t->max_rows < rows)
     t->max_rows = t->max_rows ? 2 * t->max_rows : 1024;
   for (i = 0; i < t->n_columns; i++) {
-    int64_t old = t->n_rows;
     t->data[i] = trealloc(t->data[i], sizeof(double) * (uint64_t)t->max_rows);
     memset(t->data[i] + old, 0, sizeof(double) * (uint64_t)(t->max_rows - old));
   }
@@ -680,6 +682,9 @@ int32_t SDDS_WritePage(SDDS_DATASET *t)
 }
 
 int32_t SDDS_WriteTable(SDDS_DATASET *t) { return SDDS_WritePage(t); }
+
+int32_t SDDS_GetColumnIndex(SDDS_DATASET *t, char *name) { return col_index(t, name); }
+int32_t SDDS_NumberOfErrors(void) { return 0; }
 int32_t SDDS_UpdatePage(SDDS_DATASET *t, uint32_t mode) { (void)mode; return SDDS_WritePage(t); }
 int32_t SDDS_Terminate(SDDS_DATASET *t) { (void)t; return 1; }
 

@@ -2,8 +2,9 @@
  *
  * No-op stand-ins for reference functions that perform_integration()
  * (integrate.c:149-193) calls every step but that lie outside the checked
- * per-step PIC path: field sampling/saving/output, beam snapshots, arbitrary-
- * surface emitters, resistors and the moving window.  Each is inert when its
+ * path: field sampling and saving, arbitrary-surface emitters, resistors and
+ * the moving window (beam snapshots and field output are the reference's own
+ * snapshots.c and field_output.c).  Each is inert when its
  * command was never given, which is how the checked configurations run; the
  * ones that would act bomb instead, so a checker can never silently skip
  * work.  compose_filename() stands in for the one in spiffe.c, which is not
@@ -36,21 +37,6 @@ void save_fields(FIELD_SAVING *saving_defn, FIELDS *EM_problem, long final_call)
   (void)final_call;
   if (saving_defn && saving_defn->filename)
     bomb("field saving is not part of the checked path", NULL);
-}
-
-void output_fields(FIELD_OUTPUT *output_defn, FIELDS *EM_problem)
-{
-  (void)EM_problem;
-  if (output_defn && output_defn->filename)
-    bomb("field output is not part of the checked path", NULL);
-}
-
-void take_beam_snapshot(SNAPSHOT *snapshot_defn, BEAM *beam, FIELDS *EM_problem)
-{
-  (void)beam;
-  (void)EM_problem;
-  if (snapshot_defn && snapshot_defn->filename)
-    bomb("beam snapshots are not part of the checked path", NULL);
 }
 
 void emit_electrons_from_emitter(BEAM *beam, EMITTER *emitter, FIELDS *EM_problem)

@@ -189,6 +189,45 @@ struct FieldSaving {
   spiffe_sdds::Writer out;
 };
 
+// SNAPSHOT and FIELD_OUTPUT, spiffe.h:320-398; step_interval/start_step are
+// set on the first call of the integration loop (snapshots.c:60-63,
+// field_output.c:58-61)
+struct BeamSnapshots {
+  bool defined = false;
+  std::string filename;
+  double time_interval = 0, start_time = 0;
+  long long step_interval = -1, start_step = -1, index = -1;
+  spiffe_sdds::Writer out;
+};
+
+struct FieldOutput {
+  bool defined = false;
+  std::string filename;
+  double time_interval = 0, start_time = 0;
+  long long z_interval = 1, r_interval = 1, exclude_imposed = 0, separate_imposed = 0;
+  long long step_interval = -1, start_step = -1, index = -1;
+  spiffe_sdds::Writer out;
+};
+
+// the shared schedule test of the diagnostics (field_saving.c:138-147,
+// snapshots.c:79-80, field_output.c:126-127)
+bool due(long long step, long long start_step, long long step_interval)
+{
+  return step >= start_step && (step_interval == 0 || (step - start_step) % step_interval == 0);
+}
+
+// the first step at or after `from` the schedule selects
+long long next_due(long long from, long long start_step, long long step_interval)
+{
+  long long j = from > start_step ? from : start_step;
+  if (step_interval > 0) {
+    const long long r = (j - start_step) % step_interval;
+    if (r)
+      j += step_interval - r;
+  }
+  return j;
+}
+
 const char *const kFieldNames[] = {"Ez",  "Er",  "Bphi",      "Bphi2",     "Jz",         "Jr",        "Ephi",
                                    "Jphi", "Br", "Br2",       "Bz",        "Bz2",        "EzImposed", "ErImposed",
                                    "PsiImposed", "BzImposed", "BrImposed", "Psi",        "Q"};
@@ -228,6 +267,8 @@ struct spiffe_session {
   bool pc_defined = false;
   spiffe_poisson_options pc{};
   FieldSaving saving;
+  BeamSnapshots snapshots;
+  FieldOutput field_output;
   // integrate.nl variables the reference does not reset between commands
   double ramp_time = 0, flat_top_time = 1;
   long long auto_max_dt = 0;
@@ -297,11 +338,15 @@ struct spiffe_session {
   int cmd_poisson(Args &g);
   int cmd_load_fields(Args &g);
   int cmd_field_saving(Args &g);
+  int cmd_snapshots(Args &g);
+  int cmd_field_output(Args &g);
   int cmd_integrate(Args &g);
   int execute(const std::string &text);
 
   int ensure_instance();
   int save_fields(long long step, double time, bool final_call);
+  int take_snapshot(long long step, double time);
+  int output_fields(long long step, double time);
   int flush_screens(long long step, double time);
   int status(long long step, double time);
 };
@@ -1047,8 +1092,8 @@ int spiffe_session::save_fields(long long step, double time, bool final_call)
   bool save = false;
   if (final_call && saving.save_before_exiting)
     save = true;
-  else if (step >= saving.start_step)
-    save = saving.step_interval == 0 || (step - saving.start_step) % saving.step_interval == 0;
+  else
+    save = due(step, saving.start_step, saving.step_interval);
   if (!save)
     return 0;
   S_TRY(pull());
@@ -1067,6 +1112,213 @@ int spiffe_session::save_fields(long long step, double time, bool final_call)
     return serr(SPIFFE_ERR_INVALID, "field saving: %s", err.c_str());
   say("fields saved to file %s at t=%e s\n", saving.filename.c_str(), time);
   saving.save_index++;
+  return 0;
+}
+
+// process_snapshot_definition, snapshots.c:16-40
+int spiffe_session::cmd_snapshots(Args &g)
+{
+  std::string filename;
+  double time_interval = 0, start_time = 0;
+  const bool have_file = g.str("filename", filename);
+  g.num("time_interval", time_interval);
+  g.num("start_time", start_time);
+  S_TRY(g.finish());
+  if (!have_file)
+    return serr(SPIFFE_ERR_INVALID, "no filename given for beam snapshots");
+  if (time_interval < 0)
+    return serr(SPIFFE_ERR_INVALID, "time_interval < 0 for beam snapshots");
+  snapshots.out.close();
+  snapshots.defined = true;
+  snapshots.filename = compose(filename, rootname);
+  snapshots.time_interval = time_interval;
+  snapshots.start_time = start_time;
+  snapshots.step_interval = snapshots.start_step = snapshots.index = -1;
+  return 0;
+}
+
+// take_beam_snapshot, snapshots.c:48-119: the beam at the step's start
+int spiffe_session::take_snapshot(long long step, double time)
+{
+  if (!snapshots.defined)
+    return 0;
+  using namespace spiffe_sdds;
+  BeamSnapshots &S = snapshots;
+  if (S.index == -1) {
+    S.step_interval = (long long)(S.time_interval / mesh.dt + 0.5);
+    S.start_step = (long long)((S.start_time - mesh.start_time) / mesh.dt + 0.5);
+    S.index = 0;
+    const char *q[9] = {"z", "r", "pz", "pr", "pphi", "q", "r0", "z0", "t0"};
+    const char *u[9] = {"m", "m", "m$be$nc", "m$be$nc", "m$be$nc", "C", "m", "m", "s"};
+    std::vector<Def> cols;
+    for (int k = 0; k < 9; k++)
+      cols.push_back(Def{q[k], u[k], "", T_DOUBLE});
+    cols.push_back(Def{"generation", "", "", T_SHORT});
+    cols.push_back(Def{"particleID", "", "", T_LONG});
+    cols.push_back(Def{"status", "", "", T_SHORT});
+    std::vector<Def> params = {Def{"Time", "s", "Time of snapshot", T_DOUBLE},
+                               Def{"Timestep", "", "Time-step of snapshot", T_LONG}};
+    std::string err;
+    if (!S.out.open(S.filename, "spiffe beam snapshots for run " + rootname, "", params, cols, err))
+      return serr(SPIFFE_ERR_INVALID, "beam snapshots: %s", err.c_str());
+  }
+  if (!due(step, S.start_step, S.step_interval))
+    return 0;
+  int64_t np = 0;
+  S_TRY(spiffe_gpu_counts(inst, &np, nullptr));
+  const size_t n = (size_t)np, cap = n ? n : 1;
+  std::vector<std::vector<double>> d(16, std::vector<double>(cap));
+  std::vector<int32_t> id(cap);
+  std::vector<int16_t> gen(cap);
+  std::vector<uint64_t> st(cap);
+  spiffe_beam_set b{};
+  b.capacity = (int64_t)cap;
+  double **ptr[16] = {&b.z, &b.r, &b.pz, &b.pr, &b.r_pphi, &b.vz, &b.vr, &b.vphi, &b.Q, &b.r0, &b.z0, &b.t0,
+                      &b.rmin, &b.rmax, &b.zmin, &b.zmax};
+  for (int k = 0; k < 16; k++)
+    *ptr[k] = d[(size_t)k].data();
+  b.particleID = id.data();
+  b.generation = gen.data();
+  b.status = st.data();
+  S_TRY(spiffe_gpu_download_beam(inst, &b));
+  std::vector<double> pphi(cap);
+  std::vector<int16_t> status(cap);
+  for (size_t i = 0; i < n; i++) {
+    pphi[i] = b.r[i] ? b.r_pphi[i] / b.r[i] : 0.0;
+    status[i] = (int16_t)b.status[i];
+  }
+  std::vector<const void *> cols = {b.z, b.r, b.pz, b.pr, pphi.data(), b.Q, b.r0, b.z0, b.t0,
+                                    gen.data(), id.data(), status.data()};
+  std::string err;
+  if (!S.out.write_page({time, (double)step}, {"", ""}, np, cols, err))
+    return serr(SPIFFE_ERR_INVALID, "beam snapshots: %s", err.c_str());
+  say("beam snapshot saved to file %s at t=%.16e, step %lld\n", S.filename.c_str(), time, step);
+  S.index++;
+  return 0;
+}
+
+// process_field_output_definition, field_output.c:16-43
+int spiffe_session::cmd_field_output(Args &g)
+{
+  std::string filename;
+  FieldOutput o;
+  const bool have_file = g.str("filename", filename);
+  g.num("time_interval", o.time_interval);
+  g.num("start_time", o.start_time);
+  g.integer("z_interval", o.z_interval);
+  g.integer("r_interval", o.r_interval);
+  g.integer("exclude_imposed_field", o.exclude_imposed);
+  g.integer("separate_imposed_field", o.separate_imposed);
+  S_TRY(g.finish());
+  if (!have_file)
+    return serr(SPIFFE_ERR_INVALID, "no filename given for field samples");
+  if (o.time_interval < 0)
+    return serr(SPIFFE_ERR_INVALID, "time_interval < 0 for field samples");
+  if (o.z_interval < 1 || o.r_interval < 1)
+    return serr(SPIFFE_ERR_INVALID, "z_interval and r_interval must be > 1");
+  o.defined = true;
+  o.filename = compose(filename, rootname);
+  field_output = std::move(o);
+  return 0;
+}
+
+// output_fields, field_output.c:45-214: node-centred fields every
+// z_interval-th row and r_interval-th column, single precision
+int spiffe_session::output_fields(long long step, double time)
+{
+  if (!field_output.defined)
+    return 0;
+  using namespace spiffe_sdds;
+  FieldOutput &O = field_output;
+  const spiffe_mesh &m = mesh;
+  const bool tm = m.modes & SPIFFE_FL_TM_FIELDS, te = m.modes & SPIFFE_FL_TE_FIELDS;
+  const bool sep = tm && O.separate_imposed;
+  if (O.index == -1) {
+    O.step_interval = (long long)(O.time_interval / m.dt + 0.5);
+    O.start_step = (long long)((O.start_time - m.start_time) / m.dt + 0.5);
+    O.index = 0;
+    Def v1{"Variable1Name", "", "", T_STRING}, v2{"Variable2Name", "", "", T_STRING};
+    v1.fixed = v2.fixed = true;
+    v1.fixed_value = "z";
+    v2.fixed_value = "r";
+    std::vector<Def> params = {v1, Def{"zMinimum", "m", "", T_DOUBLE}, Def{"zInterval", "m", "", T_DOUBLE},
+                               Def{"zDimension", "m", "", T_LONG}, Def{"rMinimum", "m", "", T_DOUBLE},
+                               Def{"rInterval", "m", "", T_DOUBLE}, Def{"rDimension", "m", "", T_LONG}, v2,
+                               Def{"Time", "s", "Time of output", T_DOUBLE},
+                               Def{"Timestep", "", "Time-step of output", T_LONG}};
+    std::vector<Def> cols = {Def{"z", "m", "", T_FLOAT}, Def{"r", "m", "", T_FLOAT},
+                             Def{"rho", "C/m$a3$n", "", T_FLOAT}};
+    if (tm) {
+      for (auto &c : {std::make_pair("Ez", "V/m"), std::make_pair("Er", "V/m"), std::make_pair("Bphi", "T"),
+                      std::make_pair("Jz", "A/m$a2$n"), std::make_pair("Jr", "A/m$a2$n")})
+        cols.push_back(Def{c.first, c.second, "", T_FLOAT});
+      if (sep) {
+        cols.push_back(Def{"EzImposed", "V/m", "", T_FLOAT});
+        cols.push_back(Def{"ErImposed", "V/m", "", T_FLOAT});
+      }
+    }
+    if (te)
+      for (auto &c : {std::make_pair("Ephi", "V/m"), std::make_pair("Br", "T"), std::make_pair("Bz", "T"),
+                      std::make_pair("Jphi", "A/m$a2$n")})
+        cols.push_back(Def{c.first, c.second, "", T_FLOAT});
+    std::string err;
+    if (!O.out.open(O.filename, "", "spiffe field output", params, cols, err))
+      return serr(SPIFFE_ERR_INVALID, "field output: %s", err.c_str());
+  }
+  if (!due(step, O.start_step, O.step_interval))
+    return 0;
+  O.index++;
+  S_TRY(pull());
+  const long long nz = m.nz, nr = m.nr, P = nr + 1;
+  const double dr2 = m.dr * m.dr;
+  std::vector<double> area_c((size_t)nr + 1); // calculate_areas, integrate.c:689-701
+  for (long long ir = 0; ir <= nr; ir++)
+    area_c[(size_t)ir] = ir ? SPIFFE_PIx2 * ir * dr2 : SPIFFE_PI * dr2 / 4;
+  std::vector<std::vector<float>> col(16);
+  auto A = [&](const char *n) -> const double * { return has(n) ? a[n].data() : nullptr; };
+  const double *Q = A("Q"), *Ez = A("Ez"), *Er = A("Er"), *Jz = A("Jz"), *Jr = A("Jr"), *B2 = A("Bphi2");
+  const double *EzI = A("EzImposed"), *ErI = A("ErImposed"), *Ephi = A("Ephi"), *Jphi = A("Jphi");
+  const double *Br2 = A("Br2"), *Bz2 = A("Bz2");
+  for (long long iz = 0; iz < nz; iz += O.z_interval) {
+    const float zv = (float)(iz * m.dz + m.zmin);
+    for (long long ir = 0; ir < nr; ir += O.r_interval) {
+      const size_t i = (size_t)(iz * P + ir), iu = i + (size_t)P, ir1 = i + 1;
+      int c = 0;
+      col[(size_t)c++].push_back(zv);
+      col[(size_t)c++].push_back((float)(ir * m.dr));
+      col[(size_t)c++].push_back((float)(Q[i] / (m.dz * area_c[(size_t)ir])));
+      if (tm) {
+        const float ezi = (float)((EzI[i] + EzI[iu]) / 2);
+        const float ez = (float)((Ez[i] + Ez[iu]) / 2 + (O.exclude_imposed ? 0 : ezi));
+        const float eri = (float)((ErI[i] + ErI[iu]) / 2); // as field_output.c:162, row iz+1
+        const float er = (float)((Er[i] + Er[ir1]) / 2 + (O.exclude_imposed ? 0 : eri));
+        col[(size_t)c++].push_back(ez);
+        col[(size_t)c++].push_back(er);
+        col[(size_t)c++].push_back((float)((B2[i] + B2[ir1] + B2[iu] + B2[iu + 1]) / 4));
+        col[(size_t)c++].push_back((float)((Jz[i] + Jz[iu]) / 2));
+        col[(size_t)c++].push_back((float)((Jr[i] + Jr[ir1]) / 2));
+        if (sep) {
+          col[(size_t)c++].push_back(ezi);
+          col[(size_t)c++].push_back(eri);
+        }
+      }
+      if (te) {
+        col[(size_t)c++].push_back((float)Ephi[i]);
+        col[(size_t)c++].push_back((float)((Br2[i] + Br2[iu]) / 2));
+        col[(size_t)c++].push_back((float)((Bz2[i] + Bz2[ir1]) / 2));
+        col[(size_t)c++].push_back((float)Jphi[i]);
+      }
+    }
+  }
+  const size_t ncol = 3 + (tm ? 5 + (sep ? 2 : 0) : 0) + (te ? 4 : 0);
+  std::vector<const void *> cols;
+  for (size_t k = 0; k < ncol; k++)
+    cols.push_back(col[k].data());
+  const double zdim = std::ceil(nz / (O.z_interval * 1.0)), rdim = std::ceil(nr / (O.r_interval * 1.0));
+  std::string err;
+  if (!O.out.write_page({m.zmin, m.dz * O.z_interval, zdim, 0.0, m.dr * O.r_interval, rdim, time, (double)step},
+                        {}, (int64_t)col[0].size(), cols, err))
+    return serr(SPIFFE_ERR_INVALID, "field output: %s", err.c_str());
   return 0;
 }
 
@@ -1233,18 +1485,13 @@ int spiffe_session::cmd_integrate(Args &g)
 
   S_TRY(spiffe_gpu_get_mesh(inst, &m));
   long long k = m.time_step;
+  const spiffe_poisson_options no_pc{};
   const double t0 = m.start_time, step_dt = m.dt;
   bool beam_seen = false;
   auto next_save = [&](long long from) -> long long {
     if (!saving.defined || saving.save_index == -1)
       return from;
-    long long j = from > saving.start_step ? from : saving.start_step;
-    if (saving.step_interval > 0) {
-      const long long r = (j - saving.start_step) % saving.step_interval;
-      if (r)
-        j += saving.step_interval - r;
-    }
-    return j;
+    return next_due(from, saving.start_step, saving.step_interval);
   };
   while (k < n_steps) {
     const double t = k * step_dt + t0;
@@ -1258,7 +1505,19 @@ int spiffe_session::cmd_integrate(Args &g)
       if (np && !beam_seen)
         beam_seen = true;
     }
+    // the step's imposed-field ramp comes before the diagnostics
+    // (integrate.c:136-137); run_steps then finds the factor unchanged
+    if (m.imposed_ramp_time > 0 && field_output.defined) {
+      const bool first = field_output.index == -1; // the schedule is fixed at the first output call
+      const long long fs = first ? (long long)((field_output.start_time - m.start_time) / m.dt + 0.5)
+                                 : field_output.start_step;
+      const long long fi = first ? (long long)(field_output.time_interval / m.dt + 0.5) : field_output.step_interval;
+      if (due(k, fs, fi))
+        S_TRY(spiffe_gpu_compute_imposed_efield(inst, pc_defined ? &pc : &no_pc, 0));
+    }
     S_TRY(save_fields(k, t, false));
+    S_TRY(output_fields(k, t));
+    S_TRY(take_snapshot(k, t));
     if (status_interval > 0 && k % status_interval == 0)
       S_TRY(status(k, t));
     long long next = n_steps;
@@ -1268,6 +1527,16 @@ int spiffe_session::cmd_integrate(Args &g)
       next = k + flush_steps;
     if (saving.defined) {
       const long long s = next_save(k + 1);
+      if (s < next)
+        next = s;
+    }
+    if (snapshots.defined) {
+      const long long s = next_due(k + 1, snapshots.start_step, snapshots.step_interval);
+      if (s < next)
+        next = s;
+    }
+    if (field_output.defined) {
+      const long long s = next_due(k + 1, field_output.start_step, field_output.step_interval);
       if (s < next)
         next = s;
     }
@@ -1286,6 +1555,7 @@ int spiffe_session::cmd_integrate(Args &g)
   m.time = m.time_step * m.dt + m.start_time;
   S_TRY(spiffe_gpu_set_mesh(inst, &m));
   S_TRY(save_fields(m.time_step, m.time, true));
+  S_TRY(take_snapshot(m.time_step, m.time));
   if (status_interval > 0 && m.time_step % status_interval == 0)
     S_TRY(status(m.time_step, m.time));
   return 0;
@@ -1334,7 +1604,11 @@ int spiffe_session::execute(const std::string &text)
       return SPIFFE_SESSION_STOPPED;
     } else if (c == "space_charge") {
       rc = serr(SPIFFE_ERR_INVALID, "the space_charge namelist is no longer used--use space_charge=1 in the integrate namelist");
-    } else if (c == "define_field_sampling" || c == "define_snapshots" || c == "define_field_output") {
+    } else if (c == "define_snapshots") {
+      rc = cmd_snapshots(g);
+    } else if (c == "define_field_output") {
+      rc = cmd_field_output(g);
+    } else if (c == "define_field_sampling") {
       warn("%s: diagnostic output is not produced", c.c_str());
       rc = 0;
     } else if (c == "define_resistor" || c == "load_particles" || c == "set_up_translation" || c == "translate" ||

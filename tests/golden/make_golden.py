@@ -190,6 +190,16 @@ DECK_TESTBEAM = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.
 """
 
 
+# The DC gun deck for 300 steps with beam snapshots and field output (the
+# reference's snapshots.c and field_output.c, compiled into the oracle).
+DECK_DIAG = DECK_DCGUN.replace("finish_time=300e-12", "finish_time=120e-12").replace(
+    "&integrate", '&define_snapshots filename="%s.snap", time_interval=40e-12, start_time=20e-12 &end\n'
+    '&define_field_output filename="%s.fld", time_interval=40e-12, start_time=20e-12, z_interval=2, r_interval=4, '
+    'separate_imposed_field=1 &end\n&integrate')
+sys.path.insert(0, os.path.dirname(HERE))
+from golden_columns import FLD_COLUMNS, SNAP_COLUMNS  # noqa: E402
+
+
 def decks():
     geo = str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"])
     for name, deck, screens in (("deck_dcgun", DECK_DCGUN, 1), ("deck_testbeam", DECK_TESTBEAM, 1)):
@@ -207,6 +217,16 @@ def decks():
             out.update({f"screen{i}_{k}": v for k, v in rs.items()})
         out.update(dict(zip(("Ez", "Er", "Bphi", "Psi"), fields)))
         save(name, **out)
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    cmds = [b.strip() + " &end" for b in DECK_DIAG.split("&end") if b.strip()]
+    snap, fld = pyoracle.run_reference([("command", c) for c in cmds] + [("table", 0, SNAP_COLUMNS),
+                                                                       ("table", 1, FLD_COLUMNS)],
+                                       cwd=d, capacity=20000)
+    save("deck_diagnostics", deck=np.array(DECK_DIAG), geo=np.array(geo), snap_pages=snap["pages"],
+         fld_pages=fld["pages"], **{"snap_" + k: snap[k] for k in SNAP_COLUMNS},
+         **{"fld_" + k: fld[k] for k in FLD_COLUMNS})
 
 
 if __name__ == "__main__":

@@ -383,3 +383,32 @@ def test_two_screens_record_crossings(tmp_path, monkeypatch):
     assert np.median(tf) > np.median(tn)
     steps = [p["parameters"]["Timestep"] for p in far]
     assert steps == sorted(steps)
+
+
+@pytest.mark.gpu
+def test_snapshots_and_field_output_match_reference(tmp_path, monkeypatch):
+    """define_snapshots and define_field_output through the session against the
+    reference's own take_beam_snapshot and output_fields on the same deck:
+    every row of every page, bit for bit (the charge density within single
+    precision rounding: the FP64 form removes the particles' charge from Q
+    with atomics)."""
+    from golden_columns import FLD_COLUMNS, SNAP_COLUMNS
+
+    fx = load("deck_diagnostics")
+    s = run_deck(fx, tmp_path, monkeypatch)
+    s.close()
+    snap = session.read_sdds(str(tmp_path / "spiffe.snap"))
+    fld = session.read_sdds(str(tmp_path / "spiffe.fld"))
+    assert len(snap) == int(fx["snap_pages"]) == 3 and len(fld) == int(fx["fld_pages"]) == 3
+    assert [p["parameters"]["Timestep"] for p in snap] == [50, 150, 250]
+    for c in SNAP_COLUMNS:
+        got = np.concatenate([p["columns"][c] for p in snap]).astype(np.float64)
+        assert np.array_equal(got, fx["snap_" + c]), c
+    for c in FLD_COLUMNS:
+        got = np.concatenate([p["columns"][c] for p in fld]).astype(np.float64)
+        if c == "rho":
+            assert np.allclose(got, fx["fld_" + c], rtol=2e-7, atol=0), c
+        else:
+            assert np.array_equal(got, fx["fld_" + c]), c
+    p0 = fld[0]["parameters"]
+    assert p0["Variable1Name"] == "z" and p0["zDimension"] == 76 and p0["rDimension"] == 26
