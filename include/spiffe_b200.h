@@ -123,6 +123,24 @@ int spiffe_gpu_add_antenna(spiffe_gpu_instance *inst, int32_t direction, int64_t
  * slot (particle ID 0, extrema 0, inactive until its first push). */
 int spiffe_gpu_set_test_beam(spiffe_gpu_instance *inst, const spiffe_test_beam_options *opt);
 
+/* add_on_axis_fields (process_on_axis_field_definition, onAxisFields.c:18-172)
+ * given the file's z and Ez columns (n points): z_offset is added to z, Ez
+ * is scaled to peak |Ez| = Ez_peak, three derivatives are taken, and the push
+ * then adds the field's off-axis expansion (addOffAxisExpansionFields,
+ * onAxisFields.c:208-268) to every particle's fields, as advance_particles.c
+ * :836-844 does.  phase is in degrees.  Ez_peak = 0 ignores the field (the
+ * reference warns).  Errors as the reference's: negative frequency,
+ * expansion_order outside [0, 3], n <= 4, z not increasing, points not
+ * equispaced to 1e-4.  At most 8 fields per instance. */
+int spiffe_gpu_add_on_axis_field(spiffe_gpu_instance *inst, const double *z, const double *Ez, int64_t n,
+                                 double z_offset, double Ez_peak, double frequency, double phase,
+                                 int32_t expansion_order);
+/* The summed on-axis fields' (Ez, Er, Bphi) at (z, r) and time t, as the
+ * push adds them; profile != 0 sets sine and cosine to 1 (the fields_used
+ * output, onAxisFields.c:130-170). */
+int spiffe_gpu_on_axis_fields_at(spiffe_gpu_instance *inst, double z, double r, double t, int32_t profile,
+                                 double *EzErBphi);
+
 /* perform_integration (integrate.c:24-194) on the device: configure, the
  * setup before the loop (:125-133), then any number of loop steps. */
 int spiffe_gpu_configure_run(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_push_options *push,

@@ -56,6 +56,7 @@ int ref_session_init(long particle_capacity)
     return -1;
   initialized = 1;
   memset(&EM, 0, sizeof(EM));
+  shim_n_closed_tables = 0;
   memset(&beam, 0, sizeof(beam));
   EM.run_name = "checker";
   EM.rootname = strdup("checker");
@@ -100,6 +101,8 @@ int ref_command(const char *text)
     process_snapshot_definition(&snapshot_defn, &EM, &nl);
   else if (strcmp(nl.group_name, "define_field_output") == 0)
     process_field_output_definition(&field_output_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "add_on_axis_fields") == 0)
+    process_on_axis_field_definition(&EM, &nl);
   else if (strcmp(nl.group_name, "define_test_beam") == 0)
     process_testbeam_definition(&test_beam_defn, &EM, &nl);
   else if (strcmp(nl.group_name, "integrate") == 0)
@@ -408,10 +411,27 @@ void ref_step(long space_charge, double z_forces_start)
 /* every row written to the beam-snapshot table (which 0) or the field-output
  * table (which 1), all pages in order; returns the row count, -1 for an
  * unknown column */
+/* which: 0 the beam snapshots, 1 the field output, 2 + k the k-th output
+ * table the reference closed inside a command */
+static SDDS_DATASET *ref_table(long which)
+{
+  if (which == 0)
+    return &snapshot_defn.table;
+  if (which == 1)
+    return &field_output_defn.SDDSout;
+  if (which - 2 < shim_n_closed_tables)
+    return &shim_closed_tables[which - 2];
+  return NULL;
+}
+
 int64_t ref_table_column(long which, const char *column, double *out)
 {
   double *v;
-  int64_t n = shim_sdds_column(which == 0 ? &snapshot_defn.table : &field_output_defn.SDDSout, column, &v);
+  SDDS_DATASET *t = ref_table(which);
+  int64_t n;
+  if (!t)
+    return -1;
+  n = shim_sdds_column(t, column, &v);
   if (n > 0 && v && out)
     memcpy(out, v, sizeof(double) * (size_t)n);
   return v ? n : -1;
@@ -419,7 +439,8 @@ int64_t ref_table_column(long which, const char *column, double *out)
 
 int64_t ref_table_pages(long which)
 {
-  return (which == 0 ? &snapshot_defn.table : &field_output_defn.SDDSout)->pages;
+  SDDS_DATASET *t = ref_table(which);
+  return t ? t->pages : -1;
 }
 
 /* --------------------------------------------------------------- screens */

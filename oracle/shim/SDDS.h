@@ -53,6 +53,10 @@ typedef struct {
 } SDDS_DATASET;
 typedef SDDS_DATASET SDDS_TABLE;
 
+#define SHIM_MAX_CLOSED_TABLES 16
+extern SDDS_DATASET shim_closed_tables[SHIM_MAX_CLOSED_TABLES];
+extern int shim_n_closed_tables;
+
 int32_t SDDS_InitializeOutput(SDDS_DATASET *t, int32_t data_mode, int32_t lines_per_row,
                               const char *description, const char *contents, const char *filename);
 int32_t SDDS_DefineSimpleColumn(SDDS_DATASET *t, const char *name, const char *unit, int32_t type);

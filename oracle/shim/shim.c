@@ -686,7 +686,18 @@ int32_t SDDS_WriteTable(SDDS_DATASET *t) { return SDDS_WritePage(t); }
 int32_t SDDS_GetColumnIndex(SDDS_DATASET *t, char *name) { return col_index(t, name); }
 int32_t SDDS_NumberOfErrors(void) { return 0; }
 int32_t SDDS_UpdatePage(SDDS_DATASET *t, uint32_t mode) { (void)mode; return SDDS_WritePage(t); }
-int32_t SDDS_Terminate(SDDS_DATASET *t) { (void)t; return 1; }
+/* Output tables the reference closes inside a command (a local dataset, as
+ * for add_on_axis_fields' fields_used file, onAxisFields.c:130-170) are kept
+ * here, in the order they were closed, so the checker can still read them. */
+SDDS_DATASET shim_closed_tables[SHIM_MAX_CLOSED_TABLES];
+int shim_n_closed_tables;
+
+int32_t SDDS_Terminate(SDDS_DATASET *t)
+{
+  if (!t->is_input && t->n_columns && shim_n_closed_tables < SHIM_MAX_CLOSED_TABLES)
+    shim_closed_tables[shim_n_closed_tables++] = *t;
+  return 1;
+}
 
 void SDDS_SetError(char *error_text)
 {

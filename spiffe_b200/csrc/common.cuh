@@ -14,6 +14,16 @@
 #include "../../include/spiffe_b200_types.h"
 
 // Per-instance scalars every kernel needs (the FIELDS scalars of spiffe.h).
+#define SPIFFE_MAX_ON_AXIS 8
+
+// One on-axis RF field (ON_AXIS_FIELD, spiffe.h): Ez(z) on increasing z and
+// its first three z-derivatives, n points; k = omega / c.
+struct OnAxisField {
+  const double *z, *Ez, *D1, *D2, *D3;
+  int n, order;
+  double k;
+};
+
 struct DevMesh {
   int nz, nr, pitch;
   double zmin, zmax, rmax, dz, dr, dt;
@@ -22,7 +32,76 @@ struct DevMesh {
   double constE[3], constB[3];
   short turn_off[6];
   int has_solenoid;
+  // on-axis fields (add_on_axis_fields) and, for the push being launched,
+  // sin(omega t + phase) and omega/c^2 cos(omega t + phase) of each
+  int n_onaxis;
+  const OnAxisField *onaxis;
+  double oa_sin[SPIFFE_MAX_ON_AXIS], oa_bf[SPIFFE_MAX_ON_AXIS];
 };
+
+// addOffAxisExpansionFields (onAxisFields.c:208-268) at (z, r): each of
+// the n fields expanded off axis to its order and added into Ez, Er, Bphi;
+// sin_wt[i] = sin(omega t + phase) and bf[i] = omega / c^2 cos(omega t +
+// phase) of field i.  The position search follows binaryArraySearch in
+// bracket mode (-1 below the first point, n-1 at or past the last, else the
+// last point at or below z).  As in the reference, each field that covers z
+// sets Er to zero before adding its own terms.
+__host__ __device__ inline void onaxis_expand(const OnAxisField *fields, int n_fields, const double *sin_wt,
+                                              const double *bf, double z, double r, double &Ez, double &Er, double &Bphi)
+{
+  for (int ip = 0; ip < n_fields; ip++) {
+    const OnAxisField &F = fields[ip];
+    int iz;
+    if (z < F.z[0])
+      iz = -1;
+    else if (z >= F.z[F.n - 1])
+      iz = F.n - 1;
+    else {
+      int lo = 0, hi = F.n - 1;
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (z >= F.z[mid])
+          lo = mid;
+        else
+          hi = mid;
+      }
+      iz = lo;
+    }
+    if (iz < 0 || iz >= F.n - 1)
+      continue;
+    if (!(F.z[iz] <= z && F.z[iz + 1] > z))
+      continue;
+    const double s = sin_wt[ip], BF = bf[ip], k = F.k;
+    const double dz = z - F.z[iz];
+    const double Ez0 = F.Ez[iz] + F.D1[iz] * dz;
+    Ez += Ez0 * s;
+    Er = 0;
+    if (F.order >= 1) {
+      const double DzEz = F.D1[iz] + F.D2[iz] * dz;
+      Er += -r / 2 * DzEz * s;
+      Bphi += r / 2 * Ez0 * BF;
+      if (F.order >= 2) {
+        const double Dz2Ez = F.D2[iz] + F.D3[iz] * dz;
+        Ez += -(r * r) / 4. * (Dz2Ez + k * k * Ez0) * s;
+        if (F.order >= 3) {
+          Er += (r * r * r) / 16. * (F.D3[iz] + k * k * DzEz) * s;
+          Bphi += (r * r * r) / 16. * (Dz2Ez + k * k * Ez0) * BF;
+        }
+      }
+    }
+  }
+}
+
+// The on-axis fields' contribution at a particle, summed apart and then added
+// (advance_particles.c:836-844).
+__device__ __forceinline__ void onaxis_add(const DevMesh &m, double z, double r, double &Ez, double &Er, double &Bphi)
+{
+  double EzO = 0, ErO = 0, BphiO = 0;
+  onaxis_expand(m.onaxis, m.n_onaxis, m.oa_sin, m.oa_bf, z, r, EzO, ErO, BphiO);
+  Ez += EzO;
+  Er += ErO;
+  Bphi += BphiO;
+}
 
 template <typename T>
 struct DevFields {

@@ -222,13 +222,20 @@ __device__ void gather32(const DevMesh &m, const DevFields32 &f, int iz0, float 
              wr * wa * LD(f.Bphi2, N(iz1, ir1));
     }
   }
-  // uniform fields and switches (:828-857)
+  // uniform fields, the on-axis expansion and switches (:828-857)
   Ez += (float)m.constE[0];
   Er += (float)m.constE[1];
   Ephi += (float)m.constE[2];
   Bz += (float)m.constB[0];
   Br += (float)m.constB[1];
   Bphi += (float)m.constB[2];
+  if (!DEF && m.n_onaxis) {
+    double ez = 0, er = 0, bp = 0;
+    onaxis_add(m, m.zmin + ((double)iz0 + fz) * m.dz, ((double)ir0 + fr) * m.dr, ez, er, bp);
+    Ez += (float)ez;
+    Er += (float)er;
+    Bphi += (float)bp;
+  }
   if (!DEF) {
     if (m.turn_off[0]) Ez = 0;
     if (m.turn_off[1]) Er = 0;
@@ -1173,7 +1180,7 @@ extern "C" int s32_push(const DevMesh *m, const DevFields32 *f, const DevBeam32 
     const unsigned def_modes = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_LONGIT_INTERP | SPIFFE_FL_RADIAL_INTERP;
     const unsigned mode_bits = SPIFFE_FL_TM_FIELDS | SPIFFE_FL_TE_FIELDS | SPIFFE_FL_LONGIT_INTERP |
                                SPIFFE_FL_RADIAL_INTERP | SPIFFE_FL_LONGIT_SMEAR | SPIFFE_FL_RADIAL_SMEAR;
-    bool def = (m->modes & mode_bits) == def_modes && !p->forced;
+    bool def = (m->modes & mode_bits) == def_modes && !p->forced && !m->n_onaxis;
     for (int k = 0; k < 6; k++)
       def = def && !m->turn_off[k];
     int32_t *ll = any ? w->lost_list : nullptr;

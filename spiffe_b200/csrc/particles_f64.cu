@@ -189,13 +189,15 @@ __device__ void gather(const DevMesh &m, const DevFields<double> &f, double z, d
              fr * fa * f.Bphi2[N(iz1, ir1)];
     }
   }
-  // uniform fields, switches, :828-857
+  // uniform fields, the on-axis expansion, switches, :828-857
   Ez += m.constE[0];
   Er += m.constE[1];
   Ephi += m.constE[2];
   Bz += m.constB[0];
   Br += m.constB[1];
   Bphi += m.constB[2];
+  if (m.n_onaxis)
+    onaxis_add(m, z, r, Ez, Er, Bphi);
   if (m.turn_off[0]) Ez = 0;
   if (m.turn_off[1]) Er = 0;
   if (m.turn_off[2]) Ephi = 0;

@@ -23,6 +23,7 @@
 #include "../../include/spiffe_b200_rng.h"
 
 #include "modules.cuh"
+#include "onaxis.hpp"
 #include "split32.cuh"
 
 // ---------------------------------------------------------------- errors
@@ -182,6 +183,11 @@ struct spiffe_gpu_instance {
   BirthBin *d_bins = nullptr, *h_bins = nullptr;
   size_t bins_n = 0;
   double *h_probe = nullptr; // pinned scratch for single values
+  // add_on_axis_fields: the prepared tables on the host, their device copy
+  // (z, Ez, D1, D2, D3 of each field, back to back) and the device views
+  std::vector<OnAxisProfile> onaxis;
+  double *d_onaxis_data = nullptr;
+  OnAxisField *d_onaxis = nullptr;
   PhaseTimer timer;
 };
 
@@ -230,6 +236,16 @@ static void set_devmesh(spiffe_gpu_instance *in)
   for (int k = 0; k < 6; k++)
     d.turn_off[k] = m.turn_off[k];
   d.has_solenoid = m.has_solenoid && (in->s32 ? in->s32->f.BzImposed != nullptr : in->f.BzImposed != nullptr);
+  d.n_onaxis = (int)in->onaxis.size();
+  d.onaxis = in->d_onaxis;
+}
+
+// The sine and cosine terms of every on-axis field at the push's time
+// (onAxisFields.c:229-238), into the mesh parameters the push receives.
+static void onaxis_terms(spiffe_gpu_instance *in)
+{
+  for (size_t i = 0; i < in->onaxis.size(); i++)
+    in->onaxis[i].terms(in->mesh.time, false, in->dm.oa_sin[i], in->dm.oa_bf[i]);
 }
 
 static int alloc_field(double **p, size_t n, cudaStream_t s)
@@ -747,6 +763,7 @@ static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, 
   const spiffe_mesh &m = in->mesh;
   if (o->tb_electrons_per_macroparticle)
     in->stiffness = 1; // advance_particles.c:280-281
+  onaxis_terms(in);
   Push32Params p{};
   p.time = m.time;
   p.dt = (float)m.dt;
@@ -862,7 +879,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
-               in->cnt, in->d_bins};
+               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1087,6 +1104,7 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
     return s32_push_step(in, o, 0);
   if (o->tb_electrons_per_macroparticle)
     in->stiffness = 1; // advance_particles.c:280-281
+  onaxis_terms(in);
   PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
                    o->tb_z_force, o->tb_r_force, o->tb_z_start_deceleration, o->tb_r_start_deceleration,
                    o->screen_momentum, o->compaction};
@@ -1694,6 +1712,62 @@ extern "C" int spiffe_gpu_set_test_beam(spiffe_gpu_instance *in, const spiffe_te
   return 0;
 }
 
+// process_on_axis_field_definition, onAxisFields.c:18-172, without the file
+// reading: the tables are prepared on the host and copied to the device once.
+extern "C" int spiffe_gpu_add_on_axis_field(spiffe_gpu_instance *in, const double *z, const double *Ez, int64_t n,
+                                            double z_offset, double Ez_peak, double frequency, double phase,
+                                            int32_t expansion_order)
+{
+  if (!in || !z || !Ez)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (Ez_peak == 0)
+    return 0; // ignored, onAxisFields.c:45-49
+  if (in->onaxis.size() >= SPIFFE_MAX_ON_AXIS)
+    return fail(SPIFFE_ERR_UNSUPPORTED, "more than %d on-axis fields", SPIFFE_MAX_ON_AXIS);
+  OnAxisProfile p;
+  const std::string err = onaxis_prepare(p, z, Ez, n, z_offset, Ez_peak, frequency, phase, expansion_order);
+  if (!err.empty())
+    return fail(SPIFFE_ERR_INVALID, "%s", err.c_str());
+  in->onaxis.push_back(std::move(p));
+  size_t total = 0;
+  for (const OnAxisProfile &q : in->onaxis)
+    total += q.z.size();
+  CUDA_TRY(cudaStreamSynchronize(in->stream)); // the old tables may still be read
+  cudaFree(in->d_onaxis_data);
+  cudaFree(in->d_onaxis);
+  in->d_onaxis_data = nullptr;
+  in->d_onaxis = nullptr;
+  CUDA_TRY(cudaMalloc(&in->d_onaxis_data, 5 * total * sizeof(double)));
+  CUDA_TRY(cudaMalloc(&in->d_onaxis, in->onaxis.size() * sizeof(OnAxisField)));
+  std::vector<OnAxisField> views;
+  double *d = in->d_onaxis_data;
+  for (const OnAxisProfile &q : in->onaxis) {
+    const size_t k = q.z.size();
+    OnAxisField v = q.view();
+    const std::vector<double> *src[5] = {&q.z, &q.Ez, &q.D1, &q.D2, &q.D3};
+    const double **dst[5] = {&v.z, &v.Ez, &v.D1, &v.D2, &v.D3};
+    for (int a = 0; a < 5; a++) {
+      CUDA_TRY(cudaMemcpy(d, src[a]->data(), k * sizeof(double), cudaMemcpyHostToDevice));
+      *dst[a] = d;
+      d += k;
+    }
+    views.push_back(v);
+  }
+  CUDA_TRY(cudaMemcpy(in->d_onaxis, views.data(), views.size() * sizeof(OnAxisField), cudaMemcpyHostToDevice));
+  set_devmesh(in);
+  return 0;
+}
+
+extern "C" int spiffe_gpu_on_axis_fields_at(spiffe_gpu_instance *in, double z, double r, double t, int32_t profile,
+                                            double *EzErBphi)
+{
+  if (!in || !EzErBphi)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  EzErBphi[0] = EzErBphi[1] = EzErBphi[2] = 0;
+  onaxis_eval(in->onaxis, z, r, t, profile != 0, EzErBphi[0], EzErBphi[1], EzErBphi[2]);
+  return 0;
+}
+
 // set_current_density, cathode.c:673-715
 static int set_current_density(spiffe_gpu_instance *in)
 {
@@ -1721,6 +1795,11 @@ static int set_current_density(spiffe_gpu_instance *in)
       CUDA_TRY(cudaMemcpyAsync(in->h_probe + 1, in->f.EzImposed + i, sizeof(double), cudaMemcpyDeviceToHost, in->stream));
       CUDA_TRY(cudaStreamSynchronize(in->stream));
       Ez += in->h_probe[0] + in->h_probe[1];
+    }
+    if (!in->onaxis.empty()) {
+      double dummy = 0;
+      onaxis_eval(in->onaxis, c.o.z_position, (c.o.inner_radius + c.o.outer_radius) / 2.0, m.time, false, Ez, dummy,
+                  dummy);
     }
     if (Ez >= 0 && c.initial_vz <= 0)
       continue;

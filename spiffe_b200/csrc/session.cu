@@ -22,6 +22,7 @@
 #include "../../include/spiffe_b200_session.h"
 #include "../../include/spiffe_b200_types.h"
 #include "namelist.hpp"
+#include "onaxis.hpp"
 #include "sdds.hpp"
 
 extern "C" int spiffe_set_error(int code, const char *msg);
@@ -169,6 +170,15 @@ struct SessionCathode {
   bool on_device = false;
 };
 
+// one add_on_axis_fields definition: the file's columns and the namelist
+// values, given to the device instance when it exists
+struct SessionOnAxis {
+  std::vector<double> z, Ez;
+  double z_offset = 0, Ez_peak = 0, frequency = 0, phase = 0;
+  long long order = 3;
+  bool on_device = false;
+};
+
 struct SessionAntenna {
   int direction = 0;
   long istart = 0, iend = 0, iposition = 0;
@@ -260,6 +270,8 @@ struct spiffe_session {
 
   std::vector<SessionCathode> cathodes;
   std::vector<SessionAntenna> antennas;
+  std::vector<SessionOnAxis> onaxis;
+  std::vector<OnAxisProfile> onaxis_prepared; // for the fields_used output
   std::vector<SessionScreen> screens;
   bool test_beam = false;
   spiffe_test_beam_options tb{};
@@ -333,6 +345,7 @@ struct spiffe_session {
   int cmd_solenoid(Args &g);
   int cmd_cathode(Args &g);
   int cmd_antenna(Args &g);
+  int cmd_on_axis_fields(Args &g);
   int cmd_screen(Args &g);
   int cmd_test_beam(Args &g);
   int cmd_poisson(Args &g);
@@ -627,6 +640,76 @@ int spiffe_session::cmd_cathode(Args &g)
   o.profile_t = o.profile_A = nullptr;
   c.o = o;
   cathodes.push_back(std::move(c));
+  return 0;
+}
+
+// --------------------------------------------------------- add_on_axis_fields
+
+// process_on_axis_field_definition, onAxisFields.c:18-172
+int spiffe_session::cmd_on_axis_fields(Args &g)
+{
+  std::string filename, z_name, Ez_name, fields_used;
+  SessionOnAxis d;
+  g.str("filename", filename);
+  g.str("z_name", z_name);
+  g.str("ez_name", Ez_name);
+  g.num("ez_peak", d.Ez_peak);
+  g.num("frequency", d.frequency);
+  g.num("phase", d.phase);
+  g.num("z_offset", d.z_offset);
+  g.integer("expansion_order", d.order);
+  g.str("fields_used", fields_used);
+  S_TRY(g.finish());
+  if (filename.empty())
+    return serr(SPIFFE_ERR_INVALID, "filename is blank");
+  if (z_name.empty())
+    return serr(SPIFFE_ERR_INVALID, "z_name is blank");
+  if (Ez_name.empty())
+    return serr(SPIFFE_ERR_INVALID, "Ez_name is blank");
+  if (d.Ez_peak == 0) {
+    warn("Ez_peak=0, so this field is ignored.");
+    return 0;
+  }
+  if (d.frequency == 0)
+    warn("frequency=0!");
+  std::vector<std::vector<double>> cols;
+  std::string err;
+  if (!spiffe_sdds::read_columns(filename, {z_name, Ez_name}, cols, err))
+    return serr(SPIFFE_ERR_INVALID, "add_on_axis_fields: %s", err.c_str());
+  d.z = cols[0];
+  d.Ez = cols[1];
+  OnAxisProfile p;
+  err = onaxis_prepare(p, d.z.data(), d.Ez.data(), (int64_t)d.z.size(), d.z_offset, d.Ez_peak, d.frequency, d.phase,
+                       d.order);
+  if (!err.empty())
+    return serr(SPIFFE_ERR_INVALID, "%s", err.c_str());
+  if (onaxis.size() >= SPIFFE_MAX_ON_AXIS)
+    return serr(SPIFFE_ERR_UNSUPPORTED, "more than %d on-axis fields", SPIFFE_MAX_ON_AXIS);
+  onaxis.push_back(std::move(d));
+  onaxis_prepared.push_back(std::move(p));
+  if (fields_used.empty())
+    return 0;
+  // the fields of every definition so far near the axis, sine and cosine 1
+  // (onAxisFields.c:130-170)
+  using namespace spiffe_sdds;
+  const long long nz = mesh.nz;
+  std::vector<double> zc, ez, er, bp;
+  for (long long iz = 0; iz < nz; iz++) {
+    double Ez = 0, Er = 0, Bphi = 0;
+    const double z = mesh.zmin + iz * mesh.dz;
+    onaxis_eval(onaxis_prepared, z, 1e-6, 0.0, true, Ez, Er, Bphi);
+    zc.push_back(z);
+    ez.push_back(Ez);
+    er.push_back(Er / 1e-6);
+    bp.push_back(Bphi / 1e-6);
+  }
+  Writer w;
+  if (!w.open(compose(fields_used, rootname), "", "", {},
+              {Def{"z", "m", "", T_DOUBLE}, Def{"Ez", "V/m", "", T_DOUBLE}, Def{"Er/r", "V/m$a2$n", "", T_DOUBLE},
+               Def{"Bphi/r", "T/m", "", T_DOUBLE}},
+              err) ||
+      !w.write_page({}, {}, nz, {zc.data(), ez.data(), er.data(), bp.data()}, err))
+    return serr(SPIFFE_ERR_INVALID, "add_on_axis_fields: %s", err.c_str());
   return 0;
 }
 
@@ -1350,6 +1433,12 @@ int spiffe_session::ensure_instance()
                                    an.phase, an.t.data(), an.W.data(), (int64_t)an.t.size()));
       an.on_device = true;
     }
+  for (SessionOnAxis &d : onaxis)
+    if (!d.on_device) {
+      S_TRY(spiffe_gpu_add_on_axis_field(inst, d.z.data(), d.Ez.data(), (int64_t)d.z.size(), d.z_offset, d.Ez_peak,
+                                         d.frequency, d.phase, (int32_t)d.order));
+      d.on_device = true;
+    }
   for (SessionScreen &sc : screens)
     if (!sc.on_device) {
       S_TRY(spiffe_gpu_add_screen(inst, sc.z, sc.direction, screen_capacity));
@@ -1585,6 +1674,8 @@ int spiffe_session::execute(const std::string &text)
       rc = cmd_cathode(g);
     else if (c == "define_antenna")
       rc = cmd_antenna(g);
+    else if (c == "add_on_axis_fields")
+      rc = cmd_on_axis_fields(g);
     else if (c == "define_screen")
       rc = cmd_screen(g);
     else if (c == "define_test_beam")
@@ -1612,7 +1703,7 @@ int spiffe_session::execute(const std::string &text)
       warn("%s: diagnostic output is not produced", c.c_str());
       rc = 0;
     } else if (c == "define_resistor" || c == "load_particles" || c == "set_up_translation" || c == "translate" ||
-               c == "add_on_axis_fields" || c == "define_secondary_emission" || c == "define_emitter") {
+               c == "define_secondary_emission" || c == "define_emitter") {
       rc = serr(SPIFFE_ERR_UNSUPPORTED, "%s is not supported", c.c_str());
     } else {
       rc = serr(SPIFFE_ERR_INVALID, "unknown namelist %s given", c.c_str());

@@ -197,7 +197,35 @@ DECK_DIAG = DECK_DCGUN.replace("finish_time=300e-12", "finish_time=120e-12").rep
     '&define_field_output filename="%s.fld", time_interval=40e-12, start_time=20e-12, z_interval=2, r_interval=4, '
     'separate_imposed_field=1 &end\n&integrate')
 sys.path.insert(0, os.path.dirname(HERE))
-from golden_columns import FLD_COLUMNS, SNAP_COLUMNS  # noqa: E402
+from golden_columns import FLD_COLUMNS, ONAXIS_COLUMNS, SNAP_COLUMNS  # noqa: E402
+
+# An on-axis RF field (add_on_axis_fields, onAxisFields.c) over the DC gun:
+# a synthetic two-harmonic Ez(z) table of 201 equispaced points, offset to
+# cover the cathode, pushed with the third-order off-axis expansion; the
+# cathode's Richardson-Schottky current density (cathode.c:673-715) reads
+# the same expansion at its position each step.
+DECK_ONAXIS = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02, boundary="dc.geo" &end
+&define_cathode z_position=1e-6, outer_radius=0.002, temperature=1800, work_function=2.0, start_time=0,
+    stop_time=60e-12, number_per_step=10, initial_pz=1e-6 &end
+&add_on_axis_fields filename="rf.sdds", z_name="z", Ez_name="Ez", Ez_peak=8e6, frequency=2.856e9, phase=220,
+    z_offset=-0.001, fields_used="%s.oaf" &end
+&define_screen filename="oa.sc1", z_position=0.012, direction="forward" &end
+&poisson_correction step_interval=4, accuracy=1e-4, error_charge_threshold=1e-15 &end
+&integrate dt_integration=4e-13, start_time=0, finish_time=140e-12, space_charge=1, imposed_Efield_ramp_time=20e-12 &end
+"""
+
+
+def rf_profile():
+    u = np.arange(201) / 200.0
+    return u * 0.02, np.sin(np.pi * u) + 0.3 * np.sin(2 * np.pi * u)
+
+
+def write_rf(path, z, Ez):
+    with open(path, "w") as f:
+        f.write("SDDS1\n&column name=z type=double units=m &end\n&column name=Ez type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(z, Ez):
+            f.write("%.17g %.17g\n" % (a, b))
 
 
 def decks():
@@ -227,11 +255,32 @@ def decks():
     save("deck_diagnostics", deck=np.array(DECK_DIAG), geo=np.array(geo), snap_pages=snap["pages"],
          fld_pages=fld["pages"], **{"snap_" + k: snap[k] for k in SNAP_COLUMNS},
          **{"fld_" + k: fld[k] for k in FLD_COLUMNS})
+    deck_onaxis(geo)
+
+
+def deck_onaxis(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    rz, rE = rf_profile()
+    write_rf(os.path.join(d, "rf.sdds"), rz, rE)
+    cmds = [b.strip() + " &end" for b in DECK_ONAXIS.split("&end") if b.strip()]
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("mesh",), ("get_beam",), ("screen", 0)] +
+                                 [("get_field", n) for n in ("Ez", "Er", "Bphi", "Psi")] +
+                                 [("table", 2, ONAXIS_COLUMNS)], cwd=d, capacity=20000)
+    mesh, rb, rs, oaf = res[0], res[1], res[2], res[-1]
+    out = dict(deck=np.array(DECK_ONAXIS), geo=np.array(geo), rf_z=rz, rf_Ez=rE, time=mesh["time"], **beam_out(rb))
+    out.update({"screen0_" + k: v for k, v in rs.items()})
+    out.update(dict(zip(("Ez", "Er", "Bphi", "Psi"), res[3:7])))
+    out.update({"oaf_" + k.replace("/", "_"): oaf[k] for k in ONAXIS_COLUMNS})
+    save("deck_onaxis", **out)
 
 
 if __name__ == "__main__":
     if sys.argv[1:] == ["decks"]:
         decks()
+    elif sys.argv[1:] == ["onaxis"]:
+        deck_onaxis(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     else:
         main()
         decks()

@@ -1,3 +1,6 @@
 """Column lists of the diagnostics fixture (tests/golden/make_golden.py)."""
 SNAP_COLUMNS = ["z", "r", "pz", "pr", "pphi", "q", "r0", "z0", "t0", "generation", "particleID", "status"]
 FLD_COLUMNS = ["z", "r", "rho", "Ez", "Er", "Bphi", "Jz", "Jr", "EzImposed", "ErImposed"]
+
+# add_on_axis_fields' fields_used table (onAxisFields.c:130-170)
+ONAXIS_COLUMNS = ["z", "Ez", "Er/r", "Bphi/r"]

@@ -412,3 +412,111 @@ def test_snapshots_and_field_output_match_reference(tmp_path, monkeypatch):
             assert np.array_equal(got, fx["fld_" + c]), c
     p0 = fld[0]["parameters"]
     assert p0["Variable1Name"] == "z" and p0["zDimension"] == 76 and p0["rDimension"] == 26
+
+
+def write_rf(path, z, Ez):
+    """The on-axis field table as tests/golden/make_golden.py writes it."""
+    with open(path, "w") as f:
+        f.write("SDDS1\n&column name=z type=double units=m &end\n&column name=Ez type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(z, Ez):
+            f.write("%.17g %.17g\n" % (a, b))
+
+
+def test_on_axis_profile_output_matches_reference(dcgeo):
+    """add_on_axis_fields' fields_used table (the expansion near the axis with
+    sine and cosine 1, onAxisFields.c:130-170) against the reference's, bit
+    for bit: this checks the scaling, the three derivatives and the
+    expansion's arithmetic on the host."""
+    fx = load("deck_onaxis")
+    write_rf(dcgeo / "rf.sdds", fx["rf_z"], fx["rf_Ez"])
+    deck = str(fx["deck"])
+    cmds = [b.strip() + " &end" for b in deck.split("&end") if b.strip()]
+    with session.Session(verbose=0, rootname="run") as s:
+        s.execute("\n".join(c for c in cmds if c.startswith(("&define_geometry", "&add_on_axis_fields"))))
+    pages = session.read_sdds(str(dcgeo / "run.oaf"))
+    assert len(pages) == 1
+    for c in ("z", "Ez", "Er/r", "Bphi/r"):
+        got = pages[0]["columns"][c]
+        assert len(got) == 151 and np.array_equal(got, fx["oaf_" + c.replace("/", "_")]), c
+
+
+@pytest.mark.parametrize("change,msg", [
+    ("expansion_order=4", "expansion_order must by on [0, 3]"),
+    ("frequency=-1", "frequency is negative"),
+    ("rows=4", "Too few points"),
+    ("reverse", "not monotonically increasing"),
+    ("uneven", "not equispaced"),
+])
+def test_on_axis_errors(dcgeo, change, msg):
+    z, Ez = np.linspace(0, 0.02, 41), np.sin(np.linspace(0, np.pi, 41))
+    extra = ""
+    if change == "rows=4":
+        z, Ez = z[:4], Ez[:4]
+    elif change == "reverse":
+        z = z[::-1].copy()
+    elif change == "uneven":
+        z = z.copy()
+        z[20] += 1e-5
+    else:
+        extra = ", " + change
+    write_rf(dcgeo / "rf.sdds", z, Ez)
+    with session.Session(verbose=0) as s:
+        with pytest.raises(gpu.SpiffeGpuError) as e:
+            s.execute(GEOM + '&add_on_axis_fields filename="rf.sdds", z_name="z", Ez_name="Ez", Ez_peak=1e6, '
+                      f'frequency=1e9{extra} &end\n')
+        assert msg in str(e.value), str(e.value)
+    # Ez_peak = 0 ignores the definition (onAxisFields.c:45-49)
+    write_rf(dcgeo / "rf.sdds", np.linspace(0, 0.02, 41), np.ones(41))
+    with session.Session(verbose=0) as s:
+        s.execute(GEOM + '&add_on_axis_fields filename="rf.sdds", z_name="z", Ez_name="Ez", Ez_peak=0 &end\n')
+
+
+@pytest.mark.gpu
+def test_on_axis_deck_matches_reference_bit_for_bit(tmp_path, monkeypatch):
+    """The DC gun with an RF on-axis field (add_on_axis_fields) and a
+    Richardson-Schottky cathode, in the FP64 form, against the reference's
+    perform_integration on the same deck: the push adds the third-order
+    off-axis expansion to every particle's fields, the cathode's current
+    density reads it at the cathode each step."""
+    fx = load("deck_onaxis")
+    write_rf(tmp_path / "rf.sdds", fx["rf_z"], fx["rf_Ez"])
+    s = run_deck(fx, tmp_path, monkeypatch)
+    assert s.mesh().time == float(fx["time"])
+    f = s.fields()
+    for n in ("Ez", "Er", "Bphi", "Psi"):
+        assert np.array_equal(f[n], fx[n]), n
+    g = s.instance()
+    b = g.download_beam(abi.Beam(int(fx["out_np"]) + 16))
+    assert b.np == int(fx["out_np"]) > 2000
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k][: b.np], fx["out_" + k]), k
+    pages = session.read_sdds(str(tmp_path / "oa.sc1"))
+    rec = by_id({c: np.concatenate([p["columns"][c] for p in pages]) for c in abi.SCREEN_COLUMNS + ["particleID"]})
+    ref = by_id({c: fx["screen0_" + c] for c in abi.SCREEN_COLUMNS + ["particleID"]})
+    assert len(rec["r"]) == len(ref["r"]) > 2000
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rec[c], ref[c]), c
+    s.close()
+
+
+@pytest.mark.gpu
+def test_split_form_runs_the_on_axis_deck(tmp_path, monkeypatch):
+    """The split-precision form on the on-axis deck against the FP64 form:
+    exit-screen moments within 0.5 %, the beam's count within 0.5 %."""
+    from spiffe_b200 import moments
+
+    fx = load("deck_onaxis")
+    out = {}
+    for prec, d in (("f64", "a"), ("split32", "b")):
+        (tmp_path / d).mkdir()
+        write_rf(tmp_path / d / "rf.sdds", fx["rf_z"], fx["rf_Ez"])
+        s = run_deck(fx, tmp_path / d, monkeypatch, precision=prec, compaction=abi.COMPACT_SWAP,
+                     screen_momentum=abi.SCREEN_PARTICLE)
+        pages = session.read_sdds(str(tmp_path / d / "oa.sc1"))
+        out[prec] = {c: np.concatenate([p["columns"][c] for p in pages]) for c in abi.SCREEN_COLUMNS}
+        s.close()
+    m64, m32 = moments.exit_moments(out["f64"]), moments.exit_moments(out["split32"])
+    assert m64["count"] > 2000 and abs(m32["count"] - m64["count"]) <= 0.005 * m64["count"], (m32, m64)
+    errs = moments.relative_errors(m32, m64)
+    assert max(errs.values()) < 5e-3, errs
