@@ -128,8 +128,10 @@ int spiffe_gpu_set_test_beam(spiffe_gpu_instance *inst, const spiffe_test_beam_o
  * is scaled to peak |Ez| = Ez_peak, three derivatives are taken, and the push
  * then adds the field's off-axis expansion (addOffAxisExpansionFields,
  * onAxisFields.c:208-268) to every particle's fields, as advance_particles.c
- * :836-844 does.  phase is in degrees.  Ez_peak = 0 ignores the field (the
- * reference warns).  Errors as the reference's: negative frequency,
+ * :836-844 does.  phase is in radians (ON_AXIS_FIELD.phase; the command's
+ * degrees times PI / 180).  Ez_peak = 0 ignores the field (the reference
+ * warns).  A table the reference has already prepared gives the same device
+ * field when passed with z_offset 0 and Ez_peak = its largest |Ez|.  Errors as the reference's: negative frequency,
  * expansion_order outside [0, 3], n <= 4, z not increasing, points not
  * equispaced to 1e-4.  At most 8 fields per instance. */
 int spiffe_gpu_add_on_axis_field(spiffe_gpu_instance *inst, const double *z, const double *Ez, int64_t n,

@@ -62,7 +62,7 @@ inline void onaxis_derivative(std::vector<double> &dF, const std::vector<double>
 // success, else the reference's message for the error.  Ez_peak = 0 is the
 // caller's case (the reference ignores such a field with a warning).
 inline std::string onaxis_prepare(OnAxisProfile &p, const double *z, const double *Ez, int64_t n, double z_offset,
-                                  double Ez_peak, double frequency, double phase_deg, int64_t order)
+                                  double Ez_peak, double frequency, double phase_rad, int64_t order)
 {
   if (frequency < 0)
     return "frequency is negative";
@@ -72,7 +72,7 @@ inline std::string onaxis_prepare(OnAxisProfile &p, const double *z, const doubl
     return "Too few points in file (need at least 4)";
   p.frequency = frequency;
   p.order = (int)order;
-  p.phase = phase_deg * SPIFFE_PI / 180.0;
+  p.phase = phase_rad;
   p.z.assign(z, z + n);
   p.Ez.assign(Ez, Ez + n);
   for (double &v : p.z)

@@ -174,7 +174,7 @@ struct SessionCathode {
 // values, given to the device instance when it exists
 struct SessionOnAxis {
   std::vector<double> z, Ez;
-  double z_offset = 0, Ez_peak = 0, frequency = 0, phase = 0;
+  double z_offset = 0, Ez_peak = 0, frequency = 0, phase = 0; // phase in radians once read
   long long order = 3;
   bool on_device = false;
 };
@@ -679,6 +679,7 @@ int spiffe_session::cmd_on_axis_fields(Args &g)
   d.z = cols[0];
   d.Ez = cols[1];
   OnAxisProfile p;
+  d.phase = d.phase * SPIFFE_PI / 180.0; // onAxisFields.c:70
   err = onaxis_prepare(p, d.z.data(), d.Ez.data(), (int64_t)d.z.size(), d.z_offset, d.Ez_peak, d.frequency, d.phase,
                        d.order);
   if (!err.empty())

@@ -81,6 +81,9 @@ def load():
         "spiffe_gpu_set_sort_interval": ([H, C.c_int64], C.c_int),
         "spiffe_gpu_batch_run": ([P(H), C.c_int32, P(C.c_int64), C.c_int32, C.c_int64, P(C.c_double)], C.c_int),
         "spiffe_gpu_set_test_beam": ([H, P(abi.TestBeamOptions)], C.c_int),
+        "spiffe_gpu_add_on_axis_field": ([H, P(C.c_double), P(C.c_double), C.c_int64, C.c_double, C.c_double,
+                                          C.c_double, C.c_double, C.c_int32], C.c_int),
+        "spiffe_gpu_on_axis_fields_at": ([H, C.c_double, C.c_double, C.c_double, C.c_int32, P(C.c_double)], C.c_int),
         "spiffe_session_create": ([C.c_int32, C.c_char_p, P(H)], C.c_int),
         "spiffe_session_destroy": ([H], C.c_int),
         "spiffe_session_execute": ([H, C.c_char_p], C.c_int),
@@ -256,6 +259,20 @@ class GpuInstance:
         _check(self.lib.spiffe_gpu_add_antenna(self.h, direction, istart, iend, iposition, current, frequency, phase,
                                                t.ctypes.data_as(P(C.c_double)), W.ctypes.data_as(P(C.c_double)),
                                                len(t)))
+
+    def add_on_axis_field(self, z, Ez, Ez_peak, frequency, phase_rad, z_offset=0.0, expansion_order=3):
+        """add_on_axis_fields on an Ez(z) table (phase in radians)."""
+        z = np.ascontiguousarray(z, np.float64)
+        Ez = np.ascontiguousarray(Ez, np.float64)
+        _check(self.lib.spiffe_gpu_add_on_axis_field(self.h, z.ctypes.data_as(P(C.c_double)),
+                                                     Ez.ctypes.data_as(P(C.c_double)), len(z), z_offset, Ez_peak,
+                                                     frequency, phase_rad, expansion_order))
+
+    def on_axis_fields_at(self, z, r, t, profile=False):
+        """(Ez, Er, Bphi) of the on-axis fields at (z, r) and time t."""
+        out = (C.c_double * 3)()
+        _check(self.lib.spiffe_gpu_on_axis_fields_at(self.h, z, r, t, int(profile), out))
+        return tuple(out)
 
     def configure_run(self, space_charge=1, push=None, poisson=None):
         self._push = push or abi.push_options()
