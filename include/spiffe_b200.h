@@ -137,6 +137,19 @@ int spiffe_gpu_set_test_beam(spiffe_gpu_instance *inst, const spiffe_test_beam_o
 int spiffe_gpu_add_on_axis_field(spiffe_gpu_instance *inst, const double *z, const double *Ez, int64_t n,
                                  double z_offset, double Ez_peak, double frequency, double phase,
                                  int32_t expansion_order);
+/* translate (setup_translation, translate.c:21-38): the moving window.  With
+ * enable != 0, the device loop (and spiffe_gpu_translate_problem) moves the
+ * problem by one dz whenever a particle lies past z_trigger, which must be in
+ * [zmin+dz, zmax-dz].  The reference's reduction of the integration region
+ * (z_lower, z_upper narrower than the mesh, translate.c:59-121) is not
+ * provided. */
+int spiffe_gpu_set_translation(spiffe_gpu_instance *inst, int32_t enable, double z_trigger);
+/* translate_problem, translate.c:40-197: if any particle is past the trigger,
+ * the TM (and TE) field rows move down one row (the top row zeroed), zmin,
+ * zmax and the trigger grow by dz; *translated (may be NULL) is 1 then, and
+ * *total (may be NULL) receives the total translation (FIELDS.zt).  Waits for
+ * the device (one flag is read back). */
+int spiffe_gpu_translate_problem(spiffe_gpu_instance *inst, int32_t *translated, double *total);
 /* The summed on-axis fields' (Ez, Er, Bphi) at (z, r) and time t, as the
  * push adds them; profile != 0 sets sine and cosine to 1 (the fields_used
  * output, onAxisFields.c:130-170). */

@@ -101,6 +101,8 @@ int ref_command(const char *text)
     process_snapshot_definition(&snapshot_defn, &EM, &nl);
   else if (strcmp(nl.group_name, "define_field_output") == 0)
     process_field_output_definition(&field_output_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "translate") == 0)
+    setup_translation(&EM, &nl);
   else if (strcmp(nl.group_name, "add_on_axis_fields") == 0)
     process_on_axis_field_definition(&EM, &nl);
   else if (strcmp(nl.group_name, "define_test_beam") == 0)

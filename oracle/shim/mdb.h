@@ -16,6 +16,7 @@
 #include <string.h>
 #include <math.h>
 #include <float.h>
+#include <inttypes.h>
 #include <limits.h>
 #include <stdint.h>
 

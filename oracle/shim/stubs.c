@@ -60,12 +60,3 @@ void add_resistor_currents(FIELDS *EM_problem, RESISTOR *resistor)
   (void)resistor;
   bomb("resistors are not part of the checked path", NULL);
 }
-
-void translate_problem(BEAM *beam, FIELDS *EM_problem, ANTENNA *antenna, long n_antennae, RESISTOR *resistor)
-{
-  (void)beam;
-  (void)EM_problem;
-  (void)antenna;
-  (void)n_antennae;
-  (void)resistor;
-}

@@ -95,3 +95,10 @@ extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, con
 extern "C" int spiffe_antenna64(double *J, int pitch, int direction, long istart, long iend, long iposition,
                                 double value, cudaStream_t s);
 
+// translate_problem (translate.c:51-57, :123-196): *flag = 1 when a particle
+// ip < np lies past `trigger`; rows 0..nz of an array move down one row
+// (`scratch` holds nz rows), the last row zeroed
+extern "C" int spiffe_beyond64(const double *z, const DevCounts *cnt, long long np_bound, double trigger, int *flag,
+                               cudaStream_t s);
+extern "C" int spiffe_rows_down(void *a, size_t row, int nz, void *scratch, cudaStream_t s);
+

@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -188,6 +189,12 @@ struct spiffe_gpu_instance {
   std::vector<OnAxisProfile> onaxis;
   double *d_onaxis_data = nullptr;
   OnAxisField *d_onaxis = nullptr;
+  // translate (the moving window): the trigger, the total translation, a
+  // device flag and a scratch array of nz rows
+  bool tr_on = false;
+  double tr_trigger = 0, tr_zt = 0;
+  int *d_tr_flag = nullptr;
+  void *d_tr_scratch = nullptr;
   PhaseTimer timer;
 };
 
@@ -879,7 +886,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
-               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis};
+               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1758,6 +1765,89 @@ extern "C" int spiffe_gpu_add_on_axis_field(spiffe_gpu_instance *in, const doubl
   return 0;
 }
 
+// setup_translation, translate.c:21-38; the region reduction of z_lower and
+// z_upper (translate.c:59-121) is the caller's to reject
+extern "C" int spiffe_gpu_set_translation(spiffe_gpu_instance *in, int32_t enable, double z_trigger)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const spiffe_mesh &m = in->mesh;
+  if (enable && (z_trigger < m.zmin + m.dz || z_trigger > m.zmax - m.dz))
+    return fail(SPIFFE_ERR_INVALID, "z_trigger is not in range [zmin+dz, zmax-dz]");
+  if (enable && !in->d_tr_flag) {
+    CUDA_TRY(cudaMalloc(&in->d_tr_flag, sizeof(int)));
+    CUDA_TRY(cudaMalloc(&in->d_tr_scratch, (size_t)m.nz * in->dm.pitch * sizeof(double)));
+  }
+  in->tr_on = enable != 0;
+  in->tr_trigger = z_trigger;
+  return 0;
+}
+
+// translate_problem, translate.c:40-197 (without the region reduction):
+// *translated = 1 when the problem moved by one dz
+static int translate(spiffe_gpu_instance *in, int32_t *translated)
+{
+  if (translated)
+    *translated = 0;
+  if (!in->tr_on)
+    return 0;
+  spiffe_mesh &m = in->mesh;
+  cudaStream_t s = in->stream;
+  S32State *S = in->s32;
+  int *h = (int *)in->h_probe;
+  CUDA_TRY(cudaMemsetAsync(in->d_tr_flag, 0, sizeof(int), s));
+  const int rc = S ? s32_beyond(S->b.cell, S->b.fz, in->cnt, in->np_upper, m.zmin, m.dz, in->tr_trigger, in->d_tr_flag, s)
+                   : spiffe_beyond64(in->b.z, in->cnt, in->np_upper, in->tr_trigger, in->d_tr_flag, s);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "translation test launch failed");
+  CUDA_TRY(cudaMemcpyAsync(h, in->d_tr_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  if (!*h)
+    return 0;
+  const int P = in->dm.pitch;
+  std::vector<std::pair<void *, size_t>> rows;
+  if (S) {
+    const DevFields32 &F = S->f;
+    if (m.modes & SPIFFE_FL_TM_FIELDS)
+      rows.insert(rows.end(), {{F.Ez, 4}, {F.Jz, 8}, {F.Er, 4}, {F.Jr, 8}, {F.Bphi, 4}, {F.Bphi2, 4}});
+    if (m.modes & SPIFFE_FL_TE_FIELDS)
+      rows.insert(rows.end(), {{F.Ephi, 4}, {F.Jphi, 8}, {F.Br, 4}, {F.Br2, 4}, {F.Bz, 4}, {F.Bz2, 4}});
+  } else {
+    const DevFields<double> &F = in->f;
+    if (m.modes & SPIFFE_FL_TM_FIELDS)
+      rows.insert(rows.end(), {{F.Ez, 8}, {F.Jz, 8}, {F.Er, 8}, {F.Jr, 8}, {F.Bphi, 8}, {F.Bphi2, 8}});
+    if (m.modes & SPIFFE_FL_TE_FIELDS)
+      rows.insert(rows.end(), {{F.Ephi, 8}, {F.Jphi, 8}, {F.Br, 8}, {F.Br2, 8}, {F.Bz, 8}, {F.Bz2, 8}});
+  }
+  for (auto &a : rows)
+    if (spiffe_rows_down(a.first, a.second * (size_t)P, m.nz, in->d_tr_scratch, s))
+      return fail(SPIFFE_ERR_CUDA, "translation copy failed");
+  if (S && s32_cells_down(S->b.cell, S->f.jbox, in->cnt, in->np_upper, s))
+    return fail(SPIFFE_ERR_CUDA, "translation launch failed");
+  // a screen's cell moves with the particles' cells (the split push finds
+  // crossings by cell)
+  for (int k = 0; k < in->screens.n; k++)
+    in->screens.s[k].cell -= 1;
+  m.zmin += m.dz;
+  m.zmax += m.dz;
+  in->tr_zt += m.dz;
+  in->tr_trigger += m.dz;
+  set_devmesh(in);
+  if (translated)
+    *translated = 1;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_translate_problem(spiffe_gpu_instance *in, int32_t *translated, double *total)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  RC_TRY(translate(in, translated));
+  if (total)
+    *total = in->tr_zt;
+  return 0;
+}
+
 extern "C" int spiffe_gpu_on_axis_fields_at(spiffe_gpu_instance *in, double z, double r, double t, int32_t profile,
                                             double *EzErBphi)
 {
@@ -1969,6 +2059,7 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
         S->j_state = S32_J_ZERO;
       S->since_sort++;
     }
+    RC_TRY(translate(in, nullptr));
     RC_TRY(set_current_density(in));
     m.time_step++;
   }

@@ -272,6 +272,8 @@ struct spiffe_session {
   std::vector<SessionAntenna> antennas;
   std::vector<SessionOnAxis> onaxis;
   std::vector<OnAxisProfile> onaxis_prepared; // for the fields_used output
+  bool translate_on = false, translate_set = false; // translate: the moving window
+  double z_trigger = 0;
   std::vector<SessionScreen> screens;
   bool test_beam = false;
   spiffe_test_beam_options tb{};
@@ -346,6 +348,7 @@ struct spiffe_session {
   int cmd_cathode(Args &g);
   int cmd_antenna(Args &g);
   int cmd_on_axis_fields(Args &g);
+  int cmd_translate(Args &g);
   int cmd_screen(Args &g);
   int cmd_test_beam(Args &g);
   int cmd_poisson(Args &g);
@@ -711,6 +714,33 @@ int spiffe_session::cmd_on_axis_fields(Args &g)
               err) ||
       !w.write_page({}, {}, nz, {zc.data(), ez.data(), er.data(), bp.data()}, err))
     return serr(SPIFFE_ERR_INVALID, "add_on_axis_fields: %s", err.c_str());
+  return 0;
+}
+
+// ------------------------------------------------------------------ translate
+
+// setup_translation, translate.c:21-38
+int spiffe_session::cmd_translate(Args &g)
+{
+  if (inst)
+    S_TRY(spiffe_gpu_get_mesh(inst, &mesh));
+  const spiffe_mesh &m = mesh;
+  double trig = m.zmax - 5 * m.dz, lower = m.zmin, upper = m.zmax;
+  g.num("z_trigger", trig);
+  g.num("z_lower", lower);
+  g.num("z_upper", upper);
+  S_TRY(g.finish());
+  if (trig < m.zmin + m.dz || trig > m.zmax - m.dz)
+    return serr(SPIFFE_ERR_INVALID, "z_trigger is not in range [zmin+dz, zmax-dz]");
+  if (lower != upper && !(lower <= m.zmin && upper >= m.zmax))
+    return serr(SPIFFE_ERR_UNSUPPORTED, "translate: reducing the integration region (z_lower, z_upper) is not supported");
+  translate_on = true;
+  z_trigger = trig;
+  translate_set = false;
+  if (inst) {
+    S_TRY(spiffe_gpu_set_translation(inst, 1, z_trigger));
+    translate_set = true;
+  }
   return 0;
 }
 
@@ -1446,6 +1476,10 @@ int spiffe_session::ensure_instance()
       sc.on_device = true;
     }
   S_TRY(spiffe_gpu_set_test_beam(inst, test_beam ? &tb : nullptr));
+  if (translate_on && !translate_set) {
+    S_TRY(spiffe_gpu_set_translation(inst, 1, z_trigger));
+    translate_set = true;
+  }
   return 0;
 }
 
@@ -1703,7 +1737,9 @@ int spiffe_session::execute(const std::string &text)
     } else if (c == "define_field_sampling") {
       warn("%s: diagnostic output is not produced", c.c_str());
       rc = 0;
-    } else if (c == "define_resistor" || c == "load_particles" || c == "set_up_translation" || c == "translate" ||
+    } else if (c == "translate") {
+      rc = cmd_translate(g);
+    } else if (c == "define_resistor" || c == "load_particles" ||
                c == "define_secondary_emission" || c == "define_emitter") {
       rc = serr(SPIFFE_ERR_UNSUPPORTED, "%s is not supported", c.c_str());
     } else {

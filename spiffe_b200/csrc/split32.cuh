@@ -107,6 +107,11 @@ extern "C" int s32_from_fixed(const DevMesh *m, const long long *src, double *d_
 extern "C" int s32_rescale_fixed(long long *a, size_t n, int shift, cudaStream_t s);
 extern "C" int s32_antenna(long long *J, int *jbox, int pitch, int direction, long istart, long iend, long iposition,
                            double value, double qJ, cudaStream_t s);
+// the moving window's trigger test and the particles' (and deposited
+// current rows') move down one row (translate.cu)
+extern "C" int s32_beyond(const int32_t *cell, const float *fz, const DevCounts *cnt, long long np_bound, double zmin,
+                          double dz, double trigger, int *flag, cudaStream_t s);
+extern "C" int s32_cells_down(int32_t *cell, int *jbox, const DevCounts *cnt, long long np_bound, cudaStream_t s);
 
 // particles (particles_f32.cu)
 struct Particles32Work {

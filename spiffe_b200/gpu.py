@@ -84,6 +84,8 @@ def load():
         "spiffe_gpu_add_on_axis_field": ([H, P(C.c_double), P(C.c_double), C.c_int64, C.c_double, C.c_double,
                                           C.c_double, C.c_double, C.c_int32], C.c_int),
         "spiffe_gpu_on_axis_fields_at": ([H, C.c_double, C.c_double, C.c_double, C.c_int32, P(C.c_double)], C.c_int),
+        "spiffe_gpu_set_translation": ([H, C.c_int32, C.c_double], C.c_int),
+        "spiffe_gpu_translate_problem": ([H, P(C.c_int32), P(C.c_double)], C.c_int),
         "spiffe_session_create": ([C.c_int32, C.c_char_p, P(H)], C.c_int),
         "spiffe_session_destroy": ([H], C.c_int),
         "spiffe_session_execute": ([H, C.c_char_p], C.c_int),
@@ -273,6 +275,16 @@ class GpuInstance:
         out = (C.c_double * 3)()
         _check(self.lib.spiffe_gpu_on_axis_fields_at(self.h, z, r, t, int(profile), out))
         return tuple(out)
+
+    def set_translation(self, enable, z_trigger):
+        """translate's moving window (z_trigger in [zmin+dz, zmax-dz])."""
+        _check(self.lib.spiffe_gpu_set_translation(self.h, int(enable), z_trigger))
+
+    def translate_problem(self):
+        """translate_problem: (moved this call, total translation)."""
+        moved, total = C.c_int32(), C.c_double()
+        _check(self.lib.spiffe_gpu_translate_problem(self.h, C.byref(moved), C.byref(total)))
+        return bool(moved.value), total.value
 
     def configure_run(self, space_charge=1, push=None, poisson=None):
         self._push = push or abi.push_options()

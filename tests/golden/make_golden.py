@@ -9,6 +9,7 @@ reference present.  Run from the repository root:
 
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py decks    # the input-deck fixtures only
+    python tests/golden/make_golden.py onaxis   # one deck fixture (also: translate)
 """
 import os
 import sys
@@ -215,6 +216,27 @@ DECK_ONAXIS = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02
 """
 
 
+# The DC gun deck with the moving window (translate, translate.c): once a
+# particle passes z = 8 mm the problem moves by dz each step that one lies
+# past the (moving) trigger.
+DECK_TRANSLATE = DECK_DCGUN.replace("&integrate", "&translate z_trigger=0.008 &end\n&integrate")
+
+
+def deck_translate(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    cmds = [b.strip() + " &end" for b in DECK_TRANSLATE.split("&end") if b.strip()]
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("mesh",), ("get_beam",), ("screen", 0)] +
+                                 [("get_field", n) for n in ("Ez", "Er", "Bphi", "Psi")], cwd=d, capacity=20000)
+    mesh, rb, rs = res[0], res[1], res[2]
+    out = dict(deck=np.array(DECK_TRANSLATE), geo=np.array(geo), time=mesh["time"], zmin=mesh["zmin"],
+               zmax=mesh["zmax"], **beam_out(rb))
+    out.update({"screen0_" + k: v for k, v in rs.items()})
+    out.update(dict(zip(("Ez", "Er", "Bphi", "Psi"), res[3:7])))
+    save("deck_translate", **out)
+
+
 def rf_profile():
     u = np.arange(201) / 200.0
     return u * 0.02, np.sin(np.pi * u) + 0.3 * np.sin(2 * np.pi * u)
@@ -256,6 +278,7 @@ def decks():
          fld_pages=fld["pages"], **{"snap_" + k: snap[k] for k in SNAP_COLUMNS},
          **{"fld_" + k: fld[k] for k in FLD_COLUMNS})
     deck_onaxis(geo)
+    deck_translate(geo)
 
 
 def deck_onaxis(geo):
@@ -279,6 +302,8 @@ def deck_onaxis(geo):
 if __name__ == "__main__":
     if sys.argv[1:] == ["decks"]:
         decks()
+    elif sys.argv[1:] == ["translate"]:
+        deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["onaxis"]:
         deck_onaxis(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     else:

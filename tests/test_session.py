@@ -520,3 +520,68 @@ def test_split_form_runs_the_on_axis_deck(tmp_path, monkeypatch):
     assert m64["count"] > 2000 and abs(m32["count"] - m64["count"]) <= 0.005 * m64["count"], (m32, m64)
     errs = moments.relative_errors(m32, m64)
     assert max(errs.values()) < 5e-3, errs
+
+
+def test_translate_checks(dcgeo):
+    """translate's range check (translate.c:35-36); the region reduction of
+    z_lower/z_upper is refused."""
+    with session.Session(verbose=0) as s:
+        with pytest.raises(gpu.SpiffeGpuError) as e:
+            s.execute(GEOM + "&translate z_trigger=0.0299 &end\n")
+        assert "z_trigger is not in range" in str(e.value)
+    with session.Session(verbose=0) as s:
+        with pytest.raises(gpu.SpiffeGpuError) as e:
+            s.execute(GEOM + "&translate z_trigger=0.01, z_lower=0.005 &end\n")
+        assert f"error {ERR_UNSUPPORTED}" in str(e.value) and "z_lower" in str(e.value)
+    with session.Session(verbose=0) as s:
+        s.execute(GEOM + "&translate &end\n")  # default trigger zmax - 5 dz
+
+
+@pytest.mark.gpu
+def test_translate_deck_matches_reference_bit_for_bit(tmp_path, monkeypatch):
+    """The DC gun deck with the moving window (translate) in the FP64 form
+    against the reference on the same deck: 316 translations, then the same
+    mesh position, fields, beam and screen records."""
+    fx = load("deck_translate")
+    s = run_deck(fx, tmp_path, monkeypatch)
+    m = s.mesh()
+    assert m.time == float(fx["time"]) and m.zmin == float(fx["zmin"]) and m.zmax == float(fx["zmax"])
+    assert m.zmin > 0.06
+    f = s.fields()
+    for n in ("Ez", "Er", "Bphi", "Psi"):
+        assert np.array_equal(f[n], fx[n]), n
+    b = s.instance().download_beam(abi.Beam(int(fx["out_np"]) + 16))
+    assert b.np == int(fx["out_np"]) > 800
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k][: b.np], fx["out_" + k]), k
+    pages = session.read_sdds(str(tmp_path / "deck.sc1"))
+    rec = by_id({c: np.concatenate([p["columns"][c] for p in pages]) for c in abi.SCREEN_COLUMNS + ["particleID"]})
+    ref = by_id({c: fx["screen0_" + c] for c in abi.SCREEN_COLUMNS + ["particleID"]})
+    assert len(rec["r"]) == len(ref["r"]) > 900
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rec[c], ref[c]), c
+    s.close()
+
+
+@pytest.mark.gpu
+def test_split_form_runs_the_translate_deck(tmp_path, monkeypatch):
+    """The split form (positions stored relative to the moving mesh) on the
+    moving-window deck against the FP64 form: the same number of
+    translations, exit moments within 0.5 %."""
+    from spiffe_b200 import moments
+
+    fx = load("deck_translate")
+    out, zmin = {}, {}
+    for prec, d in (("f64", "a"), ("split32", "b")):
+        (tmp_path / d).mkdir()
+        s = run_deck(fx, tmp_path / d, monkeypatch, precision=prec, compaction=abi.COMPACT_SWAP,
+                     screen_momentum=abi.SCREEN_PARTICLE)
+        zmin[prec] = s.mesh().zmin
+        pages = session.read_sdds(str(tmp_path / d / "deck.sc1"))
+        out[prec] = {c: np.concatenate([p["columns"][c] for p in pages]) for c in abi.SCREEN_COLUMNS}
+        s.close()
+    assert zmin["split32"] == zmin["f64"] > 0.06
+    m64, m32 = moments.exit_moments(out["f64"]), moments.exit_moments(out["split32"])
+    assert m64["count"] > 900 and abs(m32["count"] - m64["count"]) <= 0.005 * m64["count"], (m32, m64)
+    errs = moments.relative_errors(m32, m64)
+    assert max(errs.values()) < 5e-3, errs
