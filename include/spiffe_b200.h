@@ -150,6 +150,13 @@ int spiffe_gpu_set_translation(spiffe_gpu_instance *inst, int32_t enable, double
  * *total (may be NULL) receives the total translation (FIELDS.zt).  Waits for
  * the device (one flag is read back). */
 int spiffe_gpu_translate_problem(spiffe_gpu_instance *inst, int32_t *translated, double *total);
+/* do_status_printouts' values (status_pr.c:18-356, kinetic_energy and
+ * field_energy :358-452) for the current state; reads the fields and the
+ * beam back, so it waits for the device.  JCathode is the first cathode's
+ * current density (0 without one); EzOOEMin/Max are the last push's extremes
+ * of the summed on-axis Ez (+inf/-inf when no particle met an on-axis field,
+ * 0 before the first push). */
+int spiffe_gpu_status_report(spiffe_gpu_instance *inst, spiffe_status_row *row);
 /* The summed on-axis fields' (Ez, Er, Bphi) at (z, r) and time t, as the
  * push adds them; profile != 0 sets sine and cosine to 1 (the fields_used
  * output, onAxisFields.c:130-170). */

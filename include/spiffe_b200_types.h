@@ -179,6 +179,22 @@ typedef struct spiffe_poisson_report {
   double residual, driving; /* final sum|residual|, sum|rhs| of the solve */
 } spiffe_poisson_report;
 
+/* One status report (do_status_printouts, status_pr.c:18-356): the values of
+ * one row of the status file (setUpStatusOutputFile, status_pr.c:454-499)
+ * except NewParticles, which is the caller's (Particles minus the previous
+ * row's).  The beam moments cover all np particles, active or not, as the
+ * reference's do; Charge sums the active ones. */
+typedef struct spiffe_status_row {
+  double t, JCathode, KineticEnergy, FieldEnergy, TotalEnergy, Charge, EzAbsMax, ErAbsMax;
+  int64_t Particles, ActiveParticles, SecondaryParticles;
+  double zMax, zMin, zAve, zRMS, zStDev;
+  double rMax, rMin, rAve, rRMS, rStDev;
+  double pzMax, pzMin, pzAve, pzRMS, pzStDev;
+  double prMax, prMin, prAve, prRMS, prStDev;
+  double EzOOEMin, EzOOEMax;
+  double ElectricEnergy, MagneticEnergy; /* FieldEnergy's two parts */
+} spiffe_status_row;
+
 #ifdef __cplusplus
 }
 #endif

@@ -305,7 +305,9 @@ def _child(program, capacity, cwd):
                 d[col] = a
             out.append(d)
         elif kind == "table":
-            # ("table", which, [columns]): which 0 beam snapshots, 1 field output
+            # ("table", which, [columns]): which 0 beam snapshots, 1 field output,
+            # 2 + k the k-th table closed inside a command, 100 + k the k-th
+            # table written row by row (the status file)
             which, cols = args
             d = {"pages": lib.ref_table_pages(which)}
             for col in cols:

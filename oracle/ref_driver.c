@@ -57,6 +57,7 @@ int ref_session_init(long particle_capacity)
   initialized = 1;
   memset(&EM, 0, sizeof(EM));
   shim_n_closed_tables = 0;
+  shim_n_updated_tables = 0;
   memset(&beam, 0, sizeof(beam));
   EM.run_name = "checker";
   EM.rootname = strdup("checker");
@@ -414,13 +415,16 @@ void ref_step(long space_charge, double z_forces_start)
  * table (which 1), all pages in order; returns the row count, -1 for an
  * unknown column */
 /* which: 0 the beam snapshots, 1 the field output, 2 + k the k-th output
- * table the reference closed inside a command */
+ * table the reference closed inside a command, 100 + k the k-th table it
+ * wrote row by row (the status file) */
 static SDDS_DATASET *ref_table(long which)
 {
   if (which == 0)
     return &snapshot_defn.table;
   if (which == 1)
     return &field_output_defn.SDDSout;
+  if (which >= 100)
+    return which - 100 < shim_n_updated_tables ? &shim_updated_tables[which - 100] : NULL;
   if (which - 2 < shim_n_closed_tables)
     return &shim_closed_tables[which - 2];
   return NULL;

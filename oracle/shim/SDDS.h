@@ -39,7 +39,7 @@
 #define SDDS_CHECK_OKAY 0
 #define SDDS_CHECK_NONEXISTENT 1
 
-#define SHIM_SDDS_MAX_COLUMNS 32
+#define SHIM_SDDS_MAX_COLUMNS 64
 
 typedef struct {
   int n_columns;
@@ -56,6 +56,8 @@ typedef SDDS_DATASET SDDS_TABLE;
 #define SHIM_MAX_CLOSED_TABLES 16
 extern SDDS_DATASET shim_closed_tables[SHIM_MAX_CLOSED_TABLES];
 extern int shim_n_closed_tables;
+extern SDDS_DATASET shim_updated_tables[SHIM_MAX_CLOSED_TABLES];
+extern int shim_n_updated_tables;
 
 int32_t SDDS_InitializeOutput(SDDS_DATASET *t, int32_t data_mode, int32_t lines_per_row,
                               const char *description, const char *contents, const char *filename);

@@ -685,7 +685,32 @@ int32_t SDDS_WriteTable(SDDS_DATASET *t) { return SDDS_WritePage(t); }
 
 int32_t SDDS_GetColumnIndex(SDDS_DATASET *t, char *name) { return col_index(t, name); }
 int32_t SDDS_NumberOfErrors(void) { return 0; }
-int32_t SDDS_UpdatePage(SDDS_DATASET *t, uint32_t mode) { (void)mode; return SDDS_WritePage(t); }
+/* Tables written row by row with SDDS_UpdatePage and never closed (the
+ * status file lives on perform_integration's stack, integrate.c:50, :79-80):
+ * a copy of each, by its address, taken at every update; the rows stay on
+ * the heap after the function returns. */
+SDDS_DATASET shim_updated_tables[SHIM_MAX_CLOSED_TABLES];
+static const void *shim_updated_keys[SHIM_MAX_CLOSED_TABLES];
+int shim_n_updated_tables;
+
+int32_t SDDS_UpdatePage(SDDS_DATASET *t, uint32_t mode)
+{
+  int k;
+  (void)mode;
+  /* the rows set so far stay on the open page (row numbers count from its
+     start), so the page is not advanced */
+  for (k = 0; k < shim_n_updated_tables; k++)
+    if (shim_updated_keys[k] == t)
+      break;
+  if (k < SHIM_MAX_CLOSED_TABLES) {
+    if (k == shim_n_updated_tables)
+      shim_updated_keys[shim_n_updated_tables++] = t;
+    shim_updated_tables[k] = *t;
+    shim_updated_tables[k].n_rows = t->n_rows + t->page_len;
+    shim_updated_tables[k].pages = t->pages + 1;
+  }
+  return 1;
+}
 /* Output tables the reference closes inside a command (a local dataset, as
  * for add_on_axis_fields' fields_used file, onAxisFields.c:130-170) are kept
  * here, in the order they were closed, so the checker can still read them. */

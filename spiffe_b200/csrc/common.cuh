@@ -37,6 +37,7 @@ struct DevMesh {
   int n_onaxis;
   const OnAxisField *onaxis;
   double oa_sin[SPIFFE_MAX_ON_AXIS], oa_bf[SPIFFE_MAX_ON_AXIS];
+  double *oa_ext; // DevCounts' (oa_min, oa_max): the push's extremes of the summed on-axis Ez
 };
 
 // addOffAxisExpansionFields (onAxisFields.c:208-268) at (z, r): each of
@@ -47,7 +48,8 @@ struct DevMesh {
 // last point at or below z).  As in the reference, each field that covers z
 // sets Er to zero before adding its own terms.
 __host__ __device__ inline void onaxis_expand(const OnAxisField *fields, int n_fields, const double *sin_wt,
-                                              const double *bf, double z, double r, double &Ez, double &Er, double &Bphi)
+                                              const double *bf, double z, double r, double &Ez, double &Er, double &Bphi,
+                                              double *lo = nullptr, double *hi = nullptr)
 {
   for (int ip = 0; ip < n_fields; ip++) {
     const OnAxisField &F = fields[ip];
@@ -89,6 +91,34 @@ __host__ __device__ inline void onaxis_expand(const OnAxisField *fields, int n_f
         }
       }
     }
+    if (lo) { // EzMin, EzMax (onAxisFields.c:262-265)
+      if (*lo > Ez)
+        *lo = Ez;
+      if (*hi < Ez)
+        *hi = Ez;
+    }
+  }
+}
+
+__device__ inline void atomic_min_f64(double *a, double v)
+{
+  unsigned long long *p = (unsigned long long *)a, old = *p;
+  while (__longlong_as_double((long long)old) > v) {
+    const unsigned long long seen = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
+    if (seen == old)
+      break;
+    old = seen;
+  }
+}
+
+__device__ inline void atomic_max_f64(double *a, double v)
+{
+  unsigned long long *p = (unsigned long long *)a, old = *p;
+  while (__longlong_as_double((long long)old) < v) {
+    const unsigned long long seen = atomicCAS(p, old, (unsigned long long)__double_as_longlong(v));
+    if (seen == old)
+      break;
+    old = seen;
   }
 }
 
@@ -96,8 +126,12 @@ __host__ __device__ inline void onaxis_expand(const OnAxisField *fields, int n_f
 // (advance_particles.c:836-844).
 __device__ __forceinline__ void onaxis_add(const DevMesh &m, double z, double r, double &Ez, double &Er, double &Bphi)
 {
-  double EzO = 0, ErO = 0, BphiO = 0;
-  onaxis_expand(m.onaxis, m.n_onaxis, m.oa_sin, m.oa_bf, z, r, EzO, ErO, BphiO);
+  double EzO = 0, ErO = 0, BphiO = 0, lo = INFINITY, hi = -INFINITY;
+  onaxis_expand(m.onaxis, m.n_onaxis, m.oa_sin, m.oa_bf, z, r, EzO, ErO, BphiO, &lo, &hi);
+  if (lo <= hi) {
+    atomic_min_f64(m.oa_ext, lo);
+    atomic_max_f64(m.oa_ext + 1, hi);
+  }
   Ez += EzO;
   Er += ErO;
   Bphi += BphiO;
@@ -150,6 +184,7 @@ struct DevCounts {
   long long screen_overflow;
   double last_pz0, last_pr0, last_rpphi0; // pre-kick momenta of particle np-1
   long long pushed;                       // sum over pushes of the active count (particle-steps)
+  double oa_min, oa_max;                  // EzOOEMin, EzOOEMax of the last push (advance_particles.c:113-114)
   long long sor_halfsweeps, sor_solves;   // red-black half-sweeps and solves run
   unsigned int error;                     // SPIFFE_DEV_ERR_* bits
   unsigned int pad;

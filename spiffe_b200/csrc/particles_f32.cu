@@ -723,6 +723,8 @@ __global__ void k_reset_step_counts32(DevCounts *cnt)
   cnt->n_lost = 0;
   cnt->new_active = 0;
   cnt->pushed += cnt->npActive;
+  cnt->oa_min = INFINITY; // HUGE, advance_particles.c:113-114
+  cnt->oa_max = -INFINITY;
 }
 
 // The reference's removal: the first lost index ends the beam (:490-518 as released).

@@ -9,6 +9,7 @@
 // 116-119).  Particle counts live on the device; the host tracks an upper
 // bound for launch sizes and reads the true count only when it must.
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstddef>
@@ -245,6 +246,7 @@ static void set_devmesh(spiffe_gpu_instance *in)
   d.has_solenoid = m.has_solenoid && (in->s32 ? in->s32->f.BzImposed != nullptr : in->f.BzImposed != nullptr);
   d.n_onaxis = (int)in->onaxis.size();
   d.onaxis = in->d_onaxis;
+  d.oa_ext = in->cnt ? (double *)((char *)in->cnt + offsetof(DevCounts, oa_min)) : nullptr;
 }
 
 // The sine and cosine terms of every on-axis field at the push's time
@@ -1845,6 +1847,197 @@ extern "C" int spiffe_gpu_translate_problem(spiffe_gpu_instance *in, int32_t *tr
   RC_TRY(translate(in, translated));
   if (total)
     *total = in->tr_zt;
+  return 0;
+}
+
+// computeMoments as the checker's SDDS stand-in defines it: mean, rms about
+// zero, standard deviation with n-1 (SDDS's mdbmth, absent here)
+static void moments(const double *x, int64_t n, double &ave, double &rms, double &sd)
+{
+  double s = 0, s2 = 0, d = 0;
+  for (int64_t i = 0; i < n; i++) {
+    s += x[i];
+    s2 += x[i] * x[i];
+  }
+  const double m = s / n;
+  for (int64_t i = 0; i < n; i++)
+    d += (x[i] - m) * (x[i] - m);
+  ave = m;
+  rms = std::sqrt(s2 / n);
+  sd = n > 1 ? std::sqrt(d / (n - 1)) : 0;
+}
+
+static void min_max(const double *x, int64_t n, double &lo, double &hi)
+{
+  lo = DBL_MAX;
+  hi = -DBL_MAX;
+  for (int64_t i = 0; i < n; i++) {
+    if (x[i] < lo)
+      lo = x[i];
+    if (x[i] > hi)
+      hi = x[i];
+  }
+}
+
+// do_status_printouts, status_pr.c:18-356; kinetic_energy and field_energy,
+// :358-452
+extern "C" int spiffe_gpu_status_report(spiffe_gpu_instance *in, spiffe_status_row *st)
+{
+  if (!in || !st)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  const spiffe_mesh &m = in->mesh;
+  const int nz = m.nz, nr = m.nr, P = nr + 1;
+  const size_t nodes = (size_t)(nz + 1) * P;
+  memset(st, 0, sizeof(*st));
+  st->t = m.time;
+  st->JCathode = in->cathodes.empty() ? 0 : in->cathodes[0].current_density;
+  // the beam
+  RC_TRY(read_counts(in));
+  const int64_t np = in->h_cnt->np;
+  std::vector<double> bd[9];
+  for (auto &v : bd)
+    v.resize((size_t)np + 1);
+  std::vector<int32_t> id((size_t)np + 1);
+  std::vector<int16_t> gen((size_t)np + 1);
+  std::vector<uint64_t> status((size_t)np + 1);
+  std::vector<double> extra[7];
+  for (auto &v : extra)
+    v.resize((size_t)np + 1);
+  spiffe_beam_set b{};
+  b.capacity = np + 1;
+  b.z = bd[0].data(); b.r = bd[1].data(); b.pz = bd[2].data(); b.pr = bd[3].data(); b.r_pphi = bd[4].data();
+  b.vz = bd[5].data(); b.vr = bd[6].data(); b.vphi = bd[7].data(); b.Q = bd[8].data();
+  b.r0 = extra[0].data(); b.z0 = extra[1].data(); b.t0 = extra[2].data(); b.rmin = extra[3].data();
+  b.rmax = extra[4].data(); b.zmin = extra[5].data(); b.zmax = extra[6].data();
+  b.particleID = id.data();
+  b.generation = gen.data();
+  b.status = status.data();
+  RC_TRY(spiffe_gpu_download_beam(in, &b));
+  st->Particles = b.np;
+  st->ActiveParticles = b.npActive;
+  double KE = 0;
+  if (b.np) {
+    double Q = 0;
+    int64_t sec = 0;
+    for (int64_t ip = 0; ip < b.np; ip++)
+      if (b.status[ip] & SPIFFE_PART_ACTIVE) {
+        Q += b.Q[ip];
+        if (b.generation[ip] > 0)
+          sec++;
+      }
+    st->Charge = Q;
+    st->SecondaryParticles = sec;
+    moments(b.z, b.np, st->zAve, st->zRMS, st->zStDev);
+    min_max(b.z, b.np, st->zMin, st->zMax);
+    moments(b.r, b.np, st->rAve, st->rRMS, st->rStDev);
+    min_max(b.r, b.np, st->rMin, st->rMax);
+    moments(b.pz, b.np, st->pzAve, st->pzRMS, st->pzStDev);
+    min_max(b.pz, b.np, st->pzMin, st->pzMax);
+    moments(b.pr, b.np, st->prAve, st->prRMS, st->prStDev);
+    min_max(b.pr, b.np, st->prMin, st->prMax);
+    double sum = 0;
+    for (int64_t ip = 0; ip < b.np; ip++) {
+      const double a = b.r[ip] ? b.r_pphi[ip] / b.r[ip] : 0;
+      sum += std::sqrt(1 + b.pz[ip] * b.pz[ip] + b.pr[ip] * b.pr[ip] + a * a);
+    }
+    KE = in->stiffness * SPIFFE_ME_MKS * (SPIFFE_C_MKS * SPIFFE_C_MKS) * (sum - b.np);
+  }
+  st->KineticEnergy = KE;
+  // the fields
+  std::vector<double> F[8];
+  const bool tm = m.modes & SPIFFE_FL_TM_FIELDS, te = m.modes & SPIFFE_FL_TE_FIELDS;
+  spiffe_field_set h{};
+  double **want[8] = {&h.Ez, &h.Er, &h.Bphi2, &h.EzImposed, &h.ErImposed, &h.Ephi, &h.Br2, &h.Bz2};
+  for (int k = 0; k < 8; k++)
+    if ((k < 5 && tm) || (k >= 5 && te)) {
+      F[k].resize(nodes);
+      *want[k] = F[k].data();
+    }
+  RC_TRY(spiffe_gpu_download_fields(in, &h));
+  const int16_t *fl = in->h_flags.data();
+  auto at = [&](const std::vector<double> &a, int iz, int ir) { return a[(size_t)iz * P + ir]; };
+  auto flag = [&](int iz, int ir) { return fl[(size_t)iz * P + ir]; };
+  const double dr2 = m.dr * m.dr;
+  std::vector<double> area_c((size_t)nr + 1), area_o((size_t)nr + 1); // calculate_areas, integrate.c:689-701
+  for (int ir = 0; ir <= nr; ir++)
+    area_c[(size_t)ir] = ir ? SPIFFE_PIx2 * ir * dr2 : SPIFFE_PI * dr2 / 4;
+  area_o[0] = 0;
+  for (int ir = 1; ir <= nr; ir++)
+    area_o[(size_t)ir] = SPIFFE_PI * (2 * ir - 1) * dr2;
+  double E0 = 0, E1 = 0;
+  if (tm) {
+    double lo = DBL_MAX, hi = -DBL_MAX;
+    for (int iz = 1; iz < nz; iz++)
+      for (int ir = 0; ir < nr; ir++) {
+        const double v = at(F[0], iz, ir) + at(F[3], iz, ir);
+        if (v > hi)
+          hi = v;
+        if (v < lo)
+          lo = v;
+      }
+    st->EzAbsMax = std::fabs(lo) > std::fabs(hi) ? std::fabs(lo) : std::fabs(hi);
+    lo = DBL_MAX;
+    hi = -DBL_MAX;
+    for (int iz = 0; iz < nz; iz++)
+      for (int ir = 0; ir < nr; ir++) {
+        const double v = at(F[1], iz, ir) + at(F[4], iz, ir);
+        if (v > hi)
+          hi = v;
+        if (v < lo)
+          lo = v;
+      }
+    st->ErAbsMax = std::fabs(lo) > std::fabs(hi) ? std::fabs(lo) : std::fabs(hi);
+    for (int ir = 0; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 1; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_EZ_ZERO))
+          sum += at(F[0], iz, ir) * at(F[0], iz, ir);
+      E0 += sum * area_c[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
+    }
+    for (int ir = 1; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 0; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_ER_ZERO))
+          sum += at(F[1], iz, ir) * at(F[1], iz, ir);
+      E0 += sum * area_o[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
+    }
+    for (int ir = 1; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 1; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_BPHI_ZERO))
+          sum += at(F[2], iz, ir) * at(F[2], iz, ir);
+      E1 += sum * area_o[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
+    }
+  }
+  if (te) {
+    for (int ir = 0; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 0; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_EPHI_ZERO))
+          sum += at(F[5], iz, ir) * at(F[5], iz, ir);
+      E0 += sum * area_c[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
+    }
+    for (int ir = 0; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 1; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_BR_ZERO))
+          sum += at(F[6], iz, ir) * at(F[6], iz, ir);
+      E1 += sum * area_c[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
+    }
+    for (int ir = 1; ir < nr; ir++) {
+      double sum = 0;
+      for (int iz = 0; iz < nz; iz++)
+        if (!(flag(iz, ir) & SPIFFE_FL_BZ_ZERO))
+          sum += at(F[7], iz, ir) * at(F[7], iz, ir);
+      E1 += sum * area_o[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
+    }
+  }
+  st->ElectricEnergy = E0;
+  st->MagneticEnergy = E1;
+  st->FieldEnergy = E0 + E1;
+  st->TotalEnergy = KE + st->FieldEnergy;
+  st->EzOOEMin = in->h_cnt->oa_min;
+  st->EzOOEMax = in->h_cnt->oa_max;
   return 0;
 }
 

@@ -272,6 +272,13 @@ struct spiffe_session {
   std::vector<SessionAntenna> antennas;
   std::vector<SessionOnAxis> onaxis;
   std::vector<OnAxisProfile> onaxis_prepared; // for the fields_used output
+  // integrate's status_output: the rows so far (the file is rewritten whole
+  // after each row, so it is a complete one-page table at every point)
+  bool status_on = false;
+  std::string status_path;
+  std::vector<std::vector<double>> status_cols;
+  std::vector<std::vector<int32_t>> status_counts;
+  int64_t status_old_np = 0;
   bool translate_on = false, translate_set = false; // translate: the moving window
   double z_trigger = 0;
   std::vector<SessionScreen> screens;
@@ -365,6 +372,7 @@ struct spiffe_session {
   int output_fields(long long step, double time);
   int flush_screens(long long step, double time);
   int status(long long step, double time);
+  int write_status();
 };
 
 // ------------------------------------------------------------ define_geometry
@@ -1524,11 +1532,62 @@ int spiffe_session::flush_screens(long long step, double time)
   return 0;
 }
 
+// The status file's columns (setUpStatusOutputFile, status_pr.c:454-499):
+// the double columns, then Particles, NewParticles, SecondaryParticles
+// (long) between ErAbsMax and zMax
+static const char *const kStatusD[] = {"t", "JCathode", "KineticEnergy", "FieldEnergy", "TotalEnergy", "Charge",
+                                       "EzAbsMax", "ErAbsMax", "zMax", "zMin", "zAve", "zRMS", "zStDev", "rMax",
+                                       "rMin", "rAve", "rRMS", "rStDev", "pzMax", "pzMin", "pzAve", "pzRMS",
+                                       "pzStDev", "prMax", "prMin", "prAve", "prRMS", "prStDev", "EzOOEMin",
+                                       "EzOOEMax"};
+static const char *const kStatusDU[] = {"s", "A/m$a2$n", "J", "J", "J", "C", "V/m", "V/m", "m", "m", "m", "m", "m",
+                                        "m", "m", "m", "m", "m", "", "", "", "", "", "", "", "", "", "", "V/m", "V/m"};
+static const char *const kStatusL[] = {"Particles", "NewParticles", "SecondaryParticles"};
+
 int spiffe_session::status(long long step, double time)
 {
   int64_t np = 0, act = 0;
   S_TRY(spiffe_gpu_counts(inst, &np, &act));
   say("step %lld  t=%e s  particles %lld (%lld active)\n", step, time, (long long)np, (long long)act);
+  if (!status_on)
+    return 0;
+  // one row of do_status_printouts (status_pr.c:316-345)
+  spiffe_status_row r;
+  S_TRY(spiffe_gpu_status_report(inst, &r));
+  r.t = time; // the step about to run (integrate.c:138)
+  const double d[] = {r.t, r.JCathode, r.KineticEnergy, r.FieldEnergy, r.TotalEnergy, r.Charge, r.EzAbsMax,
+                      r.ErAbsMax, r.zMax, r.zMin, r.zAve, r.zRMS, r.zStDev, r.rMax, r.rMin, r.rAve, r.rRMS,
+                      r.rStDev, r.pzMax, r.pzMin, r.pzAve, r.pzRMS, r.pzStDev, r.prMax, r.prMin, r.prAve,
+                      r.prRMS, r.prStDev, r.EzOOEMin, r.EzOOEMax};
+  static_assert(sizeof(d) / sizeof(d[0]) == sizeof(kStatusD) / sizeof(kStatusD[0]), "status columns");
+  for (size_t k = 0; k < status_cols.size(); k++)
+    status_cols[k].push_back(d[k]);
+  status_counts[0].push_back((int32_t)r.Particles);
+  status_counts[1].push_back((int32_t)(r.Particles - status_old_np));
+  status_counts[2].push_back((int32_t)r.SecondaryParticles);
+  status_old_np = r.Particles;
+  return write_status();
+}
+
+int spiffe_session::write_status()
+{
+  using namespace spiffe_sdds;
+  std::vector<Def> cols;
+  std::vector<const void *> ptr;
+  for (size_t k = 0; k < status_cols.size(); k++) {
+    cols.push_back(Def{kStatusD[k], kStatusDU[k], "", T_DOUBLE});
+    ptr.push_back(status_cols[k].data());
+    if (k == 7) // after ErAbsMax
+      for (int c = 0; c < 3; c++) {
+        cols.push_back(Def{kStatusL[c], "", "", T_LONG});
+        ptr.push_back(status_counts[(size_t)c].data());
+      }
+  }
+  Writer w;
+  std::string err;
+  if (!w.open(status_path, "", "", {}, cols, err) ||
+      !w.write_page({}, {}, (int64_t)status_counts[0].size(), ptr, err))
+    return serr(SPIFFE_ERR_INVALID, "status_output: %s", err.c_str());
   return 0;
 }
 
@@ -1549,8 +1608,8 @@ int spiffe_session::cmd_integrate(Args &g)
   g.integer("sg_smoothing_halfwidth", sg);
   g.integer("terminate_on_total_loss", terminate);
   g.num("z_forces_start", z_forces_start);
-  if (g.str("status_output", out))
-    warn("integrate: status_output is not written");
+  std::string status_output;
+  const bool have_status = g.str("status_output", status_output);
   if (g.str("lost_particles", out))
     warn("integrate: lost_particles is not written");
   g.num("imposed_efield_ramp_time", ramp_time);
@@ -1569,6 +1628,15 @@ int spiffe_session::cmd_integrate(Args &g)
     return serr(SPIFFE_ERR_INVALID, "J_filter_multiplier must be >=0 and < 1");
   if (smoothing || j_filter || sg)
     return serr(SPIFFE_ERR_UNSUPPORTED, "integrate: current smoothing and filtering are not supported");
+  // setUpStatusOutputFile, status_pr.c:454-499 (integrate.c:79-80)
+  status_on = have_status && !status_output.empty();
+  if (status_on) {
+    status_path = compose(status_output, rootname);
+    status_cols.assign(sizeof(kStatusD) / sizeof(kStatusD[0]), {});
+    status_counts.assign(3, {});
+    status_old_np = 0;
+    S_TRY(write_status());
+  }
   if (inst)
     S_TRY(spiffe_gpu_get_mesh(inst, &mesh));
   spiffe_mesh &m = mesh;
@@ -1631,12 +1699,16 @@ int spiffe_session::cmd_integrate(Args &g)
     }
     // the step's imposed-field ramp comes before the diagnostics
     // (integrate.c:136-137); run_steps then finds the factor unchanged
-    if (m.imposed_ramp_time > 0 && field_output.defined) {
-      const bool first = field_output.index == -1; // the schedule is fixed at the first output call
-      const long long fs = first ? (long long)((field_output.start_time - m.start_time) / m.dt + 0.5)
-                                 : field_output.start_step;
-      const long long fi = first ? (long long)(field_output.time_interval / m.dt + 0.5) : field_output.step_interval;
-      if (due(k, fs, fi))
+    if (m.imposed_ramp_time > 0) {
+      bool need = status_on && status_interval > 0 && k % status_interval == 0;
+      if (field_output.defined) {
+        const bool first = field_output.index == -1; // the schedule is fixed at the first output call
+        const long long fs = first ? (long long)((field_output.start_time - m.start_time) / m.dt + 0.5)
+                                   : field_output.start_step;
+        const long long fi = first ? (long long)(field_output.time_interval / m.dt + 0.5) : field_output.step_interval;
+        need = need || due(k, fs, fi);
+      }
+      if (need)
         S_TRY(spiffe_gpu_compute_imposed_efield(inst, pc_defined ? &pc : &no_pc, 0));
     }
     S_TRY(save_fields(k, t, false));

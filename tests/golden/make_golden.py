@@ -198,7 +198,7 @@ DECK_DIAG = DECK_DCGUN.replace("finish_time=300e-12", "finish_time=120e-12").rep
     '&define_field_output filename="%s.fld", time_interval=40e-12, start_time=20e-12, z_interval=2, r_interval=4, '
     'separate_imposed_field=1 &end\n&integrate')
 sys.path.insert(0, os.path.dirname(HERE))
-from golden_columns import FLD_COLUMNS, ONAXIS_COLUMNS, SNAP_COLUMNS  # noqa: E402
+from golden_columns import FLD_COLUMNS, ONAXIS_COLUMNS, SNAP_COLUMNS, STATUS_COLUMNS  # noqa: E402
 
 # An on-axis RF field (add_on_axis_fields, onAxisFields.c) over the DC gun:
 # a synthetic two-harmonic Ez(z) table of 201 equispaced points, offset to
@@ -237,9 +237,32 @@ def deck_translate(geo):
     save("deck_translate", **out)
 
 
+# The on-axis deck with integrate's status file (status_pr.c): a row every
+# 50 steps and one after the loop.
+DECK_STATUS = None  # set after DECK_ONAXIS
+
+
+def deck_status(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    rz, rE = rf_profile()
+    write_rf(os.path.join(d, "rf.sdds"), rz, rE)
+    cmds = [b.strip() + " &end" for b in DECK_STATUS.split("&end") if b.strip()]
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("table", 100, STATUS_COLUMNS)], cwd=d,
+                                 capacity=20000)
+    st = res[0]
+    save("deck_status", deck=np.array(DECK_STATUS), geo=np.array(geo), rf_z=rz, rf_Ez=rE, rows=len(st["t"]),
+         **{"st_" + k: st[k] for k in STATUS_COLUMNS})
+
+
 def rf_profile():
     u = np.arange(201) / 200.0
     return u * 0.02, np.sin(np.pi * u) + 0.3 * np.sin(2 * np.pi * u)
+
+
+DECK_STATUS = DECK_ONAXIS.replace("space_charge=1, imposed", 'status_interval=50, status_output="%s.status", '
+                                  "space_charge=1, imposed")
 
 
 def write_rf(path, z, Ez):
@@ -279,6 +302,7 @@ def decks():
          **{"fld_" + k: fld[k] for k in FLD_COLUMNS})
     deck_onaxis(geo)
     deck_translate(geo)
+    deck_status(geo)
 
 
 def deck_onaxis(geo):
@@ -302,6 +326,8 @@ def deck_onaxis(geo):
 if __name__ == "__main__":
     if sys.argv[1:] == ["decks"]:
         decks()
+    elif sys.argv[1:] == ["status"]:
+        deck_status(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["translate"]:
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["onaxis"]:

@@ -585,3 +585,23 @@ def test_split_form_runs_the_translate_deck(tmp_path, monkeypatch):
     assert m64["count"] > 900 and abs(m32["count"] - m64["count"]) <= 0.005 * m64["count"], (m32, m64)
     errs = moments.relative_errors(m32, m64)
     assert max(errs.values()) < 5e-3, errs
+
+
+@pytest.mark.gpu
+def test_status_file_matches_reference(tmp_path, monkeypatch):
+    """integrate's status_output (do_status_printouts, status_pr.c) on the
+    on-axis deck in the FP64 form against the reference's status file: every
+    column of every row identical (energies, charge, beam moments and
+    extremes, the Schottky cathode's current density, the on-axis Ez
+    extremes of the last push)."""
+    from golden_columns import STATUS_COLUMNS
+
+    fx = load("deck_status")
+    write_rf(tmp_path / "rf.sdds", fx["rf_z"], fx["rf_Ez"])
+    s = run_deck(fx, tmp_path, monkeypatch)
+    s.close()
+    pages = session.read_sdds(str(tmp_path / "spiffe.status"))
+    assert len(pages) == 1 and int(fx["rows"]) == 8
+    for c in STATUS_COLUMNS:
+        got = np.asarray(pages[0]["columns"][c], np.float64)
+        assert len(got) == 8 and np.array_equal(got, fx["st_" + c]), (c, got, fx["st_" + c])
