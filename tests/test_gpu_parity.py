@@ -255,3 +255,54 @@ def test_counts_async_matches_counts():
     assert [tuple(r) for r in out] == seen and seen[-1][0] > 0
     g.close()
     g2.close()
+
+
+def test_on_axis_fields_at_matches_reference_profile():
+    """spiffe_gpu_add_on_axis_field and the expansion through the C ABI against
+    the reference's fields_used table (onAxisFields.c:130-170): r = 1e-6,
+    sine and cosine 1, bit for bit at every z of the DC gun mesh."""
+    fx = load("deck_onaxis")
+    f = abi.Fields(151, 101, 0.0, 0.03, 0.02)
+    g = gpu.GpuInstance(f, capacity=16)
+    g.add_on_axis_field(fx["rf_z"], fx["rf_Ez"], Ez_peak=8e6, frequency=2.856e9, phase_rad=220 * np.pi / 180,
+                        z_offset=-0.001)
+    got = np.array([g.on_axis_fields_at(z, 1e-6, 0.0, profile=True) for z in fx["oaf_z"]])
+    assert np.array_equal(got[:, 0], fx["oaf_Ez"])
+    assert np.array_equal(got[:, 1] / 1e-6, fx["oaf_Er_r"])
+    assert np.array_equal(got[:, 2] / 1e-6, fx["oaf_Bphi_r"])
+    with pytest.raises(gpu.SpiffeGpuError):
+        g.add_on_axis_field(fx["rf_z"][:4], fx["rf_Ez"][:4], Ez_peak=1e6, frequency=1e9, phase_rad=0.0)
+    g.close()
+
+
+@pytest.mark.parametrize("prec", [gpu.PRECISION_F64, gpu.PRECISION_SPLIT32])
+def test_translate_problem_moves_rows(prec):
+    """spiffe_gpu_translate_problem (translate.c:40-197): with a particle past
+    the trigger the TM field and current rows move down one row, the top row
+    is zeroed, zmin, zmax and the trigger grow by dz; without one nothing
+    moves."""
+    rng = np.random.default_rng(7)
+    f = abi.Fields(41, 31, 0.0, 0.03, 0.02)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Jz", "Jr"):
+        f[n] = rng.standard_normal(f.shape)
+    g = gpu.GpuInstance(f, capacity=64, precision=prec)
+    g.upload_fields(f)
+    b = abi.Beam(16)
+    b.set(1, z=[0.0251], r=[0.004], pz=[0.1], Q=[-1e-15], status=[1])
+    b.npActive, b.nextParticleID, b.QoMC, b.stiffness = 1, 2, -5.866e2, 1.0
+    g.upload_beam(b)
+    dz = f.mesh.dz
+    g.set_translation(1, 0.025)
+    assert g.translate_problem() == (True, dz)
+    m = g.get_mesh()
+    assert m.zmin == dz and m.zmax == 0.03 + dz
+    got = g.fields(f)
+    for n in ("Ez", "Er", "Bphi", "Bphi2"):
+        ref = f[n] if prec == gpu.PRECISION_F64 else f[n].astype(np.float32).astype(np.float64)
+        assert np.array_equal(got[n][:-1], ref[1:]), n
+        assert not got[n][-1].any(), n
+    # the particle (z = 25.1 mm) is no longer past the trigger (25 mm + dz)
+    assert g.translate_problem() == (False, dz)
+    with pytest.raises(gpu.SpiffeGpuError):  # past zmax - dz of the moved mesh
+        g.set_translation(1, 0.0301)
+    g.close()
