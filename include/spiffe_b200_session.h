@@ -17,20 +17,23 @@
  *   (poisson_correction.c:31), load_fields (load_fields.c:20),
  *   define_field_saving (field_saving.c:16; time_interval saving),
  *   define_snapshots (snapshots.c:16), define_field_output (field_output.c:16),
- *   integrate (integrate.c:24), trace (obsolete, as spiffe), stop.
+ *   add_on_axis_fields (onAxisFields.c:18, with its fields_used table),
+ *   translate (translate.c:21), integrate (integrate.c:24, with status_output,
+ *   status_pr.c:454), trace (obsolete, as spiffe), stop.
  * Accepted with a warning and no output (diagnostic files only):
  *   define_field_sampling, and the
  *   output-file variables boundary_output, urmel_boundary_output,
  *   discrete_boundary_output, interior_points, emission_log, field_output,
- *   status_output, lost_particles.
+ *   lost_particles.
  * Rejected with SPIFFE_ERR_UNSUPPORTED: define_resistor, load_particles,
- * set_up_translation, add_on_axis_fields, define_secondary_emission,
- * define_emitter, and options whose physics the device loop does not have
- * (current smoothing and filtering, test charges, thermal velocities, Halton
- * sequences, field saving on an Ez trigger).
+ * define_secondary_emission, define_emitter, translate's reduction of the
+ * integration region (z_lower, z_upper), and options whose physics the device
+ * loop does not have (current smoothing and filtering, test charges, thermal
+ * velocities, Halton sequences, field saving on an Ez trigger).
  *
- * Outputs: screens, field saves, beam snapshots and field output are SDDS1
- * binary files with the reference's columns and parameters.  A screen page holds the crossings of
+ * Outputs: screens, field saves, beam snapshots, field output, the status
+ * file and the on-axis fields_used table are SDDS1 binary files with the
+ * reference's columns and parameters.  A screen page holds the crossings of
  * one run segment (the steps between two host synchronisations, at most
  * the session's flush interval) instead of one time step.
  */
