@@ -88,12 +88,12 @@ int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *inst, int32_t target, doub
  * allocation after start-up.  All scratch lives in one fixed 352 KB array
  * that every GPU loading the library holds until exit; limits: iteration_limit
  * <= 16384, nr <= 4096, ceil((nr-1)/32)*ceil(nz/8) <= 16384.  Larger sizes
- * are rejected with an error.  The first call on a device looks up that
- * array's device address (with the device current), so make that first call
- * before any stream capture.  Every call shares the one array: calls that
- * overlap on the GPU (other threads, other streams) race and must be
- * serialised by the caller.  `stream` is a cudaStream_t (NULL: the default
- * stream); the call waits for the solve to finish. */
+ * are rejected with an error.  Each call looks up that array's device address
+ * with the caller's device and context current, copies its coefficient tables
+ * from host memory on `stream`, and waits on `stream` for the solve to finish
+ * before it returns.  Every call shares the one array: calls that overlap on
+ * the GPU (other threads, other streams) race and must be serialised by the
+ * caller.  `stream` is a cudaStream_t (NULL: the default stream). */
 int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, double *psi, const double *rhs, const int16_t *flags,
                                          double accuracy, int64_t iteration_limit, int64_t *iterations, void *stream);
 /* add_poisson_correction, poisson_correction.c:73 (interval and start-step

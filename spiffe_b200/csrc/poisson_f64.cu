@@ -755,7 +755,6 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[SPIFFE_NOALLOC_
 namespace {
 constexpr int NOALLOC_MAX_DEVICES = 64;
 std::mutex g_noalloc_mutex;
-NoallocScratch *g_noalloc_addr[NOALLOC_MAX_DEVICES];
 int g_noalloc_grid[NOALLOC_MAX_DEVICES];
 // host staging for the tables, static so the call allocates nothing
 double g_noalloc_omega[SPIFFE_NOALLOC_MAX_HALFSWEEPS];
@@ -798,15 +797,22 @@ extern "C" int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, dou
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES)
     return spiffe_set_error(-2, "no current CUDA device");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  // once per device, with that device current: the device address of the
-  // scratch array (its host-side name is not a device address)
-  if (!g_noalloc_addr[dev]) {
+  // every call, with the caller's device and context current: the device
+  // address of the scratch array (its host-side name is not a device
+  // address).  The lookup allocates nothing, and repeating it keeps the
+  // address right after a device reset or under another context.
+  NoallocScratch *sc = nullptr;
+  {
     void *p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) {
       snprintf(msg, sizeof(msg), "cudaGetSymbolAddress of the solver scratch failed: %s", cudaGetErrorString(e));
       return spiffe_set_error(-2, msg);
     }
+    sc = (NoallocScratch *)p;
+  }
+  // the cooperative grid depends on the device only
+  if (!g_noalloc_grid[dev]) {
     int sms = 0, per = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_sor, RT, 0);
@@ -816,9 +822,7 @@ extern "C" int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, dou
     if (grid > SPIFFE_NOALLOC_MAX_GRID)
       grid = SPIFFE_NOALLOC_MAX_GRID;
     g_noalloc_grid[dev] = grid;
-    g_noalloc_addr[dev] = (NoallocScratch *)p;
   }
-  NoallocScratch *sc = g_noalloc_addr[dev];
   // the tables, with the expressions of the instance path (poisson.c:342-361)
   const double dz = mesh->dz, dr = mesh->dr;
   const double rz = dz / dr;

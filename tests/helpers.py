@@ -10,6 +10,22 @@ MODES = abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP | abi.FL_LONGIT_INTERP
 QoMC = -1.602176634e-19 / (9.1093837015e-31 * 2.99792458e8)
 
 
+def reference_root():
+    """The reference checkout whose sources built oracle/_ref (SPIFFE_REFERENCE
+    overrides), or None where it is absent, as on the GPU boxes."""
+    root = os.environ.get("SPIFFE_REFERENCE")
+    if not root:
+        rec = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "reference_root.txt")
+        if os.path.exists(rec):
+            root = open(rec).read().strip()
+    return root if root and os.path.isdir(root) else None
+
+
+def reference_file(*parts):
+    root = reference_root()
+    return os.path.join(root, *parts) if root else None
+
+
 def load(name):
     with np.load(os.path.join(GOLDEN, name + ".npz")) as z:
         return {k: z[k] for k in z.files}

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 from spiffe_b200 import geometry, workloads
-from helpers import load
+from helpers import load, reference_file
 
 
 @pytest.mark.parametrize("name", ["pillbox_fdtd", "dcgun_geometry", "gun16_geometry"])
@@ -19,10 +19,10 @@ def test_flags_match_reference(name):
         assert np.array_equal(psi, fx["PsiImposed"])
 
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = reference_file("examples")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+@pytest.mark.skipif(REF_EXAMPLES is None, reason="reference examples not present")
 @pytest.mark.parametrize("rel,nz,nr,zmax,rmax", [
     ("dcGun/dc.geo", 165, 165, 0.072, 0.042),
     ("apsTCRFGun/excite/mg6mm-3.geo", 165, 165, 0.0959148653920, 0.04289777777),

@@ -15,7 +15,7 @@ import numpy as np
 import pytest
 
 from spiffe_b200 import abi, gpu, session
-from helpers import by_id, load
+from helpers import by_id, load, reference_file
 
 ERR_INVALID, ERR_UNSUPPORTED = -1, -5
 
@@ -190,10 +190,10 @@ def test_sdds_ascii_tables(dcgeo):
                       'profile="prof.sdds", profile_time_name="t", profile_factor_name="A" &end')
 
 
-REF_WF = "/root/reference/examples/apsTCRFGun/excite/spline4.wf"
+REF_WF = reference_file("examples", "apsTCRFGun", "excite", "spline4.wf")
 
 
-@pytest.mark.skipif(not os.path.exists(REF_WF), reason="reference examples not present")
+@pytest.mark.skipif(REF_WF is None or not os.path.exists(REF_WF), reason="reference examples not present")
 def test_reference_waveform_file_is_read(dcgeo):
     pages = session.read_sdds(REF_WF)
     t = pages[0]["columns"]["t"]

@@ -78,3 +78,15 @@ def test_noalloc_rejects_sizes_beyond_its_limits():
     n = C.c_int64()
     rc = fn(C.byref(f.mesh), psi.data_ptr(), None, flags.data_ptr(), 1e-6, 20000, C.byref(n), None)
     assert rc != 0 and b"exceeds" in lib.spiffe_gpu_last_error()
+    # meshes past the fixed row tables or the fixed block-sum array: each is
+    # refused on the host before anything is launched, so a one-element
+    # array stands in for the (absent) large one
+    tiny = torch.zeros(1, dtype=torch.float64, device="cuda")
+    tiny_flags = torch.zeros(1, dtype=torch.int16, device="cuda")
+    for nz, nr in ((200, 5000), (1100, 4096)):
+        mesh = abi.Mesh.from_buffer_copy(f.mesh)
+        mesh.nz, mesh.nr = nz, nr
+        n = C.c_int64(-7)
+        rc = fn(C.byref(mesh), tiny.data_ptr(), tiny.data_ptr(), tiny_flags.data_ptr(), 1e-6, 100, C.byref(n), None)
+        assert rc != 0 and b"exceeds" in lib.spiffe_gpu_last_error(), (nz, nr)
+        assert n.value == -7
