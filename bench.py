@@ -43,12 +43,14 @@ BYTES = {
         "correction": 110.0,  # per node and correction: two flux passes, rhs scaling, gradient update
     },
     "split32": {
-        "fdtd": 61.0,     # per node-step: read Ez,Er,Bphi (12) + int64 Jz,Jr (16) + mask (1); write Ez,Er,
-                          # Bphi,Bphi2 (16); zero Jz,Jr (16)
+        "fdtd": 29.0,     # per node-step: read Ez,Er,Bphi (12) + mask (1); write Ez,Er,Bphi,Bphi2 (16); the int64
+                          # current is read and cleared only on the rows the deposition touched
         "push": 86.0,     # per particle-step: read cell,fz,fr,pz,pr,r_pphi,Q,status,4 extrema (45); write all
                           # but Q (41); the next step's deposition is fused in (its J traffic stays in L2)
         "deposit": 29.0,  # per particle-step (first step only): cell, offsets, momenta, Q, status
         "sor": 7.0,       # per node and half-sweep: FP32 d and r0 (the bands live in shared memory)
+        "mg": 180.0,      # per node and V-cycle: FP64 residual (25) and fold (20), four red-black sweeps on the
+                          # mesh (56), transfers (12), the nine-point levels below (about 67)
         "correction": 90.0,  # per node and correction: flux passes, charge combine, rhs scaling, FP64 r0 and fold
     },
 }
@@ -316,6 +318,7 @@ def gpu_arm(args):
     psteps = w1["particle_steps"] - w0["particle_steps"]
     halfsweeps = w1["sor_halfsweeps"] - w0["sor_halfsweeps"]
     solves = w1["sor_solves"] - w0["sor_solves"]
+    cycles = w1["mg_cycles"] - w0["mg_cycles"]
     np_end, _ = g.counts()
     g.close()
 
@@ -367,20 +370,25 @@ def gpu_arm(args):
     cells = cfg.nz * cfg.nr * K * world / sec
 
     # --- roofline of the dominant phase
-    peak, peak_kind = measured_peak()
     nodes = (cfg.nz + 1) * (cfg.nr + 1)
     sor_nodes = cfg.nz * (cfg.nr - 1)
     work_bytes = {
         "fdtd": nbytes["fdtd"] * nodes * phases["fdtd"][1],
         "push": nbytes["push"] * psteps,
         "deposit": nbytes["deposit"] * psteps if prec == gpu.PRECISION_F64 else nbytes["deposit"] * cfg.n_macro * phases["deposit"][1],
-        "poisson": nbytes["sor"] * sor_nodes * halfsweeps + nbytes["correction"] * nodes * solves,
+        "poisson": nbytes["sor"] * sor_nodes * halfsweeps + nbytes.get("mg", 0.0) * nodes * cycles +
+                   nbytes["correction"] * nodes * solves,
         "emission": 0.0,
     }
     total_ms = sum(v[0] for v in phases.values()) or 1.0
+    peak, peak_kind = measured_peak()
     breakdown = {k: {"ms": round(v[0], 3), "launches": v[1], "share": round(v[0] / total_ms, 4),
-                     "gbs": round(work_bytes[k] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None}
+                     "gbs": round(work_bytes[k] / (v[0] / 1e3) / 1e9, 1) if v[0] > 0 else None,
+                     "frac": round(work_bytes[k] / (v[0] / 1e3) / 1e9 / peak, 3) if v[0] > 0 else None}
                  for k, v in phases.items()}
+    breakdown["poisson"]["solves"] = solves
+    breakdown["poisson"]["halfsweeps_per_solve"] = round(halfsweeps / solves, 1) if solves else 0
+    breakdown["poisson"]["vcycles_per_solve"] = round(cycles / solves, 2) if solves else 0
     dom = max(phases, key=lambda k: phases[k][0])
     dom_units = {"fdtd": phases["fdtd"][1], "push": phases["push"][1], "deposit": phases["deposit"][1],
                  "poisson": max(solves, 1), "emission": 1}[dom]
@@ -405,9 +413,19 @@ def gpu_arm(args):
                    "form": ("split precision: FP32 fields and push, cell+FP32-offset positions, 64-bit fixed-point "
                             "current, FP32 SOR in FP64 iterative refinement") if prec == gpu.PRECISION_SPLIT32
                    else "plain FP64 (bit-faithful to the reference)",
-                   "field": "analytic pi-mode standing wave, 100 MV/m on the cathode",
+                   "field": "stand-in: an analytic pi-mode standing wave, 100 MV/m on the cathode, in place of the "
+                            "30,000-step antenna build-up and reload",
+                   "beam": "stand-in: the 1 nC, 2 ps rms bunch generated already emitted (positions from uniform "
+                           "acceleration by the cathode field), so the timed steps hold no emission",
                    "particles": cfg.n_macro, "nodes": cfg.nz * cfg.nr, "steps_timed": K,
-                   "l2": "no flush: the resident state (fields ~%d MB, beam ~%d MB) exceeds the 126 MB L2"
+                   "poisson_solver": ("multigrid (FP32 V-cycles in FP64 refinement)" if prec == gpu.PRECISION_SPLIT32
+                                      else "the reference's red-black SOR"),
+                   "l2": ("no flush: each step streams the 1M-particle beam (%d MB read and written) and the fields; "
+                          "the split form keeps its ~%d MB of FP32 TM fields in an L2 persisting window on purpose, "
+                          "as it does in production" % (cfg.n_macro * 86 // 2 ** 20,
+                                                        16 * (cfg.nz + 1) * ((cfg.nr + 1 + 31) // 32 * 32) // 2 ** 20))
+                         if prec == gpu.PRECISION_SPLIT32 else
+                         "no flush: the resident state (fields ~%d MB, beam ~%d MB) exceeds the 126 MB L2"
                          % (sum(v.nbytes for v in f.a.values()) // 2 ** 20, sum(v.nbytes for v in b.a.values()) // 2 ** 20),
                    "parallelism": "replicas" if world > 1 else "single"},
         "cell_updates_per_s": round(cells, 1),

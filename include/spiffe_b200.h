@@ -196,6 +196,16 @@ int64_t spiffe_gpu_launch_count(void);
  * beam upload; this keeps the gather and the deposition of neighbouring
  * threads on the same nodes.  No effect on the FP64 form. */
 int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *inst, int64_t n);
+/* No counterpart in the reference (which has one solver).  The solver of the
+ * split-precision form's Poisson correction and of spiffe_gpu_solve_poisson_cyl
+ * with target 0: SPIFFE_POISSON_MULTIGRID (the default) solves the same
+ * equations to the same stop rule, sum|residual| < accuracy sum|rhs| with the
+ * residual over every updated node, by FP64 residual refinement around FP32
+ * multigrid V-cycles, at most min(iteration_limit, 100) of them (the count is
+ * reported in place of half-sweeps; -1 at the limit); SPIFFE_POISSON_SOR runs
+ * the reference's red-black SOR.  Laplace solves (target 1, the imposed field)
+ * always use SOR.  The FP64 form accepts SPIFFE_POISSON_SOR only. */
+int spiffe_gpu_set_poisson_solver(spiffe_gpu_instance *inst, int32_t solver);
 /* Batched execution (no counterpart in the reference, which runs one problem
  * per process): advances n independent instances concurrently, instance i by
  * steps[i] steps of spiffe_gpu_run_steps, on `workers` host threads.  Each
@@ -209,7 +219,8 @@ int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *inst, int64_t n);
 int spiffe_gpu_batch_run(spiffe_gpu_instance *const *inst, int32_t n, const int64_t *steps, int32_t workers,
                          int64_t chunk, double *done_ms);
 /* Work done so far: out[0] particle-steps (active particles summed over
- * pushes), out[1] SOR half-sweeps, out[2] SOR solves, out[3] FDTD steps. */
+ * pushes), out[1] SOR half-sweeps, out[2] Poisson solves (either solver),
+ * out[3] FDTD steps, out[4] multigrid V-cycles; out holds 5 values. */
 int spiffe_gpu_work_counters(spiffe_gpu_instance *inst, int64_t *out);
 
 #ifdef __cplusplus

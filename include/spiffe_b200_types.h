@@ -99,6 +99,10 @@ typedef struct spiffe_screen_set {
   int32_t *particleID;
 } spiffe_screen_set;
 
+/* Poisson solver of the split-precision form (spiffe_gpu_set_poisson_solver) */
+#define SPIFFE_POISSON_SOR 0       /* the reference's red-black SOR and stop rule (poisson.c:17-130) */
+#define SPIFFE_POISSON_MULTIGRID 1 /* FP32 multigrid V-cycles in FP64 refinement, the same stop rule */
+
 /* Lost-particle removal.  SPIFFE_COMPACT_REFERENCE reproduces
  * advance_particles.c:491-518 as it behaves: the loop tests is_lost[ip] but
  * never moves is_lost with the particle it copies down, so the first lost

@@ -26,6 +26,7 @@ from spiffe_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "build", "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspiffe_ref.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "libspiffe_dropin.so")
 
 P = C.POINTER
 
@@ -224,10 +225,15 @@ def _mesh(lib):
 _BEAM_INT = {"particleID": np.int32, "generation": np.int16, "status": np.uint64}
 
 
-def _child(program, capacity, cwd):
-    """Runs in a spawned process: executes `program` against the reference."""
+def _child(program, capacity, cwd, preload=()):
+    """Runs in a spawned process: executes `program` against the reference.
+    Libraries in `preload` are loaded first into the global symbol scope, so
+    their definitions take the place of the reference's own (a link-time
+    drop-in)."""
     if cwd:
         os.chdir(cwd)
+    for path in preload:
+        C.CDLL(path, mode=C.RTLD_GLOBAL)
     lib = _ref_lib()
     lib.ref_session_init(capacity)
     out = []
@@ -344,7 +350,7 @@ def _child(program, capacity, cwd):
     return out
 
 
-def run_reference(program, capacity=1 << 16, cwd=None, timeout=900, threads=1):
+def run_reference(program, capacity=1 << 16, cwd=None, timeout=900, threads=1, preload=()):
     """Runs `program` (a list of tuples) against the compiled reference in a
     fresh Python process (pickles over stdin/stdout) and returns the list of
     requested outputs.  `threads` sets OMP_NUM_THREADS: the reference's push
@@ -357,7 +363,8 @@ def run_reference(program, capacity=1 << 16, cwd=None, timeout=900, threads=1):
     env = dict(os.environ)
     env["PYTHONPATH"] = repo + os.pathsep + env.get("PYTHONPATH", "")
     env["OMP_NUM_THREADS"] = str(threads)
-    proc = subprocess.run([sys.executable, "-m", "oracle.pyoracle"], input=pickle.dumps((program, capacity, cwd)),
+    proc = subprocess.run([sys.executable, "-m", "oracle.pyoracle"],
+                          input=pickle.dumps((program, capacity, cwd, tuple(preload))),
                           capture_output=True, timeout=timeout, env=env, cwd=repo)
     if proc.returncode != 0:
         raise RuntimeError("reference run failed (%d): %s" % (proc.returncode, proc.stderr.decode()[-2000:]))
@@ -369,11 +376,11 @@ def reference_available():
 
 
 if __name__ == "__main__":
-    _program, _capacity, _cwd = pickle.loads(sys.stdin.buffer.read())
+    _program, _capacity, _cwd, _preload = pickle.loads(sys.stdin.buffer.read())
     # the reference prints progress on stdout; keep the pickle channel clean
     _real = os.dup(1)
     os.dup2(2, 1)
-    _out = _child(_program, _capacity, _cwd)
+    _out = _child(_program, _capacity, _cwd, _preload)
     sys.stdout.flush()
     os.dup2(_real, 1)
     with os.fdopen(_real, "wb") as _f:

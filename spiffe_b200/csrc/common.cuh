@@ -185,7 +185,8 @@ struct DevCounts {
   double last_pz0, last_pr0, last_rpphi0; // pre-kick momenta of particle np-1
   long long pushed;                       // sum over pushes of the active count (particle-steps)
   double oa_min, oa_max;                  // EzOOEMin, EzOOEMax of the last push (advance_particles.c:113-114)
-  long long sor_halfsweeps, sor_solves;   // red-black half-sweeps and solves run
+  long long sor_halfsweeps, sor_solves;   // red-black half-sweeps and Poisson solves run (either solver)
+  long long mg_cycles;                    // multigrid V-cycles run
   unsigned int error;                     // SPIFFE_DEV_ERR_* bits
   unsigned int pad;
 };

@@ -1,0 +1,868 @@
+// spiffe_b200/csrc/multigrid_f32.cu -- multigrid Poisson solve of the split-precision form.
+//
+// The problem is solve_poisson_cyl's (poisson.c:17-130): the five-point
+// cylindrical operator on the nodes that routine updates (rows lo..hi,
+// columns 0..nr-2, not metal; the axis row of coefficients 4c and e - 2c;
+// mirrored end rows for a "Dirichlet" end), every other node held.  The
+// reference relaxes it with red-black SOR to its stop rule
+// sum|residual| < accuracy sum|rhs|; on the meshes of the RF and DC guns
+// that rule is out of reach within its 1000 half-sweeps.  Here the same
+// equations are solved by FP64 iterative refinement around FP32 multigrid
+// V-cycles:
+//
+//   r = rhs - A Psi in FP64; stop when sum|r| < accuracy * sum|rhs|
+//   (sum|rhs| over iz < nz, ir < nr-1, as poisson.c:40-43 forms it; a
+//   Laplace solve, rhs absent, measures against its first residual);
+//   u = V-cycle(r) in FP32;  Psi += u in FP64;  repeat.
+//
+// Levels: level 0 is the mesh; level l+1 holds the nodes 2I, 2J of level l
+// (node (I, J) of level l+1 is unknown when node (2I, 2J) of level l is).
+// Transfers are bilinear interpolation P and its volume-weighted adjoint
+// R = (1/4) Vc^-1 P^T Vf (Vf, Vc: annulus volumes, the axis node's 1/8 of
+// the first ring's), and the coarse operators are the Galerkin products
+// R A P, built once per mesh on the host in FP64 (nine-point stencils).
+// Metal irises and electrodes stay in the coarse operators that way;
+// operators rediscretised on the coarse nodes instead lose them and the
+// V-cycle then reduces the residual only 0.6x per cycle on the 1.6-cell gun
+// against 0.1-0.17x with the Galerkin operators.  Smoothing is red-black
+// Gauss-Seidel on level 0 and four-colour Gauss-Seidel (colour (I&1, J&1))
+// on the nine-point levels, nu sweeps before and after each coarse
+// correction; the last pre-smoothing colour leaves a zero residual at its
+// own nodes, so the restriction evaluates the residual only at the others.
+//
+// One cooperative launch runs the whole solve.  Levels with more than
+// MG_TAIL_NODES nodes are worked by every CTA with grid barriers between the
+// colour sweeps; the smaller ones, down to the coarsest (GS sweeps, no
+// direct solve), by CTA 0 alone with CTA barriers while the others wait at
+// the next grid barrier.  Data written inside the launch are read through
+// L2 (ld.cg).  The sums that drive the stop rule are per-CTA partials added
+// in the same order by every CTA, so every CTA takes the same decision and
+// the result does not depend on timing.  Every barrier wait is bounded;
+// on time-out the kernel raises SPIFFE_DEV_ERR_BARRIER and every CTA returns.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "modules.cuh"
+#include "split32.cuh"
+
+namespace {
+
+constexpr int MG_NT = 512;            // threads per CTA
+constexpr int MG_TAIL_NODES = 12288;  // levels at most this large are worked by CTA 0 alone
+constexpr int MG_MIN_UNKNOWNS = 64;   // coarsening stops at this many unknowns
+enum { MG_INVD = 8, MG_DIAG = 9 };
+
+struct Mg32Args {
+  double *Psi;
+  const double *rhs; // null: Laplace solve
+  const uint8_t *umask;
+  float *u0, *f0;
+  const float *crow, *drow;
+  int nz, P0, lo, hi, cols;
+  float a, c4, e, e2c, inv_e, inv_e2c;   // level-0 operator in FP32
+  double a_d, e_d, c4_d, e2c_d, dr2_inv; // and in FP64 for the residual
+  int nlev, tail, nu0, nu, coarse_sweeps, max_cycles;
+  double accuracy;
+  MgLevel lev[MG_MAX_LEVELS];
+  unsigned long long *bar; // [0] arrivals, [16] abort
+  double *part;            // [grid][2]
+  PcState *st;
+  long long *iters_out;
+};
+
+__device__ __forceinline__ unsigned long long mg_ld_acquire(const unsigned long long *p)
+{
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long mg_ld_relaxed(const unsigned long long *p)
+{
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier over a monotonic arrival counter (barrier number gen, counted
+// from 1 by every thread alike).  Bounded: after 2^24 polls, or once another
+// CTA has given up, it returns false in every thread of the CTA.
+__device__ bool mg_grid_sync(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
+{
+  __shared__ int ok_sh;
+  gen++;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    asm volatile("red.relaxed.gpu.global.add.u64 [%0], %1;" ::"l"(a.bar), "l"(1ull) : "memory");
+    const unsigned long long target = (unsigned long long)gridDim.x * gen;
+    unsigned long long polls = 0;
+    while (mg_ld_acquire(a.bar) < target) {
+      if (mg_ld_relaxed(a.bar + 16)) {
+        ok = 0;
+        break;
+      }
+      if (++polls > (1ull << 24)) {
+        atomicOr(&cnt->error, SPIFFE_DEV_ERR_BARRIER);
+        asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(a.bar + 16), "l"(1ull) : "memory");
+        ok = 0;
+        break;
+      }
+      if (polls > 32)
+        __nanosleep(32);
+    }
+    ok_sh = ok;
+  }
+  __syncthreads();
+  return ok_sh != 0;
+}
+
+// A synchronisation point of a level's work: the whole grid, or CTA 0 alone.
+__device__ __forceinline__ bool mg_sync(const Mg32Args &a, bool local, unsigned &gen, DevCounts *cnt)
+{
+  if (local) {
+    __syncthreads();
+    return true;
+  }
+  return mg_grid_sync(a, gen, cnt);
+}
+
+// ---- level 0: the mesh, five-point operator
+
+__device__ __forceinline__ bool unknown0(const Mg32Args &a, int iz, int ir, size_t j)
+{
+  return iz >= a.lo && iz <= a.hi && ir < a.cols && !(a.umask[j] & S32_U_METAL);
+}
+
+// neighbour sum of the level-0 operator at an unknown node (poisson.c:57-117)
+__device__ __forceinline__ float nb0(const Mg32Args &a, const float *u, int iz, int ir, size_t j)
+{
+  const long P = a.P0;
+  const float up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? __ldcg(u + j - P) : __ldcg(u + j + P);
+  const float dn = (iz == 0 && a.lo == 0) ? __ldcg(u + j + P) : __ldcg(u + j - P);
+  if (ir == 0)
+    return a.a * (up + dn) + a.c4 * __ldcg(u + j + 1);
+  return a.a * (up + dn) + __ldg(a.crow + ir) * __ldcg(u + j + 1) + __ldg(a.drow + ir) * __ldcg(u + j - 1);
+}
+
+__device__ __forceinline__ float res0(const Mg32Args &a, int iz, int ir)
+{
+  const size_t j = node(iz, ir, a.P0);
+  if (!unknown0(a, iz, ir, j))
+    return 0.f;
+  return __ldcg(a.f0 + j) - nb0(a, a.u0, iz, ir, j) - (ir ? a.e : a.e2c) * __ldcg(a.u0 + j);
+}
+
+// one colour c of red-black Gauss-Seidel on level 0: nodes with (iz+ir)%2 == c
+__device__ void smooth0(const Mg32Args &a, int c, long t0, long dt)
+{
+  const int Hh = (a.cols + 1) >> 1;
+  const long n = (long)(a.hi - a.lo + 1) * Hh;
+  for (long t = t0; t < n; t += dt) {
+    const int row = (int)(t / Hh), k = (int)(t - (long)row * Hh);
+    const int iz = a.lo + row, ir = 2 * k + ((iz + c) & 1);
+    if (ir >= a.cols)
+      continue;
+    const size_t j = node(iz, ir, a.P0);
+    if (a.umask[j] & S32_U_METAL)
+      continue;
+    a.u0[j] = (__ldcg(a.f0 + j) - nb0(a, a.u0, iz, ir, j)) * (ir ? a.inv_e : a.inv_e2c);
+  }
+}
+
+// ---- levels >= 1: nine-point Galerkin operators
+
+__device__ __forceinline__ float nb9(const MgLevel &L, size_t idx, size_t plane)
+{
+  const float *u = L.u, *c = L.coef;
+  const long P = L.P;
+  float s = __ldg(c + idx) * __ldcg(u + idx - P - 1);
+  s += __ldg(c + plane + idx) * __ldcg(u + idx - P);
+  s += __ldg(c + 2 * plane + idx) * __ldcg(u + idx - P + 1);
+  s += __ldg(c + 3 * plane + idx) * __ldcg(u + idx - 1);
+  s += __ldg(c + 4 * plane + idx) * __ldcg(u + idx + 1);
+  s += __ldg(c + 5 * plane + idx) * __ldcg(u + idx + P - 1);
+  s += __ldg(c + 6 * plane + idx) * __ldcg(u + idx + P);
+  s += __ldg(c + 7 * plane + idx) * __ldcg(u + idx + P + 1);
+  return s;
+}
+
+__device__ __forceinline__ float res9(const MgLevel &L, int I, int J)
+{
+  const size_t plane = (size_t)(L.Z + 2) * L.P, idx = (size_t)(I + 1) * L.P + J + 1;
+  if (__ldg(L.coef + MG_INVD * plane + idx) == 0.f)
+    return 0.f;
+  return __ldcg(L.f + idx) - __ldg(L.coef + MG_DIAG * plane + idx) * (__ldcg(L.u + idx) + nb9(L, idx, plane));
+}
+
+// one colour (cz, cr) = (c >> 1, c & 1) of Gauss-Seidel on a nine-point level
+__device__ void smooth9(const MgLevel &L, int c, long t0, long dt)
+{
+  const int cz = c >> 1, cr = c & 1;
+  const int Zh = (L.Z - cz + 1) >> 1, Rh = (L.R - cr + 1) >> 1;
+  const long n = (long)Zh * Rh;
+  const size_t plane = (size_t)(L.Z + 2) * L.P;
+  for (long t = t0; t < n; t += dt) {
+    const int q = (int)(t / Rh);
+    const int I = 2 * q + cz, J = 2 * (int)(t - (long)q * Rh) + cr;
+    const size_t idx = (size_t)(I + 1) * L.P + J + 1;
+    const float id = __ldg(L.coef + MG_INVD * plane + idx);
+    if (id == 0.f)
+      continue;
+    L.u[idx] = __ldcg(L.f + idx) * id - nb9(L, idx, plane);
+  }
+}
+
+// f of level C from the residual of level 0 (C = lev[1]), u of C cleared.
+// Level 0's last colour (1) has a zero residual: only (iz+ir) even nodes.
+__device__ void restrict0(const Mg32Args &a, long t0, long dt)
+{
+  const MgLevel &C = a.lev[1];
+  const long n = (long)C.Z * C.R;
+  const size_t plane = (size_t)(C.Z + 2) * C.P;
+  for (long t = t0; t < n; t += dt) {
+    const int I = (int)(t / C.R), J = (int)(t - (long)I * C.R);
+    const size_t idx = (size_t)(I + 1) * C.P + J + 1;
+    float s = 0.f;
+    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
+      const float w0 = __ldg(C.rw + 3 * J), w1 = __ldg(C.rw + 3 * J + 1), w2 = __ldg(C.rw + 3 * J + 2);
+      const int iz = 2 * I, ir = 2 * J;
+      s = w1 * res0(a, iz, ir);
+      if (iz > 0) {
+        if (ir > 0)
+          s += 0.5f * w0 * res0(a, iz - 1, ir - 1);
+        s += 0.5f * w2 * res0(a, iz - 1, ir + 1);
+      }
+      if (iz < a.nz) {
+        if (ir > 0)
+          s += 0.5f * w0 * res0(a, iz + 1, ir - 1);
+        s += 0.5f * w2 * res0(a, iz + 1, ir + 1);
+      }
+    }
+    C.f[idx] = s;
+    C.u[idx] = 0.f;
+  }
+}
+
+// f of level C = lev[l+1] from the residual of F = lev[l], u of C cleared.
+// F's last colour (3: odd, odd) has a zero residual: its four diagonal
+// neighbours of (2I, 2J) are skipped.
+__device__ void restrict9(const MgLevel &F, const MgLevel &C, long t0, long dt)
+{
+  const long n = (long)C.Z * C.R;
+  const size_t plane = (size_t)(C.Z + 2) * C.P;
+  for (long t = t0; t < n; t += dt) {
+    const int I = (int)(t / C.R), J = (int)(t - (long)I * C.R);
+    const size_t idx = (size_t)(I + 1) * C.P + J + 1;
+    float s = 0.f;
+    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
+      const float w0 = __ldg(C.rw + 3 * J), w1 = __ldg(C.rw + 3 * J + 1), w2 = __ldg(C.rw + 3 * J + 2);
+      const int i = 2 * I, j = 2 * J;
+      s = w1 * res9(F, i, j);
+      if (j > 0)
+        s += w0 * res9(F, i, j - 1);
+      if (j + 1 < F.R)
+        s += w2 * res9(F, i, j + 1);
+      if (i > 0)
+        s += 0.5f * w1 * res9(F, i - 1, j);
+      if (i + 1 < F.Z)
+        s += 0.5f * w1 * res9(F, i + 1, j);
+    }
+    C.f[idx] = s;
+    C.u[idx] = 0.f;
+  }
+}
+
+// bilinear correction from level C at node (i, j) of the level above
+__device__ __forceinline__ float interp(const MgLevel &C, int i, int j)
+{
+  const int I = i >> 1, J = j >> 1;
+  const float *u = C.u + (size_t)(I + 1) * C.P + J + 1;
+  float v;
+  if (j & 1)
+    v = 0.5f * (__ldcg(u) + __ldcg(u + 1));
+  else
+    v = __ldcg(u);
+  if (i & 1) {
+    const float *w = u + C.P;
+    v = 0.5f * v + 0.5f * ((j & 1) ? 0.5f * (__ldcg(w) + __ldcg(w + 1)) : __ldcg(w));
+  }
+  return v;
+}
+
+__device__ void prolong0(const Mg32Args &a, long t0, long dt)
+{
+  const MgLevel &C = a.lev[1];
+  const long n = (long)(a.hi - a.lo + 1) * a.cols;
+  for (long t = t0; t < n; t += dt) {
+    const int row = (int)(t / a.cols), ir = (int)(t - (long)row * a.cols), iz = a.lo + row;
+    const size_t j = node(iz, ir, a.P0);
+    if (a.umask[j] & S32_U_METAL)
+      continue;
+    a.u0[j] = __ldcg(a.u0 + j) + interp(C, iz, ir);
+  }
+}
+
+__device__ void prolong9(const MgLevel &F, const MgLevel &C, long t0, long dt)
+{
+  const long n = (long)F.Z * F.R;
+  const size_t plane = (size_t)(F.Z + 2) * F.P;
+  for (long t = t0; t < n; t += dt) {
+    const int i = (int)(t / F.R), j = (int)(t - (long)i * F.R);
+    const size_t idx = (size_t)(i + 1) * F.P + j + 1;
+    if (__ldg(F.coef + MG_INVD * plane + idx) == 0.f)
+      continue;
+    F.u[idx] = __ldcg(F.u + idx) + interp(C, i, j);
+  }
+}
+
+// Levels l0 .. nlev-1 below a restriction into l0: descent, the coarsest
+// level's sweeps, ascent back to l0.  `local`: CTA 0 alone.
+__device__ bool sub_cycle(const Mg32Args &a, int l0, bool local, long t0, long dt, unsigned &gen, DevCounts *cnt)
+{
+  const int L = a.nlev;
+  for (int l = l0; l < L - 1; l++) {
+    for (int k = 0; k < a.nu; k++)
+      for (int c = 0; c < 4; c++) {
+        smooth9(a.lev[l], c, t0, dt);
+        if (!mg_sync(a, local, gen, cnt))
+          return false;
+      }
+    restrict9(a.lev[l], a.lev[l + 1], t0, dt);
+    if (!mg_sync(a, local, gen, cnt))
+      return false;
+  }
+  for (int k = 0; k < a.coarse_sweeps; k++)
+    for (int c = 0; c < 4; c++) {
+      smooth9(a.lev[L - 1], c, t0, dt);
+      if (!mg_sync(a, local, gen, cnt))
+        return false;
+    }
+  for (int l = L - 2; l >= l0; l--) {
+    prolong9(a.lev[l], a.lev[l + 1], t0, dt);
+    if (!mg_sync(a, local, gen, cnt))
+      return false;
+    for (int k = 0; k < a.nu; k++)
+      for (int c = 3; c >= 0; c--) {
+        smooth9(a.lev[l], c, t0, dt);
+        if (!mg_sync(a, local, gen, cnt))
+          return false;
+      }
+  }
+  return true;
+}
+
+// One V-cycle on (u0, f0), u0 = 0 on entry.
+__device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
+{
+  const long gt0 = (long)blockIdx.x * blockDim.x + threadIdx.x, gdt = (long)gridDim.x * blockDim.x;
+  const long lt0 = threadIdx.x, ldt = blockDim.x;
+  const int T = a.tail; // 1 <= T <= nlev - 1
+  for (int k = 0; k < a.nu0; k++)
+    for (int c = 0; c < 2; c++) {
+      smooth0(a, c, gt0, gdt);
+      if (!mg_grid_sync(a, gen, cnt))
+        return false;
+    }
+  restrict0(a, gt0, gdt);
+  if (!mg_grid_sync(a, gen, cnt))
+    return false;
+  // grid-wide nine-point levels 1 .. T-1
+  for (int l = 1; l < T; l++) {
+    for (int k = 0; k < a.nu; k++)
+      for (int c = 0; c < 4; c++) {
+        smooth9(a.lev[l], c, gt0, gdt);
+        if (!mg_grid_sync(a, gen, cnt))
+          return false;
+      }
+    restrict9(a.lev[l], a.lev[l + 1], gt0, gdt);
+    if (!mg_grid_sync(a, gen, cnt))
+      return false;
+  }
+  // levels T .. nlev-1 by CTA 0 while the others wait
+  if (blockIdx.x == 0 && !sub_cycle(a, T, true, lt0, ldt, gen, cnt))
+    return false;
+  if (!mg_grid_sync(a, gen, cnt))
+    return false;
+  for (int l = T - 1; l >= 1; l--) {
+    prolong9(a.lev[l], a.lev[l + 1], gt0, gdt);
+    if (!mg_grid_sync(a, gen, cnt))
+      return false;
+    for (int k = 0; k < a.nu; k++)
+      for (int c = 3; c >= 0; c--) {
+        smooth9(a.lev[l], c, gt0, gdt);
+        if (!mg_grid_sync(a, gen, cnt))
+          return false;
+      }
+  }
+  prolong0(a, gt0, gdt);
+  if (!mg_grid_sync(a, gen, cnt))
+    return false;
+  for (int k = 0; k < a.nu0; k++)
+    for (int c = 1; c >= 0; c--) {
+      smooth0(a, c, gt0, gdt);
+      if (!mg_grid_sync(a, gen, cnt))
+        return false;
+    }
+  return true;
+}
+
+// r = rhs - A Psi in FP64 over the unknown nodes into f0 (rounded), u0 = 0
+// there; this thread's sum |r| and, with first, sum |rhs| over iz < nz,
+// ir < nr-1.  With fold, Psi += u0 first (the same nodes per thread).
+__device__ void residual64(const Mg32Args &a, bool first, double *rs, double *ds)
+{
+  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, dt = (long)gridDim.x * blockDim.x;
+  const long n = (long)a.nz * a.cols, P = a.P0;
+  double r_acc = 0, d_acc = 0;
+  for (long t = t0; t < n; t += dt) {
+    const int iz = (int)(t / a.cols), ir = (int)(t - (long)iz * a.cols);
+    const size_t j = node(iz, ir, a.P0);
+    const double rh = a.rhs ? a.rhs[j] : 0.0;
+    if (first)
+      d_acc += fabs(rh);
+    if (!unknown0(a, iz, ir, j))
+      continue;
+    const double up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? __ldcg(a.Psi + j - P) : __ldcg(a.Psi + j + P);
+    const double dn = (iz == 0 && a.lo == 0) ? __ldcg(a.Psi + j + P) : __ldcg(a.Psi + j - P);
+    const double psi = __ldcg(a.Psi + j);
+    double ap;
+    if (ir == 0)
+      ap = a.a_d * (up + dn) + a.c4_d * __ldcg(a.Psi + j + 1) + a.e2c_d * psi;
+    else {
+      const double h = 0.5 / ir;
+      ap = a.a_d * (up + dn) + a.dr2_inv * (1 + h) * __ldcg(a.Psi + j + 1) +
+           a.dr2_inv * (1 - h) * __ldcg(a.Psi + j - 1) + a.e_d * psi;
+    }
+    const double r = rh - ap;
+    r_acc += fabs(r);
+    a.f0[j] = (float)r;
+    a.u0[j] = 0.f;
+  }
+  *rs = r_acc;
+  *ds = d_acc;
+}
+
+__device__ void fold(const Mg32Args &a)
+{
+  const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, dt = (long)gridDim.x * blockDim.x;
+  const long n = (long)a.nz * a.cols;
+  for (long t = t0; t < n; t += dt) {
+    const int iz = (int)(t / a.cols), ir = (int)(t - (long)iz * a.cols);
+    const size_t j = node(iz, ir, a.P0);
+    if (unknown0(a, iz, ir, j))
+      a.Psi[j] = __ldcg(a.Psi + j) + (double)__ldcg(a.u0 + j);
+  }
+}
+
+// CTA sums of two doubles into part[blockIdx][0..1] (fixed order)
+__device__ void block_sums(const Mg32Args &a, double x, double y)
+{
+  __shared__ double sh[2][MG_NT / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    x += __shfl_down_sync(0xffffffffu, x, o);
+    y += __shfl_down_sync(0xffffffffu, y, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sh[0][w] = x;
+    sh[1][w] = y;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sx = 0, sy = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+      sx += sh[0][k];
+      sy += sh[1][k];
+    }
+    a.part[2 * blockIdx.x] = sx;
+    a.part[2 * blockIdx.x + 1] = sy;
+  }
+}
+
+// the grid's totals, formed in the same order by every CTA
+__device__ void grid_totals(const Mg32Args &a, double *tx, double *ty)
+{
+  __shared__ double tot[2];
+  if (threadIdx.x < 32) {
+    double x = 0, y = 0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += 32) {
+      x += __ldcg(a.part + 2 * k);
+      y += __ldcg(a.part + 2 * k + 1);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(0xffffffffu, x, o);
+      y += __shfl_down_sync(0xffffffffu, y, o);
+    }
+    if (threadIdx.x == 0) {
+      tot[0] = x;
+      tot[1] = y;
+    }
+  }
+  __syncthreads();
+  *tx = tot[0];
+  *ty = tot[1];
+}
+
+__global__ void __launch_bounds__(MG_NT) k_mg32(Mg32Args a, DevCounts *cnt)
+{
+  if (a.st && !a.st->do_solve)
+    return;
+  unsigned gen = 0;
+  double drive = 0, total = 0;
+  long long cycles = 0;
+  bool conv = false;
+  for (;;) {
+    const bool first = cycles == 0;
+    double rs, ds;
+    residual64(a, first, &rs, &ds);
+    block_sums(a, rs, ds);
+    if (!mg_grid_sync(a, gen, cnt))
+      return;
+    double dsum;
+    grid_totals(a, &total, &dsum);
+    if (first)
+      drive = a.rhs ? dsum : total; // poisson.c:40-43; a Laplace solve: its first residual
+    if (total == 0 || total < a.accuracy * drive) {
+      conv = true;
+      break;
+    }
+    if (cycles >= a.max_cycles)
+      break;
+    // (the partials are rewritten only after the V-cycle's first barrier,
+    // which every CTA reaches after reading them)
+    if (!vcycle(a, gen, cnt))
+      return;
+    fold(a);
+    if (!mg_grid_sync(a, gen, cnt))
+      return;
+    cycles++;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const long long result = conv ? cycles : -1;
+    if (a.iters_out)
+      *a.iters_out = result;
+    if (a.st) {
+      a.st->iterations = result;
+      a.st->residual = total;
+    }
+    cnt->mg_cycles += cycles;
+    cnt->sor_solves += 1;
+  }
+}
+
+// ---- host: the level hierarchy
+
+// level-0 operator as nine-point rows (only the five-point entries are
+// nonzero): coefficient of node (iz+dz, ir+dr) at k = (dz+1)*3 + (dr+1)
+struct Stencil {
+  int Z = 0, R = 0;
+  std::vector<double> c; // [9][Z*R]
+  std::vector<uint8_t> unk;
+  double &at(int k, int i, int j) { return c[(size_t)k * Z * R + (size_t)i * R + j]; }
+  double at(int k, int i, int j) const { return c[(size_t)k * Z * R + (size_t)i * R + j]; }
+};
+
+void fine_stencil(const DevMesh &m, const int16_t *flags, int lo, int hi, Stencil &S)
+{
+  const int nz = m.nz, nr = m.nr, cols = nr - 1;
+  S.Z = nz + 1;
+  S.R = nr + 1;
+  S.c.assign((size_t)9 * S.Z * S.R, 0.0);
+  S.unk.assign((size_t)S.Z * S.R, 0);
+  for (int iz = lo; iz <= hi; iz++)
+    for (int ir = 0; ir < cols; ir++)
+      if (!(flags[(size_t)iz * (nr + 1) + ir] & (SPIFFE_FL_IS_SURFACE | SPIFFE_FL_IS_INSIDE)))
+        S.unk[(size_t)iz * S.R + ir] = 1;
+  const double a = 1 / (m.dz * m.dz), dr2 = m.dr * m.dr;
+  const double e = -2 * (1 / (m.dz * m.dz) + 1 / dr2);
+  for (int iz = lo; iz <= hi; iz++)
+    for (int ir = 0; ir < cols; ir++) {
+      if (!S.unk[(size_t)iz * S.R + ir])
+        continue;
+      double cu = a, cd = a;
+      int zu = iz + 1, zd = iz - 1;
+      if (iz == 0 && lo == 0) { // mirrored end rows (poisson.c:67-84, :102-118)
+        zd = iz + 1;
+      } else if (iz == nz - 1 && hi == nz - 1) {
+        zu = iz - 1;
+      }
+      double cr, cl, dg;
+      if (ir == 0) {
+        cr = 4 / dr2;
+        cl = 0;
+        dg = e - 2 / dr2;
+      } else {
+        cr = 1 / dr2 * (1 + 1. / (2 * ir));
+        cl = 1 / dr2 * (1 - 1. / (2 * ir));
+        dg = e;
+      }
+      auto add = [&](int z2, int r2, double v) {
+        if (v == 0 || z2 < 0 || z2 >= S.Z || r2 < 0 || r2 >= S.R || !S.unk[(size_t)z2 * S.R + r2])
+          return;
+        S.at((z2 - iz + 1) * 3 + (r2 - ir + 1), iz, ir) += v;
+      };
+      add(zu, ir, cu);
+      add(zd, ir, cd);
+      add(iz, ir + 1, cr);
+      add(iz, ir - 1, cl);
+      S.at(4, iz, ir) = dg;
+    }
+}
+
+// annulus weight of column j of a level of spacing 1 (the axis node: 1/8)
+inline double vol(int j) { return j ? (double)j : 0.125; }
+
+// Galerkin R A P from level F to C (nodes 2I, 2J of F); restriction weights
+// rw[J][3] for F columns 2J-1, 2J, 2J+1 (z weights 1/2, 1, 1/2 apply on top)
+void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
+{
+  C.Z = (F.Z + 1) / 2;
+  C.R = (F.R + 1) / 2;
+  C.c.assign((size_t)9 * C.Z * C.R, 0.0);
+  C.unk.assign((size_t)C.Z * C.R, 0);
+  for (int I = 0; I < C.Z; I++)
+    for (int J = 0; J < C.R; J++)
+      C.unk[(size_t)I * C.R + J] = F.unk[(size_t)(2 * I) * F.R + 2 * J];
+  rw.assign((size_t)3 * C.R, 0.0);
+  for (int J = 0; J < C.R; J++)
+    for (int dj = -1; dj <= 1; dj++) {
+      const int j = 2 * J + dj;
+      if (j < 0 || j >= F.R)
+        continue;
+      // fine spacing 1, coarse spacing 2: Vc(J) = 2 vol(J) (axis: 1/4)
+      const double vc = J ? 2.0 * J : 0.25;
+      rw[(size_t)3 * J + dj + 1] = (dj ? 0.5 : 1.0) * vol(j) / (4 * vc);
+    }
+  auto cunk = [&](int I, int J) { return I >= 0 && I < C.Z && J >= 0 && J < C.R && C.unk[(size_t)I * C.R + J]; };
+  for (int I = 0; I < C.Z; I++)
+    for (int J = 0; J < C.R; J++) {
+      if (!C.unk[(size_t)I * C.R + J])
+        continue;
+      double acc[9] = {0};
+      for (int di = -1; di <= 1; di++)
+        for (int dj = -1; dj <= 1; dj++) {
+          const int i = 2 * I + di, j = 2 * J + dj;
+          if (i < 0 || i >= F.Z || j < 0 || j >= F.R || !F.unk[(size_t)i * F.R + j])
+            continue;
+          const double r = (di ? 0.5 : 1.0) * rw[(size_t)3 * J + dj + 1];
+          for (int k = 0; k < 9; k++) {
+            const double v = F.at(k, i, j);
+            if (v == 0)
+              continue;
+            const int ni = i + k / 3 - 1, nj = j + k % 3 - 1; // an unknown fine node
+            // its coarse parents (bilinear interpolation)
+            const int pz0 = ni >> 1, pr0 = nj >> 1;
+            const int nzp = (ni & 1) ? 2 : 1, nrp = (nj & 1) ? 2 : 1;
+            const double wz = (ni & 1) ? 0.5 : 1.0, wr = (nj & 1) ? 0.5 : 1.0;
+            for (int pz = 0; pz < nzp; pz++)
+              for (int pr = 0; pr < nrp; pr++) {
+                const int K = pz0 + pz, Lc = pr0 + pr;
+                if (!cunk(K, Lc))
+                  continue;
+                acc[(K - I + 1) * 3 + (Lc - J + 1)] += r * v * wz * wr;
+              }
+          }
+        }
+      for (int k = 0; k < 9; k++)
+        C.at(k, I, J) = acc[k];
+      if (!(acc[4] < 0)) { // not a proper diagonal: hold the node
+        C.unk[(size_t)I * C.R + J] = 0;
+        for (int k = 0; k < 9; k++)
+          C.at(k, I, J) = 0;
+      }
+    }
+  // couplings to nodes that were held above
+  for (int I = 0; I < C.Z; I++)
+    for (int J = 0; J < C.R; J++)
+      for (int k = 0; k < 9; k++)
+        if (C.at(k, I, J) != 0 && !cunk(I + k / 3 - 1, J + k % 3 - 1))
+          C.at(k, I, J) = 0;
+}
+
+size_t unknowns(const Stencil &S)
+{
+  size_t n = 0;
+  for (uint8_t u : S.unk)
+    n += u;
+  return n;
+}
+
+} // namespace
+
+extern "C" void s32_mg_free(Mg32Work *w)
+{
+  cudaFree(w->mem);
+  *w = Mg32Work();
+}
+
+extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w, cudaStream_t s)
+{
+  s32_mg_free(w);
+  const int lo = m->left_bc == SPIFFE_DIRICHLET ? 0 : 1;
+  const int hi = m->right_bc == SPIFFE_DIRICHLET ? m->nz - 1 : m->nz - 2;
+  std::vector<Stencil> lev(1);
+  std::vector<std::vector<double>> rws(1);
+  fine_stencil(*m, flags, lo, hi, lev[0]);
+  while ((int)lev.size() < MG_MAX_LEVELS) {
+    const Stencil &F = lev.back();
+    if (F.Z < 5 || F.R < 5 || unknowns(F) <= (size_t)MG_MIN_UNKNOWNS)
+      break;
+    Stencil C;
+    std::vector<double> rw;
+    galerkin(F, C, rw);
+    if (unknowns(C) == 0)
+      break;
+    lev.push_back(std::move(C));
+    rws.push_back(std::move(rw));
+  }
+  const int L = (int)lev.size();
+  if (L < 2)
+    return (int)cudaErrorInvalidConfiguration; // a mesh too small to coarsen: the caller uses SOR
+  // device layout: level 0's u0, f0 at the mesh pitch; per coarse level u,
+  // f, MG_NCOEF coefficient planes of (Z+2) x P floats, rw of 3 R floats
+  const size_t n0 = (size_t)(m->nz + 1) * m->pitch;
+  size_t bytes = 2 * n0 * sizeof(float);
+  std::vector<size_t> off(L), coff(L), roff(L);
+  for (int l = 1; l < L; l++) {
+    const int P = (lev[l].R + 2 + 31) / 32 * 32;
+    const size_t plane = (size_t)(lev[l].Z + 2) * P;
+    off[l] = bytes;
+    bytes += 2 * plane * sizeof(float);
+    coff[l] = bytes;
+    bytes += MG_NCOEF * plane * sizeof(float);
+    roff[l] = bytes;
+    bytes += ((size_t)3 * lev[l].R * sizeof(float) + 255) / 256 * 256;
+  }
+  const size_t sums_off = bytes;
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_mg32, MG_NT, 0);
+  if (e != cudaSuccess)
+    return (int)e;
+  if (per < 1)
+    return (int)cudaErrorInvalidConfiguration;
+  const int grid = sms; // one CTA per SM: every CTA is resident
+  bytes += (size_t)2 * grid * sizeof(double) + 32 * sizeof(unsigned long long) + sizeof(long long);
+  char *mem = nullptr;
+  e = cudaMalloc(&mem, bytes);
+  if (e != cudaSuccess)
+    return (int)e;
+  e = cudaMemsetAsync(mem, 0, bytes, s); // halos, held nodes and level 0 start at zero
+  w->mem = mem;
+  w->bytes = bytes;
+  w->nlev = L;
+  w->grid = grid;
+  w->threads = MG_NT;
+  w->u0 = (float *)mem;
+  w->f0 = (float *)mem + n0;
+  w->part = (double *)(mem + sums_off);
+  w->bar = (unsigned long long *)(mem + sums_off + (size_t)2 * grid * sizeof(double));
+  w->iters = (long long *)(w->bar + 32);
+  // the first level small enough for CTA 0 alone (at least level 1, at most the coarsest)
+  int tail = L - 1;
+  for (int l = 1; l < L; l++)
+    if ((size_t)lev[l].Z * lev[l].R <= (size_t)MG_TAIL_NODES) {
+      tail = l;
+      break;
+    }
+  w->tail = tail;
+  std::vector<float> hc, hr;
+  for (int l = 1; l < L && e == cudaSuccess; l++) {
+    const Stencil &S = lev[l];
+    MgLevel &D = w->lev[l];
+    D.Z = S.Z;
+    D.R = S.R;
+    D.P = (S.R + 2 + 31) / 32 * 32;
+    const size_t plane = (size_t)(S.Z + 2) * D.P;
+    D.u = (float *)(mem + off[l]);
+    D.f = D.u + plane;
+    D.coef = (const float *)(mem + coff[l]);
+    D.rw = (const float *)(mem + roff[l]);
+    hc.assign(MG_NCOEF * plane, 0.f);
+    for (int I = 0; I < S.Z; I++)
+      for (int J = 0; J < S.R; J++) {
+        if (!S.unk[(size_t)I * S.R + J])
+          continue;
+        const size_t idx = (size_t)(I + 1) * D.P + J + 1;
+        const double dg = S.at(4, I, J);
+        int q = 0;
+        for (int k = 0; k < 9; k++) {
+          if (k == 4)
+            continue;
+          hc[(size_t)q * plane + idx] = (float)(S.at(k, I, J) / dg);
+          q++;
+        }
+        hc[(size_t)MG_INVD * plane + idx] = (float)(1 / dg);
+        hc[(size_t)MG_DIAG * plane + idx] = (float)dg;
+      }
+    hr.assign((size_t)3 * S.R, 0.f);
+    for (size_t k = 0; k < hr.size(); k++)
+      hr[k] = (float)rws[l][k];
+    e = cudaMemcpyAsync(mem + coff[l], hc.data(), hc.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(mem + roff[l], hr.data(), hr.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(s); // the host staging is reused by the next level
+  }
+  if (e != cudaSuccess)
+    s32_mg_free(w);
+  return (int)e;
+}
+
+// the solve on Psi with driving term rhs (null: Laplace), stop rule
+// sum|r| < accuracy sum|rhs|, at most max_cycles V-cycles
+extern "C" int s32_mg_solve(const DevMesh *m, Mg32Work *w, const float *crow, const float *drow, double *Psi,
+                            const double *rhs, const uint8_t *umask, double accuracy, long long max_cycles,
+                            PcState *st, long long *iters_out, DevCounts *cnt, cudaStream_t s)
+{
+  Mg32Args a{};
+  a.Psi = Psi;
+  a.rhs = rhs;
+  a.umask = umask;
+  a.u0 = w->u0;
+  a.f0 = w->f0;
+  a.crow = crow;
+  a.drow = drow;
+  a.nz = m->nz;
+  a.P0 = m->pitch;
+  a.lo = m->left_bc == SPIFFE_DIRICHLET ? 0 : 1;
+  a.hi = m->right_bc == SPIFFE_DIRICHLET ? m->nz - 1 : m->nz - 2;
+  a.cols = m->nr - 1;
+  const double dz2 = m->dz * m->dz, dr2 = m->dr * m->dr;
+  a.a_d = 1 / dz2;
+  a.e_d = -2 * (1 / dz2 + 1 / dr2);
+  a.c4_d = 4 / dr2;
+  a.e2c_d = a.e_d - 2 / dr2;
+  a.dr2_inv = 1 / dr2;
+  a.a = (float)a.a_d;
+  a.c4 = (float)a.c4_d;
+  a.e = (float)a.e_d;
+  a.e2c = (float)a.e2c_d;
+  a.inv_e = (float)(1 / a.e_d);
+  a.inv_e2c = (float)(1 / a.e2c_d);
+  a.nlev = w->nlev;
+  a.tail = w->tail;
+  a.nu0 = 2;
+  a.nu = 2;
+  a.coarse_sweeps = 24;
+  a.max_cycles = (int)std::min<long long>(max_cycles, 100);
+  a.accuracy = accuracy;
+  for (int l = 0; l < w->nlev; l++)
+    a.lev[l] = w->lev[l];
+  a.bar = w->bar;
+  a.part = w->part;
+  a.st = st;
+  a.iters_out = iters_out ? iters_out : w->iters;
+  cudaError_t e = cudaMemsetAsync(w->bar, 0, 32 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess)
+    return (int)e;
+  void *args[] = {&a, &cnt};
+  e = cudaLaunchCooperativeKernel((const void *)k_mg32, dim3(w->grid), dim3(w->threads), args, 0, s);
+  spiffe_note_launches(1);
+  return (int)e;
+}

@@ -1161,6 +1161,7 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
 
 extern "C" void s32_poisson_free(Poisson32Work *w)
 {
+  s32_mg_free(&w->mg);
   void *p[] = {w->Az, w->Ari, w->Aro, w->volume, w->crow, w->drow, w->scalars, w->qreal_fixed, w->st,
                w->iters, w->bar, w->dpart, w->xbuf, w->part, w->omega};
   for (void *q : p)
@@ -1241,6 +1242,14 @@ extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const do
   return (int)e;
 }
 
+extern "C" int s32_solve(const DevMesh *m, Poisson32Work *w, double *Psi, const double *rhs, const uint8_t *umask,
+                         double accuracy, long long limit, PcState *st, DevCounts *cnt, cudaStream_t s)
+{
+  if (w->solver == SPIFFE_POISSON_MULTIGRID && w->mg.nlev >= 2)
+    return s32_mg_solve(m, &w->mg, w->crow, w->drow, Psi, rhs, umask, accuracy, limit, st, w->iters, cnt, s);
+  return s32_sor(m, w, Psi, rhs, umask, accuracy, limit, st, cnt, s);
+}
+
 extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, const DevBeam32 *b, DevCounts *cnt,
                                       long long np_bound, const PoissonHostOptions *o, const S32Scales *sc,
                                       Poisson32Work *w, cudaStream_t s)
@@ -1271,7 +1280,7 @@ extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, co
     k_guess32<<<grid, block, 0, s>>>(*m, *f, o->guess_code, w->st);
     spiffe_note_launches(1);
   }
-  int rc = s32_sor(m, w, f->Psi, f->Q, f->umask, o->accuracy, o->maximum_iterations, w->st, cnt, s);
+  int rc = s32_solve(m, w, f->Psi, f->Q, f->umask, o->accuracy, o->maximum_iterations, w->st, cnt, s);
   if (rc)
     return rc;
   k_subtract32<<<grid, block, 0, s>>>(*m, *f, w->st);

@@ -564,6 +564,10 @@ static int s32_ensure_poisson(spiffe_gpu_instance *in)
                 "mesh %d x %d is too large for the shared-memory Poisson solver of the split-precision form",
                 in->mesh.nz, in->mesh.nr);
   RC_TRY(rc);
+  // the multigrid levels (a mesh too small to coarsen keeps SOR)
+  const int mrc = s32_mg_setup(&in->dm, in->h_flags.data(), &S.pcw.mg, in->stream);
+  if (mrc && mrc != (int)cudaErrorInvalidConfiguration)
+    return fail(SPIFFE_ERR_CUDA, "multigrid set-up failed: %s", cudaGetErrorString((cudaError_t)mrc));
   S.pc_ready = true;
   return 0;
 }
@@ -1136,8 +1140,10 @@ extern "C" int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *in, int32_t tar
   if (in->s32) {
     S32State &S = *in->s32;
     RC_TRY(s32_ensure_poisson(in));
-    const int rc = s32_sor(&in->dm, &S.pcw, target ? S.f.PsiImposed : S.f.Psi, target ? nullptr : S.f.Q, S.umask,
-                           accuracy, limit, nullptr, in->cnt, in->stream);
+    const int rc = target ? s32_sor(&in->dm, &S.pcw, S.f.PsiImposed, nullptr, S.umask, accuracy, limit, nullptr,
+                                    in->cnt, in->stream)
+                          : s32_solve(&in->dm, &S.pcw, S.f.Psi, S.f.Q, S.umask, accuracy, limit, nullptr, in->cnt,
+                                      in->stream);
     if (rc)
       return fail(SPIFFE_ERR_CUDA, "SOR launch failed: %s", cudaGetErrorString((cudaError_t)rc));
     long long it = 0;
@@ -2349,8 +2355,21 @@ extern "C" int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *in, int64_t n)
   return 0;
 }
 
+extern "C" int spiffe_gpu_set_poisson_solver(spiffe_gpu_instance *in, int32_t solver)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (solver != SPIFFE_POISSON_SOR && solver != SPIFFE_POISSON_MULTIGRID)
+    return fail(SPIFFE_ERR_INVALID, "unknown Poisson solver %d", (int)solver);
+  if (!in->s32)
+    return solver == SPIFFE_POISSON_SOR ? 0
+                                        : fail(SPIFFE_ERR_UNSUPPORTED, "the FP64 form solves with the reference's SOR");
+  in->s32->pcw.solver = solver;
+  return 0;
+}
+
 // Work done so far: [0] particle-steps (active particles summed over pushes),
-// [1] SOR half-sweeps, [2] SOR solves, [3] FDTD steps.
+// [1] SOR half-sweeps, [2] Poisson solves, [3] FDTD steps, [4] V-cycles.
 extern "C" int spiffe_gpu_work_counters(spiffe_gpu_instance *in, int64_t *out)
 {
   if (!in || !out)
@@ -2360,5 +2379,6 @@ extern "C" int spiffe_gpu_work_counters(spiffe_gpu_instance *in, int64_t *out)
   out[1] = in->h_cnt->sor_halfsweeps;
   out[2] = in->h_cnt->sor_solves;
   out[3] = in->fdtd_steps;
+  out[4] = in->h_cnt->mg_cycles;
   return 0;
 }

@@ -161,6 +161,37 @@ struct BirthParams;
 extern "C" int s32_births(const DevMesh *m, const DevFields32 *f, const DevBeam32 *b, const BirthParams *p,
                           DevCounts *cnt, const S32Scales *sc, int deposit, cudaStream_t s);
 
+// Multigrid solve (multigrid_f32.cu): level 0 is the mesh itself (the
+// five-point operator of poisson.c:57-117 in FP32 on the correction u0 with
+// right-hand side f0); each coarser level holds nodes 2I, 2J of the level
+// above, with the Galerkin operator R A P of that level (nine points) built
+// on the host.
+#define MG_MAX_LEVELS 14
+#define MG_NCOEF 10 // 8 off-diagonal coefficients divided by the diagonal, 1/diagonal, diagonal
+struct MgLevel {
+  int Z = 0, R = 0, P = 0; // nodes in z and r; row pitch with one halo node a side
+  float *u = nullptr, *f = nullptr; // (Z+2) x P, node (I, J) at (I+1) P + J + 1; halo nodes stay 0
+  const float *coef = nullptr;      // MG_NCOEF arrays of (Z+2) x P; 1/diagonal 0 marks a held node
+  const float *rw = nullptr;        // restriction weights from the level above: [J][3], columns 2J-1, 2J, 2J+1
+};
+struct Mg32Work {
+  int nlev = 0, tail = 0; // levels; first level that CTA 0 works alone
+  MgLevel lev[MG_MAX_LEVELS];
+  float *u0 = nullptr, *f0 = nullptr; // level 0 at the mesh pitch
+  void *mem = nullptr;                // every level array, one allocation
+  double *part = nullptr;             // per-CTA partial sums [grid][2]
+  unsigned long long *bar = nullptr;  // [0] barrier arrivals, [16] abort
+  long long *iters = nullptr;
+  int grid = 0, threads = 0;
+  size_t bytes = 0;
+};
+extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *host_flags, Mg32Work *w, cudaStream_t s);
+extern "C" void s32_mg_free(Mg32Work *w);
+struct PcState;
+extern "C" int s32_mg_solve(const DevMesh *m, Mg32Work *w, const float *crow, const float *drow, double *Psi,
+                            const double *rhs, const uint8_t *umask, double accuracy, long long max_cycles,
+                            PcState *st, long long *iters_out, DevCounts *cnt, cudaStream_t s);
+
 // Poisson correction (poisson_f32.cu)
 struct PcState;
 struct Poisson32Work {
@@ -181,12 +212,20 @@ struct Poisson32Work {
   int grid = 0, threads = 0, depth = 2; // depth: halo rows a side = half-sweeps per barrier
   size_t smem = 0;
   int rows_per = 0, half = 0; // rows of the widest CTA band; half-row length (nodes of one colour)
+  // solver of the Poisson correction: SPIFFE_POISSON_MULTIGRID (mg) or SPIFFE_POISSON_SOR
+  int solver = 1;
+  Mg32Work mg;
 };
+
 struct PoissonHostOptions;
 extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long np_capacity, cudaStream_t s);
 extern "C" void s32_poisson_free(Poisson32Work *w);
 extern "C" int s32_sor(const DevMesh *m, Poisson32Work *w, double *Psi, const double *rhs, const uint8_t *umask,
                        double accuracy, long long limit, PcState *st, DevCounts *cnt, cudaStream_t s);
+// the instance's solver (multigrid where it was set up, else SOR); the
+// count of half-sweeps or V-cycles, -1 at the limit, lands in w->iters
+extern "C" int s32_solve(const DevMesh *m, Poisson32Work *w, double *Psi, const double *rhs, const uint8_t *umask,
+                         double accuracy, long long limit, PcState *st, DevCounts *cnt, cudaStream_t s);
 extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, const DevBeam32 *b, DevCounts *cnt,
                                       long long np_bound, const PoissonHostOptions *o, const S32Scales *sc,
                                       Poisson32Work *w, cudaStream_t s);

@@ -21,6 +21,8 @@ LIB_PATH = os.path.join(HERE, "libspiffe_b200.so")
 
 PRECISION_F64 = 0
 PRECISION_SPLIT32 = 1
+POISSON_SOR = 0
+POISSON_MULTIGRID = 1
 
 _lib = None
 P = C.POINTER
@@ -79,6 +81,7 @@ def load():
         "spiffe_gpu_launch_count": ([], C.c_int64),
         "spiffe_gpu_work_counters": ([H, P(C.c_int64)], C.c_int),
         "spiffe_gpu_set_sort_interval": ([H, C.c_int64], C.c_int),
+        "spiffe_gpu_set_poisson_solver": ([H, C.c_int32], C.c_int),
         "spiffe_gpu_batch_run": ([P(H), C.c_int32, P(C.c_int64), C.c_int32, C.c_int64, P(C.c_double)], C.c_int),
         "spiffe_gpu_set_test_beam": ([H, P(abi.TestBeamOptions)], C.c_int),
         "spiffe_gpu_add_on_axis_field": ([H, P(C.c_double), P(C.c_double), C.c_int64, C.c_double, C.c_double,
@@ -320,10 +323,16 @@ class GpuInstance:
         return {n: (ms[i], cnt[i]) for i, n in enumerate(self.PHASES)}
 
     def work_counters(self):
-        """particle-steps, SOR half-sweeps, SOR solves, FDTD steps so far."""
-        out = (C.c_int64 * 4)()
+        """particle-steps, SOR half-sweeps, Poisson solves, FDTD steps and
+        multigrid V-cycles so far."""
+        out = (C.c_int64 * 5)()
         _check(self.lib.spiffe_gpu_work_counters(self.h, out))
-        return dict(particle_steps=out[0], sor_halfsweeps=out[1], sor_solves=out[2], fdtd_steps=out[3])
+        return dict(particle_steps=out[0], sor_halfsweeps=out[1], sor_solves=out[2], fdtd_steps=out[3],
+                    mg_cycles=out[4])
+
+    def set_poisson_solver(self, solver):
+        """POISSON_MULTIGRID (split form default) or POISSON_SOR."""
+        _check(self.lib.spiffe_gpu_set_poisson_solver(self.h, int(solver)))
 
     def counts_async(self, out):
         """Enqueues a copy of (np, npActive) into out[0:2] (an int64 numpy

@@ -41,12 +41,15 @@ from . import abi, workloads
 # device bytes of an instance: a fixed part (allocation granularity, solver
 # scratch), per mesh node (split form: FP32 E/B and imposed fields, int64
 # current and particle charge, FP64 Psi/PsiImposed/Q, flags, update mask,
-# FP64 staging) and per particle slot (the split particle layout, a second
+# FP64 staging, and the multigrid levels: FP32 correction and residual on
+# the mesh, ten coefficient planes and two arrays a quarter the size on the
+# next level, a sixteenth on the one after, padded rows) and per particle
+# slot (the split particle layout, a second
 # copy for the cell sort, sort keys, transfer staging).  An upper estimate:
 # on a B200 the measured use of eight scan instances (18k-273k nodes,
 # 39k-610k slots, a screen as large as the beam) lay 5-55 % below it.
 FIXED_BYTES = 16 << 20
-NODE_BYTES = {"split32": 160, "f64": 260}
+NODE_BYTES = {"split32": 200, "f64": 260}
 PARTICLE_BYTES = {"split32": 360, "f64": 460}
 RECORD_BYTES = 112  # one screen record slot
 

@@ -10,6 +10,7 @@ reference present.  Run from the repository root:
     python tests/golden/make_golden.py          # every fixture
     python tests/golden/make_golden.py decks    # the input-deck fixtures only
     python tests/golden/make_golden.py onaxis   # one deck fixture (also: translate)
+    python tests/golden/make_golden.py te       # the TE-field fixture
 """
 import os
 import sys
@@ -160,6 +161,72 @@ def main():
                                       workloads.gun16_geo())
     save("gun16_geometry", flags=flags3, geo=np.array(workloads.gun16_geo()), **mesh_arrays(mesh3))
     save("dcgun_geometry", flags=flags2, PsiImposed=psi_imp0, geo=np.array(geo), **mesh_arrays(mesh2))
+
+
+# TE fields (include_TE_fields=1, geometry.nl:25): the FDTD's TE part
+# (integrate.c:434-540) on the gun mesh from random fields and currents, and
+# one deposition and push whose gather reads Ephi, Br2 and Bz2
+# (advance_particles.c:649-825) and whose deposit fills Jphi
+# (space_charge.c:218).
+TE_FIELDS = ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Bz", "Br2", "Bz2")
+
+
+def f32(a):
+    return np.asarray(a, np.float32).astype(np.float64)
+
+
+def te():
+    rng = np.random.default_rng(3)
+    fx = np.load(os.path.join(HERE, "gun16_geometry.npz"))
+    cmd = workloads.geometry_command(301, 83, 0.0, 0.150, 0.041, "gun.geo")
+    d, mesh, flags, _ = geometry(cmd, "gun.geo", str(fx["geo"]))
+    assert np.array_equal(flags, fx["flags"])
+    modes = MODES | abi.FL_TE_FIELDS
+    dt, steps = 2e-13, 25
+    # inputs rounded to single precision (exact in double) keep the fixture small
+    init = {n: f32(rng.normal(size=flags.shape)) for n in TE_FIELDS + ("Jz", "Jr", "Jphi")}
+    prog = [("command", cmd), ("set_time", dt, 0.0, 0, modes)]
+    prog += [("set_field", n, a) for n, a in init.items()]
+    prog += [("call", "ref_advance_field_solutions")] * steps
+    prog += [("get_field", n) for n in TE_FIELDS]
+    out = pyoracle.run_reference(prog, cwd=d)[-len(TE_FIELDS):]
+    arrays = dict(flags=flags, dt=dt, steps=steps, modes=modes,
+                  **{"in_" + n: a.astype(np.float32) for n, a in init.items()},
+                  **dict(zip(TE_FIELDS, out)), **mesh_arrays(mesh))
+
+    # deposition and push on the pillbox mesh with TE fields present
+    cfg = workloads.PillboxConfig()
+    d2, mesh2, flags2, _ = geometry(cfg.geometry(), "pillbox.geo", cfg.geo_text())
+    shape = flags2.shape
+    scale = {"E": 1e7, "B": 0.05}
+    fields = {n: f32(rng.normal(size=shape) * scale[n[0]]) for n in TE_FIELDS}
+    fields["EzImposed"] = f32(rng.normal(size=shape) * 1e6)
+    fields["ErImposed"] = f32(rng.normal(size=shape) * 1e6)
+    fields["BzImposed"] = f32(rng.normal(size=shape) * 0.1)
+    fields["BrImposed"] = f32(rng.normal(size=shape) * 0.1)
+    N = 1500
+    beam = random_beam(rng, N, -0.0003, cfg.L + 0.0003, cfg.R)
+    beam["r_pphi"] = rng.normal(size=N) * 1e-4
+    rs = np.where(beam["r"] != 0, beam["r"], 1.0)
+    g = np.sqrt(1 + beam["pz"] ** 2 + beam["pr"] ** 2 + (beam["r_pphi"] / rs) ** 2)
+    c = 2.99792458e8
+    beam["vz"], beam["vr"], beam["vphi"] = c * beam["pz"] / g, c * beam["pr"] / g, c * beam["r_pphi"] / rs / g
+    tstep = 11
+    pmodes = modes | abi.FL_SPACE_CHARGE
+    prog = [("command", cfg.geometry()), ("set_time", cfg.dt, 0.0, tstep, pmodes)]
+    prog += [("set_field", n, a) for n, a in fields.items()]
+    # the TE current array exists when define_geometry has include_TE_fields=1
+    prog += [("set_field", "Jphi", np.zeros(shape))]
+    prog += [("set_beam", (N, int(beam["status"].sum()), 0, N + 1), (QoMC, 1.0), beam),
+             ("call", "ref_zero_current_arrays"), ("call", "ref_add_particle_currents"), ("get_field", "Jz"),
+             ("get_field", "Jr"), ("get_field", "Jphi"), ("call", "ref_advance_particles", -1.0), ("get_beam",)]
+    res = pyoracle.run_reference(prog, cwd=d2)
+    Jz, Jr, Jphi, rb = res[-5], res[-4], res[-3], res[-1]
+    arrays.update(p_flags=flags2, p_dt=cfg.dt, p_time_step=tstep, p_modes=pmodes, p_QoMC=QoMC,
+                  p_Jz=Jz, p_Jr=Jr, p_Jphi=Jphi, **{"p_f_" + k: v.astype(np.float32) for k, v in fields.items()},
+                  **{"p_in_" + k: v for k, v in beam.items()}, **{"p_" + k: v for k, v in beam_out(rb).items()},
+                  **{"p_" + k: v for k, v in mesh_arrays(mesh2).items()})
+    save("gun16_te", **arrays)
 
 
 # Input decks run through the reference's own command processors and
@@ -330,8 +397,11 @@ if __name__ == "__main__":
         deck_status(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["translate"]:
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["te"]:
+        te()
     elif sys.argv[1:] == ["onaxis"]:
         deck_onaxis(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     else:
         main()
+        te()
         decks()

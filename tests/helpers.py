@@ -62,3 +62,57 @@ def rel_l2(a, b):
 def by_id(records, key="particleID"):
     order = np.argsort(records[key], kind="stable")
     return {k: np.asarray(v)[order] for k, v in records.items()}
+
+
+TE_FIELDS = ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Bz", "Br2", "Bz2")
+
+
+def te_fdtd_state(fx):
+    """The gun16_te fixture's FDTD case: the gun mesh with TE and TM fields
+    and constant currents, before its `steps` field steps."""
+    f = fields_from(fx, modes=int(fx["modes"]), dt=float(fx["dt"]))
+    for n in TE_FIELDS + ("Jz", "Jr", "Jphi"):
+        f[n] = fx["in_" + n].astype(np.float64)
+    return f
+
+
+def te_push_state(fx):
+    """The gun16_te fixture's deposition and push case (pillbox mesh, TE and
+    TM fields, imposed fields, 1,500 particles with angular momentum)."""
+    sub = {k[2:]: v for k, v in fx.items() if k.startswith("p_")}
+    f = fields_from(sub, modes=int(sub["modes"]), dt=float(sub["dt"]))
+    f.mesh.time_step = int(sub["time_step"])
+    f.mesh.time = f.mesh.time_step * f.mesh.dt
+    for k, v in sub.items():
+        if k.startswith("f_"):
+            f[k[2:]] = v.astype(np.float64)
+    return f, beam_from(sub), sub
+
+
+def poisson_residual(f, psi, rhs):
+    """sum |rhs - A psi| over the nodes solve_poisson_cyl updates
+    (poisson.c:57-117, both colours at once) and sum |rhs| over iz < nz,
+    ir < nr-1 (poisson.c:40-43), in FP64."""
+    m = f.mesh
+    nz, nr = m.nz, m.nr
+    a = 1 / m.dz ** 2
+    dr2 = m.dr ** 2
+    e = -2 * (1 / m.dz ** 2 + 1 / dr2)
+    lo = 0 if m.left_bc == abi.DIRICHLET else 1
+    hi = nz - 1 if m.right_bc == abi.DIRICHLET else nz - 2
+    rows = np.arange(lo, hi + 1)
+    up = np.where(rows == nz - 1, rows - 1, rows + 1) if hi == nz - 1 else rows + 1
+    dn = np.where(rows == 0, rows + 1, rows - 1) if lo == 0 else rows - 1
+    cols = nr - 1
+    ir = np.arange(cols, dtype=float)
+    c = np.where(ir > 0, 1 / dr2 * (1 + 0.5 / np.maximum(ir, 1)), 4 / dr2)
+    d = np.where(ir > 0, 1 / dr2 * (1 - 0.5 / np.maximum(ir, 1)), 0.0)
+    dg = np.where(ir > 0, e, e - 2 / dr2)
+    P = psi
+    left = np.concatenate([np.zeros((len(rows), 1)), P[rows, : cols - 1]], axis=1)
+    ap = a * (P[up, :cols] + P[dn, :cols]) + c * P[rows, 1: cols + 1] + d * left + dg * P[rows, :cols]
+    rh = rhs[rows, :cols] if rhs is not None else 0.0
+    upd = (f.flags[rows, :cols] & abi.FL_IS_METAL) == 0
+    res = np.abs(np.where(upd, rh - ap, 0.0)).sum()
+    drive = np.abs(rhs[:nz, :cols]).sum() if rhs is not None else 0.0
+    return res, drive

@@ -9,7 +9,7 @@ import pytest
 
 from spiffe_b200 import abi, gpu, workloads
 from oracle import pyoracle
-from helpers import MODES, beam_from, by_id, fields_from, load, rel_l2
+from helpers import MODES, TE_FIELDS, beam_from, by_id, fields_from, load, rel_l2, te_fdtd_state, te_push_state
 
 pytestmark = pytest.mark.gpu
 
@@ -37,21 +37,50 @@ def test_fdtd_pillbox_bit_exact():
         assert np.array_equal(out[n], fx[n]), n
 
 
-def test_fdtd_te_fields_match_oracle(oracle):
-    fx = load("gun16_geometry")
-    modes = MODES | abi.FL_TE_FIELDS
-    f = fields_from(fx, modes=modes, dt=2e-13)
-    rng = np.random.default_rng(3)
-    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Bz", "Br2", "Bz2", "Jz", "Jr", "Jphi"):
-        f[n] = rng.normal(size=f.shape)
-    ref = f.copy()
+def test_fdtd_te_fields_bit_exact():
+    """TE and TM parts of advance_field_solutions (integrate.c:308-540) for
+    25 steps from random fields and currents on the gun mesh, against the
+    reference's own output (fixture gun16_te)."""
+    fx = load("gun16_te")
+    f = te_fdtd_state(fx)
     g = gpu.GpuInstance(f)
-    for _ in range(25):
+    for _ in range(int(fx["steps"])):
         g.advance_fields()
-        oracle.advance_fields(ref)
     out = g.fields(f)
-    for n in ("Ez", "Er", "Bphi", "Bphi2", "Ephi", "Br", "Br2", "Bz", "Bz2"):
-        assert np.array_equal(out[n], ref[n]), n
+    for n in TE_FIELDS:
+        assert np.array_equal(out[n], fx[n]), n
+
+
+@pytest.mark.parametrize("ordered", [1, 0])
+def test_te_deposit(ordered):
+    """Jz, Jr and Jphi (space_charge.c:34-295) with TE fields on."""
+    fx = load("gun16_te")
+    f, b, sub = te_push_state(fx)
+    g = gpu.GpuInstance(f)
+    g.set_deposit_order(ordered)
+    g.upload_beam(b)
+    g.zero_currents()
+    g.deposit()
+    out = g.fields(f)
+    for n in ("Jz", "Jr", "Jphi"):
+        if ordered:
+            assert np.array_equal(out[n], sub[n]), n
+        else:
+            assert rel_l2(out[n], sub[n]) <= ATOMIC_TOL, n
+
+
+def test_te_push_bit_exact():
+    """A push whose gather reads Ephi, Br2 and Bz2 (advance_particles.c:
+    649-825), against the reference's output."""
+    fx = load("gun16_te")
+    f, b, sub = te_push_state(fx)
+    g = gpu.GpuInstance(f)
+    g.upload_beam(b)
+    g.advance_particles(abi.push_options(compaction=abi.COMPACT_REFERENCE, screen_momentum=abi.SCREEN_REFERENCE))
+    out = g.download_beam(abi.Beam(b.capacity))
+    assert out.np == int(sub["out_np"]) and out.npActive == int(sub["out_npActive"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(out[k], sub["out_" + k]), k
 
 
 @pytest.mark.parametrize("ordered", [1, 0])

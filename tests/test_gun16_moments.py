@@ -10,6 +10,14 @@ beside them, taken half way (step 6,000, the bunch inside the gun): once the
 bunch has left, the FP64 form's correction potential falls to round-off
 (~1e-9 V) while the split form's stays at its FP32 rounding level (~0.3 V),
 so a relative Psi difference at the end measures nothing.
+
+Field tolerance.  The beam-loaded fields are chaotic in the beam: two FP64
+runs whose initial states differ only by the split form's rounding of that
+state (positions to an FP32 offset in a cell, momenta, charge and fields to
+FP32) already differ at step 6,000.  That FP64-vs-FP64 difference is the
+sensitivity floor of this workload; the split form, which rounds every step
+rather than once, must keep Ez, Er and Bphi within
+max(FIELD_TOL, FLOOR_FACTOR x floor) of the FP64 form.
 """
 import numpy as np
 import pytest
@@ -20,10 +28,12 @@ from helpers import rel_l2
 pytestmark = pytest.mark.gpu
 
 MOMENT_TOL = 5e-3
+FIELD_TOL = 1e-5
+FLOOR_FACTOR = 4.0
 STEPS = 12000  # the bunch needs about 9,000 steps of 17.7 um to reach the exit
 
 
-def run(precision, cfg, f, b):
+def run(precision, cfg, f, b, steps=STEPS):
     g = gpu.GpuInstance(f, capacity=b.capacity, precision=precision)
     g.upload_beam(b)
     g.add_screen(cfg.screen_z(), 1, capacity=b.capacity)
@@ -32,11 +42,21 @@ def run(precision, cfg, f, b):
     g.run_begin()
     g.run_steps(STEPS // 2)
     mid = g.fields(f)
-    g.run_steps(STEPS - STEPS // 2)
+    if steps > STEPS // 2:
+        g.run_steps(steps - STEPS // 2)
     rec = g.screen(0, capacity=b.capacity).records()
     np_end, _ = g.counts()
     g.close()
     return rec, mid, np_end
+
+
+def rounded_by_split_form(f, b):
+    """The initial state as the split form holds it, back in FP64."""
+    g = gpu.GpuInstance(f, capacity=b.capacity, precision=gpu.PRECISION_SPLIT32)
+    g.upload_beam(b)
+    fr, br = g.fields(f), g.download_beam(abi.Beam(b.capacity))
+    g.close()
+    return fr, br
 
 
 def test_gun16_exit_moments_split_vs_f64():
@@ -44,15 +64,21 @@ def test_gun16_exit_moments_split_vs_f64():
     f, b = cfg.state()
     r64, o64, n64 = run(gpu.PRECISION_F64, cfg, f, b)
     r32, o32, n32 = run(gpu.PRECISION_SPLIT32, cfg, f, b)
+    fr, br = rounded_by_split_form(f, b)
+    _, o64r, _ = run(gpu.PRECISION_F64, cfg, fr, br, steps=STEPS // 2)
     m64, m32 = moments.exit_moments(r64), moments.exit_moments(r32)
     err = moments.relative_errors(m32, m64)
     fields = {n: rel_l2(o32[n], o64[n]) for n in ("Ez", "Er", "Bphi", "Psi")}
+    floor = {n: rel_l2(o64r[n], o64[n]) for n in ("Ez", "Er", "Bphi", "Psi")}
     print("gun16 exit moments FP64 ", m64)
     print("gun16 exit moments split", m32)
     print("gun16 relative errors   ", err)
     print("gun16 field rel L2 (mid)", fields)
+    print("gun16 FP64 floor (mid)  ", floor)
     print("gun16 particles left    ", n64, n32)
     assert m64["count"] > 0.5 * cfg.n_macro, "the bunch has not crossed the exit screen"
     assert abs(m32["count"] - m64["count"]) <= max(2, MOMENT_TOL * m64["count"])
     for k, v in err.items():
         assert v <= MOMENT_TOL, (k, v)
+    for n in ("Ez", "Er", "Bphi"):
+        assert fields[n] <= max(FIELD_TOL, FLOOR_FACTOR * floor[n]), (n, fields[n], floor[n])

@@ -3,7 +3,7 @@ import numpy as np
 
 from spiffe_b200 import abi, workloads
 from oracle import pyoracle
-from helpers import MODES, beam_from, fields_from, load
+from helpers import MODES, TE_FIELDS, beam_from, fields_from, load, te_fdtd_state, te_push_state
 
 
 def test_fdtd_pillbox_400_steps(oracle):
@@ -78,3 +78,30 @@ def test_loop_with_emission(oracle):
     rec = sc.records()
     for c in abi.SCREEN_COLUMNS:
         assert np.array_equal(rec[c], fx["screen_" + c]), c
+
+
+def test_fdtd_te_fields_25_steps(oracle):
+    """The TE part of advance_field_solutions (integrate.c:434-540) with the
+    TM part, from random fields and currents on the gun mesh."""
+    fx = load("gun16_te")
+    f = te_fdtd_state(fx)
+    for _ in range(int(fx["steps"])):
+        oracle.advance_fields(f)
+    for n in TE_FIELDS:
+        assert np.array_equal(f[n], fx[n]), n
+
+
+def test_te_deposit_and_push(oracle):
+    """Jphi deposition (space_charge.c:218-295) and the gather of Ephi, Br2
+    and Bz2 (advance_particles.c:649-825) in a push with TE fields."""
+    fx = load("gun16_te")
+    f, b, sub = te_push_state(fx)
+    oracle.zero_currents(f)
+    oracle.deposit(f, b)
+    for n in ("Jz", "Jr", "Jphi"):
+        assert np.array_equal(f[n], sub[n]), n
+    oracle.advance_particles(f, b, [], abi.push_options(compaction=abi.COMPACT_REFERENCE,
+                                                        screen_momentum=abi.SCREEN_REFERENCE))
+    assert b.np == int(sub["out_np"]) and b.npActive == int(sub["out_npActive"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k], sub["out_" + k]), k
