@@ -100,6 +100,13 @@ int spiffe_gpu_solve_poisson_cyl_noalloc(const spiffe_mesh *mesh, double *psi, c
  * tests included; `report` may be NULL) */
 int spiffe_gpu_add_poisson_correction(spiffe_gpu_instance *inst, int32_t space_charge, const spiffe_poisson_options *opt,
                                       spiffe_poisson_report *report);
+/* No counterpart in the reference, which prints these values only when
+ * verbose.  The instance's log of Poisson corrections that ran (one row each,
+ * kept on the device so a run of steps needs no host synchronisation): rows
+ * [k*4 + 0..3] = time step, iterations (half-sweeps or V-cycles, -1 at the
+ * limit), final sum|residual|, sum|rhs| of the solve.  Copies at most
+ * max_rows of the first 65536 rows; *n_total receives how many ran. */
+int spiffe_gpu_poisson_log(spiffe_gpu_instance *inst, int64_t max_rows, double *rows, int64_t *n_total);
 /* compute_imposed_Efield, poisson_correction.c:456 */
 int spiffe_gpu_compute_imposed_efield(spiffe_gpu_instance *inst, const spiffe_poisson_options *opt, int32_t initialize);
 
@@ -108,6 +115,13 @@ int spiffe_gpu_add_screen(spiffe_gpu_instance *inst, double z_position, int32_t 
 int spiffe_gpu_screen_count(spiffe_gpu_instance *inst, int32_t screen, int64_t *nb);
 int spiffe_gpu_download_screen(spiffe_gpu_instance *inst, int32_t screen, spiffe_screen_set *host);
 int spiffe_gpu_clear_screens(spiffe_gpu_instance *inst);
+/* No counterpart in the reference, which leaves moments to external SDDS
+ * tools.  The exit-plane moments of a screen's records, reduced on the device
+ * in FP64 with weights |q|: out[0] records, [1] charge sum q, [2] mean kinetic
+ * energy m c^2 <gamma-1> (eV), [3] its rms spread (eV), [4] rms bunch length
+ * sigma_t <beta_z> c (m), [5] normalized rms emittance of the x projection,
+ * <x^2> = <r^2>/2, <px^2> = (<pr^2> + <pphi^2>)/2, <x px> = <r pr>/2 (m). */
+int spiffe_gpu_screen_moments(spiffe_gpu_instance *inst, int32_t screen, double *out);
 
 /* define_cathode (cathode.c:21) and define_antenna (antenna.c:18) for the
  * device integration loop; waveform times must already include time_offset. */

@@ -548,6 +548,7 @@ __global__ void __launch_bounds__(MG_NT) k_mg32(Mg32Args a, DevCounts *cnt)
     if (a.st) {
       a.st->iterations = result;
       a.st->residual = total;
+      a.st->driving = drive;
     }
     cnt->mg_cycles += cycles;
     cnt->sor_solves += 1;

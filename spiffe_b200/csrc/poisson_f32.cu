@@ -724,6 +724,8 @@ __global__ void __launch_bounds__(SOR_NT) k_sor32(DevMesh m, Sor32Args s, DevCou
     }
     ok_sh = ok;
     thr_sh = s.accuracy * t;
+    if (b == 0 && s.st)
+      s.st->driving = t;
     base_sh = t2;
     quantum_sh = fmax(fmax(base_sh, thr_sh), 1e-280) / 1073741824.0;
     rebase_sh = 0;
@@ -1305,7 +1307,7 @@ extern "C" int s32_poisson_report(Poisson32Work *w, spiffe_poisson_report *rep, 
   rep->Qerror = st.Qerror;
   rep->Qsurface = st.Qsurface;
   rep->residual = st.residual;
-  rep->driving = 0;
+  rep->driving = st.driving;
   return (int)e;
 }
 

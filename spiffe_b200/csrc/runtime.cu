@@ -177,6 +177,11 @@ struct spiffe_gpu_instance {
   spiffe_poisson_options pc{};
   long long pc_start_step = -1;
   double last_imposed_factor = -1;
+  // one row per Poisson correction: time step, iterations, residual, driving
+  double *d_pclog = nullptr;
+  double *d_status = nullptr; // status-row reduction scratch
+  double *d_moments = nullptr; // exit-moment reduction scratch
+  unsigned long long *d_pclog_n = nullptr;
   std::vector<HostCathode> cathodes;
   uint64_t rng_key = 0, rng_counter = 0;
   std::vector<HostAntenna> antennas;
@@ -892,7 +897,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
-               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch};
+               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1166,6 +1171,52 @@ extern "C" int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *in, int32_t tar
   return 0;
 }
 
+constexpr long long PCLOG_ROWS = 1 << 16;
+
+// appends this correction's row to the instance's log (rows past the
+// capacity are counted, not stored)
+__global__ void k_pc_log(const PcState *st, const double *driving, long long step, double *log,
+                         unsigned long long *n)
+{
+  if (!st->do_solve)
+    return;
+  const unsigned long long k = (*n)++;
+  if (k < (unsigned long long)PCLOG_ROWS) {
+    log[4 * k] = (double)step;
+    log[4 * k + 1] = (double)st->iterations;
+    log[4 * k + 2] = st->residual;
+    log[4 * k + 3] = *driving;
+  }
+}
+
+static int pc_log(spiffe_gpu_instance *in, const PcState *st, const double *driving)
+{
+  if (!in->d_pclog) {
+    CUDA_TRY(cudaMalloc(&in->d_pclog, sizeof(double) * 4 * PCLOG_ROWS + sizeof(unsigned long long)));
+    in->d_pclog_n = (unsigned long long *)(in->d_pclog + 4 * PCLOG_ROWS);
+    CUDA_TRY(cudaMemsetAsync(in->d_pclog_n, 0, sizeof(unsigned long long), in->stream));
+  }
+  k_pc_log<<<1, 1, 0, in->stream>>>(st, driving, in->mesh.time_step, in->d_pclog, in->d_pclog_n);
+  spiffe_note_launches(1);
+  return 0;
+}
+
+extern "C" int spiffe_gpu_poisson_log(spiffe_gpu_instance *in, int64_t max_rows, double *rows, int64_t *n_total)
+{
+  if (!in || (max_rows > 0 && !rows) || !n_total)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  unsigned long long n = 0;
+  if (in->d_pclog) {
+    CUDA_TRY(cudaMemcpyAsync(&n, in->d_pclog_n, sizeof(n), cudaMemcpyDeviceToHost, in->stream));
+    CUDA_TRY(cudaStreamSynchronize(in->stream));
+    const long long k = std::min<long long>(std::min<long long>((long long)n, PCLOG_ROWS), max_rows);
+    if (k > 0)
+      CUDA_TRY(cudaMemcpy(rows, in->d_pclog, sizeof(double) * 4 * (size_t)k, cudaMemcpyDeviceToHost));
+  }
+  *n_total = (int64_t)n;
+  return 0;
+}
+
 static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const spiffe_poisson_options *o)
 {
   // poisson_correction.c:84-119
@@ -1186,6 +1237,7 @@ static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const s
     const int rc = s32_poisson_correction(&in->dm, &S.f, &S.b, in->cnt, in->np_upper, &h, &S.sc, &S.pcw, in->stream);
     if (rc)
       return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+    RC_TRY(pc_log(in, S.pcw.st, &S.pcw.st->driving));
     return 1;
   }
   RC_TRY(ensure_poisson(in));
@@ -1193,6 +1245,7 @@ static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const s
   const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  RC_TRY(pc_log(in, in->pcw.st, in->pcw.scalars + 4));
   return 1;
 }
 
@@ -1310,6 +1363,22 @@ extern "C" int spiffe_gpu_screen_count(spiffe_gpu_instance *in, int32_t is, int6
   RC_TRY(read_counts(in));
   const long long n = in->h_cnt->screen_nb[is];
   *nb = n < in->screens.s[is].capacity ? n : in->screens.s[is].capacity;
+  return 0;
+}
+
+extern "C" int spiffe_screen_moments_device(const DevScreen *scr, const long long *nb, double *scratch,
+                                            double *host_out, cudaStream_t s);
+
+extern "C" int spiffe_gpu_screen_moments(spiffe_gpu_instance *in, int32_t is, double *out)
+{
+  if (!in || !out || is < 0 || is >= in->screens.n)
+    return fail(SPIFFE_ERR_INVALID, "bad screen index");
+  if (!in->d_moments)
+    CUDA_TRY(cudaMalloc(&in->d_moments, sizeof(double) * (148 * 9 + 64)));
+  const int rc = spiffe_screen_moments_device(&in->screens.s[is], &in->cnt->screen_nb[is], in->d_moments, out,
+                                              in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "screen moments failed: %s", cudaGetErrorString((cudaError_t)rc));
   return 0;
 }
 
@@ -1858,190 +1927,56 @@ extern "C" int spiffe_gpu_translate_problem(spiffe_gpu_instance *in, int32_t *tr
 
 // computeMoments as the checker's SDDS stand-in defines it: mean, rms about
 // zero, standard deviation with n-1 (SDDS's mdbmth, absent here)
-static void moments(const double *x, int64_t n, double &ave, double &rms, double &sd)
-{
-  double s = 0, s2 = 0, d = 0;
-  for (int64_t i = 0; i < n; i++) {
-    s += x[i];
-    s2 += x[i] * x[i];
-  }
-  const double m = s / n;
-  for (int64_t i = 0; i < n; i++)
-    d += (x[i] - m) * (x[i] - m);
-  ave = m;
-  rms = std::sqrt(s2 / n);
-  sd = n > 1 ? std::sqrt(d / (n - 1)) : 0;
-}
-
-static void min_max(const double *x, int64_t n, double &lo, double &hi)
-{
-  lo = DBL_MAX;
-  hi = -DBL_MAX;
-  for (int64_t i = 0; i < n; i++) {
-    if (x[i] < lo)
-      lo = x[i];
-    if (x[i] > hi)
-      hi = x[i];
-  }
-}
+extern "C" int spiffe_status_device(const DevMesh *m, bool split, const void *fields, const int16_t *flags,
+                                    int fpitch, const void *beam, const DevCounts *cnt, double stiffness,
+                                    double *scratch, double *host_out, cudaStream_t s);
 
 // do_status_printouts, status_pr.c:18-356; kinetic_energy and field_energy,
-// :358-452
+// :358-452.  The sums run on the device in the reference's order (reduce.cu);
+// only the row's values come back.
 extern "C" int spiffe_gpu_status_report(spiffe_gpu_instance *in, spiffe_status_row *st)
 {
   if (!in || !st)
     return fail(SPIFFE_ERR_INVALID, "null argument");
   const spiffe_mesh &m = in->mesh;
-  const int nz = m.nz, nr = m.nr, P = nr + 1;
-  const size_t nodes = (size_t)(nz + 1) * P;
   memset(st, 0, sizeof(*st));
   st->t = m.time;
   st->JCathode = in->cathodes.empty() ? 0 : in->cathodes[0].current_density;
-  // the beam
+  if (!in->d_status) {
+    CUDA_TRY(cudaMalloc(&in->d_status, sizeof(double) * (10 * (size_t)m.nr + 64)));
+  }
+  CUDA_TRY(cudaMemsetAsync(in->d_status, 0, sizeof(double) * (10 * (size_t)m.nr + 64), in->stream));
+  double v[4 + 23];
+  int rc;
+  if (in->s32)
+    rc = spiffe_status_device(&in->dm, true, &in->s32->f, in->d_flags, in->dm.pitch, &in->s32->b, in->cnt,
+                              in->stiffness, in->d_status, v, in->stream);
+  else
+    rc = spiffe_status_device(&in->dm, false, &in->f, in->d_flags, m.nr + 1, &in->b, in->cnt, in->stiffness,
+                              in->d_status, v, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "status reductions failed: %s", cudaGetErrorString((cudaError_t)rc));
   RC_TRY(read_counts(in));
-  const int64_t np = in->h_cnt->np;
-  std::vector<double> bd[9];
-  for (auto &v : bd)
-    v.resize((size_t)np + 1);
-  std::vector<int32_t> id((size_t)np + 1);
-  std::vector<int16_t> gen((size_t)np + 1);
-  std::vector<uint64_t> status((size_t)np + 1);
-  std::vector<double> extra[7];
-  for (auto &v : extra)
-    v.resize((size_t)np + 1);
-  spiffe_beam_set b{};
-  b.capacity = np + 1;
-  b.z = bd[0].data(); b.r = bd[1].data(); b.pz = bd[2].data(); b.pr = bd[3].data(); b.r_pphi = bd[4].data();
-  b.vz = bd[5].data(); b.vr = bd[6].data(); b.vphi = bd[7].data(); b.Q = bd[8].data();
-  b.r0 = extra[0].data(); b.z0 = extra[1].data(); b.t0 = extra[2].data(); b.rmin = extra[3].data();
-  b.rmax = extra[4].data(); b.zmin = extra[5].data(); b.zmax = extra[6].data();
-  b.particleID = id.data();
-  b.generation = gen.data();
-  b.status = status.data();
-  RC_TRY(spiffe_gpu_download_beam(in, &b));
-  st->Particles = b.np;
-  st->ActiveParticles = b.npActive;
-  double KE = 0;
-  if (b.np) {
-    double Q = 0;
-    int64_t sec = 0;
-    for (int64_t ip = 0; ip < b.np; ip++)
-      if (b.status[ip] & SPIFFE_PART_ACTIVE) {
-        Q += b.Q[ip];
-        if (b.generation[ip] > 0)
-          sec++;
-      }
-    st->Charge = Q;
-    st->SecondaryParticles = sec;
-    moments(b.z, b.np, st->zAve, st->zRMS, st->zStDev);
-    min_max(b.z, b.np, st->zMin, st->zMax);
-    moments(b.r, b.np, st->rAve, st->rRMS, st->rStDev);
-    min_max(b.r, b.np, st->rMin, st->rMax);
-    moments(b.pz, b.np, st->pzAve, st->pzRMS, st->pzStDev);
-    min_max(b.pz, b.np, st->pzMin, st->pzMax);
-    moments(b.pr, b.np, st->prAve, st->prRMS, st->prStDev);
-    min_max(b.pr, b.np, st->prMin, st->prMax);
-    double sum = 0;
-    for (int64_t ip = 0; ip < b.np; ip++) {
-      const double a = b.r[ip] ? b.r_pphi[ip] / b.r[ip] : 0;
-      sum += std::sqrt(1 + b.pz[ip] * b.pz[ip] + b.pr[ip] * b.pr[ip] + a * a);
-    }
-    KE = in->stiffness * SPIFFE_ME_MKS * (SPIFFE_C_MKS * SPIFFE_C_MKS) * (sum - b.np);
+  const double *b = v + 4;
+  st->Particles = in->h_cnt->np;
+  st->ActiveParticles = in->h_cnt->npActive;
+  if (st->Particles) {
+    st->Charge = b[0];
+    st->SecondaryParticles = (int64_t)b[1];
+    st->KineticEnergy = b[2];
+    st->zAve = b[3], st->zRMS = b[4], st->zStDev = b[5];
+    st->rAve = b[6], st->rRMS = b[7], st->rStDev = b[8];
+    st->pzAve = b[9], st->pzRMS = b[10], st->pzStDev = b[11];
+    st->prAve = b[12], st->prRMS = b[13], st->prStDev = b[14];
+    st->zMin = b[15], st->zMax = b[16], st->rMin = b[17], st->rMax = b[18];
+    st->pzMin = b[19], st->pzMax = b[20], st->prMin = b[21], st->prMax = b[22];
   }
-  st->KineticEnergy = KE;
-  // the fields
-  std::vector<double> F[8];
-  const bool tm = m.modes & SPIFFE_FL_TM_FIELDS, te = m.modes & SPIFFE_FL_TE_FIELDS;
-  spiffe_field_set h{};
-  double **want[8] = {&h.Ez, &h.Er, &h.Bphi2, &h.EzImposed, &h.ErImposed, &h.Ephi, &h.Br2, &h.Bz2};
-  for (int k = 0; k < 8; k++)
-    if ((k < 5 && tm) || (k >= 5 && te)) {
-      F[k].resize(nodes);
-      *want[k] = F[k].data();
-    }
-  RC_TRY(spiffe_gpu_download_fields(in, &h));
-  const int16_t *fl = in->h_flags.data();
-  auto at = [&](const std::vector<double> &a, int iz, int ir) { return a[(size_t)iz * P + ir]; };
-  auto flag = [&](int iz, int ir) { return fl[(size_t)iz * P + ir]; };
-  const double dr2 = m.dr * m.dr;
-  std::vector<double> area_c((size_t)nr + 1), area_o((size_t)nr + 1); // calculate_areas, integrate.c:689-701
-  for (int ir = 0; ir <= nr; ir++)
-    area_c[(size_t)ir] = ir ? SPIFFE_PIx2 * ir * dr2 : SPIFFE_PI * dr2 / 4;
-  area_o[0] = 0;
-  for (int ir = 1; ir <= nr; ir++)
-    area_o[(size_t)ir] = SPIFFE_PI * (2 * ir - 1) * dr2;
-  double E0 = 0, E1 = 0;
-  if (tm) {
-    double lo = DBL_MAX, hi = -DBL_MAX;
-    for (int iz = 1; iz < nz; iz++)
-      for (int ir = 0; ir < nr; ir++) {
-        const double v = at(F[0], iz, ir) + at(F[3], iz, ir);
-        if (v > hi)
-          hi = v;
-        if (v < lo)
-          lo = v;
-      }
-    st->EzAbsMax = std::fabs(lo) > std::fabs(hi) ? std::fabs(lo) : std::fabs(hi);
-    lo = DBL_MAX;
-    hi = -DBL_MAX;
-    for (int iz = 0; iz < nz; iz++)
-      for (int ir = 0; ir < nr; ir++) {
-        const double v = at(F[1], iz, ir) + at(F[4], iz, ir);
-        if (v > hi)
-          hi = v;
-        if (v < lo)
-          lo = v;
-      }
-    st->ErAbsMax = std::fabs(lo) > std::fabs(hi) ? std::fabs(lo) : std::fabs(hi);
-    for (int ir = 0; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 1; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_EZ_ZERO))
-          sum += at(F[0], iz, ir) * at(F[0], iz, ir);
-      E0 += sum * area_c[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
-    }
-    for (int ir = 1; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 0; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_ER_ZERO))
-          sum += at(F[1], iz, ir) * at(F[1], iz, ir);
-      E0 += sum * area_o[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
-    }
-    for (int ir = 1; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 1; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_BPHI_ZERO))
-          sum += at(F[2], iz, ir) * at(F[2], iz, ir);
-      E1 += sum * area_o[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
-    }
-  }
-  if (te) {
-    for (int ir = 0; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 0; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_EPHI_ZERO))
-          sum += at(F[5], iz, ir) * at(F[5], iz, ir);
-      E0 += sum * area_c[(size_t)ir] * m.dz * SPIFFE_EPSILON_O / 2;
-    }
-    for (int ir = 0; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 1; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_BR_ZERO))
-          sum += at(F[6], iz, ir) * at(F[6], iz, ir);
-      E1 += sum * area_c[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
-    }
-    for (int ir = 1; ir < nr; ir++) {
-      double sum = 0;
-      for (int iz = 0; iz < nz; iz++)
-        if (!(flag(iz, ir) & SPIFFE_FL_BZ_ZERO))
-          sum += at(F[7], iz, ir) * at(F[7], iz, ir);
-      E1 += sum * area_o[(size_t)ir] * m.dz / (2 * SPIFFE_MU_O);
-    }
-  }
-  st->ElectricEnergy = E0;
-  st->MagneticEnergy = E1;
-  st->FieldEnergy = E0 + E1;
-  st->TotalEnergy = KE + st->FieldEnergy;
+  st->ElectricEnergy = v[0];
+  st->MagneticEnergy = v[1];
+  st->EzAbsMax = v[2];
+  st->ErAbsMax = v[3];
+  st->FieldEnergy = v[0] + v[1];
+  st->TotalEnergy = st->KineticEnergy + st->FieldEnergy;
   st->EzOOEMin = in->h_cnt->oa_min;
   st->EzOOEMax = in->h_cnt->oa_max;
   return 0;

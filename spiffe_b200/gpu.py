@@ -82,6 +82,8 @@ def load():
         "spiffe_gpu_work_counters": ([H, P(C.c_int64)], C.c_int),
         "spiffe_gpu_set_sort_interval": ([H, C.c_int64], C.c_int),
         "spiffe_gpu_set_poisson_solver": ([H, C.c_int32], C.c_int),
+        "spiffe_gpu_poisson_log": ([H, C.c_int64, P(C.c_double), P(C.c_int64)], C.c_int),
+        "spiffe_gpu_screen_moments": ([H, C.c_int32, P(C.c_double)], C.c_int),
         "spiffe_gpu_batch_run": ([P(H), C.c_int32, P(C.c_int64), C.c_int32, C.c_int64, P(C.c_double)], C.c_int),
         "spiffe_gpu_set_test_beam": ([H, P(abi.TestBeamOptions)], C.c_int),
         "spiffe_gpu_add_on_axis_field": ([H, P(C.c_double), P(C.c_double), C.c_int64, C.c_double, C.c_double,
@@ -329,6 +331,22 @@ class GpuInstance:
         _check(self.lib.spiffe_gpu_work_counters(self.h, out))
         return dict(particle_steps=out[0], sor_halfsweeps=out[1], sor_solves=out[2], fdtd_steps=out[3],
                     mg_cycles=out[4])
+
+    def screen_moments(self, screen=0):
+        """Exit-plane moments of a screen's records, reduced on the device
+        (the keys of spiffe_b200.moments.exit_moments)."""
+        out = (C.c_double * 6)()
+        _check(self.lib.spiffe_gpu_screen_moments(self.h, int(screen), out))
+        return {"count": int(out[0]), "charge": out[1], "mean_ke_ev": out[2], "rms_energy_ev": out[3],
+                "bunch_length_m": out[4], "emittance_m": out[5]}
+
+    def poisson_log(self, max_rows=1 << 16):
+        """The Poisson corrections run so far: an (n, 4) array of time step,
+        iterations, final sum|residual| and sum|rhs|."""
+        rows = np.zeros((max_rows, 4))
+        n = C.c_int64()
+        _check(self.lib.spiffe_gpu_poisson_log(self.h, max_rows, rows.ctypes.data_as(P(C.c_double)), C.byref(n)))
+        return rows[: min(n.value, max_rows)].copy()
 
     def set_poisson_solver(self, solver):
         """POISSON_MULTIGRID (split form default) or POISSON_SOR."""
