@@ -115,6 +115,15 @@ int spiffe_gpu_add_screen(spiffe_gpu_instance *inst, double z_position, int32_t 
 int spiffe_gpu_screen_count(spiffe_gpu_instance *inst, int32_t screen, int64_t *nb);
 int spiffe_gpu_download_screen(spiffe_gpu_instance *inst, int32_t screen, spiffe_screen_set *host);
 int spiffe_gpu_clear_screens(spiffe_gpu_instance *inst);
+/* The lost-particle file's rows (integrate's lost_particles, the loss
+ * epilogue of advance_particles.c:437-487 with findLossCoordinates,
+ * secondaryEmission.c:239): capacity > 0 makes every push record up to
+ * `capacity` lost particles on the device between downloads; 0 stops it. */
+int spiffe_gpu_set_lost_log(spiffe_gpu_instance *inst, int64_t capacity);
+/* The rows recorded since the last download, in the reference's order (step,
+ * then particle index), and empties the log; an error when more particles
+ * were lost than the log or `host` holds. */
+int spiffe_gpu_download_lost(spiffe_gpu_instance *inst, spiffe_lost_set *host);
 /* No counterpart in the reference, which leaves moments to external SDDS
  * tools.  The exit-plane moments of a screen's records, reduced on the device
  * in FP64 with weights |q|: out[0] records, [1] charge sum q, [2] mean kinetic

@@ -99,6 +99,19 @@ typedef struct spiffe_screen_set {
   int32_t *particleID;
 } spiffe_screen_set;
 
+/* Rows of the lost-particle file (integrate's lost_particles;
+ * setUpLostParticleFile, advance_particles.c:577-603, and the rows of the
+ * loss epilogue, :437-487): the time, where the path left the open region
+ * (findLossCoordinates, secondaryEmission.c:239), the momenta, birth
+ * position, charge, generation and id, and the step of each row. */
+typedef struct spiffe_lost_set {
+  int64_t nb, capacity;
+  double *t, *rLost, *zLost, *pz, *pr, *z0, *r0, *q;
+  int16_t *generation;
+  int32_t *particleID;
+  int64_t *step; /* may be NULL */
+} spiffe_lost_set;
+
 /* Poisson solver of the split-precision form (spiffe_gpu_set_poisson_solver) */
 #define SPIFFE_POISSON_SOR 0       /* the reference's red-black SOR and stop rule (poisson.c:17-130) */
 #define SPIFFE_POISSON_MULTIGRID 1 /* FP32 multigrid V-cycles in FP64 refinement, the same stop rule */

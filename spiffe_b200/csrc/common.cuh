@@ -191,6 +191,108 @@ struct DevCounts {
   unsigned int pad;
 };
 
+// One particle lost in a push, with what the loss epilogue of
+// advance_particles (advance_particles.c:437-487) computes from it: the
+// point and direction where its path left the mesh's open region
+// (findLossCoordinates, below), its momentum magnitude, the pushed momenta,
+// the birth position, the charge, id and generation, and the particle's
+// index and the step, which order the records as the reference writes them.
+struct LostRecord {
+  double t, zLost, rLost, p, pz, pr, r0, z0, q;
+  long long ip, step;
+  int32_t id;
+  int16_t gen, code; // code -1: a split-form row whose values are still to be formed (cell0, fz0, fr0, neg)
+  int32_t cell0, neg;
+  float fz0, fr0;
+};
+
+// Where a push appends its lost particles (rec null: not recorded).
+struct LostLog {
+  LostRecord *rec;
+  unsigned long long *n;
+  long long cap, step;
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void lost_append(const LostLog &L, const LostRecord &r)
+{
+  const unsigned long long k = atomicAdd(L.n, 1ull);
+  if ((long long)k < L.cap)
+    L.rec[k] = r;
+}
+#endif
+
+// findLossCoordinates (secondaryEmission.c:239-352): the point where the
+// straight path from (z0, r0) to (z1, r1) leaves its cell through the face
+// it crossed, and that face's direction code (1 left, 2 right, 3 up, 4
+// down; 1 also when the particle did not move).  flags at pitch fpitch.
+#define SPIFFE_GOING_LEFT 1
+#define SPIFFE_GOING_RIGHT 2
+#define SPIFFE_GOING_UP 3
+#define SPIFFE_GOING_DOWN 4
+__host__ __device__ inline int find_loss_coordinates(double zmin, double zmax, double dz, double dr, long nr,
+                                                     const int16_t *flags, long fpitch, double z0, double r0,
+                                                     double z1, double r1, double *zr, double *rr)
+{
+  const long iz0 = (long)((z0 - zmin) / dz), ir0 = (long)(r0 / dr);
+  const long iz1 = z1 < zmin ? -1 : (long)((z1 - zmin) / dz);
+  const long ir1 = r1 < 0 ? -1 : (long)(r1 / dr);
+  auto metal = [&](long iz, long ir) { return (flags[iz * fpitch + ir] & SPIFFE_FL_IS_METAL) != 0; };
+  int code = 0;
+  if (r0 == r1 && z0 == z1) {
+    *zr = z0;
+    *rr = r0;
+    return 1;
+  }
+  if (ir0 == ir1)
+    code = iz0 > iz1 ? SPIFFE_GOING_LEFT : SPIFFE_GOING_RIGHT;
+  else if (iz0 == iz1)
+    code = ir0 > ir1 ? SPIFFE_GOING_DOWN : SPIFFE_GOING_UP;
+  else if (z1 < z0) {
+    if (z1 < 0)
+      code = SPIFFE_GOING_LEFT;
+    else if (ir0 != ir1) {
+      if (ir1 >= 0 && ir1 < nr && metal(iz0, ir1))
+        code = SPIFFE_GOING_LEFT;
+      else if (ir1 < 0 && metal(iz0, -ir1))
+        code = SPIFFE_GOING_LEFT;
+    } else if (ir0 == ir1 && (ir0 < nr - 1 && metal(iz0, ir0 + 1)))
+      code = SPIFFE_GOING_LEFT;
+    else
+      code = r1 < r0 ? SPIFFE_GOING_DOWN : SPIFFE_GOING_UP;
+  } else if (z1 > z0) {
+    if (z1 > zmax)
+      code = SPIFFE_GOING_RIGHT;
+    else if (ir0 != ir1) {
+      if (ir1 >= 0 && ir1 < nr && metal(iz1, ir1))
+        code = SPIFFE_GOING_RIGHT;
+      else if (ir1 < 0 && metal(iz1, -ir1))
+        code = SPIFFE_GOING_RIGHT;
+    } else if (ir0 == ir1 && (ir0 < nr - 1 && metal(iz1, ir0 + 1)))
+      code = SPIFFE_GOING_RIGHT;
+    else
+      code = r1 < r0 ? SPIFFE_GOING_DOWN : SPIFFE_GOING_UP;
+  } else
+    code = r1 < r0 ? SPIFFE_GOING_DOWN : SPIFFE_GOING_UP;
+  double zm, rm;
+  if (code == SPIFFE_GOING_LEFT) {
+    zm = ((long)((z0 - zmin) / dz)) * dz + zmin + dz * 1e-12;
+    rm = (r1 - r0) / (z1 - z0) * (zm - z0) + r0;
+  } else if (code == SPIFFE_GOING_RIGHT) {
+    zm = ((long)((z0 - zmin) / dz)) * dz + zmin + dz * (1 - 1e-12);
+    rm = (r1 - r0) / (z1 - z0) * (zm - z0) + r0;
+  } else if (code == SPIFFE_GOING_DOWN) {
+    rm = ((long)(r0 / dr)) * dr + dr * 1e-12;
+    zm = (z1 - z0) / (r1 - r0) * (rm - r0) + z0;
+  } else {
+    rm = ((long)(r0 / dr)) * dr + dr * (1 - 1e-12);
+    zm = (z1 - z0) / (r1 - r0) * (rm - r0) + z0;
+  }
+  *zr = zm;
+  *rr = fabs(rm);
+  return code;
+}
+
 #define SPIFFE_DEV_ERR_CAPACITY 1u
 #define SPIFFE_DEV_ERR_SCREEN 2u
 #define SPIFFE_DEV_ERR_BARRIER 4u

@@ -31,6 +31,7 @@ struct PushHostParams {
   double time, z_forces_start, QoMC, stiffness;
   double tb_epm, tb_z_force, tb_r_force, tb_z_decel, tb_r_decel;
   int screen_momentum, compaction;
+  LostLog lost;
 };
 extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const PushHostParams *hp,
                              const DevScreens *scr, DevCounts *cnt, long long np_bound, Particles64Work *w,

@@ -653,6 +653,18 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
       atomicMin(&cnt->first_lost, (long long)ip);
       if (lost_list)
         lost_list[slot] = (int32_t)ip;
+      if (p.lost.rec) { // the cell before the drift; k_lost32 forms the row after the push
+        LostRecord rec{};
+        rec.t = p.time;
+        rec.ip = ip;
+        rec.step = p.lost.step;
+        rec.code = -1;
+        rec.cell0 = s32_cell(iz0, ir0);
+        rec.fz0 = fz0;
+        rec.fr0 = fr0;
+        rec.neg = r_negative;
+        lost_append(p.lost, rec);
+      }
     }
     b.status[ip] = status;
     if (iz < -32767 || iz > 32767)
@@ -713,6 +725,41 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
   }
   if (DEP)
     deposit_particle<DEF>(m, f, dep_on, d_iz, d_fz, d_ir, d_fr, d_bz, d_br, d_bphi, d_qs);
+}
+
+// The loss epilogue of advance_particles (:437-487) for the rows this push
+// recorded, before the compaction moves the lost particles: the momentum,
+// the loss point (findLossCoordinates) from the positions before and after
+// the drift, in FP64.
+__global__ void k_lost32(DevMesh m, const int16_t *fl, DevBeam32 b, LostLog L)
+{
+  const unsigned long long n = *L.n;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L.cap || (unsigned long long)k >= n)
+    return;
+  LostRecord &r = L.rec[k];
+  if (r.code != -1)
+    return;
+  const long ip = (long)r.ip;
+  const int32_t c = b.cell[ip];
+  const double rd = ((double)s32_ir(c) + (double)b.fr[ip]) * m.dr, pz = b.pz[ip], pr = b.pr[ip];
+  const double rpp = b.rpphi[ip];
+  double pm = pz * pz + pr * pr;
+  if (rd)
+    pm += (rpp / rd) * (rpp / rd);
+  r.p = sqrt(pm);
+  r.pz = pz;
+  r.pr = pr;
+  r.r0 = b.r0[ip];
+  r.z0 = b.z0[ip];
+  r.q = b.Q[ip];
+  r.id = b.particleID[ip];
+  r.gen = b.generation[ip];
+  const double z0 = m.zmin + ((double)s32_iz(r.cell0) + (double)r.fz0) * m.dz;
+  const double r0 = ((double)s32_ir(r.cell0) + (double)r.fr0) * m.dr;
+  const double z1 = m.zmin + ((double)s32_iz(c) + (double)b.fz[ip]) * m.dz;
+  r.code = (int16_t)find_loss_coordinates(m.zmin, m.zmax, m.dz, m.dr, m.nr, fl, m.pitch, z0, r0, z1,
+                                          r.neg ? -rd : rd, &r.zLost, &r.rLost);
 }
 
 // ---- compaction
@@ -1196,6 +1243,10 @@ extern "C" int s32_push(const DevMesh *m, const DevFields32 *f, const DevBeam32 
     else
       k_push32<false, false><<<nb, T, 0, s>>>(*m, *f, *b, *p, *scr, cnt, ll, *sc);
     spiffe_note_launches(1);
+    if (p->lost.rec) {
+      k_lost32<<<blocks_for(p->lost.cap, T), T, 0, s>>>(*m, f->flags, *b, p->lost);
+      spiffe_note_launches(1);
+    }
   }
   if (!any) {
     k_compact_reference32<<<1, 1, 0, s>>>(cnt);

@@ -236,6 +236,7 @@ struct PushParams {
   double QoMC, stiffness;
   double tb_epm, tb_z_force, tb_r_force, tb_z_decel, tb_r_decel;
   int screen_momentum;
+  LostLog lost;
 };
 
 __device__ void record(const DevScreen &s, long long *nb, long long *overflow, const DevBeam64 &b, long ip,
@@ -414,6 +415,16 @@ __global__ void __launch_bounds__(T) k_push(DevMesh m, DevFields<double> f, DevB
   }
   b.status[ip] = status;
   lost_flag[ip] = lost ? 1 : 0;
+  if (lost && p.lost.rec) { // the loss epilogue, :437-487
+    double pm = pz * pz + pr * pr;
+    if (r)
+      pm += (r_pphi / r) * (r_pphi / r);
+    LostRecord rec{p.time, 0, 0, sqrt(pm), pz, pr, b.r0[ip], b.z0[ip], b.Q[ip], (long long)ip, p.lost.step,
+                   b.particleID[ip], b.generation[ip], 0, 0, 0, 0.f, 0.f};
+    rec.code = (int16_t)find_loss_coordinates(zmin, zmax, dz, dr, nr, fl, m.pitch, z0, r0s, z,
+                                              r_was_negative ? -r : r, &rec.zLost, &rec.rLost);
+    lost_append(p.lost, rec);
+  }
 
   // screen crossings, :362-434
   if (scr.n) {
@@ -899,7 +910,7 @@ extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const
   spiffe_note_launches(1);
   if (np_bound > 0) {
     PushParams p{hp->time, hp->z_forces_start, hp->QoMC, hp->stiffness, hp->tb_epm, hp->tb_z_force,
-                 hp->tb_r_force, hp->tb_z_decel, hp->tb_r_decel, hp->screen_momentum};
+                 hp->tb_r_force, hp->tb_z_decel, hp->tb_r_decel, hp->screen_momentum, hp->lost};
     if (scr->n && hp->screen_momentum == SPIFFE_SCREEN_REFERENCE)
       { k_snapshot_last<<<1, 1, 0, s>>>(*b, cnt); spiffe_note_launches(1); }
     k_push<<<blocks_for(np_bound, T), T, 0, s>>>(*m, *f, *b, p, *scr, cnt, w->lost);

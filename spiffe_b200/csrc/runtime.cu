@@ -17,6 +17,7 @@
 #include <cstring>
 #include <string>
 #include <utility>
+#include <algorithm>
 #include <vector>
 
 #include "common.cuh"
@@ -180,6 +181,9 @@ struct spiffe_gpu_instance {
   // one row per Poisson correction: time step, iterations, residual, driving
   double *d_pclog = nullptr;
   double *d_status = nullptr; // status-row reduction scratch
+  LostRecord *d_lost = nullptr; // lost-particle rows since the last download
+  unsigned long long *d_lost_n = nullptr;
+  long long lost_cap = 0;
   double *d_moments = nullptr; // exit-moment reduction scratch
   unsigned long long *d_pclog_n = nullptr;
   std::vector<HostCathode> cathodes;
@@ -775,6 +779,11 @@ static int s32_deposit_all(spiffe_gpu_instance *in)
   return 0;
 }
 
+static LostLog lost_log(const spiffe_gpu_instance *in)
+{
+  return LostLog{in->d_lost, in->d_lost_n, in->lost_cap, (long long)in->mesh.time_step};
+}
+
 static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, int deposit)
 {
   S32State &S = *in->s32;
@@ -798,6 +807,7 @@ static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, 
   p.tb_r_decel = o->tb_r_start_deceleration;
   p.screen_momentum = o->screen_momentum;
   p.deposit = deposit;
+  p.lost = lost_log(in);
   PhaseScope ps(in, PH_PUSH);
   const int rc = s32_push(&in->dm, &S.f, &S.b, &p, &in->screens, in->cnt, in->np_upper, o->compaction, &S.sc, &S.pw,
                           in->stream);
@@ -897,7 +907,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
-               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments};
+               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments, in->d_lost};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1125,7 +1135,7 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
   onaxis_terms(in);
   PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
                    o->tb_z_force, o->tb_r_force, o->tb_z_start_deceleration, o->tb_r_start_deceleration,
-                   o->screen_momentum, o->compaction};
+                   o->screen_momentum, o->compaction, lost_log(in)};
   PhaseScope ps(in, PH_PUSH);
   const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw, in->stream);
   if (rc)
@@ -1379,6 +1389,68 @@ extern "C" int spiffe_gpu_screen_moments(spiffe_gpu_instance *in, int32_t is, do
                                               in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "screen moments failed: %s", cudaGetErrorString((cudaError_t)rc));
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_lost_log(spiffe_gpu_instance *in, int64_t capacity)
+{
+  if (!in || capacity < 0)
+    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  cudaFree(in->d_lost);
+  in->d_lost = nullptr;
+  in->d_lost_n = nullptr;
+  in->lost_cap = 0;
+  if (capacity == 0)
+    return 0;
+  if (cudaMalloc(&in->d_lost, sizeof(LostRecord) * (size_t)capacity + 256) != cudaSuccess)
+    return fail(SPIFFE_ERR_NOMEM, "lost-particle log of %lld rows does not fit", (long long)capacity);
+  in->d_lost_n = (unsigned long long *)((char *)in->d_lost + sizeof(LostRecord) * (size_t)capacity);
+  CUDA_TRY(cudaMemsetAsync(in->d_lost_n, 0, sizeof(unsigned long long), in->stream));
+  in->lost_cap = capacity;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_download_lost(spiffe_gpu_instance *in, spiffe_lost_set *h)
+{
+  if (!in || !h)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  h->nb = 0;
+  if (!in->d_lost)
+    return 0;
+  unsigned long long n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, in->d_lost_n, sizeof(n), cudaMemcpyDeviceToHost, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  if ((long long)n > in->lost_cap)
+    return fail(SPIFFE_ERR_CAPACITY, "%llu particles were lost since the last download, more than the log's %lld",
+                n, in->lost_cap);
+  if ((long long)n > h->capacity)
+    return fail(SPIFFE_ERR_CAPACITY, "%llu lost-particle rows do not fit the %lld of the host buffer", n,
+                (long long)h->capacity);
+  std::vector<LostRecord> rec(n);
+  if (n)
+    CUDA_TRY(cudaMemcpy(rec.data(), in->d_lost, sizeof(LostRecord) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemsetAsync(in->d_lost_n, 0, sizeof(unsigned long long), in->stream));
+  // the reference's order: step by step, ascending particle index (advance_particles.c:437-440)
+  std::sort(rec.begin(), rec.end(), [](const LostRecord &a, const LostRecord &b) {
+    return a.step != b.step ? a.step < b.step : a.ip < b.ip;
+  });
+  for (size_t k = 0; k < rec.size(); k++) {
+    const LostRecord &r = rec[k];
+    h->t[k] = r.t;
+    h->rLost[k] = r.rLost;
+    h->zLost[k] = r.zLost;
+    h->pz[k] = r.pz;
+    h->pr[k] = r.pr;
+    h->z0[k] = r.z0;
+    h->r0[k] = r.r0;
+    h->q[k] = r.q;
+    h->generation[k] = r.gen;
+    h->particleID[k] = r.id;
+    if (h->step)
+      h->step[k] = r.step;
+  }
+  h->nb = (int64_t)n;
   return 0;
 }
 

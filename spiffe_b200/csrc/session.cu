@@ -279,6 +279,10 @@ struct spiffe_session {
   std::vector<std::vector<double>> status_cols;
   std::vector<std::vector<int32_t>> status_counts;
   int64_t status_old_np = 0;
+  // integrate's lost_particles file (setUpLostParticleFile, advance_particles.c:577-603)
+  bool lost_on = false;
+  std::string lost_path;
+  spiffe_sdds::Writer lost_out;
   bool translate_on = false, translate_set = false; // translate: the moving window
   double z_trigger = 0;
   std::vector<SessionScreen> screens;
@@ -371,6 +375,7 @@ struct spiffe_session {
   int take_snapshot(long long step, double time);
   int output_fields(long long step, double time);
   int flush_screens(long long step, double time);
+  int flush_lost();
   int status(long long step, double time);
   int write_status();
 };
@@ -1532,6 +1537,47 @@ int spiffe_session::flush_screens(long long step, double time)
   return 0;
 }
 
+// The lost particles since the last flush, written as advance_particles
+// writes them (:450-487, :529-535): each step's rows in particle order, in
+// pages of at most 1000 rows.
+int spiffe_session::flush_lost()
+{
+  if (!lost_on)
+    return 0;
+  const size_t cap = (size_t)particle_capacity;
+  std::vector<double> t(cap), rl(cap), zl(cap), pz(cap), pr(cap), z0(cap), r0(cap), q(cap);
+  std::vector<int16_t> gen(cap);
+  std::vector<int32_t> id(cap);
+  std::vector<int64_t> step(cap);
+  spiffe_lost_set h{0, (int64_t)cap, t.data(), rl.data(), zl.data(), pz.data(), pr.data(), z0.data(), r0.data(),
+                    q.data(), gen.data(), id.data(), step.data()};
+  S_TRY(spiffe_gpu_download_lost(inst, &h));
+  const size_t n = (size_t)h.nb;
+  std::vector<float> f[7];
+  for (size_t a = 0; a < n;) {
+    size_t b = a;
+    while (b < n && step[b] == step[a] && b - a < 1000)
+      b++;
+    const size_t rows = b - a;
+    const double *src[7] = {rl.data(), zl.data(), pz.data(), pr.data(), z0.data(), r0.data(), q.data()};
+    for (int c = 0; c < 7; c++) {
+      f[c].resize(rows);
+      for (size_t i = 0; i < rows; i++)
+        f[c][i] = (float)src[c][a + i];
+    }
+    std::vector<const void *> cols = {t.data() + a};
+    for (int c = 0; c < 7; c++)
+      cols.push_back(f[c].data());
+    cols.push_back(gen.data() + a);
+    cols.push_back(id.data() + a);
+    std::string err;
+    if (!lost_out.write_page({}, {}, (int64_t)rows, cols, err))
+      return serr(SPIFFE_ERR_INVALID, "lost_particles: %s", err.c_str());
+    a = b;
+  }
+  return 0;
+}
+
 // The status file's columns (setUpStatusOutputFile, status_pr.c:454-499):
 // the double columns, then Particles, NewParticles, SecondaryParticles
 // (long) between ErAbsMax and zMax
@@ -1610,8 +1656,8 @@ int spiffe_session::cmd_integrate(Args &g)
   g.num("z_forces_start", z_forces_start);
   std::string status_output;
   const bool have_status = g.str("status_output", status_output);
-  if (g.str("lost_particles", out))
-    warn("integrate: lost_particles is not written");
+  std::string lost_particles;
+  const bool have_lost = g.str("lost_particles", lost_particles);
   g.num("imposed_efield_ramp_time", ramp_time);
   g.num("imposed_efield_flat_top_time", flat_top_time);
   g.integer("auto_max_dt", auto_max_dt);
@@ -1628,6 +1674,20 @@ int spiffe_session::cmd_integrate(Args &g)
     return serr(SPIFFE_ERR_INVALID, "J_filter_multiplier must be >=0 and < 1");
   if (smoothing || j_filter || sg)
     return serr(SPIFFE_ERR_UNSUPPORTED, "integrate: current smoothing and filtering are not supported");
+  // setUpLostParticleFile, advance_particles.c:577-603 (integrate.c:81-82)
+  lost_on = have_lost && !lost_particles.empty();
+  if (lost_on) {
+    using namespace spiffe_sdds;
+    lost_path = compose(lost_particles, rootname);
+    const std::vector<Def> cols = {Def{"t", "s", "", T_DOUBLE},    Def{"rLost", "m", "", T_FLOAT},
+                                   Def{"zLost", "m", "", T_FLOAT}, Def{"pz", "", "", T_FLOAT},
+                                   Def{"pr", "", "", T_FLOAT},     Def{"z0", "m", "", T_FLOAT},
+                                   Def{"r0", "m", "", T_FLOAT},    Def{"q", "C", "", T_FLOAT},
+                                   Def{"generation", "", "", T_SHORT}, Def{"particleID", "", "", T_LONG}};
+    std::string err;
+    if (!lost_out.open(lost_path, "", "", {}, cols, err))
+      return serr(SPIFFE_ERR_INVALID, "lost_particles: %s", err.c_str());
+  }
   // setUpStatusOutputFile, status_pr.c:454-499 (integrate.c:79-80)
   status_on = have_status && !status_output.empty();
   if (status_on) {
@@ -1672,6 +1732,7 @@ int spiffe_session::cmd_integrate(Args &g)
   push.compaction = compaction >= 0 ? compaction : (f64 ? SPIFFE_COMPACT_REFERENCE : SPIFFE_COMPACT_ANY);
   push.screen_momentum = screen_momentum >= 0 ? screen_momentum : (f64 ? SPIFFE_SCREEN_REFERENCE : SPIFFE_SCREEN_PARTICLE);
   S_TRY(spiffe_gpu_configure_run(inst, sc, &push, pc_defined ? &pc : nullptr));
+  S_TRY(spiffe_gpu_set_lost_log(inst, lost_on ? particle_capacity : 0));
   S_TRY(spiffe_gpu_run_begin(inst, nullptr));
   say("integration will consist of up to %lld steps spaced by %e\n", n_steps, m.dt);
 
@@ -1744,7 +1805,13 @@ int spiffe_session::cmd_integrate(Args &g)
     S_TRY(spiffe_gpu_run_steps(inst, next - k));
     steps += next - k;
     S_TRY(flush_screens(next - 1, (next - 1) * step_dt + t0));
+    S_TRY(flush_lost());
     k = next;
+  }
+  if (lost_on) { // SDDS_Terminate, integrate.c:203
+    lost_out.close();
+    lost_on = false;
+    S_TRY(spiffe_gpu_set_lost_log(inst, 0));
   }
   // integrate.c:195-206
   S_TRY(spiffe_gpu_get_mesh(inst, &m));

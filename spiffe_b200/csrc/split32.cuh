@@ -132,6 +132,7 @@ struct Push32Params {
   double tb_z_decel, tb_r_decel;
   int screen_momentum;
   int deposit; // fused deposition of the pushed particles for the next step
+  LostLog lost;
 };
 extern "C" int s32_particles_work(Particles32Work *w, long long capacity);
 extern "C" void s32_particles_work_free(Particles32Work *w);

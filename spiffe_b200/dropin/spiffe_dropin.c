@@ -30,8 +30,7 @@
  * beam outgrows it); it uses the FP64 form, whose arithmetic is the
  * reference's, with the reference's compaction and screen-momentum
  * behaviour and the ordered deposition.  Errors call bomb() as the
- * reference does.  Not produced: the lost-particle file (a non-null
- * SDDSlost is refused), secondary emission and on-axis fields.
+ * reference does.  Not available: secondary emission and on-axis fields.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -59,6 +58,7 @@ typedef struct {
   long screen_dir[SPIFFE_MAX_SCREENS];
   spiffe_screen_set scr;      /* download buffers */
   int64_t scr_capacity;
+  int lost_on;                /* the device records lost particles */
 } Mirror;
 
 static Mirror mirrors[DROPIN_MAX];
@@ -367,6 +367,51 @@ static void screen_buffers(Mirror *M, int64_t capacity)
   M->scr_capacity = capacity;
 }
 
+/* this push's lost particles into the lost-particle table, row by row in
+ * pages of at most 1000 rows, as advance_particles.c:450-487 and :529-535
+ * write them */
+static void write_lost(Mirror *M, SDDS_DATASET *SDDSlost, FIELDS *EM_problem)
+{
+  int64_t cap = M->capacity;
+  double *v = malloc(sizeof(double) * 8 * (size_t)cap);
+  int16_t *gen = malloc(sizeof(int16_t) * (size_t)cap);
+  int32_t *id = malloc(sizeof(int32_t) * (size_t)cap);
+  if (!v || !gen || !id)
+    bomb("memory allocation failure (spiffe drop-in)", NULL);
+  spiffe_lost_set h = {0, cap, v, v + cap, v + 2 * cap, v + 3 * cap, v + 4 * cap, v + 5 * cap, v + 6 * cap,
+                       v + 7 * cap, gen, id, NULL};
+  check(spiffe_gpu_download_lost(M->inst, &h), "spiffe drop-in: lost particles");
+  long newLost = 0, maxLost = 0;
+  for (int64_t k = 0; k < h.nb; k++) {
+    if (newLost && newLost >= maxLost) {
+      if (!SDDS_WritePage(SDDSlost)) {
+        SDDS_SetError("Problem writing lost particle data.");
+        SDDS_PrintErrors(stderr, SDDS_EXIT_PrintErrors | SDDS_VERBOSE_PrintErrors);
+      }
+      newLost = maxLost = 0;
+    }
+    if (maxLost == 0 && !SDDS_StartPage(SDDSlost, maxLost = 1000)) {
+      SDDS_SetError("Problem writing lost particle data.");
+      SDDS_PrintErrors(stderr, SDDS_EXIT_PrintErrors | SDDS_VERBOSE_PrintErrors);
+    }
+    if (!SDDS_SetRowValues(SDDSlost, SDDS_SET_BY_NAME | SDDS_PASS_BY_VALUE, newLost, "t", EM_problem->time, "rLost",
+                           (float)h.rLost[k], "zLost", (float)h.zLost[k], "pz", (float)h.pz[k], "pr",
+                           (float)h.pr[k], "r0", (float)h.r0[k], "z0", (float)h.z0[k], "q", (float)h.q[k],
+                           "generation", h.generation[k], "particleID", h.particleID[k], NULL)) {
+      SDDS_SetError("Problem writing lost particle data.");
+      SDDS_PrintErrors(stderr, SDDS_EXIT_PrintErrors | SDDS_VERBOSE_PrintErrors);
+    }
+    newLost++;
+  }
+  if (newLost && !SDDS_WritePage(SDDSlost)) {
+    SDDS_SetError("Problem writing lost particle data.");
+    SDDS_PrintErrors(stderr, SDDS_EXIT_PrintErrors | SDDS_VERBOSE_PrintErrors);
+  }
+  free(v);
+  free(gen);
+  free(id);
+}
+
 /* the screen's SDDS page, as advance_particles.c:538-569 writes it */
 static void write_screen_page(SCREEN *sc, FIELDS *EM_problem)
 {
@@ -397,8 +442,6 @@ void advance_particles(BEAM *beam, FIELDS *EM_problem, TEST_BEAM_DEFN *test_beam
 {
   if (secondaryEmission && nSecondaryDefns > 0)
     bomb("secondary emission is not available in the spiffe drop-in", NULL);
-  if (SDDSlost)
-    bomb("the lost-particle file is not produced by the spiffe drop-in", NULL);
   if (EM_problem->onAxisFields > 0)
     bomb("on-axis fields are not available in the spiffe drop-in", NULL);
   if (n_screens > SPIFFE_MAX_SCREENS)
@@ -437,7 +480,13 @@ void advance_particles(BEAM *beam, FIELDS *EM_problem, TEST_BEAM_DEFN *test_beam
   }
   o.compaction = SPIFFE_COMPACT_REFERENCE;
   o.screen_momentum = SPIFFE_SCREEN_REFERENCE;
+  if (SDDSlost && !M->lost_on) {
+    check(spiffe_gpu_set_lost_log(M->inst, M->capacity), "spiffe drop-in: lost-particle log");
+    M->lost_on = 1;
+  }
   check(spiffe_gpu_advance_particles(M->inst, &o), "advance_particles");
+  if (SDDSlost)
+    write_lost(M, SDDSlost, EM_problem);
   beam_download(M, beam);
   /* this push's screen records into the reference's buffers, then its page */
   for (long is = 0; is < n_screens; is++) {

@@ -11,6 +11,7 @@ reference present.  Run from the repository root:
     python tests/golden/make_golden.py decks    # the input-deck fixtures only
     python tests/golden/make_golden.py onaxis   # one deck fixture (also: translate)
     python tests/golden/make_golden.py te       # the TE-field fixture
+    python tests/golden/make_golden.py lost     # the lost-particle deck
 """
 import os
 import sys
@@ -289,6 +290,28 @@ DECK_ONAXIS = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02
 DECK_TRANSLATE = DECK_DCGUN.replace("&integrate", "&translate z_trigger=0.008 &end\n&integrate")
 
 
+# The DC gun deck with integrate's lost_particles file (advance_particles.c:
+# 437-487, 577-603; findLossCoordinates, secondaryEmission.c:239), a cathode
+# wider than the anode hole and a stronger radial field, so particles are
+# lost on the anode plate as well as through the exit.
+DECK_LOST = DECK_DCGUN.replace("space_charge=1,", 'lost_particles="%s.lost", space_charge=1,').replace(
+    "outer_radius=0.002", "outer_radius=0.0045").replace("Br=1e-4", "Br=2e-3")
+LOST_COLUMNS = ["t", "rLost", "zLost", "pz", "pr", "z0", "r0", "q", "generation", "particleID"]
+
+
+def deck_lost(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    cmds = [b.strip() + " &end" for b in DECK_LOST.split("&end") if b.strip()]
+    # the lost-particle table is the first the reference closes (integrate.c:203)
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("table", 2, LOST_COLUMNS), ("get_beam",)], cwd=d,
+                                 capacity=20000)
+    lost, rb = res
+    save("deck_lost", deck=np.array(DECK_LOST), geo=np.array(geo), lost_pages=lost["pages"],
+         **{"lost_" + k: lost[k] for k in LOST_COLUMNS}, **beam_out(rb))
+
+
 def deck_translate(geo):
     d = tempfile.mkdtemp()
     with open(os.path.join(d, "dc.geo"), "w") as f:
@@ -370,6 +393,7 @@ def decks():
     deck_onaxis(geo)
     deck_translate(geo)
     deck_status(geo)
+    deck_lost(geo)
 
 
 def deck_onaxis(geo):
@@ -397,6 +421,8 @@ if __name__ == "__main__":
         deck_status(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["translate"]:
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["lost"]:
+        deck_lost(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["te"]:
         te()
     elif sys.argv[1:] == ["onaxis"]:

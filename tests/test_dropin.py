@@ -110,3 +110,19 @@ def test_solve_poisson_cyl(tmp_path):
     for (n_r, p_r), (n_g, p_g) in zip(ref, got):
         assert n_r == n_g
         assert np.array_equal(p_r, p_g)
+
+
+def test_lost_particle_file(tmp_path):
+    """integrate's lost_particles file through the drop-in: the reference's
+    own perform_integration hands SDDSlost to the drop-in's
+    advance_particles, which writes the rows it gets from the device."""
+    fx = load("deck_lost")
+    d = str(tmp_path)
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(str(fx["geo"]))
+    cmds = [b.strip() + " &end" for b in str(fx["deck"]).split("&end") if b.strip()]
+    cols = ["t", "rLost", "zLost", "pz", "pr", "z0", "r0", "q", "generation", "particleID"]
+    lost, = run_with_dropin([("command", c) for c in cmds] + [("table", 2, cols)], d, capacity=20000)
+    assert lost["pages"] == int(fx["lost_pages"])
+    for c in cols:
+        assert np.array_equal(lost[c], fx["lost_" + c]), c

@@ -605,3 +605,50 @@ def test_status_file_matches_reference(tmp_path, monkeypatch):
     for c in STATUS_COLUMNS:
         got = np.asarray(pages[0]["columns"][c], np.float64)
         assert len(got) == 8 and np.array_equal(got, fx["st_" + c]), (c, got, fx["st_" + c])
+
+
+LOST_COLUMNS = ["t", "rLost", "zLost", "pz", "pr", "z0", "r0", "q", "generation", "particleID"]
+
+
+@pytest.mark.gpu
+def test_lost_particle_file_matches_reference(tmp_path, monkeypatch):
+    """integrate's lost_particles file (advance_particles.c:437-487, 577-603)
+    on a DC gun deck whose cathode is wider than the anode hole: in the FP64
+    form the rows (time, the loss point of findLossCoordinates,
+    secondaryEmission.c:239, momenta, birth position, charge, generation, id)
+    and the page breaks equal the reference's."""
+    fx = load("deck_lost")
+    s = run_deck(fx, tmp_path, monkeypatch)
+    pages = session.read_sdds(str(tmp_path / "spiffe.lost"))
+    got = {c: np.concatenate([p["columns"][c] for p in pages]) for c in LOST_COLUMNS}
+    assert len(pages) == int(fx["lost_pages"])
+    assert len(got["t"]) == len(fx["lost_t"]) > 40
+    for c in LOST_COLUMNS:
+        assert np.array_equal(np.asarray(got[c], np.float64), fx["lost_" + c]), c
+    s.close()
+
+
+@pytest.mark.gpu
+def test_lost_particle_file_split_form(tmp_path, monkeypatch):
+    """The split form writes the same file: the same particles lost, on the
+    same step (or the next, one dt of 4e-13 s, for a few whose FP32 path
+    crosses a face a step apart), with loss points within 1e-5 of a cell of
+    the reference's."""
+    fx = load("deck_lost")
+    s = run_deck(fx, tmp_path, monkeypatch, precision="split32")
+    pages = session.read_sdds(str(tmp_path / "spiffe.lost"))
+    got = by_id({c: np.concatenate([p["columns"][c] for p in pages]) for c in LOST_COLUMNS}, "particleID")
+    ref = by_id({c: fx["lost_" + c] for c in LOST_COLUMNS}, "particleID")
+    # the reference ends the beam at its first lost index; the split form
+    # removes only the lost particles, so it may lose more of them later
+    common, ig, ir = np.intersect1d(got["particleID"], ref["particleID"], return_indices=True)
+    assert len(common) == len(ref["particleID"])
+    # the same step, or a neighbour where FP32 rounding moves a particle across a cell face
+    assert np.max(np.abs(got["t"][ig] - ref["t"][ir])) <= 4.1e-13
+    same = got["t"][ig] == ref["t"][ir]
+    assert same.mean() > 0.9
+    ig, ir = ig[same], ir[same]
+    dz = 0.03 / 150
+    assert np.max(np.abs(got["zLost"][ig] - ref["zLost"][ir])) <= 1e-5 * dz + 1e-9
+    assert np.max(np.abs(got["rLost"][ig] - ref["rLost"][ir])) <= 1e-5 * dz + 1e-9
+    s.close()
