@@ -98,7 +98,9 @@ int ref_command(const char *text)
   else if (strcmp(nl.group_name, "define_antenna") == 0) {
     process_antenna_definition(&antenna, n_antennae, &EM, &nl);
     n_antennae++;
-  } else if (strcmp(nl.group_name, "define_snapshots") == 0)
+  } else if (strcmp(nl.group_name, "define_field_saving") == 0)
+    process_field_saving_definition(&saving_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "define_snapshots") == 0)
     process_snapshot_definition(&snapshot_defn, &EM, &nl);
   else if (strcmp(nl.group_name, "define_field_output") == 0)
     process_field_output_definition(&field_output_defn, &EM, &nl);
@@ -415,14 +417,17 @@ void ref_step(long space_charge, double z_forces_start)
  * table (which 1), all pages in order; returns the row count, -1 for an
  * unknown column */
 /* which: 0 the beam snapshots, 1 the field output, 2 + k the k-th output
- * table the reference closed inside a command, 100 + k the k-th table it
- * wrote row by row (the status file) */
+ * table the reference closed inside a command, 3 + SHIM_MAX_CLOSED_TABLES
+ * the field saves, 100 + k the k-th table it wrote row by row (the status
+ * file) */
 static SDDS_DATASET *ref_table(long which)
 {
   if (which == 0)
     return &snapshot_defn.table;
   if (which == 1)
     return &field_output_defn.SDDSout;
+  if (which == 3 + SHIM_MAX_CLOSED_TABLES)
+    return &saving_defn.outTable;
   if (which >= 100)
     return which - 100 < shim_n_updated_tables ? &shim_updated_tables[which - 100] : NULL;
   if (which - 2 < shim_n_closed_tables)

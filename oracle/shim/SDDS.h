@@ -23,6 +23,7 @@
 #define SDDS_SHORT 4
 #define SDDS_STRING 5
 #define SDDS_LONG64 6
+#define SDDS_CHARACTER 7
 #define SDDS_ANY_FLOATING_TYPE 100
 
 #define SDDS_SET_BY_INDEX 1

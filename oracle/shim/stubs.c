@@ -31,14 +31,6 @@ void sample_fields(SAMPLE_DEFN *sample_defn, long n_sample_defns, FIELDS *EM_pro
     bomb("field sampling is not part of the checked path", NULL);
 }
 
-void save_fields(FIELD_SAVING *saving_defn, FIELDS *EM_problem, long final_call)
-{
-  (void)EM_problem;
-  (void)final_call;
-  if (saving_defn && saving_defn->filename)
-    bomb("field saving is not part of the checked path", NULL);
-}
-
 void emit_electrons_from_emitter(BEAM *beam, EMITTER *emitter, FIELDS *EM_problem)
 {
   (void)beam;

@@ -312,6 +312,34 @@ def deck_lost(geo):
          **{"lost_" + k: lost[k] for k in LOST_COLUMNS}, **beam_out(rb))
 
 
+# The DC gun deck with define_field_saving (field_saving.c:46-213): saves at
+# 0 and 100 ps and before exiting.  The saved columns are compared through
+# SHA-256 digests of their values (bit-for-bit equality needs nothing more,
+# and the fixture stays small).
+DECK_FIELDSAVE = DECK_DCGUN.replace("finish_time=300e-12", "finish_time=140e-12").replace(
+    "&integrate", '&define_field_saving filename="%s.flds", time_interval=100e-12, save_before_exiting=1 &end\n'
+    "&integrate")
+SAVE_COLUMNS = ["Ez", "Er", "Jz", "Jr", "Bphi", "Bphi2", "metalFlags"]
+
+
+def digest(a):
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(a, np.float64).tobytes()).hexdigest()
+
+
+def deck_fieldsave(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    cmds = [b.strip() + " &end" for b in DECK_FIELDSAVE.split("&end") if b.strip()]
+    t, = pyoracle.run_reference([("command", c) for c in cmds] + [("table", 3 + 16, SAVE_COLUMNS)], cwd=d,
+                                capacity=20000)
+    save("deck_fieldsave", deck=np.array(DECK_FIELDSAVE), geo=np.array(geo), pages=t["pages"], rows=len(t["Ez"]),
+         **{"sha_" + c: np.array(digest(t[c])) for c in SAVE_COLUMNS},
+         **{"head_" + c: t[c][:64] for c in SAVE_COLUMNS})
+
+
 def deck_translate(geo):
     d = tempfile.mkdtemp()
     with open(os.path.join(d, "dc.geo"), "w") as f:
@@ -394,6 +422,7 @@ def decks():
     deck_translate(geo)
     deck_status(geo)
     deck_lost(geo)
+    deck_fieldsave(geo)
 
 
 def deck_onaxis(geo):
@@ -421,6 +450,8 @@ if __name__ == "__main__":
         deck_status(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["translate"]:
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["fieldsave"]:
+        deck_fieldsave(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["lost"]:
         deck_lost(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["te"]:

@@ -652,3 +652,23 @@ def test_lost_particle_file_split_form(tmp_path, monkeypatch):
     assert np.max(np.abs(got["zLost"][ig] - ref["zLost"][ir])) <= 1e-5 * dz + 1e-9
     assert np.max(np.abs(got["rLost"][ig] - ref["rLost"][ir])) <= 1e-5 * dz + 1e-9
     s.close()
+
+
+@pytest.mark.gpu
+def test_field_saves_match_reference(tmp_path, monkeypatch):
+    """define_field_saving (field_saving.c:46-213) on the DC gun deck in the
+    FP64 form: the same pages, every column (Ez, Er, Jz, Jr, Bphi, Bphi2 and
+    the metalFlags column the reference leaves at zero) equal to the
+    reference's saves bit for bit (compared through SHA-256 digests)."""
+    import hashlib
+
+    fx = load("deck_fieldsave")
+    s = run_deck(fx, tmp_path, monkeypatch)
+    pages = session.read_sdds(str(tmp_path / "spiffe.flds"))
+    assert len(pages) == int(fx["pages"])
+    for c in ("Ez", "Er", "Jz", "Jr", "Bphi", "Bphi2", "metalFlags"):
+        v = np.concatenate([np.asarray(p["columns"][c], np.float64) for p in pages])
+        assert len(v) == int(fx["rows"])
+        assert np.array_equal(v[:64], fx["head_" + c]), c
+        assert hashlib.sha256(np.ascontiguousarray(v).tobytes()).hexdigest() == str(fx["sha_" + c]), c
+    s.close()
