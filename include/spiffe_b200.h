@@ -124,6 +124,26 @@ int spiffe_gpu_set_lost_log(spiffe_gpu_instance *inst, int64_t capacity);
  * then particle index), and empties the log; an error when more particles
  * were lost than the log or `host` holds. */
 int spiffe_gpu_download_lost(spiffe_gpu_instance *inst, spiffe_lost_set *host);
+/* The surface material of each node, (nz+1)*(nr+1) ir fastest: the
+ * materialID array of FIELDS (spiffe.h:105), from define_geometry's &po
+ * material_id (spiffe_geometry_rasterise's material output). */
+int spiffe_gpu_set_materials(spiffe_gpu_instance *inst, const int16_t *material);
+/* define_secondary_emission (secondaryEmission.c:21-118): each push queues
+ * the lost particles that hit this material (queueSecondaryEmission, :120-237)
+ * and the next step of spiffe_gpu_run_steps emits their secondaries before
+ * the cathodes' births (emitSecondaryElectrons, :374-584; integrate.c:159-163),
+ * drawing from the instance's generator in the reference's order.  With
+ * opt->log set, each emitting source is logged as the reference's log_file
+ * records it (:520-544), taking a particle ID as the reference does. */
+int spiffe_gpu_add_secondary_emission(spiffe_gpu_instance *inst, const spiffe_secondary_options *opt);
+/* The emission log of secondary-emission definition `index` (the order of
+ * spiffe_gpu_add_secondary_emission) since the last call, and empties it:
+ * *n_rows rows of SPIFFE_SECONDARY_LOG_COLS doubles, row-major (time step of
+ * the emission, z, r, t, K, yield, emitted, directionCode, generation,
+ * particleID).  With rows NULL only *n_rows is set; an error when max_rows is
+ * too small. */
+int spiffe_gpu_secondary_log(spiffe_gpu_instance *inst, int32_t index, int64_t max_rows, double *rows,
+                             int64_t *n_rows);
 /* No counterpart in the reference, which leaves moments to external SDDS
  * tools.  The exit-plane moments of a screen's records, reduced on the device
  * in FP64 with weights |q|: out[0] records, [1] charge sum q, [2] mean kinetic

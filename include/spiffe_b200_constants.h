@@ -24,5 +24,6 @@
 #define SPIFFE_KB_MKS 1.380649e-23
 #define SPIFFE_MU_O 1.2566370614359173e-06
 #define SPIFFE_EPSILON_O 8.85418781762039e-12
+#define SPIFFE_ME_MEV 0.51099895000 /* electron rest energy in MeV (secondaryEmission.c:104-105, :198) */
 
 #endif

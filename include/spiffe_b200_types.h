@@ -110,7 +110,31 @@ typedef struct spiffe_lost_set {
   int16_t *generation;
   int32_t *particleID;
   int64_t *step; /* may be NULL */
+  /* may be NULL: the impact momentum |p| (beta*gamma) and the side of the
+   * surface the particle crossed (findLossCoordinates' directionCode,
+   * secondaryEmission.c:239-352: 1 left, 2 right, 3 up, 4 down, 0 none), the
+   * arguments the reference passes to queueSecondaryEmission
+   * (advance_particles.c:443-451) */
+  double *p;
+  int16_t *direction;
 } spiffe_lost_set;
+
+/* define_secondary_emission (secondaryEmission.nl; processSecondaryEmission-
+ * Definition, secondaryEmission.c:21-118): particles lost on a surface of
+ * material `material_id` (the &po material_id of define_geometry) release a
+ * Poisson-distributed number of secondaries with mean yield(K) (linear in the
+ * table, K the impact kinetic energy in eV), each of momentum
+ * emitted_momentum (beta*gamma) in a random direction away from the surface;
+ * at most yield_limit each (0: no limit). */
+typedef struct spiffe_secondary_options {
+  int32_t material_id, verbosity;
+  double emitted_momentum;
+  int64_t yield_limit;
+  int64_t n_data;
+  const double *energy, *yield; /* energy in eV, increasing */
+  int32_t log;                  /* keep the emission log (log_file) */
+} spiffe_secondary_options;
+#define SPIFFE_SECONDARY_LOG_COLS 10
 
 /* Poisson solver of the split-precision form (spiffe_gpu_set_poisson_solver) */
 #define SPIFFE_POISSON_SOR 0       /* the reference's red-black SOR and stop rule (poisson.c:17-130) */

@@ -33,6 +33,8 @@ static RESISTOR resistor_defns;
 static FIELD_SAVING saving_defn;
 static FIELD_OUTPUT field_output_defn;
 static SNAPSHOT snapshot_defn;
+static SECONDARY_EMISSION *secondary = NULL;
+static long n_secondary = 0;
 static int initialized = 0;
 
 /* capacity of every particle and screen array: the reference sizes screen
@@ -110,10 +112,12 @@ int ref_command(const char *text)
     process_on_axis_field_definition(&EM, &nl);
   else if (strcmp(nl.group_name, "define_test_beam") == 0)
     process_testbeam_definition(&test_beam_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "define_secondary_emission") == 0)
+    processSecondaryEmissionDefinition(&secondary, &n_secondary, &nl, &EM);
   else if (strcmp(nl.group_name, "integrate") == 0)
     perform_integration(&EM, &beam, cathode, cathodes, &test_beam_defn, antenna, n_antennae, &resistor_defns,
                         NULL, 0, &saving_defn, &snapshot_defn, screen_defn, n_screen_defns,
-                        &field_output_defn, NULL, 0, NULL, 0, &nl);
+                        &field_output_defn, secondary, n_secondary, NULL, 0, &nl);
   else
     rc = -1;
   free_namelist_text(&nl);
@@ -419,7 +423,7 @@ void ref_step(long space_charge, double z_forces_start)
 /* which: 0 the beam snapshots, 1 the field output, 2 + k the k-th output
  * table the reference closed inside a command, 3 + SHIM_MAX_CLOSED_TABLES
  * the field saves, 100 + k the k-th table it wrote row by row (the status
- * file) */
+ * file), 200 + k the log_file of the k-th define_secondary_emission */
 static SDDS_DATASET *ref_table(long which)
 {
   if (which == 0)
@@ -428,6 +432,8 @@ static SDDS_DATASET *ref_table(long which)
     return &field_output_defn.SDDSout;
   if (which == 3 + SHIM_MAX_CLOSED_TABLES)
     return &saving_defn.outTable;
+  if (which >= 200)
+    return which - 200 < n_secondary && secondary[which - 200].logFile ? &secondary[which - 200].SDDSlog : NULL;
   if (which >= 100)
     return which - 100 < shim_n_updated_tables ? &shim_updated_tables[which - 100] : NULL;
   if (which - 2 < shim_n_closed_tables)

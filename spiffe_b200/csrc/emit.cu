@@ -29,6 +29,27 @@ __global__ void __launch_bounds__(T) k_births(DevMesh m, DevFields<double> f, De
   }
   const long long ip = np + k;
   const double c = SPIFFE_C_MKS;
+  if (p.mode == SPIFFE_BIRTH_LIST) {
+    // emitSecondaryElectrons (secondaryEmission.c:471-497): the host drew the
+    // momenta; position and birth position are the loss point
+    const double *L = p.list;
+    const long long n = p.total;
+    b.z[ip] = b.z0[ip] = L[k];
+    b.r[ip] = b.r0[ip] = L[n + k];
+    b.pz[ip] = L[2 * n + k];
+    b.pr[ip] = L[3 * n + k];
+    b.vz[ip] = L[4 * n + k];
+    b.vr[ip] = L[5 * n + k];
+    b.Q[ip] = L[6 * n + k];
+    b.t0[ip] = L[7 * n + k];
+    b.generation[ip] = (int16_t)L[8 * n + k];
+    b.particleID[ip] = (int32_t)L[9 * n + k];
+    b.vphi[ip] = b.r_pphi[ip] = 0;
+    b.rmin[ip] = b.zmin[ip] = 1.7976931348623157e308;
+    b.rmax[ip] = b.zmax[ip] = -1.7976931348623157e308;
+    b.status[ip] = SPIFFE_PART_ACTIVE;
+    return;
+  }
   if (p.mode == SPIFFE_BIRTH_TEST) {
     // test_beam.c:91-103 sets position, momenta, velocities and charge only;
     // every other per-particle value is what a fresh (zeroed) slot holds, and
@@ -124,15 +145,16 @@ __global__ void __launch_bounds__(T) k_births(DevMesh m, DevFields<double> f, De
   b.status[ip] = SPIFFE_PART_ACTIVE;
 }
 
-__global__ void k_births_commit(long long total, long long capacity, int test, DevCounts *cnt)
+__global__ void k_births_commit(long long total, long long capacity, int mode, DevCounts *cnt)
 {
   if (cnt->np + total > capacity)
     return;
   cnt->np += total;
-  if (test) // inactive and without an ID, test_beam.c:104
+  if (mode == SPIFFE_BIRTH_TEST) // inactive and without an ID, test_beam.c:104
     return;
   cnt->npActive += total;
-  cnt->nextParticleID += total;
+  if (mode != SPIFFE_BIRTH_LIST) // listed particles carry the IDs given at their queueing
+    cnt->nextParticleID += total;
 }
 
 __global__ void k_antenna(double *J, int P, int direction, long istart, long iend, long iposition, double value)
@@ -156,7 +178,7 @@ extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, con
     return 0;
   k_births<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt);
   spiffe_note_launches(1);
-  k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode == SPIFFE_BIRTH_TEST, cnt);
+  k_births_commit<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode, cnt);
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

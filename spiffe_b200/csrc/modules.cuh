@@ -33,6 +33,8 @@ struct PushHostParams {
   int screen_momentum, compaction;
   LostLog lost;
 };
+extern "C" int spiffe_gather_points64(const DevMesh *m, const DevFields<double> *f, const double *zr, int n, double *E,
+                                      cudaStream_t s);
 extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const PushHostParams *hp,
                              const DevScreens *scr, DevCounts *cnt, long long np_bound, Particles64Work *w,
                              cudaStream_t s);
@@ -80,6 +82,8 @@ struct BirthBin {
 // test_beam.c:57-104) at (z_position, inner_radius) with momenta pz0, pr0,
 // rpphi0, inactive until the push activates it.
 #define SPIFFE_BIRTH_TEST 3
+#define SPIFFE_BIRTH_LIST 4 // explicit particles (secondary electrons): list holds BIRTH_LIST_COLS rows of total
+#define BIRTH_LIST_COLS 10  // z, r, pz, pr, vz, vr, Q, t0, generation, particleID
 struct BirthParams {
   long long total;
   uint64_t key, counter_base;
@@ -90,6 +94,7 @@ struct BirthParams {
   double pz0, pr0, rpphi0;
   const BirthBin *bins;
   int n_bins;
+  const double *list; // SPIFFE_BIRTH_LIST
 };
 extern "C" int spiffe_births64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const BirthParams *p,
                                DevCounts *cnt, cudaStream_t s);

@@ -920,7 +920,41 @@ __global__ void __launch_bounds__(T) k_births32(DevMesh m, DevFields32 f, DevBea
   int iz = 0, ir = 0;
   float fz = 0, fr = 0, bz = 0, br = 0, bphi = 0, qs = 0;
   const bool test = p.mode == SPIFFE_BIRTH_TEST;
-  if (on && test) {
+  if (on && p.mode == SPIFFE_BIRTH_LIST) {
+    // emitSecondaryElectrons (secondaryEmission.c:471-497) from the host's list
+    const long long ip = np + k, n = p.total;
+    const double *L = p.list;
+    const double xz = (L[k] - m.zmin) / m.dz, xr = L[n + k] / m.dr;
+    iz = (int)floor(xz);
+    fz = (float)(xz - iz);
+    if (fz >= 1.f) {
+      fz = 0.f;
+      iz++;
+    }
+    ir = (int)floor(xr);
+    fr = (float)(xr - ir);
+    if (fr >= 1.f) {
+      fr = 0.f;
+      ir++;
+    }
+    b.cell[ip] = s32_cell(iz, ir);
+    b.fz[ip] = fz;
+    b.fr[ip] = fr;
+    b.pz[ip] = (float)L[2 * n + k];
+    b.pr[ip] = (float)L[3 * n + k];
+    b.rpphi[ip] = 0.f;
+    b.Q[ip] = (float)L[6 * n + k];
+    b.status[ip] = S32_ACTIVE;
+    b.rmin[ip] = b.zmin[ip] = FLT_MAX;
+    b.rmax[ip] = b.zmax[ip] = -FLT_MAX;
+    b.z0[ip] = L[k];
+    b.r0[ip] = L[n + k];
+    b.t0[ip] = L[7 * n + k];
+    b.particleID[ip] = (int32_t)L[9 * n + k];
+    b.generation[ip] = (int16_t)L[8 * n + k];
+    betas(b.pz[ip], b.pr[ip], 0.f, ((float)ir + fr) * (float)m.dr, bz, br, bphi);
+    qs = b.Q[ip] * sc.s_charge;
+  } else if (on && test) {
     // test_beam.c:91-103: position, momenta and charge; the rest as a fresh
     // slot holds it, inactive until the push activates it (no deposit)
     const long long ip = np + k;
@@ -1031,15 +1065,31 @@ __global__ void __launch_bounds__(T) k_births32(DevMesh m, DevFields32 f, DevBea
     deposit_particle<false>(m, f, on && !test, iz, fz, ir, fr, bz, br, bphi, qs);
 }
 
-__global__ void k_births_commit32(long long total, long long capacity, int test, DevCounts *cnt)
+__global__ void k_births_commit32(long long total, long long capacity, int mode, DevCounts *cnt)
 {
   if (cnt->np + total > capacity)
     return;
   cnt->np += total;
-  if (test) // inactive and without an ID, test_beam.c:104
+  if (mode == SPIFFE_BIRTH_TEST) // inactive and without an ID, test_beam.c:104
     return;
   cnt->npActive += total;
-  cnt->nextParticleID += total;
+  if (mode != SPIFFE_BIRTH_LIST) // listed particles carry the IDs given at their queueing
+    cnt->nextParticleID += total;
+}
+
+// interpolateFields at n points (zr[2i], zr[2i+1]) of the split form's
+// fields: Ez, Er into E[2i], E[2i+1]
+__global__ void k_gather_points32(DevMesh m, DevFields32 f, const double *zr, int n, double *E)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n)
+    return;
+  const double xz = (zr[2 * i] - m.zmin) / m.dz, xr = zr[2 * i + 1] / m.dr;
+  const int iz = (int)floor(xz), ir = (int)floor(xr);
+  float e[6];
+  gather32<false>(m, f, iz, (float)(xz - iz), ir, (float)(xr - ir), e);
+  E[2 * i] = e[0];
+  E[2 * i + 1] = e[1];
 }
 
 // ---- conversions between the FP64 SoA and the split beam
@@ -1287,8 +1337,18 @@ extern "C" int s32_births(const DevMesh *m, const DevFields32 *f, const DevBeam3
   if (p->total <= 0)
     return 0;
   k_births32<<<blocks_for(p->total, T), T, 0, s>>>(*m, *f, *b, *p, cnt, *sc, deposit);
-  k_births_commit32<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode == SPIFFE_BIRTH_TEST, cnt);
+  k_births_commit32<<<1, 1, 0, s>>>(p->total, b->capacity, p->mode, cnt);
   spiffe_note_launches(2);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int s32_gather_points(const DevMesh *m, const DevFields32 *f, const double *zr, int n, double *E,
+                                 cudaStream_t s)
+{
+  if (n <= 0)
+    return 0;
+  k_gather_points32<<<blocks_for(n, 128), 128, 0, s>>>(*m, *f, zr, n, E);
+  spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }
 

@@ -102,6 +102,21 @@ struct PhaseTimer {
 
 // ------------------------------------------------------------- host state
 
+// One secondary-emission material as the reference holds it
+// (SECONDARY_EMISSION, spiffe.h:293-317) with its queue of sources.
+struct HostSecondary {
+  int material = 1, verbosity = 0;
+  double em = 0; // emitted momentum, beta*gamma
+  long long limit = 0;
+  std::vector<double> E, Y; // kinetic energy (eV), mean yield
+  double pMin = 0, pMax = 0;
+  std::vector<double> qz, qr, qp, qQ;
+  std::vector<int16_t> qdir, qgen;
+  std::vector<int32_t> qid;
+  bool log = false;
+  std::vector<double> log_rows; // SPIFFE_SECONDARY_LOG_COLS per emitting source
+};
+
 // One cathode as the reference holds it (CATHODE, spiffe.h:236-262).
 struct HostCathode {
   spiffe_cathode_options o;
@@ -181,9 +196,18 @@ struct spiffe_gpu_instance {
   // one row per Poisson correction: time step, iterations, residual, driving
   double *d_pclog = nullptr;
   double *d_status = nullptr; // status-row reduction scratch
-  LostRecord *d_lost = nullptr; // lost-particle rows since the last download
+  LostRecord *d_lost = nullptr; // lost-particle rows since the last fetch
   unsigned long long *d_lost_n = nullptr;
   long long lost_cap = 0;
+  bool lost_user = false;             // the caller reads the rows (spiffe_gpu_set_lost_log)
+  std::vector<LostRecord> lost_host;  // rows fetched, not yet handed to the caller
+  // secondary emission (define_secondary_emission) and the surface materials
+  std::vector<HostSecondary> secondaries;
+  std::vector<int16_t> h_material;
+  double *d_points = nullptr;         // gather points and their fields
+  size_t points_cap = 0;
+  double *d_list = nullptr;           // births listed by the host
+  size_t list_cap = 0;
   double *d_moments = nullptr; // exit-moment reduction scratch
   unsigned long long *d_pclog_n = nullptr;
   std::vector<HostCathode> cathodes;
@@ -779,6 +803,8 @@ static int s32_deposit_all(spiffe_gpu_instance *in)
   return 0;
 }
 
+static int after_push(spiffe_gpu_instance *in);
+
 static LostLog lost_log(const spiffe_gpu_instance *in)
 {
   return LostLog{in->d_lost, in->d_lost_n, in->lost_cap, (long long)in->mesh.time_step};
@@ -814,7 +840,7 @@ static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, 
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
   S.j_state = deposit ? S32_J_DEPOSITED : S32_J_UNKNOWN;
-  return 0;
+  return after_push(in);
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -907,7 +933,8 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   DevFields<double> &f = in->f;
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
-               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments, in->d_lost};
+               in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments, in->d_lost, in->d_points,
+               in->d_list};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1136,11 +1163,14 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
   PushHostParams p{in->mesh.time, o->z_forces_start, in->QoMC, in->stiffness, o->tb_electrons_per_macroparticle,
                    o->tb_z_force, o->tb_r_force, o->tb_z_start_deceleration, o->tb_r_start_deceleration,
                    o->screen_momentum, o->compaction, lost_log(in)};
-  PhaseScope ps(in, PH_PUSH);
-  const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw, in->stream);
-  if (rc)
-    return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
-  return 0;
+  {
+    PhaseScope ps(in, PH_PUSH);
+    const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw,
+                                 in->stream);
+    if (rc)
+      return fail(SPIFFE_ERR_CUDA, "push launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  }
+  return after_push(in);
 }
 
 extern "C" int spiffe_gpu_solve_poisson_cyl(spiffe_gpu_instance *in, int32_t target, double accuracy,
@@ -1392,10 +1422,12 @@ extern "C" int spiffe_gpu_screen_moments(spiffe_gpu_instance *in, int32_t is, do
   return 0;
 }
 
-extern "C" int spiffe_gpu_set_lost_log(spiffe_gpu_instance *in, int64_t capacity)
+// The device log of lost particles runs while the caller asked for the rows
+// or secondary emission needs them; capacity: rows between fetches.
+static int lost_log_size(spiffe_gpu_instance *in, long long capacity)
 {
-  if (!in || capacity < 0)
-    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  if (capacity == in->lost_cap)
+    return 0;
   CUDA_TRY(cudaStreamSynchronize(in->stream));
   cudaFree(in->d_lost);
   in->d_lost = nullptr;
@@ -1404,11 +1436,46 @@ extern "C" int spiffe_gpu_set_lost_log(spiffe_gpu_instance *in, int64_t capacity
   if (capacity == 0)
     return 0;
   if (cudaMalloc(&in->d_lost, sizeof(LostRecord) * (size_t)capacity + 256) != cudaSuccess)
-    return fail(SPIFFE_ERR_NOMEM, "lost-particle log of %lld rows does not fit", (long long)capacity);
+    return fail(SPIFFE_ERR_NOMEM, "lost-particle log of %lld rows does not fit", capacity);
   in->d_lost_n = (unsigned long long *)((char *)in->d_lost + sizeof(LostRecord) * (size_t)capacity);
   CUDA_TRY(cudaMemsetAsync(in->d_lost_n, 0, sizeof(unsigned long long), in->stream));
   in->lost_cap = capacity;
   return 0;
+}
+
+// Moves the device's rows to lost_host, in the reference's order within each
+// step (advance_particles.c:437-440: ascending particle index).
+static int fetch_lost(spiffe_gpu_instance *in)
+{
+  if (!in->d_lost)
+    return 0;
+  unsigned long long n = 0;
+  CUDA_TRY(cudaMemcpyAsync(&n, in->d_lost_n, sizeof(n), cudaMemcpyDeviceToHost, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  if (!n)
+    return 0;
+  if ((long long)n > in->lost_cap)
+    return fail(SPIFFE_ERR_CAPACITY, "%llu particles were lost since the last download, more than the log's %lld",
+                n, in->lost_cap);
+  const size_t first = in->lost_host.size();
+  in->lost_host.resize(first + n);
+  CUDA_TRY(cudaMemcpy(in->lost_host.data() + first, in->d_lost, sizeof(LostRecord) * n, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemsetAsync(in->d_lost_n, 0, sizeof(unsigned long long), in->stream));
+  std::sort(in->lost_host.begin() + (long)first, in->lost_host.end(), [](const LostRecord &a, const LostRecord &b) {
+    return a.step != b.step ? a.step < b.step : a.ip < b.ip;
+  });
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_lost_log(spiffe_gpu_instance *in, int64_t capacity)
+{
+  if (!in || capacity < 0)
+    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  in->lost_user = capacity > 0;
+  if (!in->lost_user)
+    in->lost_host.clear();
+  const long long need = in->lost_user ? capacity : (in->secondaries.empty() ? 0 : in->capacity);
+  return lost_log_size(in, std::max<long long>(need, in->secondaries.empty() ? 0 : in->capacity));
 }
 
 extern "C" int spiffe_gpu_download_lost(spiffe_gpu_instance *in, spiffe_lost_set *h)
@@ -1416,27 +1483,13 @@ extern "C" int spiffe_gpu_download_lost(spiffe_gpu_instance *in, spiffe_lost_set
   if (!in || !h)
     return fail(SPIFFE_ERR_INVALID, "null argument");
   h->nb = 0;
-  if (!in->d_lost)
-    return 0;
-  unsigned long long n = 0;
-  CUDA_TRY(cudaMemcpyAsync(&n, in->d_lost_n, sizeof(n), cudaMemcpyDeviceToHost, in->stream));
-  CUDA_TRY(cudaStreamSynchronize(in->stream));
-  if ((long long)n > in->lost_cap)
-    return fail(SPIFFE_ERR_CAPACITY, "%llu particles were lost since the last download, more than the log's %lld",
-                n, in->lost_cap);
+  RC_TRY(fetch_lost(in));
+  const size_t n = in->lost_host.size();
   if ((long long)n > h->capacity)
-    return fail(SPIFFE_ERR_CAPACITY, "%llu lost-particle rows do not fit the %lld of the host buffer", n,
+    return fail(SPIFFE_ERR_CAPACITY, "%zu lost-particle rows do not fit the %lld of the host buffer", n,
                 (long long)h->capacity);
-  std::vector<LostRecord> rec(n);
-  if (n)
-    CUDA_TRY(cudaMemcpy(rec.data(), in->d_lost, sizeof(LostRecord) * n, cudaMemcpyDeviceToHost));
-  CUDA_TRY(cudaMemsetAsync(in->d_lost_n, 0, sizeof(unsigned long long), in->stream));
-  // the reference's order: step by step, ascending particle index (advance_particles.c:437-440)
-  std::sort(rec.begin(), rec.end(), [](const LostRecord &a, const LostRecord &b) {
-    return a.step != b.step ? a.step < b.step : a.ip < b.ip;
-  });
-  for (size_t k = 0; k < rec.size(); k++) {
-    const LostRecord &r = rec[k];
+  for (size_t k = 0; k < n; k++) {
+    const LostRecord &r = in->lost_host[k];
     h->t[k] = r.t;
     h->rLost[k] = r.rLost;
     h->zLost[k] = r.zLost;
@@ -1449,8 +1502,361 @@ extern "C" int spiffe_gpu_download_lost(spiffe_gpu_instance *in, spiffe_lost_set
     h->particleID[k] = r.id;
     if (h->step)
       h->step[k] = r.step;
+    if (h->p)
+      h->p[k] = r.p;
+    if (h->direction)
+      h->direction[k] = r.code;
   }
   h->nb = (int64_t)n;
+  in->lost_host.clear();
+  return 0;
+}
+
+static int ensure_points(spiffe_gpu_instance *in, size_t n)
+{
+  if (n <= in->points_cap)
+    return 0;
+  cudaFree(in->d_points);
+  in->d_points = nullptr;
+  const size_t cap = std::max<size_t>(n, 1024);
+  CUDA_TRY(cudaMalloc(&in->d_points, sizeof(double) * 4 * cap));
+  in->points_cap = cap;
+  return 0;
+}
+
+// queueSecondaryEmission (secondaryEmission.c:120-237) for the lost rows from
+// index `first` of lost_host (this push's, in the reference's order)
+static int queue_secondaries(spiffe_gpu_instance *in, size_t first)
+{
+  const spiffe_mesh &m = in->mesh;
+  const int nz = m.nz, nr = m.nr, P = nr + 1;
+  const int16_t *fl = in->h_flags.data();
+  const int16_t *mat = in->h_material.empty() ? nullptr : in->h_material.data();
+  struct Cand {
+    size_t row;
+    int im;
+  };
+  std::vector<Cand> cand;
+  for (size_t k = first; k < in->lost_host.size(); k++) {
+    const LostRecord &L = in->lost_host[k];
+    const double z = L.zLost, r = L.rLost;
+    if ((z + m.dz) >= m.zmax)
+      continue;
+    const long iz = (long)((z - m.zmin) / m.dz), ir = (long)(std::fabs(r) / m.dr), iz1 = iz + 1, ir1 = ir + 1;
+    if (iz >= nz || ir >= nr || iz < 0 || ir < 0)
+      continue;
+    const int16_t f0 = fl[iz * P + ir];
+    if (f0 & SPIFFE_FL_IS_INSIDE)
+      continue;
+    if (f0 & SPIFFE_FL_IS_SURFACE) {
+      if (iz1 > nz || ir1 > nr)
+        continue;
+      if (fl[iz1 * P + ir1] & SPIFFE_FL_IS_METAL && fl[iz * P + ir1] & SPIFFE_FL_IS_METAL &&
+          fl[iz1 * P + ir] & SPIFFE_FL_IS_METAL)
+        continue;
+    }
+    int material = 0;
+    if (mat) {
+      const long at[4][2] = {{iz, ir}, {iz1, ir}, {iz, ir1}, {iz1, ir1}};
+      for (int q = 0; q < 4 && material < 1; q++)
+        material = mat[at[q][0] * P + at[q][1]];
+    }
+    if (material < 1)
+      continue; // no secondary emission here
+    int im = -1;
+    for (size_t q = 0; q < in->secondaries.size(); q++)
+      if (in->secondaries[q].material == material) {
+        im = (int)q;
+        break;
+      }
+    if (im < 0)
+      return fail(SPIFFE_ERR_INVALID, "no match for material %d for r=%e, z=%e, (ir=%ld, iz=%ld)", material, r, z, ir,
+                  iz);
+    const HostSecondary &SE = in->secondaries[(size_t)im];
+    if (SE.pMin > L.p || SE.pMax < L.p)
+      continue;
+    cand.push_back(Cand{k, im});
+  }
+  if (cand.empty())
+    return 0;
+  // the fields at the loss point, as the reference asks interpolateFields
+  // for them: with z and r exchanged (secondaryEmission.c:195)
+  RC_TRY(ensure_points(in, cand.size()));
+  std::vector<double> pts(2 * cand.size()), E(2 * cand.size());
+  for (size_t c = 0; c < cand.size(); c++) {
+    pts[2 * c] = in->lost_host[cand[c].row].rLost;
+    pts[2 * c + 1] = in->lost_host[cand[c].row].zLost;
+  }
+  double *d_pts = in->d_points, *d_E = in->d_points + 2 * in->points_cap;
+  CUDA_TRY(cudaMemcpyAsync(d_pts, pts.data(), sizeof(double) * pts.size(), cudaMemcpyHostToDevice, in->stream));
+  const int rc = in->s32 ? s32_gather_points(&in->dm, &in->s32->f, d_pts, (int)cand.size(), d_E, in->stream)
+                         : spiffe_gather_points64(&in->dm, &in->f, d_pts, (int)cand.size(), d_E, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "field gather failed: %s", cudaGetErrorString((cudaError_t)rc));
+  CUDA_TRY(cudaMemcpyAsync(E.data(), d_E, sizeof(double) * E.size(), cudaMemcpyDeviceToHost, in->stream));
+  RC_TRY(read_counts(in)); // synchronises; the beam's next particle ID
+  long long next_id = in->h_cnt->nextParticleID;
+  const long long id0 = next_id;
+  for (size_t c = 0; c < cand.size(); c++) {
+    const LostRecord &L = in->lost_host[cand[c].row];
+    HostSecondary &SE = in->secondaries[(size_t)cand[c].im];
+    const double Ez = E[2 * c], Er = E[2 * c + 1];
+    const double K = SPIFFE_ME_MEV * 1e6 * (std::sqrt(SE.em * SE.em + 1) - 1);
+    if ((L.code == SPIFFE_GOING_LEFT && (Ez * m.dz * 1e-9) > K) ||
+        (L.code == SPIFFE_GOING_RIGHT && (-1 * Ez * m.dz * 1e-9) > K) ||
+        (L.code == SPIFFE_GOING_DOWN && (Er * m.dr * 1e-9) > K) ||
+        (L.code == SPIFFE_GOING_UP && (-1 * Er * m.dr * 1e-9) > K))
+      continue;
+    SE.qz.push_back(L.zLost);
+    SE.qr.push_back(L.rLost);
+    SE.qp.push_back(L.p);
+    SE.qQ.push_back(L.q);
+    SE.qdir.push_back(L.code);
+    SE.qgen.push_back(L.gen);
+    SE.qid.push_back((int32_t)next_id++);
+  }
+  if (next_id != id0) {
+    in->h_cnt->nextParticleID = next_id;
+    CUDA_TRY(cudaMemcpyAsync(&in->cnt->nextParticleID, &in->h_cnt->nextParticleID, sizeof(long long),
+                             cudaMemcpyHostToDevice, in->stream));
+    CUDA_TRY(cudaStreamSynchronize(in->stream));
+  }
+  return 0;
+}
+
+// After a push: the lost rows feed the secondary-emission queue.
+static int after_push(spiffe_gpu_instance *in)
+{
+  if (in->secondaries.empty())
+    return 0;
+  const size_t first = in->lost_host.size();
+  RC_TRY(fetch_lost(in));
+  RC_TRY(queue_secondaries(in, first));
+  if (!in->lost_user)
+    in->lost_host.clear();
+  return 0;
+}
+
+// inversePoissonCDF (secondaryEmission.c:586-601)
+static long inverse_poisson_cdf(double mu, double C)
+{
+  long r = 0, rMax = (long)(10 * mu);
+  const double expMinusMu = std::exp(-mu);
+  double sum = expMinusMu, term = 1;
+  while (r <= rMax && C > sum) {
+    term *= mu / (++r);
+    sum += term * expMinusMu;
+  }
+  return r;
+}
+
+static double rng_next(spiffe_gpu_instance *in);
+
+// emitSecondaryElectrons (secondaryEmission.c:374-584): each material's queue
+// in order, the number of secondaries of each source from its mean yield
+// (a Poisson draw), each with a random direction away from the surface it
+// hit; the births go to the device as a list.
+static int emit_secondaries(spiffe_gpu_instance *in)
+{
+  const spiffe_mesh &m = in->mesh;
+  for (HostSecondary &SE : in->secondaries) {
+    if (SE.qz.empty())
+      continue;
+    if (SE.verbosity > 0) {
+      printf("%ld secondary emission sources for material %hd\n", (long)SE.qz.size(), (short)SE.material);
+      fflush(stdout);
+    }
+    std::vector<double> col[BIRTH_LIST_COLS];
+    double qmax = 0;
+    long long log_id = 0, logged = 0; // the log takes particle IDs (secondaryEmission.c:541)
+    if (SE.log) {
+      RC_TRY(read_counts(in));
+      log_id = in->h_cnt->nextParticleID;
+    }
+    for (size_t s0 = 0; s0 < SE.qz.size(); s0++) {
+      double gamma = std::sqrt(SE.qp[s0] * SE.qp[s0] + 1);
+      const double K = (gamma - 1) * SPIFFE_ME_MEV * 1e6;
+      // interp(yieldData, energyData, n, K, 0, 1, &code): linear, code 0 outside the table
+      const std::vector<double> &x = SE.E, &y = SE.Y;
+      const long n = (long)x.size();
+      bool ok = true;
+      double Y;
+      if (K <= x[0]) {
+        ok = !(K < x[0]);
+        Y = y[0];
+      } else if (K >= x[(size_t)n - 1]) {
+        ok = !(K > x[(size_t)n - 1]);
+        Y = y[(size_t)n - 1];
+      } else {
+        long lo = 0, hi = n - 1;
+        while (hi - lo > 1) {
+          const long mid = (lo + hi) / 2;
+          if (x[(size_t)mid] <= K)
+            lo = mid;
+          else
+            hi = mid;
+        }
+        Y = y[(size_t)lo] + (y[(size_t)hi] - y[(size_t)lo]) / (x[(size_t)hi] - x[(size_t)lo]) * (K - x[(size_t)lo]);
+      }
+      if (!ok) {
+        if (SE.verbosity > 0) {
+          printf("Secondary yield curve interpolation failed for K=%e eV\n", K);
+          fflush(stdout);
+        }
+        continue;
+      }
+      long total = inverse_poisson_cdf(Y, rng_next(in));
+      if (SE.limit > 0 && total > SE.limit)
+        total = (long)SE.limit;
+      for (long q = 0; q < total; q++) {
+        double theta;
+        switch (SE.qdir[s0]) {
+        case SPIFFE_GOING_RIGHT: // the secondary goes left
+          theta = -rng_next(in) * SPIFFE_PI;
+          break;
+        case SPIFFE_GOING_LEFT:
+          theta = rng_next(in) * SPIFFE_PI;
+          break;
+        case SPIFFE_GOING_UP:
+          theta = rng_next(in) * SPIFFE_PI + SPIFFE_PI / 2;
+          break;
+        case SPIFFE_GOING_DOWN:
+          theta = rng_next(in) * SPIFFE_PI - SPIFFE_PI / 2;
+          break;
+        default:
+          theta = rng_next(in) * SPIFFE_PIx2;
+          break;
+        }
+        const double pz = SE.em * std::sin(theta), pr = SE.em * std::cos(theta);
+        gamma = std::sqrt(pz * pz + pr * pr + 1);
+        const double v[BIRTH_LIST_COLS] = {SE.qz[s0], SE.qr[s0], pz, pr, SPIFFE_C_MKS * pz / gamma,
+                                           SPIFFE_C_MKS * pr / gamma, SE.qQ[s0], m.time, (double)(SE.qgen[s0] + 1),
+                                           (double)SE.qid[s0]};
+        for (int c = 0; c < BIRTH_LIST_COLS; c++)
+          col[c].push_back(v[c]);
+        qmax = std::max(qmax, std::fabs(SE.qQ[s0]));
+      }
+      if (SE.log && total > 0) {
+        const double row[SPIFFE_SECONDARY_LOG_COLS] = {(double)m.time_step, SE.qz[s0], SE.qr[s0], m.time, K, Y,
+                                                       (double)total, (double)SE.qdir[s0], (double)(SE.qgen[s0] + 1),
+                                                       (double)(log_id + logged)};
+        SE.log_rows.insert(SE.log_rows.end(), row, row + SPIFFE_SECONDARY_LOG_COLS);
+        logged++;
+      }
+    }
+    if (logged) {
+      in->h_cnt->nextParticleID = log_id + logged;
+      CUDA_TRY(cudaMemcpyAsync(&in->cnt->nextParticleID, &in->h_cnt->nextParticleID, sizeof(long long),
+                               cudaMemcpyHostToDevice, in->stream));
+      CUDA_TRY(cudaStreamSynchronize(in->stream));
+    }
+    const size_t total = col[0].size();
+    if (total) {
+      if (in->list_cap < total) {
+        cudaFree(in->d_list);
+        in->d_list = nullptr;
+        in->list_cap = std::max<size_t>(total, 1024);
+        CUDA_TRY(cudaMalloc(&in->d_list, sizeof(double) * BIRTH_LIST_COLS * in->list_cap));
+      }
+      std::vector<double> flat;
+      flat.reserve(BIRTH_LIST_COLS * total);
+      for (int c = 0; c < BIRTH_LIST_COLS; c++)
+        flat.insert(flat.end(), col[c].begin(), col[c].end());
+      CUDA_TRY(cudaMemcpyAsync(in->d_list, flat.data(), sizeof(double) * flat.size(), cudaMemcpyHostToDevice,
+                               in->stream));
+      BirthParams p{};
+      p.total = (long long)total;
+      p.mode = SPIFFE_BIRTH_LIST;
+      p.list = in->d_list;
+      p.time = m.time;
+      int rc;
+      if (in->s32) {
+        S32State &S = *in->s32;
+        RC_TRY(s32_cover_charge(in, qmax));
+        rc = s32_births(&in->dm, &S.f, &S.b, &p, in->cnt, &S.sc,
+                        in->space_charge && S.j_state == S32_J_DEPOSITED ? 1 : 0, in->stream);
+      } else {
+        rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+      }
+      if (rc)
+        return fail(SPIFFE_ERR_CUDA, "secondary birth launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+      in->np_upper += (long long)total;
+      CUDA_TRY(cudaStreamSynchronize(in->stream)); // the host list is reused
+    }
+    if (SE.verbosity > 0) {
+      RC_TRY(read_counts(in));
+      printf("Secondary emission increased number of particles from %lld to %lld\n",
+             (long long)(in->h_cnt->np - (long long)total), (long long)in->h_cnt->np);
+      fflush(stdout);
+    }
+    SE.qz.clear();
+    SE.qr.clear();
+    SE.qp.clear();
+    SE.qQ.clear();
+    SE.qdir.clear();
+    SE.qgen.clear();
+    SE.qid.clear();
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_materials(spiffe_gpu_instance *in, const int16_t *material)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (material)
+    in->h_material.assign(material, material + in->nodes);
+  else
+    in->h_material.clear();
+  return 0;
+}
+
+extern "C" int spiffe_gpu_add_secondary_emission(spiffe_gpu_instance *in, const spiffe_secondary_options *o)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  // processSecondaryEmissionDefinition (secondaryEmission.c:21-118)
+  if (o->emitted_momentum < 0)
+    return fail(SPIFFE_ERR_INVALID, "emitted_momentum < 0");
+  if (o->n_data <= 0 || !o->energy || !o->yield)
+    return fail(SPIFFE_ERR_INVALID, "no data in yield file");
+  HostSecondary SE;
+  SE.material = o->material_id;
+  SE.em = o->emitted_momentum;
+  SE.limit = o->yield_limit;
+  SE.verbosity = o->verbosity;
+  SE.E.assign(o->energy, o->energy + o->n_data);
+  SE.Y.assign(o->yield, o->yield + o->n_data);
+  double lo = DBL_MAX, hi = -DBL_MAX;
+  for (double e : SE.E) {
+    lo = e < lo ? e : lo;
+    hi = e > hi ? e : hi;
+  }
+  SE.pMin = std::sqrt((lo / SPIFFE_ME_MEV / 1e6 + 1) * (lo / SPIFFE_ME_MEV / 1e6 + 1) - 1);
+  SE.pMax = std::sqrt((hi / SPIFFE_ME_MEV / 1e6 + 1) * (hi / SPIFFE_ME_MEV / 1e6 + 1) - 1);
+  for (size_t i = 1; i < SE.E.size(); i++)
+    if (SE.E[i - 1] >= SE.E[i])
+      return fail(SPIFFE_ERR_INVALID, "secondary emission data is not ordered by increasing energy values");
+  SE.log = o->log != 0;
+  in->secondaries.push_back(std::move(SE));
+  return lost_log_size(in, std::max<long long>(in->lost_cap, in->capacity));
+}
+
+extern "C" int spiffe_gpu_secondary_log(spiffe_gpu_instance *in, int32_t index, int64_t max_rows, double *rows,
+                                        int64_t *n_rows)
+{
+  if (!in || !n_rows || index < 0 || (size_t)index >= in->secondaries.size())
+    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  std::vector<double> &L = in->secondaries[(size_t)index].log_rows;
+  const int64_t n = (int64_t)(L.size() / SPIFFE_SECONDARY_LOG_COLS);
+  *n_rows = n;
+  if (!rows)
+    return 0;
+  if (n > max_rows)
+    return fail(SPIFFE_ERR_CAPACITY, "%lld emission-log rows do not fit the %lld of the host buffer", (long long)n,
+                (long long)max_rows);
+  std::copy(L.begin(), L.end(), rows);
+  L.clear();
   return 0;
 }
 
@@ -1635,6 +2041,7 @@ static int ensure_bins(spiffe_gpu_instance *in, size_t n)
 static int emit(spiffe_gpu_instance *in)
 {
   PhaseScope ps(in, PH_EMIT);
+  RC_TRY(emit_secondaries(in)); // integrate.c:159-163: before the cathodes
   const spiffe_mesh &m = in->mesh;
   for (HostCathode &c : in->cathodes) {
     if (c.number_per_step == 0 && c.electrons_per_macroparticle == 0)

@@ -170,6 +170,14 @@ struct SessionCathode {
   bool on_device = false;
 };
 
+// one define_secondary_emission definition with its yield table
+struct SessionSecondary {
+  spiffe_secondary_options o{};
+  std::vector<double> E, Y;
+  bool on_device = false;
+  spiffe_sdds::Writer log_out; // log_file, open from the definition on
+};
+
 // one add_on_axis_fields definition: the file's columns and the namelist
 // values, given to the device instance when it exists
 struct SessionOnAxis {
@@ -269,6 +277,8 @@ struct spiffe_session {
   std::map<std::string, std::vector<double>> a; // mesh arrays by FieldSet name
 
   std::vector<SessionCathode> cathodes;
+  std::vector<SessionSecondary> secondaries;
+  std::vector<int16_t> material; // define_geometry's surface materials (materialID)
   std::vector<SessionAntenna> antennas;
   std::vector<SessionOnAxis> onaxis;
   std::vector<OnAxisProfile> onaxis_prepared; // for the fields_used output
@@ -361,6 +371,7 @@ struct spiffe_session {
   int cmd_on_axis_fields(Args &g);
   int cmd_translate(Args &g);
   int cmd_screen(Args &g);
+  int cmd_secondary_emission(Args &g);
   int cmd_test_beam(Args &g);
   int cmd_poisson(Args &g);
   int cmd_load_fields(Args &g);
@@ -376,6 +387,7 @@ struct spiffe_session {
   int output_fields(long long step, double time);
   int flush_screens(long long step, double time);
   int flush_lost();
+  int flush_secondary_logs();
   int status(long long step, double time);
   int write_status();
 };
@@ -473,10 +485,11 @@ int spiffe_session::cmd_geometry(Args &g)
   mesh = m;
   const size_t n = nodes();
   flags.assign(n, 0);
+  material.assign(n, 0);
   a.clear();
   a["PsiImposed"].assign(n, 0.0);
   spiffe_geometry_options go{m.nz, m.nr, zmin, zmax, rmax, zr_factor};
-  S_TRY(spiffe_geometry_rasterise(&go, text.c_str(), flags.data(), a["PsiImposed"].data(), nullptr));
+  S_TRY(spiffe_geometry_rasterise(&go, text.c_str(), flags.data(), a["PsiImposed"].data(), material.data()));
   // the arrays of geometry.c:78-116 that the device problem holds
   for (const char *x : {"EzImposed", "ErImposed", "Q", "Jz"})
     a[x].assign(n, 0.0);
@@ -839,6 +852,109 @@ int spiffe_session::cmd_antenna(Args &g)
 // --------------------------------------------------------------- define_screen
 
 // process_screen_definition, screens.c:29-117
+// processSecondaryEmissionDefinition, secondaryEmission.c:21-118
+int spiffe_session::cmd_secondary_emission(Args &g)
+{
+  std::string input_file, energy_col, yield_col, log_file;
+  double yield_limit = 0, emitted_momentum = 0;
+  long long verbosity = 1, material_id = 1;
+  const bool have_input = g.str("input_file", input_file);
+  const bool have_energy = g.str("kinetic_energy_column", energy_col);
+  const bool have_yield = g.str("yield_column", yield_col);
+  g.num("yield_limit", yield_limit);
+  g.num("emitted_momentum", emitted_momentum);
+  g.integer("verbosity", verbosity);
+  g.integer("material_id", material_id);
+  const bool have_log = g.str("log_file", log_file);
+  S_TRY(g.finish());
+  if (!have_input || input_file.empty())
+    return serr(SPIFFE_ERR_INVALID, "supply an input file");
+  if (!have_energy || energy_col.empty())
+    return serr(SPIFFE_ERR_INVALID, "supply the name of a column containing energy values");
+  if (!have_yield || yield_col.empty())
+    return serr(SPIFFE_ERR_INVALID, "supply the name of a column containing yield values");
+  if (emitted_momentum < 0)
+    return serr(SPIFFE_ERR_INVALID, "emitted_momentum < 0");
+  std::vector<std::vector<double>> cols;
+  std::string err;
+  if (!spiffe_sdds::read_columns(input_file, {energy_col, yield_col}, cols, err))
+    return serr(SPIFFE_ERR_INVALID, "problem reading secondary emission yield data file: %s", err.c_str());
+  if (cols[0].empty())
+    return serr(SPIFFE_ERR_INVALID, "no data in yield file");
+  SessionSecondary d;
+  d.o.material_id = (int32_t)material_id;
+  d.o.verbosity = (int32_t)verbosity;
+  d.o.emitted_momentum = emitted_momentum;
+  d.o.yield_limit = (int64_t)yield_limit;
+  d.E = cols[0];
+  d.Y = cols[1];
+  for (size_t i = 1; i < d.E.size(); i++)
+    if (d.E[i - 1] >= d.E[i])
+      return serr(SPIFFE_ERR_INVALID, "secondary emission data is not ordered by increasing energy values");
+  if (have_log && !log_file.empty()) { // :91-114
+    using namespace spiffe_sdds;
+    const std::vector<Def> lc = {Def{"z", "m", "", T_FLOAT},      Def{"r", "m", "", T_FLOAT},
+                                 Def{"t", "s", "", T_FLOAT},      Def{"K", "eV", "", T_FLOAT},
+                                 Def{"yield", "", "", T_FLOAT},   Def{"emitted", "", "", T_SHORT},
+                                 Def{"directionCode", "", "", T_SHORT}, Def{"generation", "", "", T_SHORT},
+                                 Def{"particleID", "", "", T_LONG}};
+    if (!d.log_out.open(compose(log_file, rootname), "Primary/secondary activity due to material " + input_file + "\n",
+                        "", {}, lc, err))
+      return serr(SPIFFE_ERR_INVALID, "define_secondary_emission log_file: %s", err.c_str());
+    d.o.log = 1;
+  }
+  secondaries.push_back(std::move(d));
+  return 0;
+}
+
+// The secondary-emission log pages since the last flush: one page per
+// definition and emitting step (secondaryEmission.c:548-563).  The particleID
+// column holds the IDs the log took (:541); the reference hands the short
+// generation buffer to that long column (:557), which reads past its values.
+int spiffe_session::flush_secondary_logs()
+{
+  for (size_t k = 0; k < secondaries.size(); k++) {
+    SessionSecondary &d = secondaries[k];
+    if (!d.log_out.is_open() || !d.on_device)
+      continue;
+    int64_t n = 0;
+    S_TRY(spiffe_gpu_secondary_log(inst, (int32_t)k, 0, nullptr, &n));
+    if (!n)
+      continue;
+    std::vector<double> rows((size_t)n * SPIFFE_SECONDARY_LOG_COLS);
+    S_TRY(spiffe_gpu_secondary_log(inst, (int32_t)k, n, rows.data(), &n));
+    const size_t C = SPIFFE_SECONDARY_LOG_COLS;
+    for (size_t a = 0; a < (size_t)n;) {
+      size_t b = a;
+      while (b < (size_t)n && rows[b * C] == rows[a * C])
+        b++;
+      const size_t m = b - a;
+      std::vector<float> f[5];
+      std::vector<int16_t> h[3];
+      std::vector<int32_t> id(m);
+      for (size_t i = 0; i < m; i++) {
+        const double *r = &rows[(a + i) * C];
+        for (int c = 0; c < 5; c++)
+          f[c].push_back((float)r[1 + c]);
+        for (int c = 0; c < 3; c++)
+          h[c].push_back((int16_t)r[6 + c]);
+        id[i] = (int32_t)r[9];
+      }
+      std::vector<const void *> cols;
+      for (int c = 0; c < 5; c++)
+        cols.push_back(f[c].data());
+      for (int c = 0; c < 3; c++)
+        cols.push_back(h[c].data());
+      cols.push_back(id.data());
+      std::string err;
+      if (!d.log_out.write_page({}, {}, (int64_t)m, cols, err))
+        return serr(SPIFFE_ERR_INVALID, "define_secondary_emission log_file: %s", err.c_str());
+      a = b;
+    }
+  }
+  return 0;
+}
+
 int spiffe_session::cmd_screen(Args &g)
 {
   std::string filename, templ, direction = "forward";
@@ -1471,6 +1587,17 @@ int spiffe_session::ensure_instance()
       S_TRY(spiffe_gpu_add_cathode(inst, &o));
       c.on_device = true;
     }
+  if (!secondaries.empty() && !material.empty())
+    S_TRY(spiffe_gpu_set_materials(inst, material.data()));
+  for (SessionSecondary &d : secondaries)
+    if (!d.on_device) {
+      spiffe_secondary_options o = d.o;
+      o.n_data = (int64_t)d.E.size();
+      o.energy = d.E.data();
+      o.yield = d.Y.data();
+      S_TRY(spiffe_gpu_add_secondary_emission(inst, &o));
+      d.on_device = true;
+    }
   for (SessionAntenna &an : antennas)
     if (!an.on_device) {
       S_TRY(spiffe_gpu_add_antenna(inst, an.direction, an.istart, an.iend, an.iposition, an.current, an.frequency,
@@ -1806,6 +1933,7 @@ int spiffe_session::cmd_integrate(Args &g)
     steps += next - k;
     S_TRY(flush_screens(next - 1, (next - 1) * step_dt + t0));
     S_TRY(flush_lost());
+    S_TRY(flush_secondary_logs());
     k = next;
   }
   if (lost_on) { // SDDS_Terminate, integrate.c:203
@@ -1878,8 +2006,9 @@ int spiffe_session::execute(const std::string &text)
       rc = 0;
     } else if (c == "translate") {
       rc = cmd_translate(g);
-    } else if (c == "define_resistor" || c == "load_particles" ||
-               c == "define_secondary_emission" || c == "define_emitter") {
+    } else if (c == "define_secondary_emission") {
+      rc = cmd_secondary_emission(g);
+    } else if (c == "define_resistor" || c == "load_particles" || c == "define_emitter") {
       rc = serr(SPIFFE_ERR_UNSUPPORTED, "%s is not supported", c.c_str());
     } else {
       rc = serr(SPIFFE_ERR_INVALID, "unknown namelist %s given", c.c_str());

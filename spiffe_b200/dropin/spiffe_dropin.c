@@ -29,8 +29,11 @@
  * mirroring a problem is kept per FIELDS pointer (and created again when the
  * beam outgrows it); it uses the FP64 form, whose arithmetic is the
  * reference's, with the reference's compaction and screen-momentum
- * behaviour and the ordered deposition.  Errors call bomb() as the
- * reference does.  Not available: secondary emission and on-axis fields.
+ * behaviour and the ordered deposition.  Secondary emission stays the
+ * reference's: the device reports each lost particle's loss point and the
+ * reference's queueSecondaryEmission and emitSecondaryElectrons (which
+ * appends to the host beam) do the rest.  Errors call bomb() as the
+ * reference does.  Not available: on-axis fields.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -370,19 +373,30 @@ static void screen_buffers(Mirror *M, int64_t capacity)
 /* this push's lost particles into the lost-particle table, row by row in
  * pages of at most 1000 rows, as advance_particles.c:450-487 and :529-535
  * write them */
-static void write_lost(Mirror *M, SDDS_DATASET *SDDSlost, FIELDS *EM_problem)
+/* The push's lost particles, in the order of advance_particles.c:437-491:
+ * each one queued for secondary emission (the reference's own
+ * queueSecondaryEmission, with the loss point, impact momentum and side the
+ * device found) and written to the lost-particle file.  Runs after the beam
+ * came back, since the queue takes particle IDs from beam->nextParticleID. */
+static void handle_lost(Mirror *M, SDDS_DATASET *SDDSlost, FIELDS *EM_problem, BEAM *beam,
+                        SECONDARY_EMISSION *secondaryEmission, long nSecondaryDefns)
 {
   int64_t cap = M->capacity;
-  double *v = malloc(sizeof(double) * 8 * (size_t)cap);
-  int16_t *gen = malloc(sizeof(int16_t) * (size_t)cap);
+  double *v = malloc(sizeof(double) * 9 * (size_t)cap);
+  int16_t *gen = malloc(sizeof(int16_t) * 2 * (size_t)cap);
   int32_t *id = malloc(sizeof(int32_t) * (size_t)cap);
   if (!v || !gen || !id)
     bomb("memory allocation failure (spiffe drop-in)", NULL);
   spiffe_lost_set h = {0, cap, v, v + cap, v + 2 * cap, v + 3 * cap, v + 4 * cap, v + 5 * cap, v + 6 * cap,
-                       v + 7 * cap, gen, id, NULL};
+                       v + 7 * cap, gen, id, NULL, v + 8 * cap, gen + cap};
   check(spiffe_gpu_download_lost(M->inst, &h), "spiffe drop-in: lost particles");
   long newLost = 0, maxLost = 0;
   for (int64_t k = 0; k < h.nb; k++) {
+    if (nSecondaryDefns)
+      queueSecondaryEmission(secondaryEmission, nSecondaryDefns, h.p[k], h.zLost[k], h.rLost[k], h.direction[k],
+                             h.q[k], h.generation[k], EM_problem, beam);
+    if (!SDDSlost)
+      continue;
     if (newLost && newLost >= maxLost) {
       if (!SDDS_WritePage(SDDSlost)) {
         SDDS_SetError("Problem writing lost particle data.");
@@ -403,7 +417,7 @@ static void write_lost(Mirror *M, SDDS_DATASET *SDDSlost, FIELDS *EM_problem)
     }
     newLost++;
   }
-  if (newLost && !SDDS_WritePage(SDDSlost)) {
+  if (SDDSlost && newLost && !SDDS_WritePage(SDDSlost)) {
     SDDS_SetError("Problem writing lost particle data.");
     SDDS_PrintErrors(stderr, SDDS_EXIT_PrintErrors | SDDS_VERBOSE_PrintErrors);
   }
@@ -440,8 +454,8 @@ void advance_particles(BEAM *beam, FIELDS *EM_problem, TEST_BEAM_DEFN *test_beam
                        long n_screens, SDDS_DATASET *SDDSlost, double zForcesStart,
                        SECONDARY_EMISSION *secondaryEmission, long nSecondaryDefns)
 {
-  if (secondaryEmission && nSecondaryDefns > 0)
-    bomb("secondary emission is not available in the spiffe drop-in", NULL);
+  if (!secondaryEmission)
+    nSecondaryDefns = 0;
   if (EM_problem->onAxisFields > 0)
     bomb("on-axis fields are not available in the spiffe drop-in", NULL);
   if (n_screens > SPIFFE_MAX_SCREENS)
@@ -480,14 +494,14 @@ void advance_particles(BEAM *beam, FIELDS *EM_problem, TEST_BEAM_DEFN *test_beam
   }
   o.compaction = SPIFFE_COMPACT_REFERENCE;
   o.screen_momentum = SPIFFE_SCREEN_REFERENCE;
-  if (SDDSlost && !M->lost_on) {
+  if ((SDDSlost || nSecondaryDefns) && !M->lost_on) {
     check(spiffe_gpu_set_lost_log(M->inst, M->capacity), "spiffe drop-in: lost-particle log");
     M->lost_on = 1;
   }
   check(spiffe_gpu_advance_particles(M->inst, &o), "advance_particles");
-  if (SDDSlost)
-    write_lost(M, SDDSlost, EM_problem);
   beam_download(M, beam);
+  if (M->lost_on)
+    handle_lost(M, SDDSlost, EM_problem, beam, secondaryEmission, nSecondaryDefns);
   /* this push's screen records into the reference's buffers, then its page */
   for (long is = 0; is < n_screens; is++) {
     SCREEN *sc = screen_defn + is;

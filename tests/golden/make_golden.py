@@ -312,6 +312,58 @@ def deck_lost(geo):
          **{"lost_" + k: lost[k] for k in LOST_COLUMNS}, **beam_out(rb))
 
 
+# Secondary emission (secondaryEmission.c): the lost-particle deck with the
+# anode's face and hole edge drawn as material 1 (the &po material_id), a
+# yield table in eV and secondaries of beta*gamma 0.01 released away from
+# the surface; the gap field drives them back into the anode, so generations
+# cascade: the primaries (300 keV) release about 2.5 each, the returning
+# low-energy secondaries (tens of eV) fewer than one; at most 3 per source.
+DECK_SECONDARY = DECK_LOST.replace(
+    "&integrate", '&define_secondary_emission input_file="yield.sdds", kinetic_energy_column="K", '
+    'yield_column="Y", emitted_momentum=0.01, yield_limit=3, verbosity=0, log_file="%s.sel" &end\n&integrate')
+SECONDARY_LOG_COLUMNS = ["z", "r", "t", "K", "yield", "emitted", "directionCode", "generation"]
+SECONDARY_YIELD = (np.array([0.0, 10.0, 50.0, 200.0, 1e3, 1e4, 1e5, 5e5, 2e6]),
+                   np.array([0.0, 0.5, 0.9, 0.9, 1.0, 1.5, 2.0, 2.5, 2.0]))
+
+
+def secondary_geo(geo):
+    """The DC gun boundary with material_id=1 on the anode's face and hole edge."""
+    out = []
+    for line in geo.splitlines():
+        if line.startswith("&po x=0.01, y=0.003,") or line.startswith("&po x=0.0102, y=0.003,"):
+            line = line.replace(" &end", ", material_id=1 &end")
+        out.append(line)
+    assert sum("material_id" in x for x in out) == 2
+    return "\n".join(out) + "\n"
+
+
+def write_yield(path):
+    with open(path, "w") as f:
+        f.write("SDDS1\n&column name=K type=double units=eV &end\n&column name=Y type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(*SECONDARY_YIELD):
+            f.write("%.17g %.17g\n" % (a, b))
+
+
+def deck_secondary(geo):
+    geo = secondary_geo(geo)
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    write_yield(os.path.join(d, "yield.sdds"))
+    cmds = [b.strip() + " &end" for b in DECK_SECONDARY.split("&end") if b.strip()]
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("table", 2, LOST_COLUMNS), ("get_beam",),
+                                                                   ("screen", 0),
+                                                                   ("table", 200, SECONDARY_LOG_COLUMNS)],
+                                 cwd=d, capacity=40000)
+    lost, rb, rs, sel = res
+    out = dict(deck=np.array(DECK_SECONDARY), geo=np.array(geo), yield_K=SECONDARY_YIELD[0],
+               yield_Y=SECONDARY_YIELD[1], lost_pages=lost["pages"], **{"lost_" + k: lost[k] for k in LOST_COLUMNS},
+               **beam_out(rb), log_pages=sel["pages"], **{"log_" + k: sel[k] for k in SECONDARY_LOG_COLUMNS})
+    out.update({"screen0_" + k: v for k, v in rs.items()})
+    save("deck_secondary", **out)
+
+
 # The DC gun deck with define_field_saving (field_saving.c:46-213): saves at
 # 0 and 100 ps and before exiting.  The saved columns are compared through
 # SHA-256 digests of their values (bit-for-bit equality needs nothing more,
@@ -423,6 +475,7 @@ def decks():
     deck_status(geo)
     deck_lost(geo)
     deck_fieldsave(geo)
+    deck_secondary(geo)
 
 
 def deck_onaxis(geo):
@@ -452,6 +505,8 @@ if __name__ == "__main__":
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["fieldsave"]:
         deck_fieldsave(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["secondary"]:
+        deck_secondary(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["lost"]:
         deck_lost(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["te"]:

@@ -126,3 +126,30 @@ def test_lost_particle_file(tmp_path):
     assert lost["pages"] == int(fx["lost_pages"])
     for c in cols:
         assert np.array_equal(lost[c], fx["lost_" + c]), c
+
+
+def test_secondary_emission(tmp_path):
+    """Secondary emission through the drop-in: the device pushes and reports
+    each lost particle's loss point, impact momentum and side; the
+    reference's own queueSecondaryEmission and emitSecondaryElectrons do the
+    rest on the host beam.  The lost-particle file and the final beam equal
+    the pure reference run's."""
+    fx = load("deck_secondary")
+    d = str(tmp_path)
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(str(fx["geo"]))
+    with open(os.path.join(d, "yield.sdds"), "w") as f:
+        f.write("SDDS1\n&column name=K type=double units=eV &end\n&column name=Y type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(fx["yield_K"], fx["yield_Y"]):
+            f.write("%.17g %.17g\n" % (a, b))
+    cmds = [b.strip() + " &end" for b in str(fx["deck"]).split("&end") if b.strip()]
+    cols = ["t", "rLost", "zLost", "pz", "pr", "z0", "r0", "q", "generation", "particleID"]
+    lost, rb = run_with_dropin([("command", c) for c in cmds] + [("table", 2, cols), ("get_beam",)], d,
+                               capacity=40000)
+    assert lost["pages"] == int(fx["lost_pages"])
+    for c in cols:
+        assert np.array_equal(lost[c], fx["lost_" + c]), c
+    assert rb["np"] == int(fx["out_np"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(rb[k], fx["out_" + k]), k

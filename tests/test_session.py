@@ -654,6 +654,74 @@ def test_lost_particle_file_split_form(tmp_path, monkeypatch):
     s.close()
 
 
+def write_yield(tmp_path, fx):
+    with open(tmp_path / "yield.sdds", "w") as f:
+        f.write("SDDS1\n&column name=K type=double units=eV &end\n&column name=Y type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(fx["yield_K"], fx["yield_Y"]):
+            f.write("%.17g %.17g\n" % (a, b))
+
+
+@pytest.mark.gpu
+def test_secondary_emission_matches_reference(tmp_path, monkeypatch):
+    """define_secondary_emission (secondaryEmission.c) on the lost-particle
+    deck with the anode drawn as material 1: primaries that hit it release
+    secondaries (a Poisson number from the yield table, random directions
+    away from the face) that fall back and release more.  In the FP64 form
+    the lost-particle file (every generation), the final beam and the screen
+    equal the reference's bit for bit, so the queue, the yield draw, the
+    directions and the shared random stream all follow the reference, and
+    the emission log (log_file, which takes particle IDs) does too."""
+    fx = load("deck_secondary")
+    write_yield(tmp_path, fx)
+    s = run_deck(fx, tmp_path, monkeypatch)
+    pages = session.read_sdds(str(tmp_path / "spiffe.lost"))
+    got = {c: np.concatenate([p["columns"][c] for p in pages]) for c in LOST_COLUMNS}
+    assert len(pages) == int(fx["lost_pages"])
+    assert len(got["t"]) == len(fx["lost_t"])
+    assert np.max(fx["lost_generation"]) >= 3
+    for c in LOST_COLUMNS:
+        assert np.array_equal(np.asarray(got[c], np.float64), fx["lost_" + c]), c
+    g = s.instance()
+    b = g.download_beam(abi.Beam(max(int(fx["out_np"]), 1) + 16))
+    assert b.np == int(fx["out_np"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k][: b.np], fx["out_" + k]), k
+    # the log_file: a page per emitting step, a row per emitting source
+    log = session.read_sdds(str(tmp_path / "spiffe.sel"))
+    assert len(log) == int(fx["log_pages"])
+    for c in ("z", "r", "t", "K", "yield", "emitted", "directionCode", "generation"):
+        v = np.concatenate([np.asarray(p["columns"][c], np.float64) for p in log])
+        assert np.array_equal(v, fx["log_" + c]), c
+    s.close()
+
+
+@pytest.mark.gpu
+def test_secondary_emission_split_form(tmp_path, monkeypatch):
+    """The same deck in the split form: the primaries hit the anode on the
+    reference's step and release secondaries of generation 1 and higher,
+    which are lost on the anode face (z = 10 mm) in turn."""
+    fx = load("deck_secondary")
+    write_yield(tmp_path, fx)
+    s = run_deck(fx, tmp_path, monkeypatch, precision="split32")
+    pages = session.read_sdds(str(tmp_path / "spiffe.lost"))
+    got = {c: np.concatenate([p["columns"][c] for p in pages]) for c in LOST_COLUMNS}
+    gen = np.asarray(got["generation"])
+    prim = gen == 0
+    ref_prim = fx["lost_generation"] == 0
+    assert prim.sum() >= ref_prim.sum()
+    assert abs(np.min(got["t"][prim]) - np.min(fx["lost_t"][ref_prim])) <= 4.1e-13
+    sec = ~prim
+    assert sec.sum() >= 0.5 * (~ref_prim).sum() and gen.max() >= 2
+    on_anode = np.abs(got["zLost"][sec] - 0.01) < 1e-6
+    assert on_anode.mean() > 0.9
+    # secondary IDs are new, and each generation is lost after the one before it
+    assert not np.intersect1d(got["particleID"][sec], got["particleID"][prim]).size
+    for k in range(1, int(gen.max()) + 1):
+        assert got["t"][gen == k].min() > got["t"][gen == k - 1].min()
+    s.close()
+
+
 @pytest.mark.gpu
 def test_field_saves_match_reference(tmp_path, monkeypatch):
     """define_field_saving (field_saving.c:46-213) on the DC gun deck in the
