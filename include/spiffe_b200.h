@@ -155,6 +155,13 @@ int spiffe_gpu_screen_moments(spiffe_gpu_instance *inst, int32_t screen, double 
 /* define_cathode (cathode.c:21) and define_antenna (antenna.c:18) for the
  * device integration loop; waveform times must already include time_offset. */
 int spiffe_gpu_add_cathode(spiffe_gpu_instance *inst, const spiffe_cathode_options *opt);
+/* define_emitter (emitter.c:19-167): each step of spiffe_gpu_run_steps emits
+ * from every segment of the surface after the cathodes
+ * (emit_electrons_from_emitter, :169-390; integrate.c:164-165) and updates
+ * the current density from the fields after the step (setEmitterCurrentDensity,
+ * :392-440; integrate.c:132-133, :192-193), drawing positions from the
+ * second generator (random_2), reseeded by each definition. */
+int spiffe_gpu_add_emitter(spiffe_gpu_instance *inst, const spiffe_emitter_options *opt);
 int spiffe_gpu_add_antenna(spiffe_gpu_instance *inst, int32_t direction, int64_t istart, int64_t iend,
                            int64_t iposition, double current, double frequency, double phase, const double *t,
                            const double *W, int64_t n_points);

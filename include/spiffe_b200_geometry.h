@@ -30,6 +30,17 @@ typedef struct spiffe_geometry_options {
 int spiffe_geometry_rasterise(const spiffe_geometry_options *opt, const char *boundary_text, int16_t *flags,
                               double *psi_imposed, int16_t *material);
 
+/* getBoundaryPoints (grid_drawing.c:541-760), the surface a define_emitter of
+ * `material_id` emits from: the nodes of the first run of boundary points of
+ * that material (in drawing order, corners inserted so that one index changes
+ * at a time) and, per segment k -> k+1, the side it emits to (direction[k],
+ * SPIFFE_EMITS_* of spiffe_b200_types.h; the last entry unused).  *n_points is 0 when no boundary
+ * point has the material.  With iz, ir and direction all NULL only
+ * *n_points is set. */
+int spiffe_geometry_boundary_points(const spiffe_geometry_options *opt, const char *boundary_text, int32_t material_id,
+                                    int64_t max_points, int32_t *iz, int32_t *ir, int16_t *direction,
+                                    int64_t *n_points);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,13 @@ SPIFFE_HD uint64_t spiffe_rng_key(uint64_t seed)
   return spiffe_rng_mix64(seed * 0x9E3779B97F4A7C15ULL + 0x632BE59BD9B4E019ULL);
 }
 
+/* stream key of a seed for the second generator, as random_2(-seed) sets it
+ * (emitter.c:63; the surface emitters draw from it) */
+SPIFFE_HD uint64_t spiffe_rng_key2(uint64_t seed)
+{
+  return spiffe_rng_mix64(seed * 0x9E3779B97F4A7C15ULL + 0xD1B54A32D192ED03ULL);
+}
+
 /* draw number k >= 1 of the stream */
 SPIFFE_HD double spiffe_rng_uniform(uint64_t key, uint64_t k)
 {

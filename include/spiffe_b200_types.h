@@ -211,6 +211,31 @@ typedef struct spiffe_cathode_options {
   const double *profile_t, *profile_A;
 } spiffe_cathode_options;
 
+/* define_emitter (emitter.nl; process_emitter_definition, emitter.c:19-167):
+ * emission from the boundary segments of one material (the points and
+ * directions of spiffe_geometry_boundary_points), at a current density given,
+ * from the Richardson-Schottky law (temperature and work_function) or from
+ * field emission, scaled by an optional time profile. */
+#define SPIFFE_EMITS_RIGHT 1 /* the side a boundary segment emits to (spiffe.h:270-273) */
+#define SPIFFE_EMITS_UP 2
+#define SPIFFE_EMITS_LEFT 3
+#define SPIFFE_EMITS_DOWN 4
+typedef struct spiffe_emitter_options {
+  int32_t material_id;
+  double current_density, temperature, work_function; /* temperature already determined */
+  int32_t field_emission;
+  double field_emission_beta;
+  double electrons_per_macroparticle;
+  double start_time, stop_time;
+  double initial_p, offset_factor;
+  int32_t random_number_seed; /* random_2(-|seed|) */
+  int32_t n_profile;
+  const double *profile_t, *profile_A;
+  int64_t n_points;           /* boundary nodes, direction per segment */
+  const int32_t *iz, *ir;
+  const int16_t *direction;
+} spiffe_emitter_options;
+
 /* Result of one Poisson correction (the quantities the reference prints,
  * poisson_correction.c:254-256, :284). */
 typedef struct spiffe_poisson_report {

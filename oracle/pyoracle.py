@@ -210,6 +210,8 @@ def _ref_lib():
     lib.ref_field_energy.argtypes = [P(C.c_double)]
     lib.ref_time_step.restype = C.c_int64
     lib.ref_rng_counter.restype = C.c_uint64
+    lib.ref_boundary_points.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]
+    lib.ref_boundary_points.restype = C.c_long
     return lib
 
 
@@ -329,6 +331,11 @@ def _child(program, capacity, cwd, preload=()):
             e = (C.c_double * 2)()
             lib.ref_field_energy(e)
             out.append((e[0], e[1]))
+        elif kind == "boundary_points":
+            mx = 1 << 16
+            iz, ir, d = np.zeros(mx, np.int32), np.zeros(mx, np.int32), np.zeros(mx, np.int16)
+            n = lib.ref_boundary_points(args[0], iz.ctypes.data, ir.ctypes.data, d.ctypes.data, mx)
+            out.append((iz[:n].copy(), ir[:n].copy(), d[:n].copy()))
         elif kind == "rng_counter":
             out.append(lib.ref_rng_counter())
         elif kind == "time_steps":

@@ -35,6 +35,8 @@ static FIELD_OUTPUT field_output_defn;
 static SNAPSHOT snapshot_defn;
 static SECONDARY_EMISSION *secondary = NULL;
 static long n_secondary = 0;
+static EMITTER *emitter = NULL;
+static long n_emitters = 0;
 static int initialized = 0;
 
 /* capacity of every particle and screen array: the reference sizes screen
@@ -112,12 +114,18 @@ int ref_command(const char *text)
     process_on_axis_field_definition(&EM, &nl);
   else if (strcmp(nl.group_name, "define_test_beam") == 0)
     process_testbeam_definition(&test_beam_defn, &EM, &nl);
-  else if (strcmp(nl.group_name, "define_secondary_emission") == 0)
+  else if (strcmp(nl.group_name, "define_emitter") == 0) {
+    process_emitter_definition(&EM, &emitter, &n_emitters, &nl);
+    /* the definition leaves stop_step unset (emitter.c:65-90) and the first
+     * emission call compares it (:186): fresh heap memory holds 0 there, and
+     * the checker makes it so every time */
+    emitter[n_emitters - 1].stop_step = 0;
+  } else if (strcmp(nl.group_name, "define_secondary_emission") == 0)
     processSecondaryEmissionDefinition(&secondary, &n_secondary, &nl, &EM);
   else if (strcmp(nl.group_name, "integrate") == 0)
     perform_integration(&EM, &beam, cathode, cathodes, &test_beam_defn, antenna, n_antennae, &resistor_defns,
                         NULL, 0, &saving_defn, &snapshot_defn, screen_defn, n_screen_defns,
-                        &field_output_defn, secondary, n_secondary, NULL, 0, &nl);
+                        &field_output_defn, secondary, n_secondary, emitter, n_emitters, &nl);
   else
     rc = -1;
   free_namelist_text(&nl);
@@ -127,6 +135,25 @@ int ref_command(const char *text)
     exit(3);
   }
   return rc;
+}
+
+/* getBoundaryPoints (grid_drawing.c:541-760) of the last define_geometry:
+ * the emitter surface of `material`, up to `max` nodes; the direction of the
+ * last node, which the reference leaves unset, is reported as 0 */
+long ref_boundary_points(long material, int32_t *iz, int32_t *ir, int16_t *dir, long max)
+{
+  long *z = NULL, *r = NULL, i, n;
+  short *d = NULL;
+  n = getBoundaryPoints(material, &z, &r, &d);
+  for (i = 0; i < n && i < max; i++) {
+    iz[i] = (int32_t)z[i];
+    ir[i] = (int32_t)r[i];
+    dir[i] = i < n - 1 ? d[i] : 0;
+  }
+  free(z);
+  free(r);
+  free(d);
+  return n;
 }
 
 /* ------------------------------------------------------------------ mesh */

@@ -56,6 +56,7 @@ void **zarray_2d(uint64_t size, uint64_t n1, uint64_t n2);
 int free_zarray_2d(void **array, uint64_t n1, uint64_t n2);
 
 double random_1(long iseed);
+double random_2(long iseed);
 double gauss_rn_lim(double mean, double sigma, double limit_in_sigmas, double (*urandom)(long iseed));
 int32_t startHaltonSequence(int32_t *radix, double value);
 double nextHaltonSequencePoint(long ID);

@@ -95,6 +95,21 @@ double random_1(long iseed)
   return (double)(rng_mix64(rng_key + rng_counter * 0x9E3779B97F4A7C15ULL) >> 11) * 0x1.0p-53;
 }
 
+/* random_2, the second stream (the surface emitters', emitter.c:63, :276,
+ * :306, :328): the same generator under another key derivation */
+static uint64_t rng2_key = 0, rng2_counter = 0;
+
+double random_2(long iseed)
+{
+  if (iseed < 0) {
+    rng2_key = rng_mix64((uint64_t)(-iseed) * 0x9E3779B97F4A7C15ULL + 0xD1B54A32D192ED03ULL);
+    rng2_counter = 0;
+    return 0.0;
+  }
+  rng2_counter++;
+  return (double)(rng_mix64(rng2_key + rng2_counter * 0x9E3779B97F4A7C15ULL) >> 11) * 0x1.0p-53;
+}
+
 /* checker hook: position of the shared stream */
 uint64_t shim_rng_counter(void) { return rng_counter; }
 

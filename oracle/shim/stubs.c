@@ -2,9 +2,9 @@
  *
  * No-op stand-ins for reference functions that perform_integration()
  * (integrate.c:149-193) calls every step but that lie outside the checked
- * path: field sampling and saving, arbitrary-surface emitters, resistors and
- * the moving window (beam snapshots and field output are the reference's own
- * snapshots.c and field_output.c).  Each is inert when its
+ * path: field sampling and resistors (beam snapshots, field output, field
+ * saving, surface emitters and the moving window are the reference's own
+ * files).  Each is inert when its
  * command was never given, which is how the checked configurations run; the
  * ones that would act bomb instead, so a checker can never silently skip
  * work.  compose_filename() stands in for the one in spiffe.c, which is not
@@ -29,21 +29,6 @@ void sample_fields(SAMPLE_DEFN *sample_defn, long n_sample_defns, FIELDS *EM_pro
   (void)EM_problem;
   if (n_sample_defns)
     bomb("field sampling is not part of the checked path", NULL);
-}
-
-void emit_electrons_from_emitter(BEAM *beam, EMITTER *emitter, FIELDS *EM_problem)
-{
-  (void)beam;
-  (void)emitter;
-  (void)EM_problem;
-  bomb("surface emitters are not part of the checked path", NULL);
-}
-
-void setEmitterCurrentDensity(EMITTER *emitter, FIELDS *EM_problem)
-{
-  (void)emitter;
-  (void)EM_problem;
-  bomb("surface emitters are not part of the checked path", NULL);
 }
 
 void add_resistor_currents(FIELDS *EM_problem, RESISTOR *resistor)

@@ -45,6 +45,8 @@ struct Canvas {
   double *potential;
   int16_t *material;
   std::vector<double> xb, yb;
+  std::vector<long> ixb, iyb; // the node of each boundary point (ix_dbnd, iy_dbnd)
+  std::vector<short> mb;      // that node's material (material_bnd)
   long n_outside = 0;
   bool vacuum_defined = false;
   int ix_vac = 0, iy_vac = 0;
@@ -59,16 +61,21 @@ struct Canvas {
     if (!xb.empty() && xb.back() == x && yb.back() == y)
       return;
     const int i = (int)((x - xmin) / dx + 0.5), j = (int)((y - ymin) / dy + 0.5);
+    short m = 0;
     if (i >= 0 && j >= 0 && i < nx && j < ny) {
       L(i, j) = SPIFFE_FL_IS_SURFACE;
       Pt(i, j) = pot;
       if (Mt(i, j) == 0)
         Mt(i, j) = mat;
+      m = Mt(i, j);
     } else {
-      n_outside++;
+      n_outside++; // (the reference reads the material outside the lattice here)
     }
     xb.push_back(x);
     yb.push_back(y);
+    ixb.push_back(i);
+    iyb.push_back(j);
+    mb.push_back(m);
   }
 
   // draw_line, grid_drawing.c:215-295
@@ -290,8 +297,166 @@ using spiffe_nl::next_block;
 
 } // namespace
 
+static int rasterise(const spiffe_geometry_options *o, const char *text, int16_t *flags, double *psi,
+                     int16_t *material, Canvas &c);
+
 extern "C" int spiffe_geometry_rasterise(const spiffe_geometry_options *o, const char *text, int16_t *flags,
                                          double *psi, int16_t *material)
+{
+  Canvas c;
+  return rasterise(o, text, flags, psi, material, c);
+}
+
+// getBoundaryPoints, grid_drawing.c:541-760: the first run of consecutive
+// boundary points of material `id`, as nodes without repeats; a corner node
+// inserted wherever both indices change (passes repeat until none is added);
+// then the side each segment faces.
+static int boundary_points(Canvas &c, long id, std::vector<long> &iz, std::vector<long> &ir, std::vector<short> &dir)
+{
+  const long np = (long)c.mb.size();
+  long i = 0;
+  while (i < np && c.mb[(size_t)i] != id)
+    i++;
+  if (i == np)
+    return 0;
+  const long ip1 = i;
+  for (i += 1; i < np; i++)
+    if (c.mb[(size_t)i] != id)
+      break;
+  const long ip2 = i;
+  for (i = ip1; i < ip2; i++) {
+    if (i > ip1 && c.ixb[(size_t)i] == c.ixb[(size_t)i - 1] && c.iyb[(size_t)i] == c.iyb[(size_t)i - 1])
+      continue;
+    iz.push_back(c.ixb[(size_t)i]);
+    ir.push_back(c.iyb[(size_t)i]);
+  }
+  auto in = [&](long a, long b) { return (c.L((int)a, (int)b) & SPIFFE_FL_IS_INSIDE) != 0; };
+  auto surf = [&](long a, long b) { return (c.L((int)a, (int)b) & SPIFFE_FL_IS_SURFACE) != 0; };
+  auto metal = [&](long a, long b) { return (c.L((int)a, (int)b) & SPIFFE_FL_IS_METAL) != 0; };
+  long added;
+  do {
+    added = 0;
+    for (i = 1; i < (long)iz.size(); i++) {
+      const long iz0 = iz[(size_t)i - 1], iz1 = iz[(size_t)i], ir0 = ir[(size_t)i - 1], ir1 = ir[(size_t)i];
+      if (iz0 == iz1 || ir0 == ir1)
+        continue;
+      long izn, irn;
+      if (in(iz0, ir1)) {
+        izn = iz0;
+        irn = ir1;
+      } else if (in(iz1, ir0)) {
+        izn = iz1;
+        irn = ir0;
+      } else if (surf(iz0, ir1)) {
+        izn = iz0;
+        irn = ir1;
+      } else if (surf(iz1, ir0)) {
+        izn = iz1;
+        irn = ir0;
+      } else if (iz0 == 0) {
+        izn = iz0;
+        irn = ir1;
+      } else {
+        printf("boundary issue: (%ld, %ld) followed by (%ld, %ld)\n", iz0, ir0, iz1, ir1);
+        continue;
+      }
+      iz.insert(iz.begin() + i, izn);
+      ir.insert(ir.begin() + i, irn);
+      i++; // the pass resumes after the old point, as the reference's does
+      added++;
+    }
+    if (added)
+      printf("Added %ld boundary points\n", added);
+  } while (added);
+  const long n = (long)iz.size(), nx = c.nx, ny = c.ny;
+  dir.assign((size_t)n, 0);
+  for (i = 1; i < n; i++) {
+    const long z1 = iz[(size_t)i - 1], r1 = ir[(size_t)i - 1], z2 = iz[(size_t)i], r2 = ir[(size_t)i];
+    short &d = dir[(size_t)i - 1];
+    if (z1 == z2) { // a constant-z segment
+      if (z1 == 0 || in(z1 - 1, r2) || in(z1 - 1, r1))
+        d = SPIFFE_EMITS_RIGHT;
+      else if (z2 == nx - 1 || in(z1 + 1, r2) || in(z1 + 1, r1))
+        d = SPIFFE_EMITS_LEFT;
+      else if (z1 > 1 && (in(z1 - 2, r2) || in(z1 - 2, r1)))
+        d = SPIFFE_EMITS_RIGHT;
+      else if (z1 < nx - 2 && (in(z1 + 2, r2) || in(z1 + 2, r1)))
+        d = SPIFFE_EMITS_LEFT;
+      else if (metal(z1 - 1, r2) || metal(z1 - 1, r1))
+        d = SPIFFE_EMITS_RIGHT;
+      else if (metal(z1 + 1, r2) || metal(z1 + 1, r1))
+        d = SPIFFE_EMITS_LEFT;
+      else {
+        char buf[200];
+        snprintf(buf, sizeof(buf), "Can't determine which way constant-z surface at z=%e, r=%e, iz=%ld, ir=%ld emits.",
+                 z1 * c.dx + c.xmin, r1 * c.dy + c.ymin, z1, r1);
+        return spiffe_set_error(SPIFFE_ERR_INVALID, buf);
+      }
+    } else if (r2 == r1) { // a constant-r segment
+      if (r1 == 0 || in(z1, r1 - 1) || in(z2, r1 - 1))
+        d = SPIFFE_EMITS_UP;
+      else if (r2 == ny - 1 || in(z1, r1 + 1) || in(z2, r1 + 1))
+        d = SPIFFE_EMITS_DOWN;
+      else if (r1 > 1 && (in(z1, r1 - 2) || in(z2, r1 - 2)))
+        d = SPIFFE_EMITS_UP;
+      else if (r1 < ny - 2 && (in(z1, r1 + 2) || in(z2, r1 + 2)))
+        d = SPIFFE_EMITS_DOWN;
+      else if (metal(z1, r1 - 1) || metal(z2, r1 - 1))
+        d = SPIFFE_EMITS_UP;
+      else if (metal(z1, r1 + 1) || metal(z2, r1 + 1))
+        d = SPIFFE_EMITS_DOWN;
+      else {
+        char buf[200];
+        snprintf(buf, sizeof(buf), "Can't determine which way constant-r surface at z=%e, r=%e, iz=%ld, ir=%ld emits.",
+                 z1 * c.dx + c.xmin, r1 * c.dy + c.ymin, z1, r1);
+        return spiffe_set_error(SPIFFE_ERR_INVALID, buf);
+      }
+    } else if (i > 1) {
+      d = dir[(size_t)i - 2];
+    }
+  }
+  return (int)n;
+}
+
+extern "C" int spiffe_geometry_boundary_points(const spiffe_geometry_options *o, const char *text, int32_t material_id,
+                                               int64_t max_points, int32_t *iz, int32_t *ir, int16_t *direction,
+                                               int64_t *n_points)
+{
+  if (!o || !text || !n_points)
+    return spiffe_set_error(SPIFFE_ERR_INVALID, "null argument");
+  *n_points = 0;
+  const size_t n = (size_t)(o->nz + 1) * (o->nr + 1);
+  if (o->nz < 2 || o->nr < 2)
+    return spiffe_set_error(SPIFFE_ERR_INVALID, "nz and nr must be greater than 2");
+  std::vector<int16_t> flags(n), material(n);
+  std::vector<double> psi(n);
+  Canvas c;
+  const int rc = rasterise(o, text, flags.data(), psi.data(), material.data(), c);
+  if (rc)
+    return rc;
+  std::vector<long> vz, vr;
+  std::vector<short> vd;
+  const int np = boundary_points(c, material_id, vz, vr, vd);
+  if (np < 0)
+    return np;
+  *n_points = np;
+  if (!iz && !ir && !direction)
+    return 0;
+  if (np > max_points)
+    return spiffe_set_error(SPIFFE_ERR_CAPACITY, "more boundary points than the buffers hold");
+  for (int k = 0; k < np; k++) {
+    if (iz)
+      iz[k] = (int32_t)vz[(size_t)k];
+    if (ir)
+      ir[k] = (int32_t)vr[(size_t)k];
+    if (direction)
+      direction[k] = vd[(size_t)k];
+  }
+  return 0;
+}
+
+static int rasterise(const spiffe_geometry_options *o, const char *text, int16_t *flags, double *psi,
+                     int16_t *material, Canvas &c)
 {
   if (!o || !text || !flags || !psi)
     return spiffe_set_error(SPIFFE_ERR_INVALID, "null argument");
@@ -397,7 +562,6 @@ extern "C" int spiffe_geometry_rasterise(const spiffe_geometry_options *o, const
     return spiffe_set_error(SPIFFE_ERR_INVALID, "too few boundary points in geometry file");
 
   // set_up_drawing, grid_drawing.c:157-196
-  Canvas c;
   c.nx = nz;
   c.ny = nr;
   c.xmin = o->zmin;

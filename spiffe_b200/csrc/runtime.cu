@@ -117,6 +117,22 @@ struct HostSecondary {
   std::vector<double> log_rows; // SPIFFE_SECONDARY_LOG_COLS per emitting source
 };
 
+// One surface emitter as the reference holds it (EMITTER, spiffe.h:265-299):
+// the boundary nodes it emits from, the side of each segment, and each
+// segment's current density.
+struct HostEmitter {
+  spiffe_emitter_options o{};
+  std::vector<long> iz, ir;
+  std::vector<short> dir;
+  std::vector<double> prof_t, prof_A;
+  std::vector<double> J; // current density per segment
+  double initial_v = 0, Q = 0, QoMC = 0;
+  // stop_step is first computed by the first call that passes the profile;
+  // until then it is 0, as fresh memory holds in the reference (emitter.c:186
+  // reads it before any assignment), so a first call after step 0 emits nothing
+  long long start_step = -1, stop_step = 0, step_emission_started = -1;
+};
+
 // One cathode as the reference holds it (CATHODE, spiffe.h:236-262).
 struct HostCathode {
   spiffe_cathode_options o;
@@ -212,6 +228,11 @@ struct spiffe_gpu_instance {
   unsigned long long *d_pclog_n = nullptr;
   std::vector<HostCathode> cathodes;
   uint64_t rng_key = 0, rng_counter = 0;
+  std::vector<HostEmitter> emitters;
+  uint64_t rng2_key = 0, rng2_counter = 0; // random_2, the emitters' stream
+  long long *d_nodes = nullptr;            // node indices of field reads on the host's behalf
+  double *d_node_vals = nullptr;
+  size_t nodes_cap = 0;
   std::vector<HostAntenna> antennas;
   HostTestBeam test_beam;
   double QoMC = 0, stiffness = 1;
@@ -804,6 +825,7 @@ static int s32_deposit_all(spiffe_gpu_instance *in)
 }
 
 static int after_push(spiffe_gpu_instance *in);
+static int emit_emitters(spiffe_gpu_instance *in);
 
 static LostLog lost_log(const spiffe_gpu_instance *in)
 {
@@ -934,7 +956,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
                in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments, in->d_lost, in->d_points,
-               in->d_list};
+               in->d_list, in->d_nodes, in->d_node_vals};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1652,6 +1674,49 @@ static long inverse_poisson_cdf(double mu, double C)
 
 static double rng_next(spiffe_gpu_instance *in);
 
+// Particles the host composed (BIRTH_LIST_COLS columns of equal length)
+// appended to the beam on the device, the beam grown first if they do not fit.
+static int list_births(spiffe_gpu_instance *in, const std::vector<double> *col, double qmax)
+{
+  const size_t total = col[0].size();
+  if (!total)
+    return 0;
+  if (in->np_upper + (long long)total > in->capacity) {
+    RC_TRY(read_counts(in));
+    RC_TRY(grow_beam(in, in->h_cnt->np + (long long)total));
+  }
+  if (in->list_cap < total) {
+    cudaFree(in->d_list);
+    in->d_list = nullptr;
+    in->list_cap = std::max<size_t>(total, 1024);
+    CUDA_TRY(cudaMalloc(&in->d_list, sizeof(double) * BIRTH_LIST_COLS * in->list_cap));
+  }
+  std::vector<double> flat;
+  flat.reserve(BIRTH_LIST_COLS * total);
+  for (int c = 0; c < BIRTH_LIST_COLS; c++)
+    flat.insert(flat.end(), col[c].begin(), col[c].end());
+  CUDA_TRY(cudaMemcpyAsync(in->d_list, flat.data(), sizeof(double) * flat.size(), cudaMemcpyHostToDevice, in->stream));
+  BirthParams p{};
+  p.total = (long long)total;
+  p.mode = SPIFFE_BIRTH_LIST;
+  p.list = in->d_list;
+  p.time = in->mesh.time;
+  int rc;
+  if (in->s32) {
+    S32State &S = *in->s32;
+    RC_TRY(s32_cover_charge(in, qmax));
+    rc = s32_births(&in->dm, &S.f, &S.b, &p, in->cnt, &S.sc, in->space_charge && S.j_state == S32_J_DEPOSITED ? 1 : 0,
+                    in->stream);
+  } else {
+    rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
+  }
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "birth launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  in->np_upper += (long long)total;
+  CUDA_TRY(cudaStreamSynchronize(in->stream)); // the host list is freed on return
+  return 0;
+}
+
 // emitSecondaryElectrons (secondaryEmission.c:374-584): each material's queue
 // in order, the number of secondaries of each source from its mean yield
 // (a Poisson draw), each with a random direction away from the surface it
@@ -1751,38 +1816,7 @@ static int emit_secondaries(spiffe_gpu_instance *in)
       CUDA_TRY(cudaStreamSynchronize(in->stream));
     }
     const size_t total = col[0].size();
-    if (total) {
-      if (in->list_cap < total) {
-        cudaFree(in->d_list);
-        in->d_list = nullptr;
-        in->list_cap = std::max<size_t>(total, 1024);
-        CUDA_TRY(cudaMalloc(&in->d_list, sizeof(double) * BIRTH_LIST_COLS * in->list_cap));
-      }
-      std::vector<double> flat;
-      flat.reserve(BIRTH_LIST_COLS * total);
-      for (int c = 0; c < BIRTH_LIST_COLS; c++)
-        flat.insert(flat.end(), col[c].begin(), col[c].end());
-      CUDA_TRY(cudaMemcpyAsync(in->d_list, flat.data(), sizeof(double) * flat.size(), cudaMemcpyHostToDevice,
-                               in->stream));
-      BirthParams p{};
-      p.total = (long long)total;
-      p.mode = SPIFFE_BIRTH_LIST;
-      p.list = in->d_list;
-      p.time = m.time;
-      int rc;
-      if (in->s32) {
-        S32State &S = *in->s32;
-        RC_TRY(s32_cover_charge(in, qmax));
-        rc = s32_births(&in->dm, &S.f, &S.b, &p, in->cnt, &S.sc,
-                        in->space_charge && S.j_state == S32_J_DEPOSITED ? 1 : 0, in->stream);
-      } else {
-        rc = spiffe_births64(&in->dm, &in->f, &in->b, &p, in->cnt, in->stream);
-      }
-      if (rc)
-        return fail(SPIFFE_ERR_CUDA, "secondary birth launch failed: %s", cudaGetErrorString((cudaError_t)rc));
-      in->np_upper += (long long)total;
-      CUDA_TRY(cudaStreamSynchronize(in->stream)); // the host list is reused
-    }
+    RC_TRY(list_births(in, col, qmax));
     if (SE.verbosity > 0) {
       RC_TRY(read_counts(in));
       printf("Secondary emission increased number of particles from %lld to %lld\n",
@@ -2004,23 +2038,27 @@ extern "C" int spiffe_gpu_add_cathode(spiffe_gpu_instance *in, const spiffe_cath
   return 0;
 }
 
-static double profile_value(const HostCathode &c, double t)
+// interp(A, t, n, x, ...) of an ascending table: linear inside, the end
+// values outside
+static double interp_table(const std::vector<double> &A, const std::vector<double> &T, double t)
 {
-  const long n = (long)c.prof_t.size();
+  const long n = (long)T.size();
   long lo = 0, hi = n - 1;
-  if (t <= c.prof_t[0])
-    return c.prof_A[0];
-  if (t >= c.prof_t[hi])
-    return c.prof_A[hi];
+  if (t <= T[0])
+    return A[0];
+  if (t >= T[(size_t)hi])
+    return A[(size_t)hi];
   while (hi - lo > 1) {
     const long mid = (lo + hi) / 2;
-    if (c.prof_t[mid] <= t)
+    if (T[(size_t)mid] <= t)
       lo = mid;
     else
       hi = mid;
   }
-  return c.prof_A[lo] + (c.prof_A[hi] - c.prof_A[lo]) / (c.prof_t[hi] - c.prof_t[lo]) * (t - c.prof_t[lo]);
+  return A[(size_t)lo] + (A[(size_t)hi] - A[(size_t)lo]) / (T[(size_t)hi] - T[(size_t)lo]) * (t - T[(size_t)lo]);
 }
+
+static double profile_value(const HostCathode &c, double t) { return interp_table(c.prof_A, c.prof_t, t); }
 
 static double rng_next(spiffe_gpu_instance *in) { return spiffe_rng_uniform(in->rng_key, ++in->rng_counter); }
 
@@ -2205,6 +2243,7 @@ static int emit(spiffe_gpu_instance *in)
     in->QoMC = c.QoMC; // cathode.c:661-663
     in->stiffness = c.o.stiffness;
   }
+  RC_TRY(emit_emitters(in)); // integrate.c:164-165: after the cathodes
   return 0;
 }
 
@@ -2471,6 +2510,26 @@ extern "C" int spiffe_gpu_on_axis_fields_at(spiffe_gpu_instance *in, double z, d
   return 0;
 }
 
+// Richardson-Schottky emission (cathode.c:694-706, emitter.c:424-436) with
+// the reference's grouping of the products
+static double schottky_density(double T, double wf, double Ez)
+{
+  double c = 0.012 * std::sqrt(std::fabs(Ez * 1e-5));
+  if (c > wf)
+    c = wf;
+  return 60e4 * (T * T) * std::exp(-(wf - c) / (T * SPIFFE_KB_MKS / SPIFFE_E_MKS));
+}
+
+// fieldEmissionCurrentDensity, cathode.c:799-810
+static double field_emission_density(double E, double beta, double wf)
+{
+  E = std::fabs(E) * beta;
+  const double y = 3.79e-5 * std::sqrt(E) / wf;
+  const double t = ((-0.0020 * y + 0.0131) * y + 0.1091) * y + 0.9899;
+  const double v = ((0.0445 * y - 0.6782) * y - 0.4091) * y + 1.0437;
+  return 1.54e-6 * (E * E) / (wf * (t * t)) * std::exp(-6.83e9 * v * std::pow(wf, 1.5) / E);
+}
+
 // set_current_density, cathode.c:673-715
 static int set_current_density(spiffe_gpu_instance *in)
 {
@@ -2507,20 +2566,278 @@ static int set_current_density(spiffe_gpu_instance *in)
     if (Ez >= 0 && c.initial_vz <= 0)
       continue;
     if (schottky) {
-      double wf = 0.012 * std::sqrt(std::fabs(Ez * 1e-5));
-      if (wf > c.o.work_function)
-        wf = c.o.work_function;
-      c.current_density = 60e4 * c.o.temperature * c.o.temperature *
-                          std::exp(-(c.o.work_function - wf) / (c.o.temperature * SPIFFE_KB_MKS / SPIFFE_E_MKS));
+      if (0.012 * std::sqrt(std::fabs(Ez * 1e-5)) > c.o.work_function)
+        printf("Warning: Schottky correction exceeds work function.  Set equal to work function.\n");
+      c.current_density = schottky_density(c.o.temperature, c.o.work_function, Ez);
     } else {
-      double E = std::fabs(Ez) * c.o.field_emission_beta;
-      const double y = 3.79e-5 * std::sqrt(E) / c.o.work_function;
-      const double t = ((-0.0020 * y + 0.0131) * y + 0.1091) * y + 0.9899;
-      const double v = ((0.0445 * y - 0.6782) * y - 0.4091) * y + 1.0437;
-      c.current_density = 1.54e-6 * E * E / (c.o.work_function * t * t) *
-                          std::exp(-6.83e9 * v * std::pow(c.o.work_function, 1.5) / E);
+      c.current_density = field_emission_density(Ez, c.o.field_emission_beta, c.o.work_function);
     }
   }
+  return 0;
+}
+
+// The node values of Ez + EzImposed at `ez` and of Er + ErImposed at `er`
+// (flat indices of the reference's layout), read on the device for the host.
+template <typename T>
+__global__ void k_node_sums(const T *a, const T *ai, const T *b, const T *bi, const long long *idx, int n, int pitch,
+                            int P, double *out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 2 * n)
+    return;
+  const long long f = idx[k];
+  const size_t i = (size_t)(f / P) * (size_t)pitch + (size_t)(f % P);
+  out[k] = k < n ? (double)a[i] + (double)ai[i] : (double)b[i] + (double)bi[i];
+}
+
+static int node_sums(spiffe_gpu_instance *in, const std::vector<long long> &ez, const std::vector<long long> &er,
+                     std::vector<double> &Ez, std::vector<double> &Er)
+{
+  const size_t n = ez.size();
+  Ez.assign(n, 0);
+  Er.assign(n, 0);
+  if (!n)
+    return 0;
+  if (in->nodes_cap < n) {
+    cudaFree(in->d_nodes);
+    cudaFree(in->d_node_vals);
+    in->d_nodes = nullptr;
+    in->d_node_vals = nullptr;
+    in->nodes_cap = std::max<size_t>(n, 256);
+    CUDA_TRY(cudaMalloc(&in->d_nodes, sizeof(long long) * 2 * in->nodes_cap));
+    CUDA_TRY(cudaMalloc(&in->d_node_vals, sizeof(double) * 2 * in->nodes_cap));
+  }
+  std::vector<long long> idx(ez);
+  idx.insert(idx.end(), er.begin(), er.end());
+  CUDA_TRY(cudaMemcpyAsync(in->d_nodes, idx.data(), sizeof(long long) * 2 * n, cudaMemcpyHostToDevice, in->stream));
+  const int P = in->mesh.nr + 1, blocks = (int)((2 * n + 255) / 256);
+  if (in->s32) {
+    const DevFields32 &f = in->s32->f;
+    k_node_sums<float><<<blocks, 256, 0, in->stream>>>(f.Ez, f.EzImposed, f.Er, f.ErImposed, in->d_nodes, (int)n,
+                                                       in->dm.pitch, P, in->d_node_vals);
+  } else {
+    const DevFields<double> &f = in->f;
+    k_node_sums<double><<<blocks, 256, 0, in->stream>>>(f.Ez, f.EzImposed, f.Er, f.ErImposed, in->d_nodes, (int)n, P, P,
+                                                        in->d_node_vals);
+  }
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> v(2 * n);
+  CUDA_TRY(cudaMemcpyAsync(v.data(), in->d_node_vals, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  std::copy(v.begin(), v.begin() + (long)n, Ez.begin());
+  std::copy(v.begin() + (long)n, v.end(), Er.begin());
+  return 0;
+}
+
+// The fields an emitter segment sees at its nodes (emitter.c:210-222,
+// :405-417): constant plus (TM) node value plus on-axis expansion.
+static int segment_fields(spiffe_gpu_instance *in, const HostEmitter &e, bool shifted, std::vector<double> &Ez,
+                          std::vector<double> &Er)
+{
+  const spiffe_mesh &m = in->mesh;
+  const size_t nseg = e.iz.size() - 1;
+  const long long P = m.nr + 1;
+  std::vector<double> a, b;
+  if (m.modes & SPIFFE_FL_TM_FIELDS) {
+    std::vector<long long> ez(nseg), er(nseg);
+    for (size_t k = 0; k < nseg; k++) {
+      ez[k] = (e.iz[k] + (shifted ? 1 : 0)) * P + e.ir[k];
+      er[k] = e.iz[k] * P + e.ir[k] + (shifted ? 1 : 0);
+    }
+    RC_TRY(node_sums(in, ez, er, a, b));
+  }
+  Ez.assign(nseg, 0);
+  Er.assign(nseg, 0);
+  for (size_t k = 0; k < nseg; k++) {
+    Ez[k] = m.constant_E[0];
+    Er[k] = m.constant_E[1];
+    if (m.modes & SPIFFE_FL_TM_FIELDS) {
+      Ez[k] += a[k];
+      Er[k] += b[k];
+    }
+    if (!in->onaxis.empty()) {
+      double dummy = 0;
+      onaxis_eval(in->onaxis, e.iz[k] * m.dz + m.zmin, e.ir[k] * m.dr, m.time, false, Ez[k], Er[k], dummy);
+    }
+  }
+  return 0;
+}
+
+// setEmitterCurrentDensity, emitter.c:392-440
+static int set_emitter_current_density(spiffe_gpu_instance *in)
+{
+  for (HostEmitter &e : in->emitters) {
+    const size_t nseg = e.iz.size() - 1;
+    e.J.assign(nseg, e.o.current_density);
+    const bool schottky = e.o.temperature > 0 && e.o.work_function;
+    if (!schottky && !e.o.field_emission)
+      continue;
+    std::vector<double> Ez, Er;
+    RC_TRY(segment_fields(in, e, false, Ez, Er));
+    for (size_t k = 0; k < nseg; k++)
+      e.J[k] = schottky ? schottky_density(e.o.temperature, e.o.work_function, Ez[k])
+                        : field_emission_density(std::sqrt(Ez[k] * Ez[k] + Er[k] * Er[k]), e.o.field_emission_beta,
+                                                 e.o.work_function);
+  }
+  return 0;
+}
+
+static double rng2_next(spiffe_gpu_instance *in) { return spiffe_rng_uniform(in->rng2_key, ++in->rng2_counter); }
+
+// emit_electrons_from_emitter, emitter.c:169-390: per segment, the count
+// from area, current density and profile with random rounding, then each
+// particle spread over the segment (random_2), offset from the surface and
+// launched along its normal at initial_p; one list per emitter.
+static int emit_emitters(spiffe_gpu_instance *in)
+{
+  const spiffe_mesh &m = in->mesh;
+  for (HostEmitter &e : in->emitters) {
+    if (m.dt <= 0)
+      return fail(SPIFFE_ERR_INVALID, "integration step size is not defined (emit_electrons_from_emitter)");
+    if (e.start_step > m.time_step || e.stop_step < m.time_step)
+      continue;
+    double profile_factor = 1;
+    if (!e.prof_t.empty()) {
+      if (m.time >= e.prof_t.front() && m.time <= e.prof_t.back())
+        profile_factor = interp_table(e.prof_A, e.prof_t, m.time);
+      else
+        profile_factor = 0;
+    }
+    if (profile_factor <= 0)
+      continue;
+    e.start_step = (long long)((e.o.start_time - m.start_time) / m.dt);
+    if (e.o.stop_time && e.o.stop_time > m.start_time)
+      e.stop_step = (long long)((e.o.stop_time - m.start_time) / m.dt);
+    else
+      e.stop_step = 0x7fffffffffffffffLL;
+    if (e.start_step > m.time_step || e.stop_step < m.time_step)
+      continue;
+    const size_t nseg = e.iz.size() - 1;
+    std::vector<double> Ez, Er;
+    if (e.o.field_emission)
+      RC_TRY(segment_fields(in, e, true, Ez, Er));
+    std::vector<double> col[BIRTH_LIST_COLS];
+    for (size_t k = 0; k < nseg; k++) {
+      const long iz = e.iz[k], ir = e.ir[k], iz1 = e.iz[k + 1], ir1 = e.ir[k + 1];
+      const double z = iz * m.dz + m.zmin, r = ir * m.dr;
+      double nps = 0;
+      if (e.o.field_emission)
+        e.J[k] = field_emission_density(std::sqrt(Ez[k] * Ez[k] + Er[k] * Er[k]), e.o.field_emission_beta,
+                                        e.o.work_function);
+      const bool axial = e.dir[k] == SPIFFE_EMITS_RIGHT || e.dir[k] == SPIFFE_EMITS_LEFT;
+      const double area = axial ? SPIFFE_PI * ((r + m.dr) * (r + m.dr) - r * r) : SPIFFE_PIx2 * r * m.dz;
+      if (area > 0 && e.o.electrons_per_macroparticle)
+        nps = area * m.dt * e.J[k] / (SPIFFE_E_MKS * e.o.electrons_per_macroparticle);
+      if (e.step_emission_started < 0)
+        e.step_emission_started = m.time_step;
+      double fnumber = nps * profile_factor;
+      long total = (long)fnumber;
+      fnumber -= (long)fnumber;
+      if (fnumber && fnumber > rng2_next(in))
+        total += 1;
+      for (long q = 0; q < total; q++) {
+        double pz_, pr_, vz = 0, vr = 0, zp = z, rp = r;
+        if (axial) {
+          const double rn = rng2_next(in);
+          if (ir1 > ir)
+            rp = std::sqrt(rn * ((r + m.dr) * (r + m.dr) - r * r) + r * r);
+          else
+            rp = std::sqrt(rn * ((r + m.dr) * (r + m.dr) - r * r) + (r - m.dr) * (r - m.dr));
+          if (e.dir[k] == SPIFFE_EMITS_RIGHT) {
+            vz = e.initial_v;
+            zp += m.dz * e.o.offset_factor;
+          } else {
+            vz = -e.initial_v;
+            zp -= m.dz * e.o.offset_factor;
+          }
+        } else {
+          const double rn = rng2_next(in);
+          if (iz1 > iz)
+            zp = z + rn * m.dz;
+          else
+            zp = z - rn * m.dz;
+          if (e.dir[k] == SPIFFE_EMITS_UP) {
+            vr = e.initial_v;
+            rp += m.dr * e.o.offset_factor;
+          } else {
+            vr = -e.initial_v;
+            rp -= m.dr * e.o.offset_factor;
+          }
+        }
+        const double gamma = 1 / std::sqrt(1 - (vz / SPIFFE_C_MKS) * (vz / SPIFFE_C_MKS) -
+                                           (vr / SPIFFE_C_MKS) * (vr / SPIFFE_C_MKS) - 0.0);
+        pz_ = vz / SPIFFE_C_MKS * gamma;
+        pr_ = vr / SPIFFE_C_MKS * gamma;
+        const double v[BIRTH_LIST_COLS - 1] = {zp, rp, pz_, pr_, vz, vr, e.Q, m.time, 0.0};
+        for (int c = 0; c < BIRTH_LIST_COLS - 1; c++)
+          col[c].push_back(v[c]);
+      }
+    }
+    const size_t total = col[0].size();
+    if (!total)
+      continue;
+    // particle IDs in emission order from the beam's counter (emitter.c:300)
+    RC_TRY(read_counts(in));
+    const long long id0 = in->h_cnt->nextParticleID;
+    for (size_t q = 0; q < total; q++)
+      col[BIRTH_LIST_COLS - 1].push_back((double)(id0 + (long long)q));
+    RC_TRY(list_births(in, col, std::fabs(e.Q)));
+    in->h_cnt->nextParticleID = id0 + (long long)total;
+    CUDA_TRY(cudaMemcpyAsync(&in->cnt->nextParticleID, &in->h_cnt->nextParticleID, sizeof(long long),
+                             cudaMemcpyHostToDevice, in->stream));
+    CUDA_TRY(cudaStreamSynchronize(in->stream));
+    in->QoMC = e.QoMC; // emitter.c:381-383
+    in->stiffness = 1;
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_add_emitter(spiffe_gpu_instance *in, const spiffe_emitter_options *o)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  // process_emitter_definition, emitter.c:40-167
+  if (!o->field_emission && o->current_density <= 0 && o->electrons_per_macroparticle == 0 && o->temperature <= 0)
+    return fail(SPIFFE_ERR_INVALID, "either field_emission, current_density, electrons_per_macroparticle, or "
+                                    "temperature must be non-zero");
+  if (o->current_density < 0)
+    return fail(SPIFFE_ERR_INVALID, "the current density should be a positive quantity");
+  if (o->electrons_per_macroparticle < 0)
+    return fail(SPIFFE_ERR_INVALID, "electrons_per_macroparticle should be a positive quantity");
+  if (o->temperature < 0)
+    return fail(SPIFFE_ERR_INVALID, "temperature should be a positive quantity");
+  if (o->stop_time && o->start_time > o->stop_time)
+    return fail(SPIFFE_ERR_INVALID, "stop_time is non-zero and less than start_time");
+  if (o->n_points <= 0 || !o->iz || !o->ir || !o->direction)
+    return fail(SPIFFE_ERR_INVALID, "No surface elements found with the specified material ID");
+  if (o->electrons_per_macroparticle == 0)
+    return fail(SPIFFE_ERR_INVALID, "electrons_per_macroparticle must be nonzero");
+  HostEmitter e;
+  e.o = *o;
+  e.iz.assign(o->iz, o->iz + o->n_points);
+  e.ir.assign(o->ir, o->ir + o->n_points);
+  e.dir.assign(o->direction, o->direction + o->n_points);
+  for (int64_t k = 0; k < o->n_points; k++)
+    if (e.iz[(size_t)k] < 0 || e.iz[(size_t)k] > in->mesh.nz || e.ir[(size_t)k] < 0 || e.ir[(size_t)k] > in->mesh.nr)
+      return fail(SPIFFE_ERR_INVALID, "emitter boundary point outside the mesh");
+  if (o->n_profile > 0) {
+    e.prof_t.assign(o->profile_t, o->profile_t + o->n_profile);
+    e.prof_A.assign(o->profile_A, o->profile_A + o->n_profile);
+    for (size_t i = 1; i < e.prof_t.size(); i++)
+      if (e.prof_t[i - 1] >= e.prof_t[i])
+        return fail(SPIFFE_ERR_INVALID, "profile data is not ordered by increasing time values");
+  }
+  e.o.iz = e.o.ir = nullptr;
+  e.o.direction = nullptr;
+  e.o.profile_t = e.o.profile_A = nullptr;
+  e.initial_v = std::fabs(o->initial_p / std::sqrt(1 + o->initial_p * o->initial_p) * SPIFFE_C_MKS);
+  e.Q = -SPIFFE_E_MKS * o->electrons_per_macroparticle;
+  e.QoMC = -SPIFFE_E_MKS / (SPIFFE_ME_MKS * SPIFFE_C_MKS);
+  e.J.assign(e.iz.size() > 1 ? e.iz.size() - 1 : 0, o->current_density);
+  const long long seed = o->random_number_seed < 0 ? -(long long)o->random_number_seed : o->random_number_seed;
+  in->rng2_key = spiffe_rng_key2((uint64_t)seed); // random_2(-abs(seed)), emitter.c:63
+  in->rng2_counter = 0;
+  in->emitters.push_back(std::move(e));
   return 0;
 }
 
@@ -2622,6 +2939,7 @@ extern "C" int spiffe_gpu_run_begin(spiffe_gpu_instance *in, spiffe_poisson_repo
                      : spiffe_poisson64_report(&in->pcw, rep, in->stream));
   }
   RC_TRY(set_current_density(in));
+  RC_TRY(set_emitter_current_density(in));
   return 0;
 }
 
@@ -2674,6 +2992,7 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
     }
     RC_TRY(translate(in, nullptr));
     RC_TRY(set_current_density(in));
+    RC_TRY(set_emitter_current_density(in));
     m.time_step++;
   }
   return 0;

@@ -170,6 +170,15 @@ struct SessionCathode {
   bool on_device = false;
 };
 
+// one define_emitter definition with its surface and profile
+struct SessionEmitter {
+  spiffe_emitter_options o{};
+  std::vector<int32_t> iz, ir;
+  std::vector<int16_t> dir;
+  std::vector<double> t, A;
+  bool on_device = false;
+};
+
 // one define_secondary_emission definition with its yield table
 struct SessionSecondary {
   spiffe_secondary_options o{};
@@ -278,6 +287,9 @@ struct spiffe_session {
 
   std::vector<SessionCathode> cathodes;
   std::vector<SessionSecondary> secondaries;
+  std::vector<SessionEmitter> emitters;
+  spiffe_geometry_options geo_opts{}; // define_geometry's drawing, for the emitters' surfaces
+  std::string geo_text;
   std::vector<int16_t> material; // define_geometry's surface materials (materialID)
   std::vector<SessionAntenna> antennas;
   std::vector<SessionOnAxis> onaxis;
@@ -372,6 +384,7 @@ struct spiffe_session {
   int cmd_translate(Args &g);
   int cmd_screen(Args &g);
   int cmd_secondary_emission(Args &g);
+  int cmd_emitter(Args &g);
   int cmd_test_beam(Args &g);
   int cmd_poisson(Args &g);
   int cmd_load_fields(Args &g);
@@ -490,6 +503,8 @@ int spiffe_session::cmd_geometry(Args &g)
   a["PsiImposed"].assign(n, 0.0);
   spiffe_geometry_options go{m.nz, m.nr, zmin, zmax, rmax, zr_factor};
   S_TRY(spiffe_geometry_rasterise(&go, text.c_str(), flags.data(), a["PsiImposed"].data(), material.data()));
+  geo_opts = go;
+  geo_text = text;
   // the arrays of geometry.c:78-116 that the device problem holds
   for (const char *x : {"EzImposed", "ErImposed", "Q", "Jz"})
     a[x].assign(n, 0.0);
@@ -669,6 +684,118 @@ int spiffe_session::cmd_cathode(Args &g)
   o.profile_t = o.profile_A = nullptr;
   c.o = o;
   cathodes.push_back(std::move(c));
+  return 0;
+}
+
+// ------------------------------------------------------------- define_emitter
+
+// process_emitter_definition, emitter.c:19-167; the surface is
+// getBoundaryPoints' (spiffe_geometry_boundary_points)
+int spiffe_session::cmd_emitter(Args &g)
+{
+  spiffe_emitter_options o{};
+  long long material_id = -1, determine_temperature = 0, add_thermal = 0, field_emission = 0;
+  long long halton_dt = 0, halton_r = 0, halton_z = 0, seed = 987654321;
+  double number_per_step = 0;
+  o.field_emission_beta = 1;
+  o.offset_factor = 1e-2;
+  std::string profile, tname, fname, log;
+  g.integer("material_id", material_id);
+  g.num("current_density", o.current_density);
+  g.num("temperature", o.temperature);
+  g.integer("determine_temperature", determine_temperature);
+  g.num("work_function", o.work_function);
+  g.integer("add_thermal_velocities", add_thermal);
+  g.integer("field_emission", field_emission);
+  g.num("field_emission_beta", o.field_emission_beta);
+  g.num("electrons_per_macroparticle", o.electrons_per_macroparticle);
+  g.num("start_time", o.start_time);
+  g.num("stop_time", o.stop_time);
+  g.num("number_per_step", number_per_step); // declared by emitter.nl, read by no code
+  g.num("initial_p", o.initial_p);
+  g.num("offset_factor", o.offset_factor);
+  g.integer("random_number_seed", seed);
+  g.integer("halton_radix_dt", halton_dt);
+  g.integer("halton_radix_r", halton_r);
+  g.integer("halton_radix_z", halton_z);
+  const bool have_profile = g.str("profile", profile);
+  g.str("profile_time_name", tname);
+  g.str("profile_factor_name", fname);
+  if (g.str("emission_log", log))
+    warn("define_emitter: emission_log is not written");
+  S_TRY(g.finish());
+  o.field_emission = (int32_t)field_emission;
+  if (!field_emission && o.current_density <= 0 && o.electrons_per_macroparticle == 0 && o.temperature <= 0)
+    return serr(SPIFFE_ERR_INVALID,
+                "either field_emission, current_density, electrons_per_macroparticle, or temperature must be non-zero");
+  if (field_emission && (determine_temperature || o.current_density || have_profile))
+    return serr(SPIFFE_ERR_INVALID, "field_emission is incompatible with determine_temperature, current_density, and profile");
+  if (field_emission && !o.electrons_per_macroparticle)
+    return serr(SPIFFE_ERR_INVALID, "specify electrons_per_macroparticle with field_emission");
+  if (field_emission && !o.work_function)
+    return serr(SPIFFE_ERR_INVALID, "specify work_function with field_emission");
+  if (o.current_density < 0)
+    return serr(SPIFFE_ERR_INVALID, "the current density should be a positive quantity");
+  if (o.electrons_per_macroparticle < 0)
+    return serr(SPIFFE_ERR_INVALID, "electrons_per_macroparticle should be a positive quantity");
+  if (o.temperature < 0)
+    return serr(SPIFFE_ERR_INVALID, "temperature should be a positive quantity");
+  if (o.stop_time && o.start_time > o.stop_time)
+    return serr(SPIFFE_ERR_INVALID, "stop_time is non-zero and less than start_time");
+  if (add_thermal && !(o.temperature > 0 || determine_temperature))
+    return serr(SPIFFE_ERR_INVALID, "add_thermal_velocities is nonzero but the temperature is not positive");
+  if (add_thermal)
+    return serr(SPIFFE_ERR_UNSUPPORTED, "define_emitter: add_thermal_velocities is not supported");
+  if (halton_dt || halton_r || halton_z)
+    return serr(SPIFFE_ERR_UNSUPPORTED, "define_emitter: Halton sequences are not supported");
+  if (seed == 0)
+    return serr(SPIFFE_ERR_UNSUPPORTED, "define_emitter: a clock-generated random_number_seed (0) is not supported");
+  o.random_number_seed = (int32_t)seed;
+  if (!have_geometry)
+    return serr(SPIFFE_ERR_INVALID, "define_emitter before define_geometry: No surface elements found");
+  SessionEmitter e;
+  int64_t n = 0;
+  S_TRY(spiffe_geometry_boundary_points(&geo_opts, geo_text.c_str(), (int32_t)material_id, 0, nullptr, nullptr,
+                                        nullptr, &n));
+  if (n == 0)
+    return serr(SPIFFE_ERR_INVALID, "No surface elements found with the specified material ID");
+  e.iz.resize((size_t)n);
+  e.ir.resize((size_t)n);
+  e.dir.resize((size_t)n);
+  S_TRY(spiffe_geometry_boundary_points(&geo_opts, geo_text.c_str(), (int32_t)material_id, n, e.iz.data(),
+                                        e.ir.data(), e.dir.data(), &n));
+  o.material_id = (int32_t)material_id;
+  if (o.electrons_per_macroparticle == 0)
+    return serr(SPIFFE_ERR_INVALID, "electrons_per_macroparticle must be nonzero");
+  if (determine_temperature) {
+    // emitter.c:98-113, Richardson-Dushman solved for T by iteration
+    if (o.work_function <= 0 || o.current_density <= 0)
+      return serr(SPIFFE_ERR_INVALID, "to determine temperature, must have positive work function and current density");
+    double last = 1273, t = last;
+    for (int i = 0; i < 100; i++) {
+      t = -SPIFFE_E_MKS * o.work_function / SPIFFE_KB_MKS / std::log(o.current_density / 60e4 / (last * last));
+      if (std::fabs(last - t) < 0.01)
+        break;
+      last = t;
+    }
+    o.temperature = t;
+    say("Temperature determined to be %f K\n", t);
+  }
+  if (have_profile) {
+    std::vector<std::vector<double>> cols;
+    std::string err;
+    if (!spiffe_sdds::read_columns(profile, {tname, fname}, cols, err))
+      return serr(SPIFFE_ERR_INVALID, "define_emitter: %s", err.c_str());
+    if (cols[0].empty())
+      return serr(SPIFFE_ERR_INVALID, "no data in profile file");
+    for (size_t i = 1; i < cols[0].size(); i++)
+      if (cols[0][i - 1] >= cols[0][i])
+        return serr(SPIFFE_ERR_INVALID, "profile data is not ordered by increasing time values");
+    e.t = cols[0];
+    e.A = cols[1];
+  }
+  e.o = o;
+  emitters.push_back(std::move(e));
   return 0;
 }
 
@@ -1587,6 +1714,19 @@ int spiffe_session::ensure_instance()
       S_TRY(spiffe_gpu_add_cathode(inst, &o));
       c.on_device = true;
     }
+  for (SessionEmitter &e : emitters)
+    if (!e.on_device) {
+      spiffe_emitter_options o = e.o;
+      o.n_points = (int64_t)e.iz.size();
+      o.iz = e.iz.data();
+      o.ir = e.ir.data();
+      o.direction = e.dir.data();
+      o.n_profile = (int32_t)e.t.size();
+      o.profile_t = e.t.empty() ? nullptr : e.t.data();
+      o.profile_A = e.A.empty() ? nullptr : e.A.data();
+      S_TRY(spiffe_gpu_add_emitter(inst, &o));
+      e.on_device = true;
+    }
   if (!secondaries.empty() && !material.empty())
     S_TRY(spiffe_gpu_set_materials(inst, material.data()));
   for (SessionSecondary &d : secondaries)
@@ -2008,7 +2148,9 @@ int spiffe_session::execute(const std::string &text)
       rc = cmd_translate(g);
     } else if (c == "define_secondary_emission") {
       rc = cmd_secondary_emission(g);
-    } else if (c == "define_resistor" || c == "load_particles" || c == "define_emitter") {
+    } else if (c == "define_emitter") {
+      rc = cmd_emitter(g);
+    } else if (c == "define_resistor" || c == "load_particles") {
       rc = serr(SPIFFE_ERR_UNSUPPORTED, "%s is not supported", c.c_str());
     } else {
       rc = serr(SPIFFE_ERR_INVALID, "unknown namelist %s given", c.c_str());

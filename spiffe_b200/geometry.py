@@ -30,6 +30,26 @@ def rasterise(nz, nr, zmin, zmax, rmax, boundary_text, zr_factor=1.0):
     return flags, psi
 
 
+def boundary_points(nz, nr, zmin, zmax, rmax, boundary_text, material_id, zr_factor=1.0):
+    """The emitter surface of a material (getBoundaryPoints): (iz, ir,
+    direction) arrays, one entry per node, direction[k] the side segment
+    k -> k+1 emits to (abi.EMITS_*), the last entry 0."""
+    lib = gpu.load()
+    fn = lib.spiffe_geometry_boundary_points
+    fn.argtypes = [C.POINTER(GeometryOptions), C.c_char_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
+                   C.c_void_p, C.POINTER(C.c_int64)]
+    fn.restype = C.c_int
+    o = GeometryOptions(nz, nr, zmin, zmax, rmax, zr_factor)
+    n = C.c_int64(0)
+    if fn(C.byref(o), boundary_text.encode(), material_id, 0, None, None, None, C.byref(n)) != 0:
+        raise gpu.SpiffeGpuError(f"define_emitter: {lib.spiffe_gpu_last_error().decode()}")
+    iz, ir, d = np.zeros(n.value, np.int32), np.zeros(n.value, np.int32), np.zeros(n.value, np.int16)
+    if n.value and fn(C.byref(o), boundary_text.encode(), material_id, n.value, iz.ctypes.data, ir.ctypes.data,
+                      d.ctypes.data, C.byref(n)) != 0:
+        raise gpu.SpiffeGpuError(f"define_emitter: {lib.spiffe_gpu_last_error().decode()}")
+    return iz, ir, d
+
+
 def fields_for(nz, nr, zmin, zmax, rmax, boundary_text, modes=abi.FL_TM_FIELDS | abi.FL_RADIAL_INTERP |
                abi.FL_LONGIT_INTERP, **bcs):
     """An abi.Fields whose flags and PsiImposed come from the boundary text."""

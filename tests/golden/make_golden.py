@@ -364,6 +364,62 @@ def deck_secondary(geo):
     save("deck_secondary", **out)
 
 
+# Surface emitters (emitter.c): the DC gun's cathode plane drawn as material
+# 2 out to r = 1 mm and material 3 out to 2 mm; no define_cathode.  Material
+# 2 emits thermionically (Richardson-Schottky, with a time profile),
+# material 3 by field emission; both from the emitter surface the boundary
+# list yields (getBoundaryPoints).
+DECK_EMITTER = """&define_geometry nz=151, nr=101, zmin=0.0, zmax=0.03, rmax=0.02, boundary="dc.geo" &end
+&define_emitter material_id=2, temperature=2500, work_function=3.0, electrons_per_macroparticle=1e7,
+    start_time=0, stop_time=40e-12, initial_p=1e-3, random_number_seed=12345,
+    profile="prof.sdds", profile_time_name="t", profile_factor_name="A" &end
+&define_emitter material_id=3, field_emission=1, work_function=4.5, field_emission_beta=100,
+    electrons_per_macroparticle=1e6, stop_time=60e-12, initial_p=1e-3, random_number_seed=777 &end
+&define_screen filename="deck.sc1", z_position=0.012, direction="forward" &end
+&poisson_correction step_interval=4, accuracy=1e-4, error_charge_threshold=1e-15 &end
+&integrate dt_integration=4e-13, start_time=0, finish_time=150e-12, space_charge=1, imposed_Efield_ramp_time=20e-12 &end
+"""
+EMITTER_PROFILE = (np.array([0.0, 20e-12, 40e-12]), np.array([0.5, 1.0, 0.8]))
+
+
+def emitter_geo(geo):
+    """The DC gun boundary with the cathode plane split at r = 1 and 2 mm into
+    materials 2 and 3."""
+    lines = geo.splitlines()
+    assert lines[0].startswith("&po x=0.0, y=0.0,") and lines[1].startswith("&po x=0.0, y=0.02,")
+    extra = ["&po x=0.0, y=0.001, potential=0.0, material_id=2 &end",
+             "&po x=0.0, y=0.002, potential=0.0, material_id=3 &end"]
+    return "\n".join(lines[:1] + extra + lines[1:]) + "\n"
+
+
+def write_profile(path, t, A):
+    with open(path, "w") as f:
+        f.write("SDDS1\n&column name=t type=double &end\n&column name=A type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(t, A):
+            f.write("%.17g %.17g\n" % (a, b))
+
+
+def deck_emitter(geo):
+    geo = emitter_geo(geo)
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    write_profile(os.path.join(d, "prof.sdds"), *EMITTER_PROFILE)
+    cmds = [b.strip() + " &end" for b in DECK_EMITTER.split("&end") if b.strip()]
+    res = pyoracle.run_reference([("command", c) for c in cmds] + [("mesh",), ("get_beam",), ("screen", 0)] +
+                                 [("get_field", n) for n in ("Ez", "Er", "Bphi", "Psi")] +
+                                 [("boundary_points", m) for m in (2, 3)], cwd=d, capacity=40000)
+    mesh, rb, rs = res[0], res[1], res[2]
+    out = dict(deck=np.array(DECK_EMITTER), geo=np.array(geo), prof_t=EMITTER_PROFILE[0],
+               prof_A=EMITTER_PROFILE[1], time=mesh["time"], **beam_out(rb))
+    for m, (iz, ir, dr) in zip((2, 3), res[7:9]):
+        out.update({f"bp{m}_iz": iz, f"bp{m}_ir": ir, f"bp{m}_dir": dr})
+    out.update({"screen0_" + k: v for k, v in rs.items()})
+    out.update(dict(zip(("Ez", "Er", "Bphi", "Psi"), res[3:7])))
+    save("deck_emitter", **out)
+
+
 # The DC gun deck with define_field_saving (field_saving.c:46-213): saves at
 # 0 and 100 ps and before exiting.  The saved columns are compared through
 # SHA-256 digests of their values (bit-for-bit equality needs nothing more,
@@ -476,6 +532,7 @@ def decks():
     deck_lost(geo)
     deck_fieldsave(geo)
     deck_secondary(geo)
+    deck_emitter(geo)
 
 
 def deck_onaxis(geo):
@@ -505,6 +562,8 @@ if __name__ == "__main__":
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["fieldsave"]:
         deck_fieldsave(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["emitter"]:
+        deck_emitter(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["secondary"]:
         deck_secondary(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["lost"]:

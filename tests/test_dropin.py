@@ -153,3 +153,27 @@ def test_secondary_emission(tmp_path):
     assert rb["np"] == int(fx["out_np"])
     for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
         assert np.array_equal(rb[k], fx["out_" + k]), k
+
+
+def test_emitters(tmp_path):
+    """Surface emitters through the drop-in: the reference's own
+    emit_electrons_from_emitter and setEmitterCurrentDensity read the host
+    fields the drop-in brings back each step and append to the host beam;
+    fields, beam and screen equal the pure reference run's."""
+    fx = load("deck_emitter")
+    d = str(tmp_path)
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(str(fx["geo"]))
+    write_profile(d, fx["prof_t"], fx["prof_A"])
+    cmds = [b.strip() + " &end" for b in str(fx["deck"]).split("&end") if b.strip()]
+    res = run_with_dropin([("command", c) for c in cmds] + [("mesh",), ("get_beam",), ("screen", 0)] +
+                          [("get_field", n) for n in ("Ez", "Er", "Bphi", "Psi")], d, capacity=40000)
+    mesh, rb, rs = res[0], res[1], res[2]
+    assert mesh["time"] == float(fx["time"])
+    for n, a in zip(("Ez", "Er", "Bphi", "Psi"), res[3:7]):
+        assert np.array_equal(a, fx[n]), n
+    assert rb["np"] == int(fx["out_np"])
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(rb[k], fx["out_" + k]), k
+    for c in abi.SCREEN_COLUMNS:
+        assert np.array_equal(rs[c], fx["screen0_" + c]), c

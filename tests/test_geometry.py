@@ -45,3 +45,38 @@ def test_reference_example_geometries(rel, nz, nr, zmax, rmax, tmp_path):
 def test_bad_boundary_is_rejected():
     with pytest.raises(Exception):
         geometry.rasterise(20, 20, 0.0, 0.01, 0.01, "&po x=0, y=0 &end\n&po x=0.5, y=0 &end\n")
+
+
+def test_emitter_surfaces_match_reference_fixture():
+    """getBoundaryPoints (grid_drawing.c:541-760) on the emitter deck's
+    boundary: the nodes and emission sides of materials 2 and 3 equal the
+    reference's."""
+    fx = load("deck_emitter")
+    for m in (2, 3):
+        iz, ir, d = geometry.boundary_points(151, 101, 0.0, 0.03, 0.02, str(fx["geo"]), m)
+        assert np.array_equal(iz, fx[f"bp{m}_iz"]) and np.array_equal(ir, fx[f"bp{m}_ir"]), m
+        assert np.array_equal(d, fx[f"bp{m}_dir"]), m
+
+
+@pytest.mark.skipif(REF_EXAMPLES is None, reason="reference examples not present")
+@pytest.mark.parametrize("tag", [(5, (2, 3, 4, 5)), (6, (10, 11)), (7, (8, 9, 10, 11, 12))])
+def test_emitter_surfaces_match_reference(tag, tmp_path):
+    """The reference's DC gun example boundary with some of its points tagged
+    as a material: a slanted line and an arc (corner nodes inserted), the
+    anode nose, the anode face and drift pipe.  Both give the same surface
+    nodes and emission sides."""
+    from oracle import pyoracle
+
+    material, rows = tag
+    lines = open(os.path.join(REF_EXAMPLES, "dcGun/dc.geo")).read().splitlines()
+    for k in rows:
+        lines[k] = lines[k].replace("&end", ", material_id=%d &end" % material)
+    text = "\n".join(lines) + "\n"
+    (tmp_path / "b.geo").write_text(text)
+    nz, nr, zmax, rmax = 165, 165, 0.072, 0.042
+    cmd = workloads.geometry_command(nz, nr, 0.0, zmax, rmax, "b.geo")
+    (riz, rir, rd), = pyoracle.run_reference([("command", cmd), ("boundary_points", material)], cwd=str(tmp_path))
+    iz, ir, d = geometry.boundary_points(nz, nr, 0.0, zmax, rmax, text, material)
+    assert len(riz) > 3
+    assert np.array_equal(iz, riz) and np.array_equal(ir, rir)
+    assert np.array_equal(d, rd)

@@ -65,7 +65,9 @@ def test_geometry_switches(dcgeo):
     ("&define_cathode z_position=0, outer_radius=0.001, current_density=1e6 &end", ERR_INVALID, "before"),
     ("&frobnicate a=1 &end", ERR_INVALID, "unknown namelist frobnicate"),
     ("&space_charge &end", ERR_INVALID, "no longer used"),
-    ("&define_emitter &end", ERR_UNSUPPORTED, "not supported"),
+    ("&define_emitter &end", ERR_INVALID, "must be non-zero"),
+    ("&define_emitter current_density=1e6, electrons_per_macroparticle=1e6 &end", ERR_INVALID, "before"),
+    ("&define_resistor &end", ERR_UNSUPPORTED, "not supported"),
 ])
 def test_command_errors(dcgeo, text, code, msg):
     with session.Session(verbose=0) as s:
@@ -87,6 +89,11 @@ def test_checks_after_geometry(dcgeo):
             ("&poisson_correction accuracy=0 &end", "accuracy <= 0"),
             ('&poisson_correction guess_type="psychic" &end', "unknown guess type"),
             ("&define_test_beam start_time=0, stop_time=1e-12, initial_z=0.001 &end", "electrons_per_macroparticle"),
+            ("&define_emitter material_id=9, current_density=1e6, electrons_per_macroparticle=1e6 &end",
+             "No surface elements"),
+            ("&define_emitter material_id=9, current_density=1e6, electrons_per_macroparticle=1e6, "
+             "add_thermal_velocities=1, temperature=1000 &end", "not supported"),
+            ('&define_secondary_emission input_file="y.sdds" &end', "column containing energy values"),
             ("&integrate dt_integration=0 &end", "dt_integration <= 0"),
             ("&integrate dt_integration=1e-12, finish_time=1e-10 &end", "stable integration"),
             ("&integrate dt_integration=1e-13, finish_time=1e-11, smoothing_parameter=0.1 &end", "not supported"),
@@ -719,6 +726,58 @@ def test_secondary_emission_split_form(tmp_path, monkeypatch):
     assert not np.intersect1d(got["particleID"][sec], got["particleID"][prim]).size
     for k in range(1, int(gen.max()) + 1):
         assert got["t"][gen == k].min() > got["t"][gen == k - 1].min()
+    s.close()
+
+
+def write_emitter_inputs(tmp_path, fx):
+    with open(tmp_path / "prof.sdds", "w") as f:
+        f.write("SDDS1\n&column name=t type=double &end\n&column name=A type=double &end\n"
+                "&data mode=ascii no_row_counts=1 &end\n")
+        for a, b in zip(fx["prof_t"], fx["prof_A"]):
+            f.write("%.17g %.17g\n" % (a, b))
+
+
+@pytest.mark.gpu
+def test_emitters_match_reference(tmp_path, monkeypatch):
+    """define_emitter (emitter.c) on the DC gun with the cathode plane split
+    into two materials: a thermionic emitter with a time profile and a
+    field emitter, each emitting from the segments of its surface
+    (getBoundaryPoints) with random_2 positions.  In the FP64 form the fields,
+    the beam (IDs in emission order) and the screen equal the reference's bit
+    for bit."""
+    fx = load("deck_emitter")
+    write_emitter_inputs(tmp_path, fx)
+    s = run_deck(fx, tmp_path, monkeypatch)
+    assert s.mesh().time == float(fx["time"])
+    f = s.fields()
+    for n in ("Ez", "Er", "Bphi", "Psi"):
+        assert np.array_equal(f[n], fx[n]), n
+    g = s.instance()
+    b = g.download_beam(abi.Beam(int(fx["out_np"]) + 16))
+    assert b.np == int(fx["out_np"]) > 500
+    for k in abi.BEAM_DOUBLES + ["particleID", "status"]:
+        assert np.array_equal(b[k][: b.np], fx["out_" + k]), k
+    s.close()
+
+
+@pytest.mark.gpu
+def test_emitters_split_form(tmp_path, monkeypatch):
+    """The same deck in the split form: the same emission (counts, birth
+    points and times come from the host in FP64 with the same draws while the
+    field-dependent current densities see FP32 fields), so the particle count
+    is within 2% of the reference's and every particle was born on the
+    emitter surface within the reference's birth-time window."""
+    fx = load("deck_emitter")
+    write_emitter_inputs(tmp_path, fx)
+    s = run_deck(fx, tmp_path, monkeypatch, precision="split32")
+    g = s.instance()
+    b = g.download_beam(abi.Beam(2 * int(fx["out_np"]) + 16))
+    n_ref = int(fx["out_np"])
+    assert abs(b.np - n_ref) <= 0.02 * n_ref
+    np_ = b.np
+    assert np.all(b["z0"][:np_] == fx["out_z0"][0])
+    assert b["r0"][:np_].min() >= 0.0002 - 1e-12 and b["r0"][:np_].max() <= 0.002 + 1e-12
+    assert b["t0"][:np_].min() == fx["out_t0"].min() and b["t0"][:np_].max() <= fx["out_t0"].max() + 4.1e-13
     s.close()
 
 
