@@ -136,6 +136,19 @@ int spiffe_gpu_set_materials(spiffe_gpu_instance *inst, const int16_t *material)
  * opt->log set, each emitting source is logged as the reference's log_file
  * records it (:520-544), taking a particle ID as the reference does. */
 int spiffe_gpu_add_secondary_emission(spiffe_gpu_instance *inst, const spiffe_secondary_options *opt);
+/* define_field_sampling (field_sampling.c:53-101): adds a sampling
+ * definition (checked as the reference checks it against the mesh's field
+ * modes); *index receives its number.  spiffe_gpu_run_steps samples at the
+ * top of every step (integrate.c:149) on the device, into a buffer the host
+ * drains with spiffe_gpu_download_samples; spiffe_gpu_sample_fields samples
+ * at the current time (the call after the loop, integrate.c:196). */
+int spiffe_gpu_add_field_sampling(spiffe_gpu_instance *inst, const spiffe_sample_options *opt, int32_t *index);
+int spiffe_gpu_sample_fields(spiffe_gpu_instance *inst);
+/* The samples of definition `index` taken since the last download, and
+ * empties them (sample_fields, field_sampling.c:103-1097: the rows and
+ * values the reference writes).  With out->max_samples 0 only n_samples and
+ * n_rows are set. */
+int spiffe_gpu_download_samples(spiffe_gpu_instance *inst, int32_t index, spiffe_sample_set *out);
 /* The emission log of secondary-emission definition `index` (the order of
  * spiffe_gpu_add_secondary_emission) since the last call, and empties it:
  * *n_rows rows of SPIFFE_SECONDARY_LOG_COLS doubles, row-major (time step of

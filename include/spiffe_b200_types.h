@@ -236,6 +236,43 @@ typedef struct spiffe_emitter_options {
   const int16_t *direction;
 } spiffe_emitter_options;
 
+/* define_field_sampling (field_sampling.nl; process_sampling_definition,
+ * field_sampling.c:53-101): the component codes, in the order of the
+ * component names of field_sampling.c:28-29.  (The reference's own macros
+ * call 4 SAMPLE_BPHI and 5 SAMPLE_BR, so its TE check, :80-85, applies to
+ * "Bphi" and not to "Br"; the values are those the names say.) */
+#define SPIFFE_SAMPLE_EZ 0
+#define SPIFFE_SAMPLE_ER 1
+#define SPIFFE_SAMPLE_EPHI 2
+#define SPIFFE_SAMPLE_BZ 3
+#define SPIFFE_SAMPLE_BR 4
+#define SPIFFE_SAMPLE_BPHI 5
+#define SPIFFE_SAMPLE_JZ 6
+#define SPIFFE_SAMPLE_JR 7
+#define SPIFFE_SAMPLE_PHI 8
+#define SPIFFE_SAMPLE_Q 9
+#define SPIFFE_SAMPLE_E 10 /* Ez, Er, Ephi */
+#define SPIFFE_SAMPLE_B 11 /* Bz, Br, Bphi */
+typedef struct spiffe_sample_options {
+  int32_t component; /* SPIFFE_SAMPLE_* */
+  int32_t direction; /* 0: along z at r = position; 1: along r at z = position */
+  double min_coord, max_coord, position, time_interval, start_time;
+  int32_t time_sequence; /* one row per sample (the average over the range) instead of one page */
+} spiffe_sample_options;
+
+/* Samples taken since the last download, one entry per sample: its time,
+ * its parameters (param[3k]: the rSample/zSample value, then for a time
+ * sequence the start and stop of the range) and its rows (rows[k]), whose
+ * coordinate (z or r; for a time sequence the row's time) goes to x and
+ * whose values go to v[0..2] (one column, or three for SPIFFE_SAMPLE_E/B). */
+typedef struct spiffe_sample_set {
+  int64_t n_samples, n_rows;        /* filled in */
+  int64_t max_samples, max_rows;    /* capacity of the arrays below */
+  double *t, *param;                /* max_samples, 3*max_samples */
+  int64_t *rows;                    /* max_samples */
+  double *x, *v[3];                 /* max_rows */
+} spiffe_sample_set;
+
 /* Result of one Poisson correction (the quantities the reference prints,
  * poisson_correction.c:254-256, :284). */
 typedef struct spiffe_poisson_report {

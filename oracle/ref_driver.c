@@ -37,6 +37,8 @@ static SECONDARY_EMISSION *secondary = NULL;
 static long n_secondary = 0;
 static EMITTER *emitter = NULL;
 static long n_emitters = 0;
+static SAMPLE_DEFN *sample_defn = NULL;
+static long n_sample_defns = 0;
 static int initialized = 0;
 
 /* capacity of every particle and screen array: the reference sizes screen
@@ -114,6 +116,8 @@ int ref_command(const char *text)
     process_on_axis_field_definition(&EM, &nl);
   else if (strcmp(nl.group_name, "define_test_beam") == 0)
     process_testbeam_definition(&test_beam_defn, &EM, &nl);
+  else if (strcmp(nl.group_name, "define_field_sampling") == 0)
+    process_sampling_definition(&sample_defn, n_sample_defns++, &EM, &nl);
   else if (strcmp(nl.group_name, "define_emitter") == 0) {
     process_emitter_definition(&EM, &emitter, &n_emitters, &nl);
     /* the definition leaves stop_step unset (emitter.c:65-90) and the first
@@ -124,7 +128,7 @@ int ref_command(const char *text)
     processSecondaryEmissionDefinition(&secondary, &n_secondary, &nl, &EM);
   else if (strcmp(nl.group_name, "integrate") == 0)
     perform_integration(&EM, &beam, cathode, cathodes, &test_beam_defn, antenna, n_antennae, &resistor_defns,
-                        NULL, 0, &saving_defn, &snapshot_defn, screen_defn, n_screen_defns,
+                        sample_defn, n_sample_defns, &saving_defn, &snapshot_defn, screen_defn, n_screen_defns,
                         &field_output_defn, secondary, n_secondary, emitter, n_emitters, &nl);
   else
     rc = -1;
@@ -450,7 +454,8 @@ void ref_step(long space_charge, double z_forces_start)
 /* which: 0 the beam snapshots, 1 the field output, 2 + k the k-th output
  * table the reference closed inside a command, 3 + SHIM_MAX_CLOSED_TABLES
  * the field saves, 100 + k the k-th table it wrote row by row (the status
- * file), 200 + k the log_file of the k-th define_secondary_emission */
+ * file), 200 + k the log_file of the k-th define_secondary_emission, 300 + k
+ * the file of the k-th define_field_sampling */
 static SDDS_DATASET *ref_table(long which)
 {
   if (which == 0)
@@ -459,6 +464,8 @@ static SDDS_DATASET *ref_table(long which)
     return &field_output_defn.SDDSout;
   if (which == 3 + SHIM_MAX_CLOSED_TABLES)
     return &saving_defn.outTable;
+  if (which >= 300)
+    return which - 300 < n_sample_defns ? &sample_defn[which - 300].outTable : NULL;
   if (which >= 200)
     return which - 200 < n_secondary && secondary[which - 200].logFile ? &secondary[which - 200].SDDSlog : NULL;
   if (which >= 100)

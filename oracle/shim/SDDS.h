@@ -82,6 +82,7 @@ int32_t SDDS_SetParameters(SDDS_DATASET *t, int32_t mode, ...);
 int32_t SDDS_WritePage(SDDS_DATASET *t);
 int32_t SDDS_WriteTable(SDDS_DATASET *t);
 int32_t SDDS_UpdatePage(SDDS_DATASET *t, uint32_t mode);
+#define SDDS_UpdateTable(t) SDDS_UpdatePage(t, 0)
 int32_t SDDS_Terminate(SDDS_DATASET *t);
 void SDDS_SetError(char *error_text);
 void SDDS_PrintErrors(FILE *fp, int32_t mode);

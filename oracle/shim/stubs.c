@@ -2,8 +2,8 @@
  *
  * No-op stand-ins for reference functions that perform_integration()
  * (integrate.c:149-193) calls every step but that lie outside the checked
- * path: field sampling and resistors (beam snapshots, field output, field
- * saving, surface emitters and the moving window are the reference's own
+ * path: resistors (beam snapshots, field output, field saving and
+ * sampling, surface emitters and the moving window are the reference's own
  * files).  Each is inert when its
  * command was never given, which is how the checked configurations run; the
  * ones that would act bomb instead, so a checker can never silently skip
@@ -21,14 +21,6 @@ char *compose_filename(char *template, char *root_name)
     return ptr;
   }
   return template;
-}
-
-void sample_fields(SAMPLE_DEFN *sample_defn, long n_sample_defns, FIELDS *EM_problem)
-{
-  (void)sample_defn;
-  (void)EM_problem;
-  if (n_sample_defns)
-    bomb("field sampling is not part of the checked path", NULL);
 }
 
 void add_resistor_currents(FIELDS *EM_problem, RESISTOR *resistor)

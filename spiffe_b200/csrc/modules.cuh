@@ -33,8 +33,8 @@ struct PushHostParams {
   int screen_momentum, compaction;
   LostLog lost;
 };
-extern "C" int spiffe_gather_points64(const DevMesh *m, const DevFields<double> *f, const double *zr, int n, double *E,
-                                      cudaStream_t s);
+extern "C" int spiffe_gather_points64(const DevMesh *m, const DevFields<double> *f, const double *zr, int n, int ncomp,
+                                      double *E, cudaStream_t s);
 extern "C" int spiffe_push64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b, const PushHostParams *hp,
                              const DevScreens *scr, DevCounts *cnt, long long np_bound, Particles64Work *w,
                              cudaStream_t s);

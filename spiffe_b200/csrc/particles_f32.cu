@@ -1079,7 +1079,7 @@ __global__ void k_births_commit32(long long total, long long capacity, int mode,
 
 // interpolateFields at n points (zr[2i], zr[2i+1]) of the split form's
 // fields: Ez, Er into E[2i], E[2i+1]
-__global__ void k_gather_points32(DevMesh m, DevFields32 f, const double *zr, int n, double *E)
+__global__ void k_gather_points32(DevMesh m, DevFields32 f, const double *zr, int n, int ncomp, double *E)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n)
@@ -1088,8 +1088,8 @@ __global__ void k_gather_points32(DevMesh m, DevFields32 f, const double *zr, in
   const int iz = (int)floor(xz), ir = (int)floor(xr);
   float e[6];
   gather32<false>(m, f, iz, (float)(xz - iz), ir, (float)(xr - ir), e);
-  E[2 * i] = e[0];
-  E[2 * i + 1] = e[1];
+  for (int c = 0; c < ncomp; c++)
+    E[(size_t)ncomp * i + c] = e[c];
 }
 
 // ---- conversions between the FP64 SoA and the split beam
@@ -1342,12 +1342,12 @@ extern "C" int s32_births(const DevMesh *m, const DevFields32 *f, const DevBeam3
   return (int)cudaGetLastError();
 }
 
-extern "C" int s32_gather_points(const DevMesh *m, const DevFields32 *f, const double *zr, int n, double *E,
+extern "C" int s32_gather_points(const DevMesh *m, const DevFields32 *f, const double *zr, int n, int ncomp, double *E,
                                  cudaStream_t s)
 {
   if (n <= 0)
     return 0;
-  k_gather_points32<<<blocks_for(n, 128), 128, 0, s>>>(*m, *f, zr, n, E);
+  k_gather_points32<<<blocks_for(n, 128), 128, 0, s>>>(*m, *f, zr, n, ncomp < 6 ? ncomp : 6, E);
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

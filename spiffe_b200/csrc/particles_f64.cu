@@ -903,25 +903,26 @@ extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, co
 
 
 namespace {
-// interpolateFields at n points (zr[2i], zr[2i+1]): Ez, Er into E[2i], E[2i+1]
-__global__ void k_gather_points64(DevMesh m, DevFields<double> f, const double *zr, int n, double *E)
+// interpolateFields at n points (zr[2i], zr[2i+1]): the first ncomp of
+// Ez, Er, Ephi, Bz, Br, Bphi into E[ncomp*i ...]
+__global__ void k_gather_points64(DevMesh m, DevFields<double> f, const double *zr, int n, int ncomp, double *E)
 {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n)
     return;
   double e[6];
   gather(m, f, zr[2 * i], zr[2 * i + 1], e);
-  E[2 * i] = e[0];
-  E[2 * i + 1] = e[1];
+  for (int c = 0; c < ncomp; c++)
+    E[(size_t)ncomp * i + c] = e[c];
 }
 } // namespace
 
-extern "C" int spiffe_gather_points64(const DevMesh *m, const DevFields<double> *f, const double *zr, int n, double *E,
-                                      cudaStream_t s)
+extern "C" int spiffe_gather_points64(const DevMesh *m, const DevFields<double> *f, const double *zr, int n, int ncomp,
+                                      double *E, cudaStream_t s)
 {
   if (n <= 0)
     return 0;
-  k_gather_points64<<<blocks_for(n, 128), 128, 0, s>>>(*m, *f, zr, n, E);
+  k_gather_points64<<<blocks_for(n, 128), 128, 0, s>>>(*m, *f, zr, n, ncomp < 6 ? ncomp : 6, E);
   spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }

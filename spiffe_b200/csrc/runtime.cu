@@ -133,6 +133,26 @@ struct HostEmitter {
   long long start_step = -1, stop_step = 0, step_emission_started = -1;
 };
 
+// One field sample waiting for download: its rows' coordinates and where
+// its values sit in the device sample buffer (6 per gathered point, or 1
+// per node read).
+struct SampleEvent {
+  double t = 0, param[3] = {0, 0, 0};
+  std::vector<double> x; // row coordinates (snapshot pages)
+  bool gathered = false; // interpolated at points, else read at nodes
+  size_t offset = 0, n = 0;
+  long long div = 1; // a time sequence's divisor, iz1 - iz0 + 1
+};
+
+// One define_field_sampling (SAMPLE_DEFN, spiffe.h:338-349).
+struct HostSampling {
+  spiffe_sample_options o{};
+  long long step_interval = -1, start_step = -1, sample_index = -1;
+  bool initialized = false; // fileInitialized: the parameters are fixed from the first sample
+  double param[3] = {0, 0, 0};
+  std::vector<SampleEvent> events;
+};
+
 // One cathode as the reference holds it (CATHODE, spiffe.h:236-262).
 struct HostCathode {
   spiffe_cathode_options o;
@@ -230,6 +250,12 @@ struct spiffe_gpu_instance {
   uint64_t rng_key = 0, rng_counter = 0;
   std::vector<HostEmitter> emitters;
   uint64_t rng2_key = 0, rng2_counter = 0; // random_2, the emitters' stream
+  std::vector<HostSampling> samplings;
+  double *d_samples = nullptr; // sampled values not yet downloaded
+  size_t samples_cap = 0, samples_used = 0;
+  long long *d_sample_idx = nullptr;
+  double *d_sample_pts = nullptr;
+  size_t sample_pts_cap = 0;
   long long *d_nodes = nullptr;            // node indices of field reads on the host's behalf
   double *d_node_vals = nullptr;
   size_t nodes_cap = 0;
@@ -956,7 +982,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
   void *p[] = {f.Ez, f.Er, f.Bphi, f.Bphi2, f.Jz, f.Jr, f.Ephi, f.Jphi, f.Br, f.Br2, f.Bz, f.Bz2,
                f.EzImposed, f.ErImposed, f.PsiImposed, f.BzImposed, f.BrImposed, f.Psi, f.Q, in->d_flags,
                in->cnt, in->d_bins, in->d_onaxis_data, in->d_onaxis, in->d_tr_flag, in->d_tr_scratch, in->d_pclog, in->d_status, in->d_moments, in->d_lost, in->d_points,
-               in->d_list, in->d_nodes, in->d_node_vals};
+               in->d_list, in->d_nodes, in->d_node_vals, in->d_samples, in->d_sample_idx, in->d_sample_pts};
   for (void *q : p)
     cudaFree(q);
   for (int k = 0; k < in->screens.n; k++) {
@@ -1611,8 +1637,8 @@ static int queue_secondaries(spiffe_gpu_instance *in, size_t first)
   }
   double *d_pts = in->d_points, *d_E = in->d_points + 2 * in->points_cap;
   CUDA_TRY(cudaMemcpyAsync(d_pts, pts.data(), sizeof(double) * pts.size(), cudaMemcpyHostToDevice, in->stream));
-  const int rc = in->s32 ? s32_gather_points(&in->dm, &in->s32->f, d_pts, (int)cand.size(), d_E, in->stream)
-                         : spiffe_gather_points64(&in->dm, &in->f, d_pts, (int)cand.size(), d_E, in->stream);
+  const int rc = in->s32 ? s32_gather_points(&in->dm, &in->s32->f, d_pts, (int)cand.size(), 2, d_E, in->stream)
+                         : spiffe_gather_points64(&in->dm, &in->f, d_pts, (int)cand.size(), 2, d_E, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "field gather failed: %s", cudaGetErrorString((cudaError_t)rc));
   CUDA_TRY(cudaMemcpyAsync(E.data(), d_E, sizeof(double) * E.size(), cudaMemcpyDeviceToHost, in->stream));
@@ -2792,6 +2818,418 @@ static int emit_emitters(spiffe_gpu_instance *in)
   return 0;
 }
 
+// ------------------------------------------------------------ field sampling
+
+// node reads of the sampled arrays: a[i] + (b ? b[i] : 0.0), field_sampling.c:331
+__global__ void k_sample_nodes(const double *a, const double *b, const long long *idx, int n, double *out)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n)
+    return;
+  const long long i = idx[k];
+  out[k] = a[i] + (b ? b[i] : 0.0);
+}
+
+// Room for `need` more values in the sample buffer; a larger buffer keeps
+// the values not yet downloaded.
+static int sample_room(spiffe_gpu_instance *in, size_t need)
+{
+  if (in->samples_used + need <= in->samples_cap)
+    return 0;
+  const size_t cap = std::max<size_t>(2 * (in->samples_used + need), 4096);
+  double *p = nullptr;
+  CUDA_TRY(cudaMalloc(&p, sizeof(double) * cap));
+  if (in->samples_used)
+    CUDA_TRY(cudaMemcpyAsync(p, in->d_samples, sizeof(double) * in->samples_used, cudaMemcpyDeviceToDevice,
+                             in->stream));
+  CUDA_TRY(cudaStreamSynchronize(in->stream));
+  cudaFree(in->d_samples);
+  in->d_samples = p;
+  in->samples_cap = cap;
+  return 0;
+}
+
+static int sample_staging(spiffe_gpu_instance *in, size_t n)
+{
+  if (n <= in->sample_pts_cap)
+    return 0;
+  CUDA_TRY(cudaStreamSynchronize(in->stream)); // the old staging may still be read
+  cudaFree(in->d_sample_idx);
+  cudaFree(in->d_sample_pts);
+  in->d_sample_idx = nullptr;
+  in->d_sample_pts = nullptr;
+  in->sample_pts_cap = std::max<size_t>(n, 1024);
+  CUDA_TRY(cudaMalloc(&in->d_sample_idx, sizeof(long long) * in->sample_pts_cap));
+  CUDA_TRY(cudaMalloc(&in->d_sample_pts, sizeof(double) * 2 * in->sample_pts_cap));
+  return 0;
+}
+
+// interpolateFields at the points (z, r) on the device into a new event
+static int sample_gather(spiffe_gpu_instance *in, const std::vector<double> &zr, SampleEvent &ev)
+{
+  const size_t n = zr.size() / 2;
+  ev.gathered = true;
+  ev.n = n;
+  RC_TRY(sample_room(in, 6 * n));
+  ev.offset = in->samples_used;
+  if (!n)
+    return 0;
+  RC_TRY(sample_staging(in, n));
+  CUDA_TRY(cudaMemcpyAsync(in->d_sample_pts, zr.data(), sizeof(double) * zr.size(), cudaMemcpyHostToDevice,
+                           in->stream));
+  // (pageable source: the call returns with the points copied out of `zr`;
+  // the next sample's copy into the staging buffer is ordered after this
+  // launch on the stream)
+  double *out = in->d_samples + ev.offset;
+  const int rc = in->s32 ? s32_gather_points(&in->dm, &in->s32->f, in->d_sample_pts, (int)n, 6, out, in->stream)
+                         : spiffe_gather_points64(&in->dm, &in->f, in->d_sample_pts, (int)n, 6, out, in->stream);
+  if (rc)
+    return fail(SPIFFE_ERR_CUDA, "field sampling launch failed: %s", cudaGetErrorString((cudaError_t)rc));
+  in->samples_used += 6 * n;
+  return 0;
+}
+
+// node values data[iz][ir] + data1[iz][ir] at (iz, ir) pairs into a new event
+static int sample_nodes(spiffe_gpu_instance *in, const double *data, const double *data1,
+                        const std::vector<long long> &izir, SampleEvent &ev)
+{
+  const size_t n = izir.size() / 2;
+  ev.gathered = false;
+  ev.n = n;
+  RC_TRY(sample_room(in, n));
+  ev.offset = in->samples_used;
+  if (!n)
+    return 0;
+  RC_TRY(sample_staging(in, n));
+  const long long P = in->s32 ? in->dm.pitch : in->mesh.nr + 1;
+  std::vector<long long> idx(n);
+  for (size_t k = 0; k < n; k++)
+    idx[k] = izir[2 * k] * P + izir[2 * k + 1];
+  CUDA_TRY(cudaMemcpyAsync(in->d_sample_idx, idx.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, in->stream));
+  k_sample_nodes<<<(unsigned)((n + 255) / 256), 256, 0, in->stream>>>(data, data1, in->d_sample_idx, (int)n,
+                                                                     in->d_samples + ev.offset);
+  CUDA_TRY(cudaGetLastError());
+  spiffe_note_launches(1);
+  in->samples_used += n;
+  return 0;
+}
+
+// sample_fields, field_sampling.c:103-1097.  The reference keeps iz0, iz1,
+// ir and data1 as locals of the whole call, so a definition may see what an
+// earlier one of the same call left there (the r-direction time sequence
+// averages over the z range and radius last set; Jz, Jr and Q add
+// PsiImposed after a Phi definition); the call state below carries them the
+// same way.
+static int sample_fields(spiffe_gpu_instance *in)
+{
+  if (in->samplings.empty())
+    return 0;
+  const spiffe_mesh &m = in->mesh;
+  const long nz = m.nz, nr = m.nr;
+  const double dz = m.dz, dr = m.dr, zmin = m.zmin;
+  long iz0 = 0, iz1 = 0, ir = 0, ir0 = 0, ir1 = 0, iz = 0;
+  bool data1 = false;
+  const double *F = nullptr, *Fimp = nullptr, *Fj[2] = {nullptr, nullptr}, *Fq = nullptr;
+  if (in->s32) {
+    F = in->s32->f.Psi;
+    Fimp = in->s32->f.PsiImposed;
+    Fq = in->s32->f.Q;
+  } else {
+    F = in->f.Psi;
+    Fimp = in->f.PsiImposed;
+    Fj[0] = in->f.Jz;
+    Fj[1] = in->f.Jr;
+    Fq = in->f.Q;
+  }
+  for (HostSampling &S : in->samplings) {
+    if (S.sample_index == -1) {
+      S.step_interval = (long long)(S.o.time_interval / m.dt + 0.5);
+      S.start_step = (long long)((S.o.start_time - m.start_time) / m.dt + 0.5);
+      S.sample_index = 0;
+    }
+    const int c = S.o.component;
+    const double *data = nullptr;
+    if (c == SPIFFE_SAMPLE_JZ)
+      data = Fj[0];
+    else if (c == SPIFFE_SAMPLE_JR)
+      data = Fj[1];
+    else if (c == SPIFFE_SAMPLE_PHI) {
+      data = F;
+      data1 = true;
+    } else if (c == SPIFFE_SAMPLE_Q)
+      data = Fq;
+    if (!(m.time_step >= S.start_step &&
+          (S.step_interval == 0 || (m.time_step - S.start_step) % S.step_interval == 0)))
+      continue;
+    const bool field = c <= SPIFFE_SAMPLE_BPHI || c == SPIFFE_SAMPLE_E || c == SPIFFE_SAMPLE_B;
+    const bool zdir = S.o.direction == 0;
+    SampleEvent ev;
+    char pbuf[64];
+    auto fixed = [&](const char *fmt, double v) { // the parameter as its header text reads back
+      snprintf(pbuf, sizeof(pbuf), fmt, v);
+      return std::strtod(pbuf, nullptr);
+    };
+    if (!S.o.time_sequence) {
+      ev.t = m.time;
+      std::vector<double> zr;
+      std::vector<long long> nodes;
+      if (field) {
+        if (zdir) {
+          if ((ir = (long)(S.o.position / dr)) < 0 || ir > nr - 1)
+            return fail(SPIFFE_ERR_INVALID, "sampling position out of range for Ez, Er, Ephi, Bz, Br, or Bphi samples vs z");
+          if ((iz0 = (long)((S.o.min_coord - zmin) / dz + 0.5)) <= 0 || iz0 > nz - 1)
+            iz0 = iz0 <= 0 ? 1 : nz - 1;
+          if ((iz1 = (long)((S.o.max_coord - zmin) / dz + 0.5)) <= 0 || iz1 > nz - 1)
+            iz1 = iz1 <= 0 ? 1 : nz - 1;
+          ev.param[0] = fixed("%21.15e", ir * dr);
+          for (iz = iz0; iz <= iz1; iz++) {
+            ev.x.push_back(zmin + iz * dz);
+            zr.push_back(zmin + iz * dz);
+            zr.push_back(ir * dr);
+          }
+        } else {
+          iz = (long)((S.o.position - zmin) / dz + 0.5);
+          if (iz <= 0 || iz > nz)
+            return fail(SPIFFE_ERR_INVALID, "sampling position out of range for Ez, Er, Ephi, Bz, Br, or Bphi samples vs z");
+          if ((ir0 = (long)(S.o.min_coord / dr)) < 0 || ir0 >= nr)
+            ir0 = ir0 < 0 ? 0 : nr - 1;
+          if ((ir1 = (long)(S.o.max_coord / dr)) < 0 || ir1 >= nr)
+            ir1 = ir1 < 0 ? 0 : nr - 1;
+          ev.param[0] = fixed("%21.15e", zmin + (iz - 0.5) * dz);
+          for (ir = ir0; ir <= ir1; ir++) {
+            ev.x.push_back(ir * dr);
+            zr.push_back(zmin + iz * dz);
+            zr.push_back(ir * dr);
+          }
+        }
+        RC_TRY(sample_gather(in, zr, ev));
+      } else {
+        if (!data)
+          return fail(SPIFFE_ERR_INVALID, "field sampling: this array is not held in this precision");
+        const bool jz = c == SPIFFE_SAMPLE_JZ, jr = c == SPIFFE_SAMPLE_JR;
+        if (zdir) {
+          if ((ir = (long)(jr ? S.o.position / dr + 0.5 : S.o.position / dr)) < 0 || ir > nr - 1)
+            return fail(SPIFFE_ERR_INVALID, jz ? "sampling position out of range for Ez/Jz/Br samples vs z"
+                                            : jr ? "sampling position out of range for Er/Jr/Bz samples vs z"
+                                                 : "sampling position out of range for potential/Ephi samples vs z");
+          if (jz) {
+            if ((iz0 = (long)((S.o.min_coord - zmin) / dz + 0.5)) <= 0 || iz0 > nz - 1)
+              iz0 = iz0 <= 0 ? 1 : nz - 1;
+            if ((iz1 = (long)((S.o.max_coord - zmin) / dz + 0.5)) <= 0 || iz1 > nz - 1)
+              iz1 = iz1 <= 0 ? 1 : nz - 1;
+          } else {
+            if ((iz0 = (long)((S.o.min_coord - zmin) / dz)) < 0 || iz0 > nz - 1)
+              iz0 = iz0 < 0 ? 0 : nz - 1;
+            if ((iz1 = (long)((S.o.max_coord - zmin) / dz)) < 0 || iz1 > nz - 1)
+              iz1 = iz1 < 0 ? 0 : nz - 1;
+          }
+          ev.param[0] = fixed("%21.15e", jr ? (ir - 0.5) * dr : ir * dr);
+          for (iz = iz0; iz <= iz1; iz++) {
+            ev.x.push_back(jz ? zmin + (iz - 0.5) * dz : zmin + iz * dz);
+            nodes.push_back(iz);
+            nodes.push_back(ir);
+          }
+        } else {
+          if (jz) {
+            iz = (long)((S.o.position - zmin) / dz + 0.5);
+            if (iz <= 0 || iz > nz)
+              return fail(SPIFFE_ERR_INVALID, "sampling position out of range for Ez/Jz/Br samples vs r");
+          } else {
+            iz = (long)((S.o.position - zmin) / dz);
+            if (iz < 0 || iz >= nz)
+              return fail(SPIFFE_ERR_INVALID, jr ? "sampling position out of range for Er/Jr/Bz samples vs r"
+                                                 : "sampling position out of range for potential/Ephi samples vs r");
+          }
+          if (jr) {
+            if ((ir0 = (long)(S.o.min_coord / dr + 0.5)) < 1 || ir0 > nr)
+              ir0 = ir0 < 1 ? 1 : nr;
+            if ((ir1 = (long)(S.o.max_coord / dr + 0.5)) < 1 || ir1 > nr)
+              ir1 = ir1 < 1 ? 1 : nr;
+          } else {
+            if ((ir0 = (long)(S.o.min_coord / dr)) < 0 || ir0 >= nr)
+              ir0 = ir0 < 0 ? 0 : nr - 1;
+            if ((ir1 = (long)(S.o.max_coord / dr)) < 0 || ir1 >= nr)
+              ir1 = ir1 < 0 ? 0 : nr - 1;
+          }
+          ev.param[0] = fixed("%21.15e", jz ? zmin + (iz - 0.5) * dz : zmin + iz * dz);
+          for (ir = ir0; ir <= ir1; ir++) {
+            ev.x.push_back(jr ? dr * (ir - 0.5) : dr * ir);
+            nodes.push_back(iz);
+            nodes.push_back(ir);
+          }
+        }
+        RC_TRY(sample_nodes(in, data, data1 ? Fimp : nullptr, nodes, ev));
+      }
+      if (!S.initialized) {
+        std::copy(ev.param, ev.param + 3, S.param);
+        S.initialized = true;
+      }
+      S.sample_index++;
+    } else {
+      // time sequence: the average of the interpolated fields over the range
+      if (!field || c == SPIFFE_SAMPLE_B)
+        return fail(SPIFFE_ERR_UNSUPPORTED, "time-sequence samples of this component are not supported");
+      ev.t = m.time_step * m.dt + m.start_time;
+      std::vector<double> zr;
+      if (zdir) {
+        if ((ir = (long)(S.o.position / dr)) < 0 || ir > nr - 1)
+          return fail(SPIFFE_ERR_INVALID, "sampling position out of range for Ez/Jz/Br time-sequence samples vs z");
+        if ((iz0 = (long)((S.o.min_coord - zmin) / dz + 0.5)) < 0 || iz0 > nz - 1)
+          return fail(SPIFFE_ERR_INVALID, "initial sampling coordinate out of range for Ez/Jz/Br samples vs z");
+        if ((iz1 = (long)((S.o.max_coord - zmin) / dz + 0.5)) < 0 || iz1 > nz - 1)
+          return fail(SPIFFE_ERR_INVALID, "final sampling coordinate out of range for Ez/Jz/Br time-sequence samples vs z");
+        if (iz0 <= 0)
+          iz0 = 1;
+        if (iz1 <= 0)
+          iz1 = 1;
+        if (!S.initialized) {
+          S.param[0] = fixed("%e", ir * dr);
+          S.param[1] = fixed("%e", iz0 * dz + zmin);
+          S.param[2] = fixed("%e", iz1 * dz + zmin);
+          S.initialized = true;
+          S.sample_index = 0;
+        }
+      } else {
+        iz = (long)((S.o.position - zmin) / dz + 0.5);
+        if (iz <= 0 || iz > nz)
+          return fail(SPIFFE_ERR_INVALID, "sampling position out of range for Ez/Jz/Br samples vs r");
+        if ((ir0 = (long)(S.o.min_coord / dr)) < 0 || ir0 >= nr)
+          ir0 = ir0 < 0 ? 0 : nr - 1;
+        if ((ir1 = (long)(S.o.max_coord / dr)) < 0 || ir1 >= nr)
+          ir1 = ir1 < 0 ? 0 : nr - 1;
+        if (!S.initialized) {
+          S.param[0] = fixed("%e", iz * dz + zmin);
+          S.param[1] = fixed("%e", ir0 * dr);
+          S.param[2] = fixed("%e", ir1 * dr);
+          S.initialized = true;
+          S.sample_index = 0;
+        }
+      }
+      // both directions average over iz0..iz1 at radius ir (field_sampling.c:756-767, :793-804)
+      for (iz = iz0; iz <= iz1; iz++) {
+        zr.push_back(zmin + iz * dz);
+        zr.push_back(ir * dr);
+      }
+      ev.div = iz1 - iz0 + 1;
+      RC_TRY(sample_gather(in, zr, ev));
+      std::copy(S.param, S.param + 3, ev.param);
+      S.sample_index++;
+    }
+    S.events.push_back(std::move(ev));
+  }
+  return 0;
+}
+
+extern "C" int spiffe_gpu_add_field_sampling(spiffe_gpu_instance *in, const spiffe_sample_options *o, int32_t *index)
+{
+  if (!in || !o)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  // process_sampling_definition, field_sampling.c:53-101
+  if (!in->mesh.nr || !in->mesh.nz)
+    return fail(SPIFFE_ERR_INVALID, "you must defined the problem geometry before specifying field sampling");
+  if (o->component < 0 || o->component > SPIFFE_SAMPLE_B)
+    return fail(SPIFFE_ERR_INVALID, "field component name is not recognized");
+  const int c = o->component;
+  if (c == SPIFFE_SAMPLE_EPHI || c == SPIFFE_SAMPLE_BPHI || c == SPIFFE_SAMPLE_BZ) { // codes 2, 5, 3
+    if (!(in->mesh.modes & SPIFFE_FL_TE_FIELDS))
+      return fail(SPIFFE_ERR_INVALID, "can't sample TE fields unless they are enabled in define_geometry namelist");
+  } else if (!(in->mesh.modes & SPIFFE_FL_TM_FIELDS)) {
+    return fail(SPIFFE_ERR_INVALID, "can't sample TM fields/potential unless they are enabled in define_geometry namelist");
+  }
+  if (o->direction < 0 || o->direction > 1)
+    return fail(SPIFFE_ERR_INVALID, "direction name is not recognized");
+  if (o->min_coord > o->max_coord)
+    return fail(SPIFFE_ERR_INVALID, "min_coord > max_coord for field samples");
+  if (o->time_interval <= 0)
+    return fail(SPIFFE_ERR_INVALID, "time_interval <=0 for field samples");
+  if (o->time_sequence && (c == SPIFFE_SAMPLE_B || c == SPIFFE_SAMPLE_JZ || c == SPIFFE_SAMPLE_JR ||
+                           c == SPIFFE_SAMPLE_PHI || c == SPIFFE_SAMPLE_Q))
+    return fail(SPIFFE_ERR_UNSUPPORTED, "time-sequence samples of BAll, Jz, Jr, Phi and Q are not supported");
+  if (in->s32 && (c == SPIFFE_SAMPLE_JZ || c == SPIFFE_SAMPLE_JR))
+    return fail(SPIFFE_ERR_UNSUPPORTED, "Jz and Jr samples are not available in the split-precision form");
+  HostSampling S;
+  S.o = *o;
+  in->samplings.push_back(S);
+  if (index)
+    *index = (int32_t)in->samplings.size() - 1;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_sample_fields(spiffe_gpu_instance *in)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  return sample_fields(in);
+}
+
+extern "C" int spiffe_gpu_download_samples(spiffe_gpu_instance *in, int32_t index, spiffe_sample_set *h)
+{
+  if (!in || !h || index < 0 || (size_t)index >= in->samplings.size())
+    return fail(SPIFFE_ERR_INVALID, "bad argument");
+  HostSampling &S = in->samplings[(size_t)index];
+  const bool seq = S.o.time_sequence != 0;
+  const int ncol = S.o.component == SPIFFE_SAMPLE_E || S.o.component == SPIFFE_SAMPLE_B ? 3 : 1;
+  int64_t rows = 0;
+  for (const SampleEvent &ev : S.events)
+    rows += seq ? 1 : (int64_t)ev.x.size();
+  h->n_samples = (int64_t)S.events.size();
+  h->n_rows = rows;
+  if (h->max_samples == 0)
+    return 0;
+  if (h->n_samples > h->max_samples || rows > h->max_rows)
+    return fail(SPIFFE_ERR_CAPACITY, "%lld samples of %lld rows do not fit the host buffers",
+                (long long)h->n_samples, (long long)rows);
+  // every value of the buffer belongs to some definition: copy it all once
+  std::vector<double> v(in->samples_used);
+  if (!v.empty()) {
+    CUDA_TRY(cudaMemcpyAsync(v.data(), in->d_samples, sizeof(double) * v.size(), cudaMemcpyDeviceToHost, in->stream));
+    CUDA_TRY(cudaStreamSynchronize(in->stream));
+  }
+  // which of interpolateFields' outputs (Ez, Er, Ephi, Bz, Br, Bphi) a column
+  // takes (field_sampling.c:233-246, :1035-1088): fieldValue[component]
+  int pick[3] = {S.o.component, 0, 0};
+  if (S.o.component == SPIFFE_SAMPLE_E)
+    pick[0] = 0, pick[1] = 1, pick[2] = 2;
+  else if (S.o.component == SPIFFE_SAMPLE_B)
+    pick[0] = 3, pick[1] = 4, pick[2] = 5;
+  int64_t r = 0;
+  for (size_t k = 0; k < S.events.size(); k++) {
+    const SampleEvent &ev = S.events[k];
+    h->t[k] = ev.t;
+    for (int q = 0; q < 3; q++)
+      h->param[3 * k + q] = ev.param[q];
+    const double *src = v.data() + ev.offset;
+    if (seq) {
+      double sum[6] = {0, 0, 0, 0, 0, 0};
+      for (size_t i = 0; i < ev.n; i++)
+        for (int q = 0; q < 6; q++)
+          sum[q] += src[6 * i + q];
+      h->rows[k] = 1;
+      h->x[r] = ev.t;
+      for (int q = 0; q < ncol; q++)
+        if (h->v[q])
+          h->v[q][r] = sum[pick[q]] / (double)ev.div;
+      r++;
+    } else {
+      h->rows[k] = (int64_t)ev.x.size();
+      for (size_t i = 0; i < ev.x.size(); i++, r++) {
+        h->x[r] = ev.x[i];
+        for (int q = 0; q < ncol; q++)
+          if (h->v[q])
+            h->v[q][r] = ev.gathered ? src[6 * i + pick[q]] : src[i];
+      }
+    }
+  }
+  S.events.clear();
+  // the buffer empties once no definition holds samples in it
+  bool any = false;
+  for (const HostSampling &o : in->samplings)
+    any = any || !o.events.empty();
+  if (!any)
+    in->samples_used = 0;
+  return 0;
+}
+
 extern "C" int spiffe_gpu_add_emitter(spiffe_gpu_instance *in, const spiffe_emitter_options *o)
 {
   if (!in || !o)
@@ -2953,6 +3391,7 @@ extern "C" int spiffe_gpu_run_steps(spiffe_gpu_instance *in, int64_t n_steps)
     if (m.imposed_ramp_time > 0)
       RC_TRY(imposed_efield(in, &in->pc, 0));
     m.time = m.time_step * m.dt + m.start_time;
+    RC_TRY(sample_fields(in)); // integrate.c:149
     RC_TRY(emit(in));
     RC_TRY(emit_test(in));
     S32State *S = in->s32;

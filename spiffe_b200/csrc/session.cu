@@ -170,6 +170,17 @@ struct SessionCathode {
   bool on_device = false;
 };
 
+// one define_field_sampling definition and its file
+struct SessionSampling {
+  spiffe_sample_options o{};
+  std::string path;
+  int32_t index = -1; // on the device
+  spiffe_sdds::Writer out;
+  bool opened = false;
+  std::vector<double> seq_t, seq_v[3]; // a time sequence's rows so far
+  double seq_param[3] = {0, 0, 0};
+};
+
 // one define_emitter definition with its surface and profile
 struct SessionEmitter {
   spiffe_emitter_options o{};
@@ -275,6 +286,7 @@ double **slot(spiffe_field_set &f, const std::string &n)
 struct spiffe_session {
   int precision = SPIFFE_PRECISION_F64;
   std::string rootname = "spiffe";
+  std::string run_name = "spiffe"; // EM_problem->run_name: the input file (spiffe.c:204)
   int verbose = 1;
   int deposit_order = 1;
   long long particle_capacity = 1 << 16, screen_capacity = 1 << 20, flush_steps = 512;
@@ -288,6 +300,7 @@ struct spiffe_session {
   std::vector<SessionCathode> cathodes;
   std::vector<SessionSecondary> secondaries;
   std::vector<SessionEmitter> emitters;
+  std::vector<SessionSampling> samplings;
   spiffe_geometry_options geo_opts{}; // define_geometry's drawing, for the emitters' surfaces
   std::string geo_text;
   std::vector<int16_t> material; // define_geometry's surface materials (materialID)
@@ -385,6 +398,8 @@ struct spiffe_session {
   int cmd_screen(Args &g);
   int cmd_secondary_emission(Args &g);
   int cmd_emitter(Args &g);
+  int cmd_field_sampling(Args &g);
+  int flush_samples();
   int cmd_test_beam(Args &g);
   int cmd_poisson(Args &g);
   int cmd_load_fields(Args &g);
@@ -684,6 +699,156 @@ int spiffe_session::cmd_cathode(Args &g)
   o.profile_t = o.profile_A = nullptr;
   c.o = o;
   cathodes.push_back(std::move(c));
+  return 0;
+}
+
+// ------------------------------------------------------ define_field_sampling
+
+// the component and direction names of field_sampling.c:28-44 (units of the
+// single-component columns)
+static const std::vector<std::string> SAMPLE_NAMES = {"Ez", "Er", "Ephi", "Bz", "Br", "Bphi",
+                                                      "Jz", "Jr", "Phi", "Q", "EAll", "BAll"};
+static const char *SAMPLE_UNITS[10] = {"V/m", "V/m", "V/m", "T", "T", "T", "A/m$a2$n", "A/m$a2$n", "V", "C"};
+
+// process_sampling_definition, field_sampling.c:53-101
+int spiffe_session::cmd_field_sampling(Args &g)
+{
+  std::string filename, component, direction;
+  spiffe_sample_options o{};
+  const bool have_file = g.str("filename", filename);
+  const bool have_comp = g.str("component", component);
+  const bool have_dir = g.str("direction", direction);
+  long long seq = 0;
+  g.num("min_coord", o.min_coord);
+  g.num("max_coord", o.max_coord);
+  g.num("position", o.position);
+  g.num("time_interval", o.time_interval);
+  g.num("start_time", o.start_time);
+  g.integer("time_sequence", seq);
+  S_TRY(g.finish());
+  if (!have_geometry)
+    return serr(SPIFFE_ERR_INVALID, "you must defined the problem geometry before specifying field sampling");
+  if (!have_file)
+    return serr(SPIFFE_ERR_INVALID, "no filename given for field samples");
+  if (!have_comp)
+    return serr(SPIFFE_ERR_INVALID, "no field component named for field samples");
+  if ((o.component = match(component, SAMPLE_NAMES)) < 0)
+    return serr(SPIFFE_ERR_INVALID, "field component name is not recognized");
+  if (o.component == SPIFFE_SAMPLE_EPHI || o.component == SPIFFE_SAMPLE_BPHI || o.component == SPIFFE_SAMPLE_BZ) {
+    if (!(mesh.modes & SPIFFE_FL_TE_FIELDS))
+      return serr(SPIFFE_ERR_INVALID, "can't sample TE fields unless they are enabled in define_geometry namelist");
+  } else if (!(mesh.modes & SPIFFE_FL_TM_FIELDS)) {
+    return serr(SPIFFE_ERR_INVALID, "can't sample TM fields/potential unless they are enabled in define_geometry namelist");
+  }
+  if (!have_dir)
+    return serr(SPIFFE_ERR_INVALID, "no direction named for field samples");
+  if ((o.direction = match(direction, {"z", "r"})) < 0)
+    return serr(SPIFFE_ERR_INVALID, "direction name is not recognized");
+  if (o.min_coord > o.max_coord)
+    return serr(SPIFFE_ERR_INVALID, "min_coord > max_coord for field samples");
+  if (o.time_interval <= 0)
+    return serr(SPIFFE_ERR_INVALID, "time_interval <=0 for field samples");
+  o.time_sequence = (int32_t)seq;
+  SessionSampling d;
+  d.o = o;
+  d.path = compose(filename, rootname);
+  samplings.push_back(std::move(d));
+  return 0;
+}
+
+// The samples since the last flush, written as sample_fields writes them:
+// a page per sample (z or r, then the component columns; rSample or zSample
+// fixed, runName, tSample per page), or for a time sequence one page of rows
+// (t and the component columns) rewritten with the rows so far.
+int spiffe_session::flush_samples()
+{
+  using namespace spiffe_sdds;
+  for (SessionSampling &d : samplings) {
+    if (d.index < 0)
+      continue;
+    spiffe_sample_set h{};
+    S_TRY(spiffe_gpu_download_samples(inst, d.index, &h));
+    if (!h.n_samples)
+      continue;
+    const int64_t ns = h.n_samples, nr = h.n_rows;
+    std::vector<double> t((size_t)ns), param(3 * (size_t)ns), x((size_t)nr), v[3];
+    std::vector<int64_t> rows((size_t)ns);
+    const int c = d.o.component, ncol = c == SPIFFE_SAMPLE_E || c == SPIFFE_SAMPLE_B ? 3 : 1;
+    for (int q = 0; q < ncol; q++)
+      v[q].resize((size_t)nr);
+    h.max_samples = ns;
+    h.max_rows = nr;
+    h.t = t.data();
+    h.param = param.data();
+    h.rows = rows.data();
+    h.x = x.data();
+    for (int q = 0; q < ncol; q++)
+      h.v[q] = v[q].data();
+    S_TRY(spiffe_gpu_download_samples(inst, d.index, &h));
+    // column names: the component, or its three (field_sampling.c:179-203)
+    std::vector<Def> cols;
+    const bool zdir = d.o.direction == 0, seq = d.o.time_sequence != 0;
+    cols.push_back(seq ? Def{"t", "s", "", T_DOUBLE} : Def{zdir ? "z" : "r", "m", "", T_DOUBLE});
+    if (ncol == 3) {
+      const int base = c == SPIFFE_SAMPLE_E ? 0 : 3;
+      for (int q = 0; q < 3; q++)
+        cols.push_back(Def{SAMPLE_NAMES[(size_t)(base + q)], SAMPLE_UNITS[base + q], "", T_DOUBLE});
+    } else {
+      cols.push_back(Def{SAMPLE_NAMES[(size_t)c], SAMPLE_UNITS[c], "", T_DOUBLE});
+    }
+    auto fixed = [](const char *name, const char *units, const char *fmt, double value) {
+      Def p{name, units, "", T_DOUBLE};
+      char buf[64];
+      snprintf(buf, sizeof(buf), fmt, value);
+      p.fixed = true;
+      p.fixed_value = buf;
+      return p;
+    };
+    Def run{"runName", "", "", T_STRING};
+    run.fixed = true;
+    run.fixed_value = run_name;
+    std::string err;
+    if (!seq) {
+      if (!d.opened) {
+        // the parameter values come back parsed from the same text, so they print the same
+        std::vector<Def> params = {fixed(zdir ? "rSample" : "zSample", "m", "%21.15e", param[0]), run,
+                                   Def{"tSample", "s", "", T_DOUBLE}};
+        if (!d.out.open(d.path, "", "", params, cols, err))
+          return serr(SPIFFE_ERR_INVALID, "define_field_sampling: %s", err.c_str());
+        d.opened = true;
+      }
+      int64_t r = 0;
+      for (int64_t k = 0; k < ns; k++) {
+        std::vector<const void *> cp = {x.data() + r};
+        for (int q = 0; q < ncol; q++)
+          cp.push_back(v[q].data() + r);
+        if (!d.out.write_page({t[(size_t)k]}, {}, rows[(size_t)k], cp, err))
+          return serr(SPIFFE_ERR_INVALID, "define_field_sampling: %s", err.c_str());
+        r += rows[(size_t)k];
+      }
+    } else {
+      if (d.seq_t.empty())
+        std::copy(param.begin(), param.begin() + 3, d.seq_param);
+      d.seq_t.insert(d.seq_t.end(), x.begin(), x.end());
+      for (int q = 0; q < ncol; q++)
+        d.seq_v[q].insert(d.seq_v[q].end(), v[q].begin(), v[q].end());
+      Def dir{"scanDirection", "", "", T_STRING};
+      dir.fixed = true;
+      dir.fixed_value = zdir ? "z" : "r";
+      std::vector<Def> params = {run, dir, fixed(zdir ? "rSample" : "zSample", "m", "%e", d.seq_param[0]),
+                                 fixed(zdir ? "zStart" : "rStart", "m", "%e", d.seq_param[1]),
+                                 fixed(zdir ? "zStop" : "rStop", "m", "%e", d.seq_param[2])};
+      Writer w; // the whole page again, as the reference's updated page reads at the end
+      if (!w.open(d.path, "", "", params, cols, err))
+        return serr(SPIFFE_ERR_INVALID, "define_field_sampling: %s", err.c_str());
+      std::vector<const void *> cp = {d.seq_t.data()};
+      for (int q = 0; q < ncol; q++)
+        cp.push_back(d.seq_v[q].data());
+      if (!w.write_page({}, {}, (int64_t)d.seq_t.size(), cp, err))
+        return serr(SPIFFE_ERR_INVALID, "define_field_sampling: %s", err.c_str());
+      w.close();
+    }
+  }
   return 0;
 }
 
@@ -1714,6 +1879,9 @@ int spiffe_session::ensure_instance()
       S_TRY(spiffe_gpu_add_cathode(inst, &o));
       c.on_device = true;
     }
+  for (SessionSampling &d : samplings)
+    if (d.index < 0)
+      S_TRY(spiffe_gpu_add_field_sampling(inst, &d.o, &d.index));
   for (SessionEmitter &e : emitters)
     if (!e.on_device) {
       spiffe_emitter_options o = e.o;
@@ -2074,6 +2242,7 @@ int spiffe_session::cmd_integrate(Args &g)
     S_TRY(flush_screens(next - 1, (next - 1) * step_dt + t0));
     S_TRY(flush_lost());
     S_TRY(flush_secondary_logs());
+    S_TRY(flush_samples());
     k = next;
   }
   if (lost_on) { // SDDS_Terminate, integrate.c:203
@@ -2085,6 +2254,8 @@ int spiffe_session::cmd_integrate(Args &g)
   S_TRY(spiffe_gpu_get_mesh(inst, &m));
   m.time = m.time_step * m.dt + m.start_time;
   S_TRY(spiffe_gpu_set_mesh(inst, &m));
+  S_TRY(spiffe_gpu_sample_fields(inst));
+  S_TRY(flush_samples());
   S_TRY(save_fields(m.time_step, m.time, true));
   S_TRY(take_snapshot(m.time_step, m.time));
   if (status_interval > 0 && m.time_step % status_interval == 0)
@@ -2142,8 +2313,7 @@ int spiffe_session::execute(const std::string &text)
     } else if (c == "define_field_output") {
       rc = cmd_field_output(g);
     } else if (c == "define_field_sampling") {
-      warn("%s: diagnostic output is not produced", c.c_str());
-      rc = 0;
+      rc = cmd_field_sampling(g);
     } else if (c == "translate") {
       rc = cmd_translate(g);
     } else if (c == "define_secondary_emission") {
@@ -2335,6 +2505,7 @@ extern "C" int spiffe_session_run_file(spiffe_session *s, const char *path)
   std::string text, err;
   if (!read_text(path, text, err))
     return serr(SPIFFE_ERR_INVALID, "%s", err.c_str());
+  s->run_name = path;
   return s->execute(text);
 }
 

@@ -144,7 +144,7 @@ extern "C" int s32_deposit(const DevMesh *m, const DevFields32 *f, const DevBeam
 extern "C" int s32_push(const DevMesh *m, const DevFields32 *f, const DevBeam32 *b, const Push32Params *p,
                         const DevScreens *scr, DevCounts *cnt, long long np_bound, int compaction,
                         const S32Scales *sc, Particles32Work *w, cudaStream_t s);
-extern "C" int s32_gather_points(const DevMesh *m, const DevFields32 *f, const double *zr, int n, double *E,
+extern "C" int s32_gather_points(const DevMesh *m, const DevFields32 *f, const double *zr, int n, int ncomp, double *E,
                                  cudaStream_t s);
 extern "C" int s32_sort(const DevMesh *m, DevBeam32 *b, DevCounts *cnt, long long np_bound, Particles32Work *w,
                         cudaStream_t s);

@@ -420,6 +420,55 @@ def deck_emitter(geo):
     save("deck_emitter", **out)
 
 
+# Field sampling (field_sampling.c) on the DC gun deck: pages of Ez, all of
+# E, Br (the TM-only one of Br and Bphi, field_sampling.c:80-85), Phi (plus the imposed
+# potential), Q (which, after a Phi definition, also gets the imposed
+# potential added), Jz and Jr at 40 ps intervals; time sequences of Ez
+# along z and of Er along r (which averages over the last z range and
+# radius the call set) every 4 and 8 ps.
+DECK_SAMPLING = DECK_DCGUN.replace("finish_time=300e-12", "finish_time=160e-12").replace(
+    "&integrate",
+    '&define_field_sampling filename="%s.ez", component="Ez", direction="z", min_coord=0, max_coord=0.03, '
+    'position=0.001, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.e", component="EAll", direction="r", min_coord=0, max_coord=0.01, '
+    'position=0.005, time_interval=40e-12, start_time=20e-12 &end\n'
+    '&define_field_sampling filename="%s.br", component="Br", direction="z", min_coord=0.002, max_coord=0.02, '
+    'position=0.002, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.phi", component="Phi", direction="r", min_coord=0, max_coord=0.015, '
+    'position=0.008, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.q", component="Q", direction="z", min_coord=0, max_coord=0.012, '
+    'position=0.0005, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.jz", component="Jz", direction="z", min_coord=0, max_coord=0.012, '
+    'position=0.0004, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.jr", component="Jr", direction="r", min_coord=0, max_coord=0.004, '
+    'position=0.003, time_interval=40e-12 &end\n'
+    '&define_field_sampling filename="%s.ezt", component="Ez", direction="z", min_coord=0.002, max_coord=0.004, '
+    'position=0.001, time_interval=4e-12, time_sequence=1 &end\n'
+    '&define_field_sampling filename="%s.ert", component="Er", direction="r", min_coord=0, max_coord=0.004, '
+    'position=0.006, time_interval=8e-12, time_sequence=1 &end\n'
+    "&integrate")
+SAMPLING_PAGES = [("ez", ["z", "Ez"]), ("e", ["r", "Ez", "Er", "Ephi"]), ("br", ["z", "Br"]), ("phi", ["r", "Phi"]),
+                  ("q", ["z", "Q"]), ("jz", ["z", "Jz"]), ("jr", ["r", "Jr"])]
+SAMPLING_SEQ = [("ezt", ["t", "Ez"]), ("ert", ["t", "Er"])]
+
+
+def deck_sampling(geo):
+    d = tempfile.mkdtemp()
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(geo)
+    cmds = [b.strip() + " &end" for b in DECK_SAMPLING.split("&end") if b.strip()]
+    prog = [("command", c) for c in cmds]
+    prog += [("table", 300 + k, cols) for k, (_, cols) in enumerate(SAMPLING_PAGES)]
+    prog += [("table", 100 + k, cols) for k, (_, cols) in enumerate(SAMPLING_SEQ)]
+    res = pyoracle.run_reference(prog, cwd=d, capacity=20000)
+    out = dict(deck=np.array(DECK_SAMPLING), geo=np.array(geo))
+    for (name, cols), t in zip(SAMPLING_PAGES + SAMPLING_SEQ, res):
+        out[name + "_pages"] = t["pages"]
+        for c in cols:
+            out[name + "_" + c] = t[c]
+    save("deck_sampling", **out)
+
+
 # The DC gun deck with define_field_saving (field_saving.c:46-213): saves at
 # 0 and 100 ps and before exiting.  The saved columns are compared through
 # SHA-256 digests of their values (bit-for-bit equality needs nothing more,
@@ -533,6 +582,7 @@ def decks():
     deck_fieldsave(geo)
     deck_secondary(geo)
     deck_emitter(geo)
+    deck_sampling(geo)
 
 
 def deck_onaxis(geo):
@@ -562,6 +612,8 @@ if __name__ == "__main__":
         deck_translate(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["fieldsave"]:
         deck_fieldsave(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
+    elif sys.argv[1:] == ["sampling"]:
+        deck_sampling(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["emitter"]:
         deck_emitter(str(np.load(os.path.join(HERE, "dcgun_geometry.npz"))["geo"]))
     elif sys.argv[1:] == ["secondary"]:

@@ -177,3 +177,24 @@ def test_emitters(tmp_path):
         assert np.array_equal(rb[k], fx["out_" + k]), k
     for c in abi.SCREEN_COLUMNS:
         assert np.array_equal(rs[c], fx["screen0_" + c]), c
+
+
+def test_field_sampling(tmp_path):
+    """Field sampling through the drop-in: the reference's own sample_fields
+    reads the host fields the drop-in brings back each step; every sampled
+    file equals the pure reference run's."""
+    fx = load("deck_sampling")
+    d = str(tmp_path)
+    with open(os.path.join(d, "dc.geo"), "w") as f:
+        f.write(str(fx["geo"]))
+    pages = [("ez", ["z", "Ez"]), ("e", ["r", "Ez", "Er", "Ephi"]), ("br", ["z", "Br"]), ("phi", ["r", "Phi"]),
+             ("q", ["z", "Q"]), ("jz", ["z", "Jz"]), ("jr", ["r", "Jr"])]
+    seq = [("ezt", ["t", "Ez"]), ("ert", ["t", "Er"])]
+    cmds = [b.strip() + " &end" for b in str(fx["deck"]).split("&end") if b.strip()]
+    prog = [("command", c) for c in cmds] + [("table", 300 + k, cols) for k, (_, cols) in enumerate(pages)]
+    prog += [("table", 100 + k, cols) for k, (_, cols) in enumerate(seq)]
+    res = run_with_dropin(prog, d, capacity=20000)
+    for (name, cols), t in zip(pages + seq, res):
+        assert t["pages"] == int(fx[name + "_pages"]), name
+        for c in cols:
+            assert np.array_equal(t[c], fx[name + "_" + c]), (name, c)

@@ -781,6 +781,54 @@ def test_emitters_split_form(tmp_path, monkeypatch):
     s.close()
 
 
+SAMPLING_PAGES = [("ez", ["z", "Ez"]), ("e", ["r", "Ez", "Er", "Ephi"]), ("br", ["z", "Br"]), ("phi", ["r", "Phi"]),
+                  ("q", ["z", "Q"]), ("jz", ["z", "Jz"]), ("jr", ["r", "Jr"])]
+SAMPLING_SEQ = [("ezt", ["t", "Ez"]), ("ert", ["t", "Er"])]
+
+
+@pytest.mark.gpu
+def test_field_sampling_matches_reference(tmp_path, monkeypatch):
+    """define_field_sampling (field_sampling.c) on the DC gun deck, sampled on
+    the device at the top of each step: pages of interpolated fields (Ez,
+    all of E, Br), of node arrays (Phi with the imposed potential, Q, Jz,
+    Jr) and time sequences of range averages equal the reference's files in
+    the FP64 form, including its call-wide state (Q after a Phi definition
+    gets the imposed potential added; the r-direction time sequence averages
+    over the last z range and radius set)."""
+    fx = load("deck_sampling")
+    s = run_deck(fx, tmp_path, monkeypatch)
+    for name, cols in SAMPLING_PAGES + SAMPLING_SEQ:
+        pages = session.read_sdds(str(tmp_path / ("spiffe." + name)))
+        assert len(pages) == int(fx[name + "_pages"]), name
+        for c in cols:
+            got = np.concatenate([np.asarray(p["columns"][c], np.float64) for p in pages])
+            assert np.array_equal(got, fx[name + "_" + c]), (name, c)
+    s.close()
+
+
+@pytest.mark.gpu
+def test_field_sampling_split_form(tmp_path, monkeypatch):
+    """The same sampling in the split form (Jz and Jr are not held in FP64
+    there and are dropped from the deck): the same pages and rows, and the
+    sampled fields within 1e-4 of the largest magnitude of the reference's."""
+    fx = load("deck_sampling")
+    deck = "\n".join(l for l in str(fx["deck"]).split("\n") if 'component="J' not in l)
+    fx = dict(fx)
+    fx["deck"] = np.array(deck)
+    s = run_deck(fx, tmp_path, monkeypatch, precision="split32")
+    for name, cols in SAMPLING_PAGES + SAMPLING_SEQ:
+        if name in ("jz", "jr"):
+            continue
+        pages = session.read_sdds(str(tmp_path / ("spiffe." + name)))
+        assert len(pages) == int(fx[name + "_pages"]), name
+        for c in cols:
+            got = np.concatenate([np.asarray(p["columns"][c], np.float64) for p in pages])
+            ref = fx[name + "_" + c]
+            assert got.shape == ref.shape, (name, c)
+            assert np.max(np.abs(got - ref)) <= 1e-4 * max(np.max(np.abs(ref)), 1e-30), (name, c)
+    s.close()
+
+
 @pytest.mark.gpu
 def test_field_saves_match_reference(tmp_path, monkeypatch):
     """define_field_saving (field_saving.c:46-213) on the DC gun deck in the
