@@ -269,6 +269,10 @@ int spiffe_gpu_set_sort_interval(spiffe_gpu_instance *inst, int64_t n);
  * the reference's red-black SOR.  Laplace solves (target 1, the imposed field)
  * always use SOR.  The FP64 form accepts SPIFFE_POISSON_SOR only. */
 int spiffe_gpu_set_poisson_solver(spiffe_gpu_instance *inst, int32_t solver);
+/* The split form's TM field update (integrate.c:308-433), one of
+ * SPIFFE_FDTD_* (spiffe_b200_types.h).  All give the same bits.  The FP64
+ * form accepts SPIFFE_FDTD_AUTO only. */
+int spiffe_gpu_set_fdtd_kernel(spiffe_gpu_instance *inst, int32_t kernel);
 /* Batched execution (no counterpart in the reference, which runs one problem
  * per process): advances n independent instances concurrently, instance i by
  * steps[i] steps of spiffe_gpu_run_steps, on `workers` host threads.  Each

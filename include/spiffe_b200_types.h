@@ -136,6 +136,11 @@ typedef struct spiffe_secondary_options {
 } spiffe_secondary_options;
 #define SPIFFE_SECONDARY_LOG_COLS 10
 
+/* TM field update of the split-precision form (spiffe_gpu_set_fdtd_kernel) */
+#define SPIFFE_FDTD_AUTO 0        /* the fused kernel on meshes of 2^18 nodes and more, else two kernels */
+#define SPIFFE_FDTD_TWO_KERNELS 1 /* an E and a B kernel over 2-D tiles */
+#define SPIFFE_FDTD_FUSED 2       /* one persistent kernel sweeping bands of rows staged by bulk copies */
+
 /* Poisson solver of the split-precision form (spiffe_gpu_set_poisson_solver) */
 #define SPIFFE_POISSON_SOR 0       /* the reference's red-black SOR and stop rule (poisson.c:17-130) */
 #define SPIFFE_POISSON_MULTIGRID 1 /* FP32 multigrid V-cycles in FP64 refinement, the same stop rule */

@@ -297,6 +297,7 @@ __host__ __device__ inline int find_loss_coordinates(double zmin, double zmax, d
 #define SPIFFE_DEV_ERR_SCREEN 2u
 #define SPIFFE_DEV_ERR_BARRIER 4u
 #define SPIFFE_DEV_ERR_INDEX 8u
+#define SPIFFE_DEV_ERR_WAIT 16u // a bounded wait inside a persistent kernel ran out
 
 __host__ __device__ inline size_t node(int iz, int ir, int pitch) { return (size_t)iz * (size_t)pitch + (size_t)ir; }
 

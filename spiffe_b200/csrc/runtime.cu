@@ -186,6 +186,7 @@ struct S32State {
   DevBeam32 b{};
   uint8_t *umask = nullptr;
   Fdtd32Tables fdtd;
+  int fdtd_mode = SPIFFE_FDTD_AUTO;
   double fdtd_dt = -1;
   Particles32Work pw;
   Poisson32Work pcw;
@@ -404,6 +405,8 @@ static int read_counts(spiffe_gpu_instance *in)
     return fail(SPIFFE_ERR_CAPACITY, "particle capacity exceeded on the device");
   if (in->h_cnt->error & SPIFFE_DEV_ERR_BARRIER)
     return fail(SPIFFE_ERR_DEVICE, "Poisson solver grid barrier timed out");
+  if (in->h_cnt->error & SPIFFE_DEV_ERR_WAIT)
+    return fail(SPIFFE_ERR_DEVICE, "a bounded wait of the fused FDTD kernel ran out");
   if (in->h_cnt->error & SPIFFE_DEV_ERR_INDEX)
     return fail(SPIFFE_ERR_INVALID, "a particle moved more than 32767 cells outside the mesh (split-precision cell range)");
   if (in->h_cnt->screen_overflow)
@@ -832,7 +835,8 @@ static int s32_fdtd(spiffe_gpu_instance *in, int zero_j)
   RC_TRY(s32_ensure_fdtd(in));
   PhaseScope ps(in, PH_FDTD);
   in->fdtd_steps++;
-  const int rc = s32_fdtd_step(&in->dm, &S.f, &S.fdtd, S.sc.kJ, zero_j, in->stream);
+  S.fdtd.mode = S.fdtd_mode;
+  const int rc = s32_fdtd_step(&in->dm, &S.f, &S.fdtd, S.sc.kJ, zero_j, &in->cnt->error, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "FDTD launch failed: %s", cudaGetErrorString((cudaError_t)rc));
   if (zero_j)
@@ -3537,6 +3541,19 @@ extern "C" int spiffe_gpu_set_poisson_solver(spiffe_gpu_instance *in, int32_t so
     return solver == SPIFFE_POISSON_SOR ? 0
                                         : fail(SPIFFE_ERR_UNSUPPORTED, "the FP64 form solves with the reference's SOR");
   in->s32->pcw.solver = solver;
+  return 0;
+}
+
+extern "C" int spiffe_gpu_set_fdtd_kernel(spiffe_gpu_instance *in, int32_t kernel)
+{
+  if (!in)
+    return fail(SPIFFE_ERR_INVALID, "null argument");
+  if (kernel != SPIFFE_FDTD_AUTO && kernel != SPIFFE_FDTD_TWO_KERNELS && kernel != SPIFFE_FDTD_FUSED)
+    return fail(SPIFFE_ERR_INVALID, "unknown FDTD kernel choice %d", (int)kernel);
+  if (!in->s32)
+    return kernel == SPIFFE_FDTD_AUTO ? 0 : fail(SPIFFE_ERR_UNSUPPORTED, "the FP64 form has one FDTD path");
+  in->s32->fdtd_mode = kernel;
+  in->s32->fdtd.fused = -1; // planned again at the next step
   return 0;
 }
 

@@ -89,12 +89,21 @@ struct Fdtd32Tables {
   float *cpd = nullptr, *cmd = nullptr; // dt * Ez metric coefficients per ir (integrate.c:327-340)
   float *bzf = nullptr;                 // Bz factor per ir (integrate.c:515)
   float fEr = 0, topf = 0, fEphi = 0;   // dt/(mu0 eps0 dz), (rmax-dr/2)/(rmax+dr/2), dt/(eps0 mu0)
+  // the fused TM kernel (fdtd_f32.cu k_tm_fused32): bands of rows, the Er
+  // row each band publishes to the next, the bands' epoch flags
+  int fused = -1;                       // -1 not yet decided, 0 two kernels, 1 fused
+  int mode = 0;                         // SPIFFE_FDTD_*
+  int bands = 0, rows_per = 0, threads = 0;
+  size_t smem = 0;
+  float *pub = nullptr;
+  unsigned *flag = nullptr, *arrivals = nullptr;
+  unsigned epoch = 0;
 };
 extern "C" int s32_fdtd_tables(const DevMesh *m, const int16_t *host_flags, Fdtd32Tables *t, uint8_t *d_umask,
                                cudaStream_t s);
 extern "C" void s32_fdtd_tables_free(Fdtd32Tables *t);
-extern "C" int s32_fdtd_step(const DevMesh *m, const DevFields32 *f, const Fdtd32Tables *t, float kJ, int zero_j,
-                             cudaStream_t s);
+extern "C" int s32_fdtd_step(const DevMesh *m, const DevFields32 *f, Fdtd32Tables *t, float kJ, int zero_j,
+                             unsigned *err, cudaStream_t s);
 // jbox = [lo, hi] (rows; lo > hi: empty)
 extern "C" int s32_jbox_set(int *jbox, int lo, int hi, cudaStream_t s);
 // FP64 host array (pitch nr+1) <-> FP32 device array (pitch P) through a device staging buffer

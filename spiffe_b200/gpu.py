@@ -23,6 +23,9 @@ PRECISION_F64 = 0
 PRECISION_SPLIT32 = 1
 POISSON_SOR = 0
 POISSON_MULTIGRID = 1
+FDTD_AUTO = 0
+FDTD_TWO_KERNELS = 1
+FDTD_FUSED = 2
 
 _lib = None
 P = C.POINTER
@@ -347,6 +350,10 @@ class GpuInstance:
         n = C.c_int64()
         _check(self.lib.spiffe_gpu_poisson_log(self.h, max_rows, rows.ctypes.data_as(P(C.c_double)), C.byref(n)))
         return rows[: min(n.value, max_rows)].copy()
+
+    def set_fdtd_kernel(self, kernel):
+        """FDTD_AUTO, FDTD_TWO_KERNELS or FDTD_FUSED (split form)."""
+        _check(self.lib.spiffe_gpu_set_fdtd_kernel(self.h, int(kernel)))
 
     def set_poisson_solver(self, solver):
         """POISSON_MULTIGRID (split form default) or POISSON_SOR."""

@@ -31,8 +31,10 @@ def load(name):
         return {k: z[k] for k in z.files}
 
 
-def fields_from(fx, modes=MODES, dt=None):
+def fields_from(fx, modes=MODES, dt=None, **bcs):
+    """abi.Fields of a fixture's mesh; left_bc / right_bc override the fixture's."""
     lo, up, right, left = (int(v) for v in fx["bcs"])
+    left, right = bcs.get("left_bc", left), bcs.get("right_bc", right)
     f = abi.Fields(int(fx["nz"]), int(fx["nr"]), float(fx["zmin"]), float(fx["zmax"]), float(fx["rmax"]),
                    modes=modes, left_bc=left, right_bc=right, lower_bc=lo, upper_bc=up, flags=fx["flags"])
     assert f.mesh.dz == float(fx["dz"]) and f.mesh.dr == float(fx["dr"])

@@ -438,3 +438,68 @@ def test_pillbox_exit_moments_within_half_percent():
     assert abs(m32["count"] - m64["count"]) <= max(2, 0.005 * m64["count"])
     for k, v in err.items():
         assert v <= MOMENT_TOL, (k, v)
+
+
+# ---- the fused TM kernel gives the two kernels' bits
+
+def fdtd_pair(f, steps, beam=None, run=None):
+    """The same state advanced by the two-kernel and the fused TM update."""
+    out = []
+    for kernel in (gpu.FDTD_TWO_KERNELS, gpu.FDTD_FUSED):
+        g = split(f, capacity=(beam.capacity if beam is not None else 1024))
+        g.set_fdtd_kernel(kernel)
+        if beam is None:
+            for _ in range(steps):
+                g.advance_fields()
+        else:
+            g.upload_beam(beam)
+            run(g)
+        out.append((g, g.fields(f)))
+    return out
+
+
+@pytest.mark.parametrize("bcs", [{}, {"left_bc": abi.NEUMANN, "right_bc": abi.NEUMANN},
+                                 {"left_bc": abi.NEUMANN, "right_bc": abi.DIRICHLET}])
+def test_fused_fdtd_pillbox_is_bit_identical(bcs):
+    """The pillbox's free oscillation for 300 steps (104 x 160 rows and
+    columns, every end-row, axis and top copy of integrate.c:391-432), with
+    the boundary conditions at both ends varied."""
+    fx = load("pillbox_fdtd")
+    f = fields_from(fx, dt=float(fx["dt"]), **bcs)
+    f["Ez"] = fx["Ez0"]
+    (_, a), (_, b) = fdtd_pair(f, 300)
+    for n in ("Ez", "Er", "Bphi", "Bphi2"):
+        assert np.array_equal(a[n], b[n]), n
+
+
+def test_fused_fdtd_with_te_fields_is_bit_identical():
+    """TM fused beside the TE kernels on the gun mesh with constant currents
+    (J read on every row; the TE kernels empty the current box)."""
+    fx = load("gun16_te")
+    f = te_fdtd_state(fx)
+    (_, a), (_, b) = fdtd_pair(f, int(fx["steps"]))
+    for n in TE_FIELDS:
+        assert np.array_equal(a[n], b[n]), n
+
+
+def test_fused_fdtd_gun_with_beam_is_bit_identical():
+    """The benchmark's gun (3001 x 821 nodes, the fused kernel's own size
+    range) with its 1M-particle bunch and solenoid for 200 steps of the
+    device loop: deposition into the fused kernel's current rows, pushes in
+    its fields.  Fields and particles equal the two-kernel run's bit for bit."""
+    cfg = workloads.Gun16Config()
+    f, b = cfg.state()
+
+    def run(g):
+        g.configure_run(space_charge=1, push=abi.push_options(abi.COMPACT_SWAP, abi.SCREEN_PARTICLE),
+                        poisson=cfg.poisson())
+        g.run_begin()
+        g.run_steps(200)
+
+    (g1, a), (g2, b2) = fdtd_pair(f, 0, beam=b, run=run)
+    for n in ("Ez", "Er", "Bphi", "Bphi2", "Jz", "Jr"):
+        assert np.array_equal(a[n], b2[n]), n
+    x1, x2 = g1.download_beam(abi.Beam(b.capacity)), g2.download_beam(abi.Beam(b.capacity))
+    assert x1.np == x2.np > 0
+    for k in ("z", "r", "pz", "pr", "particleID"):
+        assert np.array_equal(x1[k][: x1.np], x2[k][: x2.np]), k
