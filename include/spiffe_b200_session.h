@@ -77,7 +77,8 @@ int spiffe_session_run_file(spiffe_session *s, const char *path);
  *   "compaction"         SPIFFE_COMPACT_* (default: REFERENCE for FP64, ANY for
  *                        the split form)
  *   "screen_momentum"    SPIFFE_SCREEN_* (default: REFERENCE for FP64, PARTICLE
- *                        for the split form) */
+ *                        for the split form)
+ *   "poisson_solver"     split form: SPIFFE_POISSON_* (default MULTIGRID) */
 int spiffe_session_set(spiffe_session *s, const char *name, double value);
 
 /* The mesh after define_geometry (time and step after the last integrate). */

@@ -166,10 +166,12 @@ struct DevScreen {
   double *rmin, *rmax, *zmin, *zmax;
   int16_t *generation;
   int32_t *particleID;
+  long long *order; // (time step << 32) | particle index: the reference's record order (advance_particles.c:362-434)
 };
 
 struct DevScreens {
   int n;
+  long long step; // the push's time step
   DevScreen s[SPIFFE_MAX_SCREENS];
 };
 

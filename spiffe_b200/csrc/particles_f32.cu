@@ -457,14 +457,15 @@ struct ScreenCtx {
   int momentum_policy;
 };
 
-__device__ void record32(const DevScreen &s, long long *nb, long long *overflow, const DevBeam32 &b, long ip,
-                         const double *q, float zmn, float zmx, float rmn, float rmx)
+__device__ void record32(const DevScreen &s, long long step, long long *nb, long long *overflow, const DevBeam32 &b,
+                         long ip, const double *q, float zmn, float zmx, float rmn, float rmx)
 {
   const long long k = atomic_add_ll(nb, 1LL);
   if (k >= s.capacity) {
     atomic_add_ll(overflow, 1LL);
     return;
   }
+  s.order[k] = (step << 32) | (long long)ip;
   for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
     s.col[c][k] = q[c];
   s.rmin[k] = rmn == FLT_MAX ? DBL_MAX : (double)rmn;
@@ -697,7 +698,7 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
           q[5] = b.Q[ip];
           q[6] = b.r0[ip];
           q[7] = b.t0[ip];
-          record32(s, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q, zmn, zmx, rmn, rmx);
+          record32(s, scr.step, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q, zmn, zmx, rmn, rmx);
         } else if (s.z_position >= zd && s.z_position < z0d && s.direction == -1) {
           const double dtp = (s.z_position - z0d) / vzd;
           r0 += vrd * dtp;
@@ -709,7 +710,7 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
           q[5] = b.Q[ip];
           q[6] = b.r0[ip];
           q[7] = b.t0[ip];
-          record32(s, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q, zmn, zmx, rmn, rmx);
+          record32(s, scr.step, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q, zmn, zmx, rmn, rmx);
         }
       }
     }

@@ -239,14 +239,15 @@ struct PushParams {
   LostLog lost;
 };
 
-__device__ void record(const DevScreen &s, long long *nb, long long *overflow, const DevBeam64 &b, long ip,
-                       const double *q)
+__device__ void record(const DevScreen &s, long long step, long long *nb, long long *overflow, const DevBeam64 &b,
+                       long ip, const double *q)
 {
   const long long k = atomic_add_ll(nb, 1LL);
   if (k >= s.capacity) {
     atomic_add_ll(overflow, 1LL);
     return;
   }
+  s.order[k] = (step << 32) | (long long)ip;
   for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
     s.col[c][k] = q[c];
   s.rmin[k] = b.rmin[ip];
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(T) k_push(DevMesh m, DevFields<double> f, DevB
         q[5] = b.Q[ip];
         q[6] = b.r0[ip];
         q[7] = b.t0[ip];
-        record(s, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q);
+        record(s, scr.step, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q);
       } else if (s.z_position >= z && s.z_position < z0 && s.direction == -1) {
         const double dtp = (s.z_position - z0) / vz;
         r0 += vr * dtp;
@@ -458,7 +459,7 @@ __global__ void __launch_bounds__(T) k_push(DevMesh m, DevFields<double> f, DevB
         q[5] = b.Q[ip];
         q[6] = b.r0[ip];
         q[7] = b.t0[ip];
-        record(s, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q);
+        record(s, scr.step, &cnt->screen_nb[is], &cnt->screen_overflow, b, ip, q);
       }
     }
   }

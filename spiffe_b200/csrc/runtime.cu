@@ -18,6 +18,7 @@
 #include <string>
 #include <utility>
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -887,6 +888,7 @@ static int s32_push_step(spiffe_gpu_instance *in, const spiffe_push_options *o, 
   p.deposit = deposit;
   p.lost = lost_log(in);
   PhaseScope ps(in, PH_PUSH);
+  in->screens.step = in->mesh.time_step;
   const int rc = s32_push(&in->dm, &S.f, &S.b, &p, &in->screens, in->cnt, in->np_upper, o->compaction, &S.sc, &S.pw,
                           in->stream);
   if (rc)
@@ -999,6 +1001,7 @@ extern "C" int spiffe_gpu_destroy(spiffe_gpu_instance *in)
     cudaFree(sc.zmax);
     cudaFree(sc.generation);
     cudaFree(sc.particleID);
+    cudaFree(sc.order);
   }
   free_beam(&in->b);
   spiffe_fdtd64_tables_free(&in->fdtd);
@@ -1217,6 +1220,7 @@ extern "C" int spiffe_gpu_advance_particles(spiffe_gpu_instance *in, const spiff
                    o->screen_momentum, o->compaction, lost_log(in)};
   {
     PhaseScope ps(in, PH_PUSH);
+    in->screens.step = in->mesh.time_step;
     const int rc = spiffe_push64(&in->dm, &in->f, &in->b, &p, &in->screens, in->cnt, in->np_upper, &in->pw,
                                  in->stream);
     if (rc)
@@ -1444,6 +1448,7 @@ extern "C" int spiffe_gpu_add_screen(spiffe_gpu_instance *in, double z_position,
   CUDA_TRY(cudaMalloc(&sc.zmax, n * sizeof(double)));
   CUDA_TRY(cudaMalloc(&sc.generation, n * sizeof(int16_t)));
   CUDA_TRY(cudaMalloc(&sc.particleID, n * sizeof(int32_t)));
+  CUDA_TRY(cudaMalloc(&sc.order, n * sizeof(long long)));
   in->screens.n++;
   return 0;
 }
@@ -1947,7 +1952,34 @@ extern "C" int spiffe_gpu_download_screen(spiffe_gpu_instance *in, int32_t is, s
     if (h->particleID)
       CUDA_TRY(cudaMemcpyAsync(h->particleID, sc.particleID, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   }
+  std::vector<long long> order(n);
+  if (n > 1)
+    CUDA_TRY(cudaMemcpyAsync(order.data(), sc.order, n * sizeof(long long), cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
+  // the pushes append crossings as they happen; the reference records them
+  // step by step in particle order (advance_particles.c:362-434)
+  if (n > 1 && !std::is_sorted(order.begin(), order.end())) {
+    std::vector<size_t> perm(n);
+    for (size_t i = 0; i < n; i++)
+      perm[i] = i;
+    std::sort(perm.begin(), perm.end(), [&](size_t a, size_t b) { return order[a] < order[b]; });
+    auto apply = [&](auto *p) {
+      if (!p)
+        return;
+      using T = std::remove_pointer_t<decltype(p)>;
+      std::vector<T> tmp(p, p + n);
+      for (size_t i = 0; i < n; i++)
+        p[i] = tmp[perm[i]];
+    };
+    for (int c = 0; c < SPIFFE_SCREEN_QUANS; c++)
+      apply(h->col[c]);
+    apply(h->rmin);
+    apply(h->rmax);
+    apply(h->zmin);
+    apply(h->zmax);
+    apply(h->generation);
+    apply(h->particleID);
+  }
   h->nb = nb;
   h->z_position = sc.z_position;
   h->direction = sc.direction;

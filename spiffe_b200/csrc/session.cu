@@ -291,6 +291,7 @@ struct spiffe_session {
   int deposit_order = 1;
   long long particle_capacity = 1 << 16, screen_capacity = 1 << 20, flush_steps = 512;
   int compaction = -1, screen_momentum = -1;
+  int poisson_solver = -1; // SPIFFE_POISSON_* of the split form (-1: the instance's default)
 
   bool have_geometry = false;
   spiffe_mesh mesh{};
@@ -1190,7 +1191,7 @@ int spiffe_session::cmd_secondary_emission(Args &g)
                                  Def{"yield", "", "", T_FLOAT},   Def{"emitted", "", "", T_SHORT},
                                  Def{"directionCode", "", "", T_SHORT}, Def{"generation", "", "", T_SHORT},
                                  Def{"particleID", "", "", T_LONG}};
-    if (!d.log_out.open(compose(log_file, rootname), "Primary/secondary activity due to material " + input_file + "\n",
+    if (!d.log_out.open(compose(log_file, rootname), "Primary/secondary activity due to material " + input_file,
                         "", {}, lc, err))
       return serr(SPIFFE_ERR_INVALID, "define_secondary_emission log_file: %s", err.c_str());
     d.o.log = 1;
@@ -1867,6 +1868,8 @@ int spiffe_session::ensure_instance()
     S_TRY(spiffe_gpu_upload_fields(inst, &f));
     if (precision == SPIFFE_PRECISION_F64)
       S_TRY(spiffe_gpu_set_deposit_order(inst, deposit_order));
+    if (precision == SPIFFE_PRECISION_SPLIT32 && poisson_solver >= 0)
+      S_TRY(spiffe_gpu_set_poisson_solver(inst, poisson_solver));
   } else {
     S_TRY(spiffe_gpu_set_mesh(inst, &mesh));
   }
@@ -2528,6 +2531,8 @@ extern "C" int spiffe_session_set(spiffe_session *s, const char *name, double v)
     s->compaction = (int)v;
   else if (n == "screen_momentum" && v >= 0 && v <= 1)
     s->screen_momentum = (int)v;
+  else if (n == "poisson_solver" && (v == SPIFFE_POISSON_SOR || v == SPIFFE_POISSON_MULTIGRID))
+    s->poisson_solver = (int)v;
   else
     return serr(SPIFFE_ERR_INVALID, "unknown session setting %s or bad value", name);
   if (s->inst && n == "deposit_order" && s->precision == SPIFFE_PRECISION_F64)

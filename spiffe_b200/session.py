@@ -25,7 +25,7 @@ import numpy as np
 from . import abi, gpu
 
 SETTINGS = ("verbose", "deposit_order", "particle_capacity", "screen_capacity", "flush_steps", "compaction",
-            "screen_momentum")
+            "screen_momentum", "poisson_solver")
 
 
 class Session:
