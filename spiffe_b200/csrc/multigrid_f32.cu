@@ -49,9 +49,10 @@
 
 namespace {
 
-constexpr int MG_NT = 512;            // threads per CTA
-constexpr int MG_TAIL_NODES = 12288;  // levels at most this large are worked by CTA 0 alone
+constexpr int MG_NT = 1024;           // threads per CTA
+constexpr int MG_TAIL_NODES = 3000;   // levels at most this large are worked by CTA 0 alone
 constexpr int MG_MIN_UNKNOWNS = 64;   // coarsening stops at this many unknowns
+constexpr int MG_MAX_DIRECT = 1024;   // a coarsest level of at most this many unknowns is solved exactly
 enum { MG_INVD = 8, MG_DIAG = 9 };
 
 struct Mg32Args {
@@ -64,6 +65,9 @@ struct Mg32Args {
   float a, c4, e, e2c, inv_e, inv_e2c;   // level-0 operator in FP32
   double a_d, e_d, c4_d, e2c_d, dr2_inv; // and in FP64 for the residual
   int nlev, tail, nu0, nu, coarse_sweeps, max_cycles;
+  const float *cinv; // the coarsest level's inverse, cn x cn row-major (null: coarse sweeps)
+  const int *cidx;   // its unknowns' array indices on that level
+  int cn;
   double accuracy;
   MgLevel lev[MG_MAX_LEVELS];
   unsigned long long *bar; // [0] arrivals, [16] abort
@@ -141,11 +145,11 @@ __device__ __forceinline__ bool unknown0(const Mg32Args &a, int iz, int ir, size
 __device__ __forceinline__ float nb0(const Mg32Args &a, const float *u, int iz, int ir, size_t j)
 {
   const long P = a.P0;
-  const float up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? __ldcg(u + j - P) : __ldcg(u + j + P);
-  const float dn = (iz == 0 && a.lo == 0) ? __ldcg(u + j + P) : __ldcg(u + j - P);
+  const float up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? *(u + j - P) : *(u + j + P);
+  const float dn = (iz == 0 && a.lo == 0) ? *(u + j + P) : *(u + j - P);
   if (ir == 0)
-    return a.a * (up + dn) + a.c4 * __ldcg(u + j + 1);
-  return a.a * (up + dn) + __ldg(a.crow + ir) * __ldcg(u + j + 1) + __ldg(a.drow + ir) * __ldcg(u + j - 1);
+    return a.a * (up + dn) + a.c4 * *(u + j + 1);
+  return a.a * (up + dn) + __ldg(a.crow + ir) * *(u + j + 1) + __ldg(a.drow + ir) * *(u + j - 1);
 }
 
 __device__ __forceinline__ float res0(const Mg32Args &a, int iz, int ir)
@@ -153,23 +157,45 @@ __device__ __forceinline__ float res0(const Mg32Args &a, int iz, int ir)
   const size_t j = node(iz, ir, a.P0);
   if (!unknown0(a, iz, ir, j))
     return 0.f;
-  return __ldcg(a.f0 + j) - nb0(a, a.u0, iz, ir, j) - (ir ? a.e : a.e2c) * __ldcg(a.u0 + j);
+  return *(a.f0 + j) - nb0(a, a.u0, iz, ir, j) - (ir ? a.e : a.e2c) * *(a.u0 + j);
 }
 
-// one colour c of red-black Gauss-Seidel on level 0: nodes with (iz+ir)%2 == c
+// one colour c of red-black Gauss-Seidel on level 0: nodes with (iz+ir)%2 == c.
+// A thread takes four consecutive columns of a row (16-byte loads of u on
+// the row and its neighbours, of f and of the mask) and updates the two of
+// its colour; the other two, which this colour's updates only read, are
+// written back unchanged.
 __device__ void smooth0(const Mg32Args &a, int c, long t0, long dt)
 {
-  const int Hh = (a.cols + 1) >> 1;
-  const long n = (long)(a.hi - a.lo + 1) * Hh;
+  const int G = (a.cols + 3) >> 2; // column groups per row
+  const long n = (long)(a.hi - a.lo + 1) * G;
+  const long P = a.P0;
   for (long t = t0; t < n; t += dt) {
-    const int row = (int)(t / Hh), k = (int)(t - (long)row * Hh);
-    const int iz = a.lo + row, ir = 2 * k + ((iz + c) & 1);
-    if (ir >= a.cols)
-      continue;
-    const size_t j = node(iz, ir, a.P0);
-    if (a.umask[j] & S32_U_METAL)
-      continue;
-    a.u0[j] = (__ldcg(a.f0 + j) - nb0(a, a.u0, iz, ir, j)) * (ir ? a.inv_e : a.inv_e2c);
+    const int row = (int)(t / G), g = (int)(t - (long)row * G);
+    const int iz = a.lo + row, c0 = 4 * g;
+    const size_t j = node(iz, c0, a.P0);
+    const bool top = iz == a.nz - 1 && a.hi == a.nz - 1, bottom = iz == 0 && a.lo == 0;
+    const float4 um = *reinterpret_cast<const float4 *>(a.u0 + (top ? j - P : j + P));
+    const float4 dm = *reinterpret_cast<const float4 *>(a.u0 + (bottom ? j + P : j - P));
+    const float4 u = *reinterpret_cast<const float4 *>(a.u0 + j);
+    const float4 f = *reinterpret_cast<const float4 *>(a.f0 + j);
+    const uchar4 mk = *reinterpret_cast<const uchar4 *>(a.umask + j);
+    const float left = c0 > 0 ? a.u0[j - 1] : 0.f, right = a.u0[j + 4];
+    const float uu[6] = {left, u.x, u.y, u.z, u.w, right};
+    const float ups[4] = {um.x, um.y, um.z, um.w}, dns[4] = {dm.x, dm.y, dm.z, dm.w};
+    const float fs[4] = {f.x, f.y, f.z, f.w};
+    const uint8_t ms[4] = {mk.x, mk.y, mk.z, mk.w};
+    for (int q = ((iz + c - c0) & 1); q < 4; q += 2) {
+      const int ir = c0 + q;
+      if (ir >= a.cols || (ms[q] & S32_U_METAL))
+        continue;
+      float nb;
+      if (ir == 0)
+        nb = a.a * (ups[q] + dns[q]) + a.c4 * uu[q + 2];
+      else
+        nb = a.a * (ups[q] + dns[q]) + __ldg(a.crow + ir) * uu[q + 2] + __ldg(a.drow + ir) * uu[q];
+      a.u0[j + q] = (fs[q] - nb) * (ir ? a.inv_e : a.inv_e2c);
+    }
   }
 }
 
@@ -179,14 +205,14 @@ __device__ __forceinline__ float nb9(const MgLevel &L, size_t idx, size_t plane)
 {
   const float *u = L.u, *c = L.coef;
   const long P = L.P;
-  float s = __ldg(c + idx) * __ldcg(u + idx - P - 1);
-  s += __ldg(c + plane + idx) * __ldcg(u + idx - P);
-  s += __ldg(c + 2 * plane + idx) * __ldcg(u + idx - P + 1);
-  s += __ldg(c + 3 * plane + idx) * __ldcg(u + idx - 1);
-  s += __ldg(c + 4 * plane + idx) * __ldcg(u + idx + 1);
-  s += __ldg(c + 5 * plane + idx) * __ldcg(u + idx + P - 1);
-  s += __ldg(c + 6 * plane + idx) * __ldcg(u + idx + P);
-  s += __ldg(c + 7 * plane + idx) * __ldcg(u + idx + P + 1);
+  float s = __ldg(c + idx) * *(u + idx - P - 1);
+  s += __ldg(c + plane + idx) * *(u + idx - P);
+  s += __ldg(c + 2 * plane + idx) * *(u + idx - P + 1);
+  s += __ldg(c + 3 * plane + idx) * *(u + idx - 1);
+  s += __ldg(c + 4 * plane + idx) * *(u + idx + 1);
+  s += __ldg(c + 5 * plane + idx) * *(u + idx + P - 1);
+  s += __ldg(c + 6 * plane + idx) * *(u + idx + P);
+  s += __ldg(c + 7 * plane + idx) * *(u + idx + P + 1);
   return s;
 }
 
@@ -195,7 +221,7 @@ __device__ __forceinline__ float res9(const MgLevel &L, int I, int J)
   const size_t plane = (size_t)(L.Z + 2) * L.P, idx = (size_t)(I + 1) * L.P + J + 1;
   if (__ldg(L.coef + MG_INVD * plane + idx) == 0.f)
     return 0.f;
-  return __ldcg(L.f + idx) - __ldg(L.coef + MG_DIAG * plane + idx) * (__ldcg(L.u + idx) + nb9(L, idx, plane));
+  return *(L.f + idx) - __ldg(L.coef + MG_DIAG * plane + idx) * (*(L.u + idx) + nb9(L, idx, plane));
 }
 
 // one colour (cz, cr) = (c >> 1, c & 1) of Gauss-Seidel on a nine-point level
@@ -212,7 +238,7 @@ __device__ void smooth9(const MgLevel &L, int c, long t0, long dt)
     const float id = __ldg(L.coef + MG_INVD * plane + idx);
     if (id == 0.f)
       continue;
-    L.u[idx] = __ldcg(L.f + idx) * id - nb9(L, idx, plane);
+    L.u[idx] = *(L.f + idx) * id - nb9(L, idx, plane);
   }
 }
 
@@ -283,12 +309,12 @@ __device__ __forceinline__ float interp(const MgLevel &C, int i, int j)
   const float *u = C.u + (size_t)(I + 1) * C.P + J + 1;
   float v;
   if (j & 1)
-    v = 0.5f * (__ldcg(u) + __ldcg(u + 1));
+    v = 0.5f * (*(u) + *(u + 1));
   else
-    v = __ldcg(u);
+    v = *(u);
   if (i & 1) {
     const float *w = u + C.P;
-    v = 0.5f * v + 0.5f * ((j & 1) ? 0.5f * (__ldcg(w) + __ldcg(w + 1)) : __ldcg(w));
+    v = 0.5f * v + 0.5f * ((j & 1) ? 0.5f * (*(w) + *(w + 1)) : *(w));
   }
   return v;
 }
@@ -302,7 +328,7 @@ __device__ void prolong0(const Mg32Args &a, long t0, long dt)
     const size_t j = node(iz, ir, a.P0);
     if (a.umask[j] & S32_U_METAL)
       continue;
-    a.u0[j] = __ldcg(a.u0 + j) + interp(C, iz, ir);
+    a.u0[j] = *(a.u0 + j) + interp(C, iz, ir);
   }
 }
 
@@ -315,7 +341,7 @@ __device__ void prolong9(const MgLevel &F, const MgLevel &C, long t0, long dt)
     const size_t idx = (size_t)(i + 1) * F.P + j + 1;
     if (__ldg(F.coef + MG_INVD * plane + idx) == 0.f)
       continue;
-    F.u[idx] = __ldcg(F.u + idx) + interp(C, i, j);
+    F.u[idx] = *(F.u + idx) + interp(C, i, j);
   }
 }
 
@@ -335,12 +361,29 @@ __device__ bool sub_cycle(const Mg32Args &a, int l0, bool local, long t0, long d
     if (!mg_sync(a, local, gen, cnt))
       return false;
   }
-  for (int k = 0; k < a.coarse_sweeps; k++)
-    for (int c = 0; c < 4; c++) {
-      smooth9(a.lev[L - 1], c, t0, dt);
-      if (!mg_sync(a, local, gen, cnt))
-        return false;
+  if (a.cinv && local) {
+    // the coarsest level solved exactly: u = A^-1 f over its unknowns
+    __shared__ float fc[MG_MAX_DIRECT];
+    const MgLevel &C = a.lev[L - 1];
+    for (int i = (int)t0; i < a.cn; i += (int)dt)
+      fc[i] = C.f[a.cidx[i]];
+    __syncthreads();
+    for (int i = (int)t0; i < a.cn; i += (int)dt) {
+      const float *row = a.cinv + (size_t)i * a.cn;
+      float acc = 0.f;
+      for (int k = 0; k < a.cn; k++)
+        acc += __ldg(row + k) * fc[k];
+      C.u[a.cidx[i]] = acc;
     }
+    __syncthreads();
+  } else {
+    for (int k = 0; k < a.coarse_sweeps; k++)
+      for (int c = 0; c < 4; c++) {
+        smooth9(a.lev[L - 1], c, t0, dt);
+        if (!mg_sync(a, local, gen, cnt))
+          return false;
+      }
+  }
   for (int l = L - 2; l >= l0; l--) {
     prolong9(a.lev[l], a.lev[l + 1], t0, dt);
     if (!mg_sync(a, local, gen, cnt))
@@ -426,16 +469,16 @@ __device__ void residual64(const Mg32Args &a, bool first, double *rs, double *ds
       d_acc += fabs(rh);
     if (!unknown0(a, iz, ir, j))
       continue;
-    const double up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? __ldcg(a.Psi + j - P) : __ldcg(a.Psi + j + P);
-    const double dn = (iz == 0 && a.lo == 0) ? __ldcg(a.Psi + j + P) : __ldcg(a.Psi + j - P);
-    const double psi = __ldcg(a.Psi + j);
+    const double up = (iz == a.nz - 1 && a.hi == a.nz - 1) ? *(a.Psi + j - P) : *(a.Psi + j + P);
+    const double dn = (iz == 0 && a.lo == 0) ? *(a.Psi + j + P) : *(a.Psi + j - P);
+    const double psi = *(a.Psi + j);
     double ap;
     if (ir == 0)
-      ap = a.a_d * (up + dn) + a.c4_d * __ldcg(a.Psi + j + 1) + a.e2c_d * psi;
+      ap = a.a_d * (up + dn) + a.c4_d * *(a.Psi + j + 1) + a.e2c_d * psi;
     else {
       const double h = 0.5 / ir;
-      ap = a.a_d * (up + dn) + a.dr2_inv * (1 + h) * __ldcg(a.Psi + j + 1) +
-           a.dr2_inv * (1 - h) * __ldcg(a.Psi + j - 1) + a.e_d * psi;
+      ap = a.a_d * (up + dn) + a.dr2_inv * (1 + h) * *(a.Psi + j + 1) +
+           a.dr2_inv * (1 - h) * *(a.Psi + j - 1) + a.e_d * psi;
     }
     const double r = rh - ap;
     r_acc += fabs(r);
@@ -454,7 +497,7 @@ __device__ void fold(const Mg32Args &a)
     const int iz = (int)(t / a.cols), ir = (int)(t - (long)iz * a.cols);
     const size_t j = node(iz, ir, a.P0);
     if (unknown0(a, iz, ir, j))
-      a.Psi[j] = __ldcg(a.Psi + j) + (double)__ldcg(a.u0 + j);
+      a.Psi[j] = *(a.Psi + j) + (double)*(a.u0 + j);
   }
 }
 
@@ -697,8 +740,80 @@ size_t unknowns(const Stencil &S)
 extern "C" void s32_mg_free(Mg32Work *w)
 {
   cudaFree(w->mem);
+  cudaFree(w->cinv);
+  cudaFree(w->cidx);
   *w = Mg32Work();
 }
+
+namespace {
+// The inverse of the coarsest level's operator over its unknowns (Gauss-Jordan
+// with partial pivoting in FP64), for the exact coarse solve; false when the
+// level has more than MG_MAX_DIRECT unknowns or the matrix is singular.
+bool coarse_inverse(const Stencil &S, int P, std::vector<float> &inv, std::vector<int> &idx)
+{
+  std::vector<int> num((size_t)S.Z * S.R, -1);
+  idx.clear();
+  for (int I = 0; I < S.Z; I++)
+    for (int J = 0; J < S.R; J++)
+      if (S.unk[(size_t)I * S.R + J]) {
+        num[(size_t)I * S.R + J] = (int)idx.size();
+        idx.push_back((I + 1) * P + J + 1);
+      }
+  const int n = (int)idx.size();
+  if (n == 0 || n > MG_MAX_DIRECT)
+    return false;
+  std::vector<double> A((size_t)n * n, 0.0), X((size_t)n * n, 0.0);
+  for (int I = 0; I < S.Z; I++)
+    for (int J = 0; J < S.R; J++) {
+      const int r = num[(size_t)I * S.R + J];
+      if (r < 0)
+        continue;
+      for (int k = 0; k < 9; k++) {
+        const int i2 = I + k / 3 - 1, j2 = J + k % 3 - 1;
+        if (i2 < 0 || i2 >= S.Z || j2 < 0 || j2 >= S.R)
+          continue;
+        const int c = num[(size_t)i2 * S.R + j2];
+        if (c >= 0)
+          A[(size_t)r * n + c] += S.at(k, I, J);
+      }
+    }
+  for (int i = 0; i < n; i++)
+    X[(size_t)i * n + i] = 1.0;
+  for (int col = 0; col < n; col++) {
+    int piv = col;
+    for (int r = col + 1; r < n; r++)
+      if (std::fabs(A[(size_t)r * n + col]) > std::fabs(A[(size_t)piv * n + col]))
+        piv = r;
+    if (A[(size_t)piv * n + col] == 0)
+      return false;
+    if (piv != col)
+      for (int k = 0; k < n; k++) {
+        std::swap(A[(size_t)piv * n + k], A[(size_t)col * n + k]);
+        std::swap(X[(size_t)piv * n + k], X[(size_t)col * n + k]);
+      }
+    const double d = 1 / A[(size_t)col * n + col];
+    for (int k = 0; k < n; k++) {
+      A[(size_t)col * n + k] *= d;
+      X[(size_t)col * n + k] *= d;
+    }
+    for (int r = 0; r < n; r++) {
+      if (r == col)
+        continue;
+      const double fct = A[(size_t)r * n + col];
+      if (fct == 0)
+        continue;
+      for (int k = 0; k < n; k++) {
+        A[(size_t)r * n + k] -= fct * A[(size_t)col * n + k];
+        X[(size_t)r * n + k] -= fct * X[(size_t)col * n + k];
+      }
+    }
+  }
+  inv.assign((size_t)n * n, 0.f);
+  for (size_t k = 0; k < inv.size(); k++)
+    inv[k] = (float)X[k];
+  return true;
+}
+} // namespace
 
 extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w, cudaStream_t s)
 {
@@ -810,6 +925,21 @@ extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w,
     if (e == cudaSuccess)
       e = cudaStreamSynchronize(s); // the host staging is reused by the next level
   }
+  // the coarsest level's inverse for its exact solve
+  std::vector<float> cinv;
+  std::vector<int> cidx;
+  if (e == cudaSuccess && coarse_inverse(lev[L - 1], w->lev[L - 1].P, cinv, cidx)) {
+    e = cudaMalloc(&w->cinv, cinv.size() * sizeof(float));
+    if (e == cudaSuccess)
+      e = cudaMalloc(&w->cidx, cidx.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(w->cinv, cinv.data(), cinv.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(w->cidx, cidx.data(), cidx.size() * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(s);
+    w->cn = (int)cidx.size();
+  }
   if (e != cudaSuccess)
     s32_mg_free(w);
   return (int)e;
@@ -851,6 +981,9 @@ extern "C" int s32_mg_solve(const DevMesh *m, Mg32Work *w, const float *crow, co
   a.nu0 = 2;
   a.nu = 2;
   a.coarse_sweeps = 24;
+  a.cinv = w->cinv;
+  a.cidx = w->cidx;
+  a.cn = w->cn;
   a.max_cycles = (int)std::min<long long>(max_cycles, 100);
   a.accuracy = accuracy;
   for (int l = 0; l < w->nlev; l++)

@@ -196,6 +196,9 @@ struct Mg32Work {
   long long *iters = nullptr;
   int grid = 0, threads = 0;
   size_t bytes = 0;
+  float *cinv = nullptr; // the coarsest level's inverse (exact coarse solve), cn x cn
+  int *cidx = nullptr;   // its unknowns' array indices
+  int cn = 0;
 };
 extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *host_flags, Mg32Work *w, cudaStream_t s);
 extern "C" void s32_mg_free(Mg32Work *w);
