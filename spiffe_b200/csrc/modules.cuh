@@ -67,9 +67,16 @@ extern "C" int spiffe_poisson64_setup(const DevMesh *m, Poisson64Work *w, long l
 extern "C" void spiffe_poisson64_free(Poisson64Work *w);
 extern "C" int spiffe_sor64(const DevMesh *m, Poisson64Work *w, double *Psi, const double *rhs, const int16_t *flags,
                             double accuracy, long long limit, DevCounts *cnt, long long *iterations, cudaStream_t s);
+// ordered: the particles' charge leaves Q through the ordered reduction on
+// pw's key/value buffers (sized by spiffe_particles64_work with ordered set)
+// instead of FP64 atomics.
 extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b,
                                            DevCounts *cnt, long long np_bound, const PoissonHostOptions *o,
-                                           Poisson64Work *w, cudaStream_t s);
+                                           Poisson64Work *w, Particles64Work *pw, bool ordered, cudaStream_t s);
+// Applies n (node, value) entries held in w->keys / w->vals to dst: a stable
+// sort by node, then each node's values added in entry order starting from
+// dst's current value.  INT_MAX keys are skipped.
+extern "C" int spiffe_ordered_add64(Particles64Work *w, long long n, double *dst, cudaStream_t s);
 extern "C" int spiffe_poisson64_report(Poisson64Work *w, spiffe_poisson_report *rep, cudaStream_t s);
 extern "C" int spiffe_imposed_field64(const DevMesh *m, const DevFields<double> *f, double factor, cudaStream_t s);
 

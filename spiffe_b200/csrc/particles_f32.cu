@@ -369,7 +369,10 @@ __device__ void contrib32(const DevMesh &m, int comp, int iz0, float fz, int ir0
 // Every lane of the warp must call this (node -1 = nothing to add).
 __device__ __forceinline__ void warp_add(long long *J, int nd, long long v)
 {
-  const unsigned grp = __match_any_sync(0xffffffffu, nd);
+  // cell-sorted particles: a warp's lanes usually share the node, and one
+  // vote settles that without the node-matching step
+  const int nd0 = __shfl_sync(0xffffffffu, nd, 0);
+  const unsigned grp = __all_sync(0xffffffffu, nd == nd0) ? 0xffffffffu : __match_any_sync(0xffffffffu, nd);
   const unsigned long long biased = (unsigned long long)(v + (1LL << 42));
   const unsigned lo = (unsigned)(biased & ((1u << 22) - 1)), hi = (unsigned)(biased >> 22);
   const unsigned slo = __reduce_add_sync(grp, lo), shi = __reduce_add_sync(grp, hi);
@@ -509,13 +512,14 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
     float pz = b.pz[ip], pr = b.pr[ip], rpp = b.rpphi[ip];
     const float pz0 = pz, pr0 = pr, rpp0 = rpp;
     float zmx = b.zmax[ip], zmn = b.zmin[ip], rmx = b.rmax[ip], rmn = b.rmin[ip];
+    unsigned moved = 0; // extrema that changed: bit 0 zmax, 1 zmin, 2 rmax, 3 rmin
     const float zmin = (float)m.zmin;
     // position before the drift and the stored (old) velocities
     const float zo = zmin + ((float)iz0 + fz0) * dz, ro = ((float)ir0 + fr0) * dr;
-    if (zo > zmx) zmx = zo;
-    if (zo < zmn) zmn = zo;
-    if (ro > rmx) rmx = ro;
-    if (ro < rmn) rmn = ro;
+    if (zo > zmx) { zmx = zo; moved |= 1u; }
+    if (zo < zmn) { zmn = zo; moved |= 2u; }
+    if (ro > rmx) { rmx = ro; moved |= 4u; }
+    if (ro < rmn) { rmn = ro; moved |= 8u; }
     float bz, br, bphi;
     betas(pz, pr, rpp, ro, bz, br, bphi);
     // drift with the old velocities (:157-158)
@@ -597,10 +601,10 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
     const float r = ((float)ir + fr) * dr;
     if (!lost && active) {
       const float zn = zmin + ((float)iz + fz) * dz;
-      if (zn > zmx) zmx = zn;
-      if (zn < zmn) zmn = zn;
-      if (r > rmx) rmx = r;
-      if (r < rmn) rmn = r;
+      if (zn > zmx) { zmx = zn; moved |= 1u; }
+      if (zn < zmn) { zmn = zn; moved |= 2u; }
+      if (r > rmx) { rmx = r; moved |= 4u; }
+      if (r < rmn) { rmn = r; moved |= 8u; }
     }
     if (DEF || !p.forced) {
       // momentum kick with the old velocities (:270-287)
@@ -643,10 +647,15 @@ __global__ void __launch_bounds__(T, 5) k_push32(DevMesh m, DevFields32 f, DevBe
     b.pz[ip] = pz;
     b.pr[ip] = pr;
     b.rpphi[ip] = rpp;
-    b.zmax[ip] = zmx;
-    b.zmin[ip] = zmn;
-    b.rmax[ip] = rmx;
-    b.rmin[ip] = rmn;
+    // extrema change rarely except the leading one: store only what moved
+    if (moved & 1u)
+      b.zmax[ip] = zmx;
+    if (moved & 2u)
+      b.zmin[ip] = zmn;
+    if (moved & 4u)
+      b.rmax[ip] = rmx;
+    if (moved & 8u)
+      b.rmin[ip] = rmn;
     if (lost) {
       status &= ~S32_ACTIVE;
       status |= S32_LOST;

@@ -890,15 +890,29 @@ extern "C" int spiffe_deposit64(const DevMesh *m, const DevFields<double> *f, co
     const int n = (int)(4 * np_bound);
     k_deposit<<<nb, T, 0, s>>>(*m, *f, *b, cnt, comp, w->keys, w->vals, np_bound);
     spiffe_note_launches(1);
-    // stable LSD radix sort keeps particle order inside each node's run;
-    // the INT_MAX pad key sorts last within the 31-bit key space
-    size_t bytes = w->cub_bytes;
-    cub::DeviceRadixSort::SortPairs(w->cub_tmp, bytes, w->keys, w->keys_alt, w->vals, w->vals_alt, n, 0, 31, s);
     double *J = comp == 0 ? f->Jz : (comp == 1 ? f->Jr : f->Jphi);
-    k_ordered_sum<<<blocks_for(n, T), T, 0, s>>>(w->keys_alt, w->vals_alt, n, J);
-    spiffe_note_launches(1);
+    if (int rc = spiffe_ordered_add64(w, n, J, s))
+      return rc;
     (void)bits;
   }
+  return (int)cudaGetLastError();
+}
+
+extern "C" int spiffe_ordered_add64(Particles64Work *w, long long n, double *dst, cudaStream_t s)
+{
+  if (n <= 0)
+    return 0;
+  if (!w->keys || n > 4 * w->capacity)
+    return (int)cudaErrorInvalidValue;
+  // stable LSD radix sort keeps entry order inside each node's run; the
+  // INT_MAX pad key sorts last within the 31-bit key space
+  size_t bytes = w->cub_bytes;
+  cudaError_t e = cub::DeviceRadixSort::SortPairs(w->cub_tmp, bytes, w->keys, w->keys_alt, w->vals, w->vals_alt,
+                                                  (int)n, 0, 31, s);
+  if (e != cudaSuccess)
+    return (int)e;
+  k_ordered_sum<<<blocks_for(n, T), T, 0, s>>>(w->keys_alt, w->vals_alt, n, dst);
+  spiffe_note_launches(1);
   return (int)cudaGetLastError();
 }
 

@@ -89,14 +89,22 @@ __global__ void __launch_bounds__(BX *BY) k_apparent_charge(DevMesh m, DevFields
   }
 }
 
-// Removal of the particles' own charge (:190-242), FP64 atomics; Qreal partial
-// sums per block.
+// Removal of the particles' own charge (:190-242); Qreal partial sums per
+// block.  With keys null each share is subtracted by an FP64 atomic, whose
+// order varies between runs once three or more particles share a node; with
+// keys set, particle ip writes its four (node, -share) pairs to entries
+// 4 ip .. 4 ip + 3 (unused ones keyed INT_MAX) for an ordered reduction that
+// applies them in particle order, the reference's serial Q[iz][ir] -= ...
+// sequence.
 __global__ void __launch_bounds__(RT) k_remove_charge(DevMesh m, DevFields<double> f, DevBeam64 b,
-                                                       const DevCounts *cnt, double *part)
+                                                       const DevCounts *cnt, double *part, int *keys, double *vals,
+                                                       long np_bound)
 {
   __shared__ double sh[RT];
   const long ip = (long)blockIdx.x * RT + threadIdx.x;
   double qreal = 0;
+  int at[4] = {0x7fffffff, 0x7fffffff, 0x7fffffff, 0x7fffffff};
+  double share[4] = {0, 0, 0, 0};
   if (ip < (long)cnt->np && (b.status[ip] & SPIFFE_PART_ACTIVE)) {
     const long nz = m.nz, nr = m.nr;
     const int P = m.pitch;
@@ -123,23 +131,39 @@ __global__ void __launch_bounds__(RT) k_remove_charge(DevMesh m, DevFields<doubl
         fr = 0;
       }
       const int16_t *F = f.flags;
-      if (!((F[node(iz, ir, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr - 1 && un))) {
-        atomicAdd(f.Q + node(iz, ir, P), -(Q * fb * fl));
-        qreal += Q * fb * fl;
+      const int n0 = node(iz, ir, P), n1 = node(iz + 1, ir, P), n2 = node(iz, ir + 1, P), n3 = node(iz + 1, ir + 1, P);
+      if (!((F[n0] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr - 1 && un))) {
+        at[0] = n0;
+        share[0] = Q * fb * fl;
+        qreal += share[0];
       }
-      if (!((F[node(iz + 1, ir, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr - 1 && un))) {
-        atomicAdd(f.Q + node(iz + 1, ir, P), -(Q * fb * fr));
-        qreal += Q * fb * fr;
+      if (!((F[n1] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr - 1 && un))) {
+        at[1] = n1;
+        share[1] = Q * fb * fr;
+        qreal += share[1];
       }
-      if (!((F[node(iz, ir + 1, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr && un))) {
-        atomicAdd(f.Q + node(iz, ir + 1, P), -(Q * fa * fl));
-        qreal += Q * fa * fl;
+      if (!((F[n2] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz - 1 && rn) || (ir >= nr && un))) {
+        at[2] = n2;
+        share[2] = Q * fa * fl;
+        qreal += share[2];
       }
-      if (!((F[node(iz + 1, ir + 1, P)] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr && un))) {
-        atomicAdd(f.Q + node(iz + 1, ir + 1, P), -(Q * fa * fr));
-        qreal += Q * fa * fr;
+      if (!((F[n3] & SPIFFE_FL_IS_METAL) || (iz == 0 && ln) || (iz >= nz && rn) || (ir >= nr && un))) {
+        at[3] = n3;
+        share[3] = Q * fa * fr;
+        qreal += share[3];
       }
     }
+  }
+  if (keys) {
+    if (ip < np_bound)
+      for (int k = 0; k < 4; k++) {
+        keys[4 * ip + k] = at[k];
+        vals[4 * ip + k] = at[k] == 0x7fffffff ? 0.0 : -share[k];
+      }
+  } else {
+    for (int k = 0; k < 4; k++)
+      if (at[k] != 0x7fffffff)
+        atomicAdd(f.Q + at[k], -share[k]);
   }
   const double s = block_sum(qreal, sh);
   if (threadIdx.x == 0)
@@ -643,8 +667,17 @@ extern "C" int spiffe_sor64(const DevMesh *m, Poisson64Work *w, double *Psi, con
 // One add_poisson_correction pass (the interval test is the caller's).
 extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<double> *f, const DevBeam64 *b,
                                            DevCounts *cnt, long long np_bound, const PoissonHostOptions *o,
-                                           Poisson64Work *w, cudaStream_t s)
+                                           Poisson64Work *w, Particles64Work *pw, bool ordered, cudaStream_t s)
 {
+  if (ordered && (!pw || !pw->keys || pw->capacity < np_bound))
+    return (int)cudaErrorInvalidValue;
+  // the particles' own charge leaves Q (:190-242)
+  auto remove_charge = [&]() -> int {
+    k_remove_charge<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, w->part, ordered ? pw->keys : nullptr,
+                                                            ordered ? pw->vals : nullptr, (long)np_bound);
+    spiffe_note_launches(1);
+    return ordered ? spiffe_ordered_add64(pw, 4 * np_bound, f->Q, s) : 0;
+  };
   dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
   const int nblk = grid.x * grid.y;
   // apparent charge, then the particles' own charge
@@ -656,8 +689,8 @@ extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<dou
   spiffe_note_launches(1);
   if (o->space_charge && np_bound > 0) {
     const unsigned pb = blocks_for(np_bound, RT);
-    k_remove_charge<<<pb, RT, 0, s>>>(*m, *f, *b, cnt, w->part);
-    spiffe_note_launches(1);
+    if (int rc = remove_charge())
+      return rc;
     k_finish_sum<<<1, 1024, 0, s>>>(w->part, (int)pb, 1, w->scalars + 2);
     spiffe_note_launches(1);
   } else {
@@ -685,7 +718,8 @@ extern "C" int spiffe_poisson_correction64(const DevMesh *m, const DevFields<dou
   k_apparent_charge<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 1, w->part);
   spiffe_note_launches(1);
   if (o->space_charge && np_bound > 0)
-    { k_remove_charge<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, w->part); spiffe_note_launches(1); }
+    if (int rc = remove_charge())
+      return rc;
   return (int)cudaGetLastError();
 }
 

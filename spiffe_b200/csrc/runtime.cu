@@ -1338,7 +1338,8 @@ static int poisson_correction(spiffe_gpu_instance *in, int space_charge, const s
   }
   RC_TRY(ensure_poisson(in));
   PhaseScope ps(in, PH_POISSON);
-  const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, in->stream);
+  const int rc = spiffe_poisson_correction64(&in->dm, &in->f, &in->b, in->cnt, in->np_upper, &h, &in->pcw, &in->pw,
+                                                 in->deposit_ordered, in->stream);
   if (rc)
     return fail(SPIFFE_ERR_CUDA, "Poisson correction launch failed: %s", cudaGetErrorString((cudaError_t)rc));
   RC_TRY(pc_log(in, in->pcw.st, in->pcw.scalars + 4));
