@@ -32,13 +32,22 @@
 //
 // One cooperative launch runs the whole solve.  Levels with more than
 // MG_TAIL_NODES nodes are worked by every CTA with grid barriers between the
-// colour sweeps; the smaller ones, down to the coarsest (GS sweeps, no
-// direct solve), by CTA 0 alone with CTA barriers while the others wait at
-// the next grid barrier.  Data written inside the launch are read through
-// L2 (ld.cg).  The sums that drive the stop rule are per-CTA partials added
-// in the same order by every CTA, so every CTA takes the same decision and
-// the result does not depend on timing.  Every barrier wait is bounded;
-// on time-out the kernel raises SPIFFE_DEV_ERR_BARRIER and every CTA returns.
+// colour sweeps; on the nine-point ones each CTA owns a band of rows, so the
+// two colours of one row parity, which depend on each other only within a
+// row, need a CTA barrier between them and a grid barrier only before the
+// other parity (two grid barriers a sweep, not four, same update order).
+// The residual pass also makes level 0's first colour-0 sweep (from u = 0
+// it needs no neighbours) and the last post-smoothing sweep adds u to Psi,
+// saving two passes and two barriers a cycle.  The smaller levels, down to
+// the coarsest (solved exactly by its precomputed inverse when it has at
+// most MG_MAX_DIRECT unknowns, else by Gauss-Seidel sweeps), are worked by
+// CTA 0 alone with CTA barriers while the others wait at the next grid
+// barrier.  Data written inside the launch are read after the acquire of a
+// grid barrier.  The sums that drive the stop rule are per-CTA partials
+// added in the same order by every CTA, so every CTA takes the same
+// decision and the result does not depend on timing.  Every barrier wait is
+// bounded; on time-out the kernel raises SPIFFE_DEV_ERR_BARRIER and every
+// CTA returns.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -124,16 +133,6 @@ __device__ bool mg_grid_sync(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
   return ok_sh != 0;
 }
 
-// A synchronisation point of a level's work: the whole grid, or CTA 0 alone.
-__device__ __forceinline__ bool mg_sync(const Mg32Args &a, bool local, unsigned &gen, DevCounts *cnt)
-{
-  if (local) {
-    __syncthreads();
-    return true;
-  }
-  return mg_grid_sync(a, gen, cnt);
-}
-
 // ---- level 0: the mesh, five-point operator
 
 __device__ __forceinline__ bool unknown0(const Mg32Args &a, int iz, int ir, size_t j)
@@ -160,42 +159,91 @@ __device__ __forceinline__ float res0(const Mg32Args &a, int iz, int ir)
   return *(a.f0 + j) - nb0(a, a.u0, iz, ir, j) - (ir ? a.e : a.e2c) * *(a.u0 + j);
 }
 
-// one colour c of red-black Gauss-Seidel on level 0: nodes with (iz+ir)%2 == c.
-// A thread takes four consecutive columns of a row (16-byte loads of u on
-// the row and its neighbours, of f and of the mask) and updates the two of
-// its colour; the other two, which this colour's updates only read, are
-// written back unchanged.
+// Four consecutive columns c0 .. c0+3 of a level-0 row: what a colour
+// sweep reads: 16-byte loads of u on the row and its two neighbours, of f
+// and of the mask; the scalars left and right of the group.
+struct Cols0 {
+  float4 um, dm, u, f;
+  uchar4 mk;
+  float left, right;
+  int j, iz, c0; // j: array index (level 0 has fewer than 2^31 nodes)
+};
+
+__device__ __forceinline__ void cols0_load(const Mg32Args &a, long t, int G, Cols0 &k)
+{
+  const long P = a.P0;
+  const int row = (int)(t / G), g = (int)(t - (long)row * G);
+  k.iz = a.lo + row;
+  k.c0 = 4 * g;
+  k.j = (int)node(k.iz, k.c0, a.P0);
+  const bool top = k.iz == a.nz - 1 && a.hi == a.nz - 1, bottom = k.iz == 0 && a.lo == 0;
+  k.um = *reinterpret_cast<const float4 *>(a.u0 + (top ? k.j - P : k.j + P));
+  k.dm = *reinterpret_cast<const float4 *>(a.u0 + (bottom ? k.j + P : k.j - P));
+  k.u = *reinterpret_cast<const float4 *>(a.u0 + k.j);
+  k.f = *reinterpret_cast<const float4 *>(a.f0 + k.j);
+  k.mk = *reinterpret_cast<const uchar4 *>(a.umask + k.j);
+  k.left = k.c0 > 0 ? a.u0[k.j - 1] : 0.f;
+  k.right = a.u0[k.j + 4];
+}
+
+// New values of the group's nodes of colour c ((iz+ir)%2 == c); fin keeps
+// the others' values.  Bit q of the result: node c0+q is an unknown.
+// Every index into the small arrays is a compile-time constant, so they
+// live in registers.
+__device__ __forceinline__ unsigned cols0_relax(const Mg32Args &a, int c, const Cols0 &k, float fin[4])
+{
+  const float uu[6] = {k.left, k.u.x, k.u.y, k.u.z, k.u.w, k.right};
+  const float ups[4] = {k.um.x, k.um.y, k.um.z, k.um.w}, dns[4] = {k.dm.x, k.dm.y, k.dm.z, k.dm.w};
+  const float fs[4] = {k.f.x, k.f.y, k.f.z, k.f.w};
+  const uint8_t ms[4] = {k.mk.x, k.mk.y, k.mk.z, k.mk.w};
+  fin[0] = k.u.x;
+  fin[1] = k.u.y;
+  fin[2] = k.u.z;
+  fin[3] = k.u.w;
+  unsigned unk = 0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int ir = k.c0 + q;
+    if (ir >= a.cols || (ms[q] & S32_U_METAL))
+      continue;
+    unk |= 1u << q;
+    if (((k.iz + ir) & 1) != c)
+      continue;
+    float nb;
+    if (ir == 0)
+      nb = a.a * (ups[q] + dns[q]) + a.c4 * uu[q + 2];
+    else
+      nb = a.a * (ups[q] + dns[q]) + __ldg(a.crow + ir) * uu[q + 2] + __ldg(a.drow + ir) * uu[q];
+    fin[q] = (fs[q] - nb) * (ir ? a.inv_e : a.inv_e2c);
+  }
+  return unk;
+}
+
+// One colour c of red-black Gauss-Seidel on level 0: nodes with (iz+ir)%2 ==
+// c, a group of four columns per task; the group's other two nodes, which
+// this colour's updates only read, are left as they are.  With FOLD (the
+// V-cycle's last sweep) the thread also adds the group's four final values
+// to Psi in FP64: the other colour's are final before this sweep and its own
+// after it.
+template <bool FOLD>
 __device__ void smooth0(const Mg32Args &a, int c, long t0, long dt)
 {
   const int G = (a.cols + 3) >> 2; // column groups per row
   const long n = (long)(a.hi - a.lo + 1) * G;
-  const long P = a.P0;
   for (long t = t0; t < n; t += dt) {
-    const int row = (int)(t / G), g = (int)(t - (long)row * G);
-    const int iz = a.lo + row, c0 = 4 * g;
-    const size_t j = node(iz, c0, a.P0);
-    const bool top = iz == a.nz - 1 && a.hi == a.nz - 1, bottom = iz == 0 && a.lo == 0;
-    const float4 um = *reinterpret_cast<const float4 *>(a.u0 + (top ? j - P : j + P));
-    const float4 dm = *reinterpret_cast<const float4 *>(a.u0 + (bottom ? j + P : j - P));
-    const float4 u = *reinterpret_cast<const float4 *>(a.u0 + j);
-    const float4 f = *reinterpret_cast<const float4 *>(a.f0 + j);
-    const uchar4 mk = *reinterpret_cast<const uchar4 *>(a.umask + j);
-    const float left = c0 > 0 ? a.u0[j - 1] : 0.f, right = a.u0[j + 4];
-    const float uu[6] = {left, u.x, u.y, u.z, u.w, right};
-    const float ups[4] = {um.x, um.y, um.z, um.w}, dns[4] = {dm.x, dm.y, dm.z, dm.w};
-    const float fs[4] = {f.x, f.y, f.z, f.w};
-    const uint8_t ms[4] = {mk.x, mk.y, mk.z, mk.w};
-    for (int q = ((iz + c - c0) & 1); q < 4; q += 2) {
-      const int ir = c0 + q;
-      if (ir >= a.cols || (ms[q] & S32_U_METAL))
-        continue;
-      float nb;
-      if (ir == 0)
-        nb = a.a * (ups[q] + dns[q]) + a.c4 * uu[q + 2];
-      else
-        nb = a.a * (ups[q] + dns[q]) + __ldg(a.crow + ir) * uu[q + 2] + __ldg(a.drow + ir) * uu[q];
-      a.u0[j + q] = (fs[q] - nb) * (ir ? a.inv_e : a.inv_e2c);
-    }
+    Cols0 k;
+    cols0_load(a, t, G, k);
+    float fin[4];
+    const unsigned unk = cols0_relax(a, c, k, fin);
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+      if ((unk >> q & 1) && ((k.iz + k.c0 + q) & 1) == c)
+        a.u0[k.j + q] = fin[q];
+    if (FOLD)
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        if (unk >> q & 1)
+          a.Psi[k.j + q] = a.Psi[k.j + q] + (double)fin[q];
   }
 }
 
@@ -239,6 +287,37 @@ __device__ void smooth9(const MgLevel &L, int c, long t0, long dt)
     if (id == 0.f)
       continue;
     L.u[idx] = *(L.f + idx) * id - nb9(L, idx, plane);
+  }
+}
+
+// Two colours (cz, cr) then (cz, 1-cr) of Gauss-Seidel on a nine-point level
+// over this CTA's rows (a band of ceil(Z / grid) rows).  A node of colour
+// (cz, 1-cr) reads the just-updated colour (cz, cr) only at its left and
+// right neighbours, in its own row, so a CTA barrier between the two
+// colours suffices; the colours of the other row parity read rows I +- 1
+// and follow a grid barrier.  The update order, and so every value, is the
+// four-colour sweep's.
+__device__ void smooth9_rows(const MgLevel &L, int cz, int cr)
+{
+  const int nbl = (L.Z + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int I0 = (int)blockIdx.x * nbl, I1 = min(I0 + nbl, L.Z);
+  const int r0 = I0 + ((I0 & 1) != cz); // first own row of parity cz
+  const int nrows = r0 < I1 ? (I1 - r0 + 1) >> 1 : 0;
+  const size_t plane = (size_t)(L.Z + 2) * L.P;
+  for (int h = 0; h < 2; h++) {
+    const int c = h ? 1 - cr : cr;
+    const int Rh = (L.R - c + 1) >> 1;
+    const long n = (long)nrows * Rh;
+    for (long t = threadIdx.x; t < n; t += blockDim.x) {
+      const int q = (int)(t / Rh);
+      const int I = r0 + 2 * q, J = 2 * (int)(t - (long)q * Rh) + c;
+      const size_t idx = (size_t)(I + 1) * L.P + J + 1;
+      const float id = __ldg(L.coef + MG_INVD * plane + idx);
+      if (id == 0.f)
+        continue;
+      L.u[idx] = *(L.f + idx) * id - nb9(L, idx, plane);
+    }
+    __syncthreads();
   }
 }
 
@@ -345,68 +424,72 @@ __device__ void prolong9(const MgLevel &F, const MgLevel &C, long t0, long dt)
   }
 }
 
-// Levels l0 .. nlev-1 below a restriction into l0: descent, the coarsest
-// level's sweeps, ascent back to l0.  `local`: CTA 0 alone.
-__device__ bool sub_cycle(const Mg32Args &a, int l0, bool local, long t0, long dt, unsigned &gen, DevCounts *cnt)
+__shared__ float mg_coarse_f[MG_MAX_DIRECT]; // the coarsest level's f, gathered for its exact solve
+
+// Levels l0 .. nlev-1 below a restriction into l0, by CTA 0 alone with CTA
+// barriers: descent, the coarsest level's solve, ascent back to l0.
+__device__ void sub_cycle(const Mg32Args &a, int l0)
 {
+  const MgLevel *lv = a.lev;
+  const long t0 = threadIdx.x, dt = blockDim.x;
   const int L = a.nlev;
   for (int l = l0; l < L - 1; l++) {
     for (int k = 0; k < a.nu; k++)
       for (int c = 0; c < 4; c++) {
-        smooth9(a.lev[l], c, t0, dt);
-        if (!mg_sync(a, local, gen, cnt))
-          return false;
+        smooth9(lv[l], c, t0, dt);
+        __syncthreads();
       }
-    restrict9(a.lev[l], a.lev[l + 1], t0, dt);
-    if (!mg_sync(a, local, gen, cnt))
-      return false;
+    restrict9(lv[l], lv[l + 1], t0, dt);
+    __syncthreads();
   }
-  if (a.cinv && local) {
+  if (a.cinv) {
     // the coarsest level solved exactly: u = A^-1 f over its unknowns
-    __shared__ float fc[MG_MAX_DIRECT];
-    const MgLevel &C = a.lev[L - 1];
+    float *fc = mg_coarse_f;
+    const MgLevel &C = lv[L - 1];
     for (int i = (int)t0; i < a.cn; i += (int)dt)
       fc[i] = C.f[a.cidx[i]];
     __syncthreads();
-    for (int i = (int)t0; i < a.cn; i += (int)dt) {
+    // a warp per row: coalesced reads of the row, the lanes' partial sums
+    // added by shuffles
+    const int lane = (int)t0 & 31, warp = (int)t0 >> 5, nwarps = (int)dt >> 5;
+    for (int i = warp; i < a.cn; i += nwarps) {
       const float *row = a.cinv + (size_t)i * a.cn;
       float acc = 0.f;
-      for (int k = 0; k < a.cn; k++)
+      for (int k = lane; k < a.cn; k += 32)
         acc += __ldg(row + k) * fc[k];
-      C.u[a.cidx[i]] = acc;
+      for (int o = 16; o > 0; o >>= 1)
+        acc += __shfl_down_sync(0xffffffffu, acc, o);
+      if (lane == 0)
+        C.u[a.cidx[i]] = acc;
     }
     __syncthreads();
   } else {
     for (int k = 0; k < a.coarse_sweeps; k++)
       for (int c = 0; c < 4; c++) {
-        smooth9(a.lev[L - 1], c, t0, dt);
-        if (!mg_sync(a, local, gen, cnt))
-          return false;
+        smooth9(lv[L - 1], c, t0, dt);
+        __syncthreads();
       }
   }
   for (int l = L - 2; l >= l0; l--) {
-    prolong9(a.lev[l], a.lev[l + 1], t0, dt);
-    if (!mg_sync(a, local, gen, cnt))
-      return false;
+    prolong9(lv[l], lv[l + 1], t0, dt);
+    __syncthreads();
     for (int k = 0; k < a.nu; k++)
       for (int c = 3; c >= 0; c--) {
-        smooth9(a.lev[l], c, t0, dt);
-        if (!mg_sync(a, local, gen, cnt))
-          return false;
+        smooth9(lv[l], c, t0, dt);
+        __syncthreads();
       }
   }
-  return true;
 }
 
 // One V-cycle on (u0, f0), u0 = 0 on entry.
 __device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
 {
   const long gt0 = (long)blockIdx.x * blockDim.x + threadIdx.x, gdt = (long)gridDim.x * blockDim.x;
-  const long lt0 = threadIdx.x, ldt = blockDim.x;
   const int T = a.tail; // 1 <= T <= nlev - 1
+  // the first colour-0 sweep from u0 = 0 was made by residual64
   for (int k = 0; k < a.nu0; k++)
-    for (int c = 0; c < 2; c++) {
-      smooth0(a, c, gt0, gdt);
+    for (int c = k ? 0 : 1; c < 2; c++) {
+      smooth0<false>(a, c, gt0, gdt);
       if (!mg_grid_sync(a, gen, cnt))
         return false;
     }
@@ -416,8 +499,8 @@ __device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
   // grid-wide nine-point levels 1 .. T-1
   for (int l = 1; l < T; l++) {
     for (int k = 0; k < a.nu; k++)
-      for (int c = 0; c < 4; c++) {
-        smooth9(a.lev[l], c, gt0, gdt);
+      for (int cz = 0; cz < 2; cz++) { // colours (cz, 0), (cz, 1)
+        smooth9_rows(a.lev[l], cz, 0);
         if (!mg_grid_sync(a, gen, cnt))
           return false;
       }
@@ -426,8 +509,8 @@ __device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
       return false;
   }
   // levels T .. nlev-1 by CTA 0 while the others wait
-  if (blockIdx.x == 0 && !sub_cycle(a, T, true, lt0, ldt, gen, cnt))
-    return false;
+  if (blockIdx.x == 0)
+    sub_cycle(a, T);
   if (!mg_grid_sync(a, gen, cnt))
     return false;
   for (int l = T - 1; l >= 1; l--) {
@@ -435,8 +518,8 @@ __device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
     if (!mg_grid_sync(a, gen, cnt))
       return false;
     for (int k = 0; k < a.nu; k++)
-      for (int c = 3; c >= 0; c--) {
-        smooth9(a.lev[l], c, gt0, gdt);
+      for (int cz = 1; cz >= 0; cz--) { // colours (cz, 1), (cz, 0)
+        smooth9_rows(a.lev[l], cz, 1);
         if (!mg_grid_sync(a, gen, cnt))
           return false;
       }
@@ -446,16 +529,20 @@ __device__ bool vcycle(const Mg32Args &a, unsigned &gen, DevCounts *cnt)
     return false;
   for (int k = 0; k < a.nu0; k++)
     for (int c = 1; c >= 0; c--) {
-      smooth0(a, c, gt0, gdt);
+      if (k == a.nu0 - 1 && c == 0)
+        smooth0<true>(a, c, gt0, gdt); // Psi += u0 on the way
+      else
+        smooth0<false>(a, c, gt0, gdt);
       if (!mg_grid_sync(a, gen, cnt))
         return false;
     }
   return true;
 }
 
-// r = rhs - A Psi in FP64 over the unknown nodes into f0 (rounded), u0 = 0
-// there; this thread's sum |r| and, with first, sum |rhs| over iz < nz,
-// ir < nr-1.  With fold, Psi += u0 first (the same nodes per thread).
+// r = rhs - A Psi in FP64 over the unknown nodes into f0 (rounded), and u0
+// as the first colour-0 Gauss-Seidel sweep from u0 = 0 leaves it: f0 / e at
+// (iz+ir) even nodes (their neighbour sum is zero), 0 at the others; this
+// thread's sum |r| and, with first, sum |rhs| over iz < nz, ir < nr-1.
 __device__ void residual64(const Mg32Args &a, bool first, double *rs, double *ds)
 {
   const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, dt = (long)gridDim.x * blockDim.x;
@@ -482,8 +569,9 @@ __device__ void residual64(const Mg32Args &a, bool first, double *rs, double *ds
     }
     const double r = rh - ap;
     r_acc += fabs(r);
-    a.f0[j] = (float)r;
-    a.u0[j] = 0.f;
+    const float rf = (float)r;
+    a.f0[j] = rf;
+    a.u0[j] = (a.nu0 && !((iz + ir) & 1)) ? rf * (ir ? a.inv_e : a.inv_e2c) : 0.f;
   }
   *rs = r_acc;
   *ds = d_acc;
@@ -579,9 +667,11 @@ __global__ void __launch_bounds__(MG_NT) k_mg32(Mg32Args a, DevCounts *cnt)
     // which every CTA reaches after reading them)
     if (!vcycle(a, gen, cnt))
       return;
-    fold(a);
-    if (!mg_grid_sync(a, gen, cnt))
-      return;
+    if (a.nu0 == 0) { // no sweep to fold into
+      fold(a);
+      if (!mg_grid_sync(a, gen, cnt))
+        return;
+    }
     cycles++;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {

@@ -48,6 +48,8 @@ STEPS = 12000  # the bunch needs about 9,000 steps of 17.7 um to reach the exit
 
 def run(precision, cfg, f, b, steps=STEPS, solver=None, corrections=True):
     g = gpu.GpuInstance(f, capacity=b.capacity, precision=precision)
+    if precision == gpu.PRECISION_F64:
+        g.set_deposit_order(1)  # the reference's particle-order sums: a deterministic FP64 run
     if solver is not None:
         g.set_poisson_solver(solver)
     g.upload_beam(b)
