@@ -102,14 +102,14 @@ __global__ void __launch_bounds__(BX *BY) k_apparent32(DevMesh m, DevFields32 f,
 __global__ void __launch_bounds__(RT) k_remove32(DevMesh m, DevFields32 f, DevBeam32 b, const DevCounts *cnt,
                                                   S32Scales sc, long long *qreal_fixed)
 {
-  __shared__ double sh[RT];
+  __shared__ long long sh[RT / 32];
   const long ip = (long)blockIdx.x * RT + threadIdx.x;
+  const bool lsm = m.modes & SPIFFE_FL_LONGIT_SMEAR, rsm = m.modes & SPIFFE_FL_RADIAL_SMEAR;
   int nodes[4] = {-1, -1, -1, -1};
   long long q[4] = {0, 0, 0, 0};
   long long mine = 0;
   if (ip < (long)cnt->np && (b.status[ip] & S32_ACTIVE)) {
     const int nz = m.nz, nr = m.nr, P = m.pitch;
-    const bool lsm = m.modes & SPIFFE_FL_LONGIT_SMEAR, rsm = m.modes & SPIFFE_FL_RADIAL_SMEAR;
     const bool ln = m.left_bc == SPIFFE_NEUMANN, rn = m.right_bc == SPIFFE_NEUMANN, un = m.upper_bc == SPIFFE_NEUMANN;
     const int32_t c = b.cell[ip];
     const int cz = s32_iz(c), cr = s32_ir(c);
@@ -171,9 +171,18 @@ __global__ void __launch_bounds__(RT) k_remove32(DevMesh m, DevFields32 f, DevBe
           mine += q[k];
     }
   }
+#pragma unroll
   for (int k = 0; k < 4; k++) {
-    // same grouping as the current deposition
-    const unsigned grp = __match_any_sync(0xffffffffu, nodes[k]);
+    // slots 1 and 3 carry charge only with longitudinal smearing, 2 and 3
+    // only with radial smearing (their weight is zero otherwise); the flags
+    // are the mesh's, the same in every lane
+    if (((k & 1) && !lsm) || ((k & 2) && !rsm))
+      continue;
+    // same grouping as the current deposition; cell-sorted particles
+    // usually share the node across the warp, which one vote settles
+    const int nd0 = __shfl_sync(0xffffffffu, nodes[k], 0);
+    const unsigned grp =
+        __all_sync(0xffffffffu, nodes[k] == nd0) ? 0xffffffffu : __match_any_sync(0xffffffffu, nodes[k]);
     const unsigned long long biased = (unsigned long long)(q[k] + (1LL << 42));
     const unsigned lo = (unsigned)(biased & ((1u << 22) - 1)), hi = (unsigned)(biased >> 22);
     const unsigned slo = __reduce_add_sync(grp, lo), shi = __reduce_add_sync(grp, hi);
@@ -183,10 +192,19 @@ __global__ void __launch_bounds__(RT) k_remove32(DevMesh m, DevFields32 f, DevBe
         atomic_add_ll(f.Qp + nodes[k], tot);
     }
   }
-  // exact integer total of the removed charge
-  const double s = block_sum_d((double)mine, sh); // |per-block sum| < 2^53
-  if (threadIdx.x == 0 && s != 0)
-    atomic_add_ll(qreal_fixed, (long long)s);
+  // exact integer total of the removed charge: warp sums, then the CTA's
+  for (int o = 16; o > 0; o >>= 1)
+    mine += __shfl_down_sync(0xffffffffu, mine, o);
+  if ((threadIdx.x & 31) == 0)
+    sh[threadIdx.x >> 5] = mine;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int w = 0; w < RT / 32; w++)
+      s += sh[w];
+    if (s)
+      atomic_add_ll(qreal_fixed, s);
+  }
 }
 
 // Q -= particle charge (the FP64 form's atomics on Q) over all nodes; partial
