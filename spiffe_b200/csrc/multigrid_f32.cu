@@ -61,6 +61,7 @@ namespace {
 constexpr int MG_NT = 1024;           // threads per CTA
 constexpr int MG_TAIL_NODES = 3000;   // levels at most this large are worked by CTA 0 alone
 constexpr int MG_MIN_UNKNOWNS = 64;   // coarsening stops at this many unknowns
+constexpr int MG_NODES_PER_CTA = 8192; // mesh nodes per CTA below one CTA per SM
 constexpr int MG_MAX_DIRECT = 1024;   // a coarsest level of at most this many unknowns is solved exactly
 enum { MG_INVD = 8, MG_DIAG = 9 };
 
@@ -952,7 +953,11 @@ extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w,
     return (int)e;
   if (per < 1)
     return (int)cudaErrorInvalidConfiguration;
-  const int grid = sms; // one CTA per SM: every CTA is resident
+  // one CTA per SM at most (every CTA resident), and no more CTAs than the
+  // mesh gives work: a small mesh's solve then pays for fewer barrier
+  // arrivals and leaves the other SMs to other instances' kernels
+  const size_t mesh_nodes = (size_t)(m->nz + 1) * (m->nr + 1);
+  const int grid = (int)std::min<size_t>((size_t)sms, std::max<size_t>(1, (mesh_nodes + MG_NODES_PER_CTA - 1) / MG_NODES_PER_CTA));
   bytes += (size_t)2 * grid * sizeof(double) + 32 * sizeof(unsigned long long) + sizeof(long long);
   char *mem = nullptr;
   e = cudaMalloc(&mem, bytes);
