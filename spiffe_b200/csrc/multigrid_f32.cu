@@ -51,6 +51,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "modules.cuh"
@@ -691,6 +692,27 @@ __global__ void __launch_bounds__(MG_NT) k_mg32(Mg32Args a, DevCounts *cnt)
 
 // ---- host: the level hierarchy
 
+// fn(lo, hi) over [0, n) in contiguous chunks on up to 16 host threads (the
+// hierarchy of a 2.5M-node mesh takes over half a second on one core)
+template <class Fn>
+void parallel_rows(int n, Fn fn)
+{
+  const int nt = std::max(1, std::min({16, (int)std::thread::hardware_concurrency(), n / 8}));
+  if (nt <= 1) {
+    fn(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const int chunk = (n + nt - 1) / nt;
+  for (int t = 0; t < nt; t++) {
+    const int lo = t * chunk, hi = std::min(n, lo + chunk);
+    if (lo < hi)
+      pool.emplace_back(fn, lo, hi);
+  }
+  for (std::thread &th : pool)
+    th.join();
+}
+
 // level-0 operator as nine-point rows (only the five-point entries are
 // nonzero): coefficient of node (iz+dz, ir+dr) at k = (dz+1)*3 + (dr+1)
 struct Stencil {
@@ -714,7 +736,9 @@ void fine_stencil(const DevMesh &m, const int16_t *flags, int lo, int hi, Stenci
         S.unk[(size_t)iz * S.R + ir] = 1;
   const double a = 1 / (m.dz * m.dz), dr2 = m.dr * m.dr;
   const double e = -2 * (1 / (m.dz * m.dz) + 1 / dr2);
-  for (int iz = lo; iz <= hi; iz++)
+  // each node writes only its own stencil row
+  parallel_rows(hi - lo + 1, [&](int r0, int r1) {
+  for (int iz = lo + r0; iz < lo + r1; iz++)
     for (int ir = 0; ir < cols; ir++) {
       if (!S.unk[(size_t)iz * S.R + ir])
         continue;
@@ -746,6 +770,7 @@ void fine_stencil(const DevMesh &m, const int16_t *flags, int lo, int hi, Stenci
       add(iz, ir - 1, cl);
       S.at(4, iz, ir) = dg;
     }
+  });
 }
 
 // annulus weight of column j of a level of spacing 1 (the axis node: 1/8)
@@ -773,7 +798,14 @@ void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
       rw[(size_t)3 * J + dj + 1] = (dj ? 0.5 : 1.0) * vol(j) / (4 * vc);
     }
   auto cunk = [&](int I, int J) { return I >= 0 && I < C.Z && J >= 0 && J < C.R && C.unk[(size_t)I * C.R + J]; };
-  for (int I = 0; I < C.Z; I++)
+  // coarse rows in parallel: each node writes only its own stencil and flag,
+  // and reads the neighbours' flags as they were before any hold below (a
+  // coupling to a node held here is removed by the pass after, so the
+  // stencils do not depend on the order the rows are done in)
+  const std::vector<uint8_t> unk0 = C.unk;
+  auto cunk0 = [&](int I, int J) { return I >= 0 && I < C.Z && J >= 0 && J < C.R && unk0[(size_t)I * C.R + J]; };
+  parallel_rows(C.Z, [&](int I0, int I1) {
+  for (int I = I0; I < I1; I++)
     for (int J = 0; J < C.R; J++) {
       if (!C.unk[(size_t)I * C.R + J])
         continue;
@@ -796,7 +828,7 @@ void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
             for (int pz = 0; pz < nzp; pz++)
               for (int pr = 0; pr < nrp; pr++) {
                 const int K = pz0 + pz, Lc = pr0 + pr;
-                if (!cunk(K, Lc))
+                if (!cunk0(K, Lc))
                   continue;
                 acc[(K - I + 1) * 3 + (Lc - J + 1)] += r * v * wz * wr;
               }
@@ -810,12 +842,15 @@ void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
           C.at(k, I, J) = 0;
       }
     }
-  // couplings to nodes that were held above
-  for (int I = 0; I < C.Z; I++)
-    for (int J = 0; J < C.R; J++)
-      for (int k = 0; k < 9; k++)
-        if (C.at(k, I, J) != 0 && !cunk(I + k / 3 - 1, J + k % 3 - 1))
-          C.at(k, I, J) = 0;
+  });
+  // couplings to nodes that were held above (after every row's hold)
+  parallel_rows(C.Z, [&](int I0, int I1) {
+    for (int I = I0; I < I1; I++)
+      for (int J = 0; J < C.R; J++)
+        for (int k = 0; k < 9; k++)
+          if (C.at(k, I, J) != 0 && !cunk(I + k / 3 - 1, J + k % 3 - 1))
+            C.at(k, I, J) = 0;
+  });
 }
 
 size_t unknowns(const Stencil &S)
