@@ -411,7 +411,7 @@ def gpu_arm(args):
         "config": {"workload": "1.6-cell RF gun, 3001x821 nodes at 50um, 1,000,000 macroparticles, "
                                "Poisson correction every 20 steps, solenoid",
                    "form": ("split precision: FP32 fields and push, cell+FP32-offset positions, 64-bit fixed-point "
-                            "current, FP32 SOR in FP64 iterative refinement") if prec == gpu.PRECISION_SPLIT32
+                            "current, FP32 multigrid in FP64 iterative refinement") if prec == gpu.PRECISION_SPLIT32
                    else "plain FP64 (bit-faithful to the reference)",
                    "field": "stand-in: an analytic pi-mode standing wave, 100 MV/m on the cathode, in place of the "
                             "30,000-step antenna build-up and reload",
