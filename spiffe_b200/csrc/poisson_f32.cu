@@ -33,68 +33,10 @@ namespace {
 
 constexpr int BX = 32, BY = 8, RT = 256;
 
-__device__ double block_sum_d(double v, double *sh)
-{
-  const int t = threadIdx.y * blockDim.x + threadIdx.x, n = blockDim.x * blockDim.y;
-  sh[t] = v;
-  __syncthreads();
-  for (int s = 512; s > 0; s >>= 1) {
-    if (t < s && t + s < n)
-      sh[t] += sh[t + s];
-    __syncthreads();
-  }
-  const double r = sh[0];
-  __syncthreads();
-  return r;
-}
-
 __device__ bool surface_cell(const DevMesh &m, int16_t fl, int iz, int ir)
 {
   return (fl & SPIFFE_FL_IS_METAL) || (iz == 0 && m.left_bc == SPIFFE_NEUMANN) ||
          (iz == m.nz - 1 && m.right_bc == SPIFFE_NEUMANN) || (ir == m.nr - 1 && m.upper_bc == SPIFFE_NEUMANN);
-}
-
-// Apparent charge from the flux of E (poisson_correction.c:141-182, second
-// pass :335-375), in FP64 from the FP32 fields.
-__global__ void __launch_bounds__(BX *BY) k_apparent32(DevMesh m, DevFields32 f, const double *Az_, const double *Ari,
-                                                        const double *Aro, int second, double *part)
-{
-  __shared__ double sh[BX * BY];
-  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
-  const int nz = m.nz, nr = m.nr, P = m.pitch;
-  const double eps = SPIFFE_EPSILON_O;
-  double qs = 0, cen = 0;
-  if (ir < nr && iz < nz) {
-    const size_t i = node(iz, ir, P);
-    const double Az = Az_[ir], Ar_inner = Ari[ir], Ar_outer = Aro[ir];
-    const double Ez0 = f.Ez[i], Ez1 = f.Ez[i + P], Er0 = f.Er[i], Er1 = f.Er[i + 1];
-    double dQ;
-    if (ir == 0)
-      dQ = (Er1 * Ar_outer + (Ez1 - Ez0) * Az) * eps;
-    else
-      dQ = (Er1 * Ar_outer - Er0 * Ar_inner + (Ez1 - Ez0) * Az) * eps;
-    if (surface_cell(m, f.flags[i], iz, ir)) {
-      if (iz == 0)
-        dQ += Ez0 * Az * eps;
-      if (iz == nz - 1)
-        dQ -= Ez1 * Az * eps;
-      if (ir == nr - 1) {
-        const double e = (double)f.Ez[i + 1] * Ar_outer * eps;
-        dQ += second ? -e : e;
-      }
-      qs = dQ;
-      f.Q[i] = 0;
-    } else {
-      f.Q[i] = dQ;
-      cen = dQ * (iz * m.dz + m.zmin);
-    }
-  }
-  const double s0 = block_sum_d(qs, sh), s1 = block_sum_d(cen, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
-    const int b = blockIdx.y * gridDim.x + blockIdx.x;
-    part[2 * b] = s0;
-    part[2 * b + 1] = s1;
-  }
 }
 
 // The particles' own charge (:190-242) in fixed point: Qp[node] receives the
@@ -207,71 +149,120 @@ __global__ void __launch_bounds__(RT) k_remove32(DevMesh m, DevFields32 f, DevBe
   }
 }
 
-// Q -= particle charge (the FP64 form's atomics on Q) over all nodes; partial
-// sums of Q over iz < nz, ir < nr for Qerror (:244-256).
-__global__ void __launch_bounds__(BX *BY) k_combine32(DevMesh m, DevFields32 f, double qQ, int space_charge,
-                                                       double *part)
+// One pass of the correction's charge: the apparent charge from the flux of
+// E (poisson_correction.c:141-182, second pass :335-375) in FP64 from the
+// FP32 fields, minus the particles' fixed-point charge per node (the FP64
+// form's subtraction on Q, :190-242), and on the first pass the solver's
+// right-hand side -Q/(V eps0) over iz < nz, ir < nr (:268-274) with the
+// per-block sums of the surface charge, its centroid moment and the error
+// charge (:244-256) taken before the scaling.  The scaling is unconditional:
+// the pass after the solve recomputes every node it touched, so a solve
+// skipped by the threshold test leaves the same Q.  Nodes outside iz < nz,
+// ir < nr keep their Q minus the particles' charge.
+__global__ void __launch_bounds__(BX *BY) k_charge32(DevMesh m, DevFields32 f, const double *Az_, const double *Ari,
+                                                      const double *Aro, const double *volume, int second, double qQ,
+                                                      int space_charge, double *part)
 {
-  __shared__ double sh[BX * BY];
   const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
-  double v = 0;
-  if (ir <= m.nr && iz <= m.nz) {
-    const size_t i = node(iz, ir, m.pitch);
-    double q = f.Q[i];
-    if (space_charge) {
-      const long long p = f.Qp[i];
-      if (p)
-        q -= (double)p * qQ;
-      f.Q[i] = q;
+  const int nz = m.nz, nr = m.nr, P = m.pitch;
+  const double eps = SPIFFE_EPSILON_O;
+  double qs = 0, cen = 0, qe = 0;
+  if (ir <= nr && iz <= nz) {
+    const size_t i = node(iz, ir, P);
+    const bool inner = ir < nr && iz < nz;
+    double q;
+    if (inner) {
+      const double Az = Az_[ir], Ar_inner = Ari[ir], Ar_outer = Aro[ir];
+      const double Ez0 = f.Ez[i], Ez1 = f.Ez[i + P], Er0 = f.Er[i], Er1 = f.Er[i + 1];
+      double dQ;
+      if (ir == 0)
+        dQ = (Er1 * Ar_outer + (Ez1 - Ez0) * Az) * eps;
+      else
+        dQ = (Er1 * Ar_outer - Er0 * Ar_inner + (Ez1 - Ez0) * Az) * eps;
+      if (surface_cell(m, f.flags[i], iz, ir)) {
+        if (iz == 0)
+          dQ += Ez0 * Az * eps;
+        if (iz == nz - 1)
+          dQ -= Ez1 * Az * eps;
+        if (ir == nr - 1) {
+          const double e = (double)f.Ez[i + 1] * Ar_outer * eps;
+          dQ += second ? -e : e;
+        }
+        qs = dQ;
+        q = 0;
+      } else {
+        q = dQ;
+        cen = dQ * (iz * m.dz + m.zmin);
+      }
+    } else {
+      q = f.Q[i];
     }
-    if (ir < m.nr && iz < m.nz)
-      v = q;
+    if (space_charge) {
+      const long long pq = f.Qp[i];
+      if (pq)
+        q -= (double)pq * qQ;
+    }
+    if (inner)
+      qe = q;
+    f.Q[i] = (!second && inner) ? -q / (volume[ir] * SPIFFE_EPSILON_O) : q;
   }
-  const double s = block_sum_d(v, sh);
-  if (threadIdx.x == 0 && threadIdx.y == 0)
-    part[blockIdx.y * gridDim.x + blockIdx.x] = s;
+  if (second)
+    return;
+  // fixed-order block sums of (qs, cen, qe)
+  __shared__ double sh[3][BX * BY / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    qs += __shfl_down_sync(0xffffffffu, qs, o);
+    cen += __shfl_down_sync(0xffffffffu, cen, o);
+    qe += __shfl_down_sync(0xffffffffu, qe, o);
+  }
+  const int t = threadIdx.y * BX + threadIdx.x;
+  if ((t & 31) == 0) {
+    sh[0][t >> 5] = qs;
+    sh[1][t >> 5] = cen;
+    sh[2][t >> 5] = qe;
+  }
+  __syncthreads();
+  if (t < 3) {
+    double v = 0;
+    for (int w = 0; w < BX * BY / 32; w++)
+      v += sh[t][w];
+    part[3 * (blockIdx.y * gridDim.x + blockIdx.x) + t] = v;
+  }
 }
 
-__global__ void k_finish_sum32(const double *part, int n, int stride, double *out)
+// The grid's sums of k_charge32's partials (fixed order) into sc[0]
+// (Qsurface), sc[1] (centroid moment), sc[3] (Qerror), then the correction's
+// state and the error-charge threshold decision.
+__global__ void k_charge_state32(const double *part, int n, double *sc, PcState *st, const long long *qreal_fixed,
+                                 double qQ, int space_charge, double threshold)
 {
-  __shared__ double sh[1024];
-  double v = 0;
+  __shared__ double sh[3][1024];
+  double v[3] = {0, 0, 0};
   for (int i = threadIdx.x; i < n; i += blockDim.x)
-    v += part[(size_t)i * stride];
-  sh[threadIdx.x] = v;
+    for (int k = 0; k < 3; k++)
+      v[k] += part[3 * (size_t)i + k];
+  for (int k = 0; k < 3; k++)
+    sh[k][threadIdx.x] = v[k];
   __syncthreads();
   for (int s = blockDim.x / 2; s > 0; s >>= 1) {
     if (threadIdx.x < s)
-      sh[threadIdx.x] += sh[threadIdx.x + s];
+      for (int k = 0; k < 3; k++)
+        sh[k][threadIdx.x] += sh[k][threadIdx.x + s];
     __syncthreads();
   }
-  if (threadIdx.x == 0)
-    *out = sh[0];
-}
-
-__global__ void k_state32(PcState *st, const double *sc, const long long *qreal_fixed, double qQ, int space_charge,
-                          double threshold)
-{
-  st->Qsurface = sc[0];
-  st->centroid = sc[1];
-  st->Qreal = space_charge ? (double)*qreal_fixed * qQ : 0.0;
-  st->Qerror = sc[3];
-  const double Qerror = st->Qerror, Qreal = st->Qreal;
-  // error-charge threshold test (:258-265)
-  const int skip = (threshold > 0 && fabs(Qerror) < threshold) ||
-                   (threshold < 0 && (Qreal == 0 || fabs(Qerror / Qreal) < fabs(threshold)));
-  st->do_solve = !skip;
-}
-
-// Q -> -Q/(V eps0) over iz < nz, ir < nr (:268-274)
-__global__ void __launch_bounds__(BX *BY) k_scale32(DevMesh m, DevFields32 f, const double *volume, const PcState *st)
-{
-  if (!st->do_solve)
-    return;
-  const int ir = blockIdx.x * BX + threadIdx.x, iz = blockIdx.y * BY + threadIdx.y;
-  if (ir < m.nr && iz < m.nz) {
-    const size_t i = node(iz, ir, m.pitch);
-    f.Q[i] = -f.Q[i] / (volume[ir] * SPIFFE_EPSILON_O);
+  if (threadIdx.x == 0) {
+    sc[0] = sh[0][0];
+    sc[1] = sh[1][0];
+    sc[3] = sh[2][0];
+    st->Qsurface = sc[0];
+    st->centroid = sc[1];
+    st->Qreal = space_charge ? (double)*qreal_fixed * qQ : 0.0;
+    st->Qerror = sc[3];
+    const double Qerror = st->Qerror, Qreal = st->Qreal;
+    // error-charge threshold test (:258-265)
+    const int skip = (threshold > 0 && fabs(Qerror) < threshold) ||
+                     (threshold < 0 && (Qreal == 0 || fabs(Qerror / Qreal) < fabs(threshold)));
+    st->do_solve = !skip;
   }
 }
 
@@ -1149,7 +1140,7 @@ extern "C" int s32_poisson_setup(const DevMesh *m, Poisson32Work *w, long long n
     e = cudaErrorInvalidConfiguration;
   w->half = H;
   const size_t gx = (nr + 1 + BX - 1) / BX, gy = (nz + 1 + BY - 1) / BY;
-  size_t parts = std::max<size_t>(2 * gx * gy, 4096);
+  size_t parts = std::max<size_t>(3 * gx * gy, 4096);
   (void)np_capacity;
   if (e == cudaSuccess && !w->Az) {
     e = cudaMalloc(&w->Az, sizeof(double) * (nr + 1));
@@ -1277,10 +1268,8 @@ extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, co
   const dim3 block(BX, BY), grid((m->nr + 1 + BX - 1) / BX, (m->nz + 1 + BY - 1) / BY);
   const int nblk = grid.x * grid.y;
   const bool sc_on = o->space_charge && np_bound > 0;
-  k_apparent32<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 0, w->part);
-  k_finish_sum32<<<1, 1024, 0, s>>>(w->part, nblk, 2, w->scalars + 0);
-  k_finish_sum32<<<1, 1024, 0, s>>>(w->part + 1, nblk, 2, w->scalars + 1);
-  spiffe_note_launches(3);
+  // the particles' charge first (it reads only the beam), then one pass of
+  // apparent charge, particle charge, sums and right-hand side
   cudaError_t e = cudaMemsetAsync(w->qreal_fixed, 0, sizeof(long long), s);
   if (e != cudaSuccess)
     return (int)e;
@@ -1291,11 +1280,10 @@ extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, co
     k_remove32<<<blocks_for(np_bound, RT), RT, 0, s>>>(*m, *f, *b, cnt, *sc, w->qreal_fixed);
     spiffe_note_launches(1);
   }
-  k_combine32<<<grid, block, 0, s>>>(*m, *f, sc->qQ, sc_on ? 1 : 0, w->part);
-  k_finish_sum32<<<1, 1024, 0, s>>>(w->part, nblk, 1, w->scalars + 3);
-  k_state32<<<1, 1, 0, s>>>(w->st, w->scalars, w->qreal_fixed, sc->qQ, o->space_charge, o->error_charge_threshold);
-  k_scale32<<<grid, block, 0, s>>>(*m, *f, w->volume, w->st);
-  spiffe_note_launches(4);
+  k_charge32<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, w->volume, 0, sc->qQ, sc_on ? 1 : 0, w->part);
+  k_charge_state32<<<1, 1024, 0, s>>>(w->part, nblk, w->scalars, w->st, w->qreal_fixed, sc->qQ, o->space_charge,
+                                      o->error_charge_threshold);
+  spiffe_note_launches(2);
   if (o->guess_code) {
     k_guess32<<<grid, block, 0, s>>>(*m, *f, o->guess_code, w->st);
     spiffe_note_launches(1);
@@ -1306,9 +1294,8 @@ extern "C" int s32_poisson_correction(const DevMesh *m, const DevFields32 *f, co
   k_subtract32<<<grid, block, 0, s>>>(*m, *f, w->st);
   // the reference recomputes the apparent charge afterwards (:333-439); the
   // particles have not moved, so their charge per node is the same Qp
-  k_apparent32<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, 1, w->part);
-  k_combine32<<<grid, block, 0, s>>>(*m, *f, sc->qQ, sc_on ? 1 : 0, w->part);
-  spiffe_note_launches(3);
+  k_charge32<<<grid, block, 0, s>>>(*m, *f, w->Az, w->Ari, w->Aro, w->volume, 1, sc->qQ, sc_on ? 1 : 0, nullptr);
+  spiffe_note_launches(2);
   return (int)cudaGetLastError();
 }
 
