@@ -63,6 +63,7 @@ constexpr int MG_NT = 1024;           // threads per CTA
 constexpr int MG_TAIL_NODES = 3000;   // levels at most this large are worked by CTA 0 alone
 constexpr int MG_MIN_UNKNOWNS = 64;   // coarsening stops at this many unknowns
 constexpr int MG_NODES_PER_CTA = 8192; // mesh nodes per CTA below one CTA per SM
+constexpr int MG_SMALL_MESH = 200000;  // meshes of at most this many nodes smooth four times
 constexpr int MG_MAX_DIRECT = 1024;   // a coarsest level of at most this many unknowns is solved exactly
 enum { MG_INVD = 8, MG_DIAG = 9 };
 
@@ -334,7 +335,18 @@ __device__ void restrict0(const Mg32Args &a, long t0, long dt)
     const int I = (int)(t / C.R), J = (int)(t - (long)I * C.R);
     const size_t idx = (size_t)(I + 1) * C.P + J + 1;
     float s = 0.f;
-    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
+    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f && (C.cz != 2 || C.cr != 2)) {
+      // semi-coarsened: the three fine nodes along the coarsened direction
+      const float w[3] = {__ldg(C.rw + 3 * J), __ldg(C.rw + 3 * J + 1), __ldg(C.rw + 3 * J + 2)};
+      const int iz = C.cz * I, ir = C.cr * J;
+#pragma unroll
+      for (int d = -1; d <= 1; d++) {
+        const int z = C.cz == 2 ? iz + d : iz, r = C.cr == 2 ? ir + d : ir;
+        if (z < 0 || z > a.nz || r < 0)
+          continue;
+        s += (C.cz == 2 ? (d ? 0.5f : 1.f) * w[1] : w[d + 1]) * res0(a, z, r);
+      }
+    } else if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
       const float w0 = __ldg(C.rw + 3 * J), w1 = __ldg(C.rw + 3 * J + 1), w2 = __ldg(C.rw + 3 * J + 2);
       const int iz = 2 * I, ir = 2 * J;
       s = w1 * res0(a, iz, ir);
@@ -365,7 +377,18 @@ __device__ void restrict9(const MgLevel &F, const MgLevel &C, long t0, long dt)
     const int I = (int)(t / C.R), J = (int)(t - (long)I * C.R);
     const size_t idx = (size_t)(I + 1) * C.P + J + 1;
     float s = 0.f;
-    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
+    if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f && (C.cz != 2 || C.cr != 2)) {
+      // semi-coarsened: the three fine nodes along the coarsened direction
+      const float w[3] = {__ldg(C.rw + 3 * J), __ldg(C.rw + 3 * J + 1), __ldg(C.rw + 3 * J + 2)};
+      const int i = C.cz * I, j = C.cr * J;
+#pragma unroll
+      for (int d = -1; d <= 1; d++) {
+        const int z = C.cz == 2 ? i + d : i, r = C.cr == 2 ? j + d : j;
+        if (z < 0 || z >= F.Z || r < 0 || r >= F.R)
+          continue;
+        s += (C.cz == 2 ? (d ? 0.5f : 1.f) * w[1] : w[d + 1]) * res9(F, z, r);
+      }
+    } else if (__ldg(C.coef + MG_INVD * plane + idx) != 0.f) {
       const float w0 = __ldg(C.rw + 3 * J), w1 = __ldg(C.rw + 3 * J + 1), w2 = __ldg(C.rw + 3 * J + 2);
       const int i = 2 * I, j = 2 * J;
       s = w1 * res9(F, i, j);
@@ -384,18 +407,20 @@ __device__ void restrict9(const MgLevel &F, const MgLevel &C, long t0, long dt)
 }
 
 // bilinear correction from level C at node (i, j) of the level above
+// (linear along a direction C does not coarsen: the node itself)
 __device__ __forceinline__ float interp(const MgLevel &C, int i, int j)
 {
-  const int I = i >> 1, J = j >> 1;
+  const bool hz = C.cz == 2 && (i & 1), hr = C.cr == 2 && (j & 1); // half-way nodes
+  const int I = C.cz == 2 ? i >> 1 : i, J = C.cr == 2 ? j >> 1 : j;
   const float *u = C.u + (size_t)(I + 1) * C.P + J + 1;
   float v;
-  if (j & 1)
+  if (hr)
     v = 0.5f * (*(u) + *(u + 1));
   else
     v = *(u);
-  if (i & 1) {
+  if (hz) {
     const float *w = u + C.P;
-    v = 0.5f * v + 0.5f * ((j & 1) ? 0.5f * (*(w) + *(w + 1)) : *(w));
+    v = 0.5f * v + 0.5f * (hr ? 0.5f * (*(w) + *(w + 1)) : *(w));
   }
   return v;
 }
@@ -776,25 +801,28 @@ void fine_stencil(const DevMesh &m, const int16_t *flags, int lo, int hi, Stenci
 // annulus weight of column j of a level of spacing 1 (the axis node: 1/8)
 inline double vol(int j) { return j ? (double)j : 0.125; }
 
-// Galerkin R A P from level F to C (nodes 2I, 2J of F); restriction weights
-// rw[J][3] for F columns 2J-1, 2J, 2J+1 (z weights 1/2, 1, 1/2 apply on top)
-void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
+// Galerkin R A P from level F to C (nodes cz I, cr J of F: cz, cr = 2 to
+// coarsen a direction, 1 to keep it); restriction weights rw[J][3] for F
+// columns cr J - 1, cr J, cr J + 1 (with cz = 2 the z weights 1/2, 1, 1/2
+// apply on top)
+void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw, int cz, int cr)
 {
-  C.Z = (F.Z + 1) / 2;
-  C.R = (F.R + 1) / 2;
+  C.Z = cz == 2 ? (F.Z + 1) / 2 : F.Z;
+  C.R = cr == 2 ? (F.R + 1) / 2 : F.R;
   C.c.assign((size_t)9 * C.Z * C.R, 0.0);
   C.unk.assign((size_t)C.Z * C.R, 0);
   for (int I = 0; I < C.Z; I++)
     for (int J = 0; J < C.R; J++)
-      C.unk[(size_t)I * C.R + J] = F.unk[(size_t)(2 * I) * F.R + 2 * J];
+      C.unk[(size_t)I * C.R + J] = F.unk[(size_t)(cz * I) * F.R + cr * J];
   rw.assign((size_t)3 * C.R, 0.0);
   for (int J = 0; J < C.R; J++)
     for (int dj = -1; dj <= 1; dj++) {
-      const int j = 2 * J + dj;
-      if (j < 0 || j >= F.R)
+      const int j = cr * J + dj;
+      if (j < 0 || j >= F.R || (cr == 1 && dj))
         continue;
-      // fine spacing 1, coarse spacing 2: Vc(J) = 2 vol(J) (axis: 1/4)
-      const double vc = J ? 2.0 * J : 0.25;
+      // in fine units: coarse spacing 2, Vc(J) = 2 vc with vc = 2J (axis:
+      // 1/4); coarse spacing 1, Vc(J) = vol(J) = 2 vc
+      const double vc = cr == 2 ? (J ? 2.0 * J : 0.25) : 0.5 * vol(J);
       rw[(size_t)3 * J + dj + 1] = (dj ? 0.5 : 1.0) * vol(j) / (4 * vc);
     }
   auto cunk = [&](int I, int J) { return I >= 0 && I < C.Z && J >= 0 && J < C.R && C.unk[(size_t)I * C.R + J]; };
@@ -810,9 +838,10 @@ void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
       if (!C.unk[(size_t)I * C.R + J])
         continue;
       double acc[9] = {0};
-      for (int di = -1; di <= 1; di++)
-        for (int dj = -1; dj <= 1; dj++) {
-          const int i = 2 * I + di, j = 2 * J + dj;
+      const int dz0 = cz == 2 ? -1 : 0, dr0 = cr == 2 ? -1 : 0;
+      for (int di = dz0; di <= -dz0; di++)
+        for (int dj = dr0; dj <= -dr0; dj++) {
+          const int i = cz * I + di, j = cr * J + dj;
           if (i < 0 || i >= F.Z || j < 0 || j >= F.R || !F.unk[(size_t)i * F.R + j])
             continue;
           const double r = (di ? 0.5 : 1.0) * rw[(size_t)3 * J + dj + 1];
@@ -821,10 +850,12 @@ void galerkin(const Stencil &F, Stencil &C, std::vector<double> &rw)
             if (v == 0)
               continue;
             const int ni = i + k / 3 - 1, nj = j + k % 3 - 1; // an unknown fine node
-            // its coarse parents (bilinear interpolation)
-            const int pz0 = ni >> 1, pr0 = nj >> 1;
-            const int nzp = (ni & 1) ? 2 : 1, nrp = (nj & 1) ? 2 : 1;
-            const double wz = (ni & 1) ? 0.5 : 1.0, wr = (nj & 1) ? 0.5 : 1.0;
+            // its coarse parents (bilinear interpolation; along a direction
+            // kept, the node itself)
+            const bool hz = cz == 2 && (ni & 1), hr = cr == 2 && (nj & 1);
+            const int pz0 = cz == 2 ? ni >> 1 : ni, pr0 = cr == 2 ? nj >> 1 : nj;
+            const int nzp = hz ? 2 : 1, nrp = hr ? 2 : 1;
+            const double wz = hz ? 0.5 : 1.0, wr = hr ? 0.5 : 1.0;
             for (int pz = 0; pz < nzp; pz++)
               for (int pr = 0; pr < nrp; pr++) {
                 const int K = pz0 + pz, Lc = pr0 + pr;
@@ -949,17 +980,31 @@ extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w,
   std::vector<Stencil> lev(1);
   std::vector<std::vector<double>> rws(1);
   fine_stencil(*m, flags, lo, hi, lev[0]);
+  // Semi-coarsening: where the spacing in one direction is at least twice
+  // the other's, the operator couples nodes far more strongly along the
+  // finer direction, point Gauss-Seidel smooths the error only along it,
+  // and only that direction is coarsened (on a 165 x 357 gun mesh with
+  // dz = 8 dr, 64 V-cycles a correction with both directions coarsened).
+  std::vector<int> czs(1, 2), crs(1, 2);
+  double sz = m->dz, sr = m->dr; // the finest level's spacings so far
   while ((int)lev.size() < MG_MAX_LEVELS) {
     const Stencil &F = lev.back();
-    if (F.Z < 5 || F.R < 5 || unknowns(F) <= (size_t)MG_MIN_UNKNOWNS)
+    if (unknowns(F) <= (size_t)MG_MIN_UNKNOWNS)
+      break;
+    const int cz = sz >= 2 * sr ? 1 : 2, cr = sr >= 2 * sz ? 1 : 2;
+    if ((cz == 2 && F.Z < 5) || (cr == 2 && F.R < 5))
       break;
     Stencil C;
     std::vector<double> rw;
-    galerkin(F, C, rw);
+    galerkin(F, C, rw, cz, cr);
     if (unknowns(C) == 0)
       break;
     lev.push_back(std::move(C));
     rws.push_back(std::move(rw));
+    czs.push_back(cz);
+    crs.push_back(cr);
+    sz *= cz;
+    sr *= cr;
   }
   const int L = (int)lev.size();
   if (L < 2)
@@ -1023,6 +1068,8 @@ extern "C" int s32_mg_setup(const DevMesh *m, const int16_t *flags, Mg32Work *w,
     MgLevel &D = w->lev[l];
     D.Z = S.Z;
     D.R = S.R;
+    D.cz = czs[l];
+    D.cr = crs[l];
     D.P = (S.R + 2 + 31) / 32 * 32;
     const size_t plane = (size_t)(S.Z + 2) * D.P;
     D.u = (float *)(mem + off[l]);
@@ -1108,8 +1155,12 @@ extern "C" int s32_mg_solve(const DevMesh *m, Mg32Work *w, const float *crow, co
   a.inv_e2c = (float)(1 / a.e2c_d);
   a.nlev = w->nlev;
   a.tail = w->tail;
-  a.nu0 = 2;
-  a.nu = 2;
+  // V(2,2); V(4,4) on small meshes, whose sweeps cost little beside their
+  // barriers and whose coarse levels carry thin metal coarsely (on a 120 x
+  // 101 gun mesh 22 V(2,2) cycles a correction, 10 V(4,4))
+  const bool small = (size_t)(m->nz + 1) * (m->nr + 1) <= (size_t)MG_SMALL_MESH;
+  a.nu0 = small ? 4 : 2;
+  a.nu = small ? 4 : 2;
   a.coarse_sweeps = 24;
   a.cinv = w->cinv;
   a.cidx = w->cidx;

@@ -184,7 +184,8 @@ struct MgLevel {
   int Z = 0, R = 0, P = 0; // nodes in z and r; row pitch with one halo node a side
   float *u = nullptr, *f = nullptr; // (Z+2) x P, node (I, J) at (I+1) P + J + 1; halo nodes stay 0
   const float *coef = nullptr;      // MG_NCOEF arrays of (Z+2) x P; 1/diagonal 0 marks a held node
-  const float *rw = nullptr;        // restriction weights from the level above: [J][3], columns 2J-1, 2J, 2J+1
+  const float *rw = nullptr;        // restriction weights from the level above: [J][3], columns cr J - 1, cr J, cr J + 1
+  int cz = 2, cr = 2;               // coarsening from the level above in z and r: node (I, J) is its (cz I, cr J)
 };
 struct Mg32Work {
   int nlev = 0, tail = 0; // levels; first level that CTA 0 works alone

@@ -300,10 +300,13 @@ def test_multigrid_meets_the_stop_rule(oracle):
     assert err <= MG_TOL
 
 
-@pytest.mark.parametrize("case", [("pillbox", 601, 321), ("gun", 1400, 200), ("gun", 3001, 821)])
+@pytest.mark.parametrize("case", [("pillbox", 601, 321), ("gun", 1400, 200), ("gun", 3001, 821), ("gun", 300, 411)])
 def test_multigrid_multi_cta(oracle, case):
     """Meshes whose finer levels are worked by every SM (grid barriers) and
-    whose coarser levels by one CTA: a Gaussian charge from a cold start."""
+    whose coarser levels by one CTA: a Gaussian charge from a cold start.
+    The 300 x 411 gun mesh has dz = 5 dr: its first levels coarsen r only
+    (with both directions coarsened such meshes needed 25 to 64 V-cycles a
+    correction)."""
     kind, nz, nr = case
     if kind == "pillbox":
         cfg = workloads.PillboxConfig(nz=nz, nr=nr)
@@ -325,6 +328,9 @@ def test_multigrid_multi_cta(oracle, case):
     res, drive = poisson_residual(f, out["Psi"], f["Q"])
     print(case, "multigrid cycles", n, "residual", res / drive)
     assert 0 < n < 30 and res < 1e-6 * drive
+    if case == ("gun", 300, 411):
+        assert n <= 12, n
+        return  # the FP64 residual above is the check; the CPU SOR converges slowly on this mesh
     if cfg.nz < 2000:  # the CPU reference solution of the full gun mesh takes minutes
         assert rel_l2(out["Psi"], converged(oracle, f, 1e-9)) <= MG_TOL
 
