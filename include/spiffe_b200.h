@@ -254,7 +254,7 @@ int spiffe_gpu_set_profiling(spiffe_gpu_instance *inst, int32_t on);
 int spiffe_gpu_phase_times(spiffe_gpu_instance *inst, double *ms, int64_t *count);
 int64_t spiffe_gpu_launch_count(void);
 /* Split-precision form only (no counterpart in the reference): reorder the
- * particles by mesh cell every n steps of spiffe_gpu_run_steps (default 20;
+ * particles by mesh cell every n steps of spiffe_gpu_run_steps (default 40;
  * 0 never), starting with the next step, and on the first step after each
  * beam upload; this keeps the gather and the deposition of neighbouring
  * threads on the same nodes.  No effect on the FP64 form. */
