@@ -63,7 +63,6 @@ constexpr int MG_NT = 1024;           // threads per CTA
 constexpr int MG_TAIL_NODES = 3000;   // levels at most this large are worked by CTA 0 alone
 constexpr int MG_MIN_UNKNOWNS = 64;   // coarsening stops at this many unknowns
 constexpr int MG_NODES_PER_CTA = 8192; // mesh nodes per CTA below one CTA per SM
-constexpr int MG_SMALL_MESH = 200000;  // meshes of at most this many nodes smooth four times
 constexpr int MG_MAX_DIRECT = 1024;   // a coarsest level of at most this many unknowns is solved exactly
 enum { MG_INVD = 8, MG_DIAG = 9 };
 
@@ -1155,12 +1154,8 @@ extern "C" int s32_mg_solve(const DevMesh *m, Mg32Work *w, const float *crow, co
   a.inv_e2c = (float)(1 / a.e2c_d);
   a.nlev = w->nlev;
   a.tail = w->tail;
-  // V(2,2); V(4,4) on small meshes, whose sweeps cost little beside their
-  // barriers and whose coarse levels carry thin metal coarsely (on a 120 x
-  // 101 gun mesh 22 V(2,2) cycles a correction, 10 V(4,4))
-  const bool small = (size_t)(m->nz + 1) * (m->nr + 1) <= (size_t)MG_SMALL_MESH;
-  a.nu0 = small ? 4 : 2;
-  a.nu = small ? 4 : 2;
+  a.nu0 = 2;
+  a.nu = 2;
   a.coarse_sweeps = 24;
   a.cinv = w->cinv;
   a.cidx = w->cidx;
