@@ -300,6 +300,35 @@ def test_multigrid_meets_the_stop_rule(oracle):
     assert err <= MG_TOL
 
 
+def test_multigrid_follows_end_conditions_set_after_configuration():
+    """The multigrid's operators hold the end rows' conditions (mirrored rows
+    of a Dirichlet end, poisson.c:67-84, :102-118), and the run's
+    configuration builds them: an instance configured with Neumann ends and
+    then given Dirichlet ends by set_mesh solves exactly as one created with
+    Dirichlet ends, and meets the stop rule of the new equations."""
+    fx = load("dcgun_poisson")
+    f = fields_from(fx, modes=MODES, dt=float(fx["dt"]))
+    rng = np.random.default_rng(11)
+    f["Q"] = rng.normal(size=f.shape) * 1e4
+    f["Psi"] = np.zeros(f.shape)
+    f.mesh.left_bc = f.mesh.right_bc = abi.NEUMANN
+    fd = f.copy()
+    fd.mesh.left_bc = fd.mesh.right_bc = abi.DIRICHLET
+    pc = abi.poisson_options(step_interval=1, accuracy=1e-6, maximum_iterations=1000)
+    a = split(f)
+    a.configure_run(space_charge=0, poisson=pc)
+    m = a.get_mesh()
+    m.left_bc = m.right_bc = abi.DIRICHLET
+    a.set_mesh(m)
+    b = split(fd)
+    b.configure_run(space_charge=0, poisson=pc)
+    na, nb = a.solve_poisson(0, 1e-6, 1000), b.solve_poisson(0, 1e-6, 1000)
+    pa, pb = a.fields(fd)["Psi"], b.fields(fd)["Psi"]
+    assert na == nb and np.array_equal(pa, pb)
+    res, drive = poisson_residual(fd, pa, fd["Q"])
+    assert 0 < na < 30 and res < 1e-6 * drive
+
+
 @pytest.mark.parametrize("case", [("pillbox", 601, 321), ("gun", 1400, 200), ("gun", 3001, 821), ("gun", 300, 411)])
 def test_multigrid_multi_cta(oracle, case):
     """Meshes whose finer levels are worked by every SM (grid barriers) and
