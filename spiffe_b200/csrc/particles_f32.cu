@@ -23,6 +23,8 @@
 
 #include <cfloat>
 
+#include <cub/block/block_radix_sort.cuh>
+
 namespace {
 
 constexpr int T = 256;
@@ -817,33 +819,48 @@ __device__ __forceinline__ void move32(const DevBeam32 &b, long dst, long src)
 }
 
 // Removes exactly the lost particles (order not kept): the lost slots below
-// the new count are refilled from the survivors above it.  One block; the
-// pairing is built with block-wide prefix counts in chunks.
-constexpr int CT = 1024;
+// the new count are refilled from the survivors above it, the k-th hole in
+// ascending index order from the k-th survivor in ascending order, so the
+// result does not depend on the order the push appended the losses (which
+// follows the timing of its blocks).  One block; the lists are built with
+// block-wide prefix counts in chunks; the holes, collected from the push's
+// list, are put in order by a block radix sort when there are at most
+// CT * CT_ITEMS of them, else collected again by a scan of the statuses.
+constexpr int CT = 1024, CT_ITEMS = 4;
 __global__ void __launch_bounds__(CT) k_compact_any32(DevBeam32 b, const int32_t *lost_list, DevCounts *cnt,
                                                        int32_t *holes, int32_t *donors)
 {
   __shared__ int warp_tot[CT / 32];
-  __shared__ int base_sh;
+  __shared__ int base_sh, n_holes_sh;
+  typedef cub::BlockRadixSort<int, CT, CT_ITEMS> HoleSort;
+  __shared__ typename HoleSort::TempStorage sort_tmp;
   const long long n_lost = cnt->n_lost, np = cnt->np, new_np = np - n_lost;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   if (n_lost > 0) {
-    // two lists with block-wide compaction: holes (lost slots < new_np) and donors (survivors >= new_np)
-    for (int list = 0; list < 2; list++) {
+    // list 0: holes (lost slots < new_np) from the push's list; list 1:
+    // donors (survivors >= new_np) in index order; list 2: holes again, in
+    // index order, from the statuses (only when too many to sort)
+    for (int list = 0; list < 3; list++) {
+      if (list == 2 && n_holes_sh <= CT * CT_ITEMS)
+        break;
       if (tid == 0)
         base_sh = 0;
       __syncthreads();
-      for (long long c0 = 0; c0 < n_lost; c0 += CT) {
+      const long long span = list == 2 ? new_np : n_lost;
+      for (long long c0 = 0; c0 < span; c0 += CT) {
         const long long i = c0 + tid;
         bool take = false;
         int val = 0;
-        if (i < n_lost) {
+        if (i < span) {
           if (list == 0) {
             val = lost_list[i];
             take = val < new_np;
-          } else {
+          } else if (list == 1) {
             val = (int)(new_np + i);
             take = !(b.status[val] & S32_LOST);
+          } else {
+            val = (int)i;
+            take = b.status[val] & S32_LOST;
           }
         }
         const unsigned bal = __ballot_sync(0xffffffffu, take);
@@ -857,11 +874,34 @@ __global__ void __launch_bounds__(CT) k_compact_any32(DevBeam32 b, const int32_t
         }
         const int base = base_sh;
         if (take)
-          (list == 0 ? holes : donors)[base + before + __popc(bal & ((1u << lane) - 1))] = val;
+          (list == 1 ? donors : holes)[base + before + __popc(bal & ((1u << lane) - 1))] = val;
         __syncthreads();
         if (tid == 0)
           base_sh = base + total;
         __syncthreads();
+      }
+      if (list == 0) {
+        if (tid == 0)
+          n_holes_sh = base_sh;
+        __syncthreads();
+        const int nh = n_holes_sh;
+        if (nh <= CT * CT_ITEMS) {
+          // the holes in ascending order (INT_MAX pads sort last)
+          int k[CT_ITEMS];
+#pragma unroll
+          for (int q = 0; q < CT_ITEMS; q++) {
+            const int at = tid * CT_ITEMS + q;
+            k[q] = at < nh ? holes[at] : 0x7fffffff;
+          }
+          HoleSort(sort_tmp).Sort(k);
+#pragma unroll
+          for (int q = 0; q < CT_ITEMS; q++) {
+            const int at = tid * CT_ITEMS + q;
+            if (at < nh)
+              holes[at] = k[q];
+          }
+          __syncthreads();
+        }
       }
     }
     const int n_move = base_sh; // equal counts: every hole has a donor

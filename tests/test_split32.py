@@ -436,6 +436,50 @@ def test_poisson_correction_within_tolerance():
     assert rel_l2(out["Psi"], fx["Psi"]) <= 1e-5
 
 
+@pytest.mark.parametrize("n, n_lost", [(5000, 600), (20000, 6000)])
+def test_compaction_pairs_holes_and_survivors_in_index_order(n, n_lost):
+    """The split form removes lost particles by refilling the lost slots below
+    the new count from the survivors above it.  The push appends the losses in
+    the order its blocks happen to run, so the pairing must not follow that
+    list: the k-th hole in ascending index order takes the k-th survivor in
+    ascending order, whatever else runs on the GPU (a batched scan found
+    exit moments that changed in the mix before this).  Above 4096 holes in
+    a step the holes are collected by a scan of the statuses instead of
+    being sorted, which the second case covers."""
+    cfg = workloads.PillboxConfig()
+    f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(), modes=MODES)
+    f.mesh.dt = cfg.dt
+    rng = np.random.default_rng(3)
+    lost = np.sort(rng.choice(n, n_lost, replace=False))
+    z = np.full(n, 0.5 * (cfg.zmin + cfg.zmax))
+    z[lost] = cfg.zmax - 0.1 * cfg.dz  # leaves the mesh in one step at pz = 10
+    pz = np.zeros(n)
+    pz[lost] = 10.0
+    b = abi.Beam(n + 16)
+    b.QoMC = QoMC
+    b.set(n, z=z, r=np.full(n, 0.2 * cfg.rmax), pz=pz, Q=np.full(n, -1e-16), particleID=np.arange(1, n + 1),
+          status=np.full(n, abi.PART_ACTIVE, np.uint64))
+    b.npActive = n
+    g = gpu.GpuInstance(f, capacity=b.capacity, precision=gpu.PRECISION_SPLIT32)
+    g.set_sort_interval(0)
+    g.upload_beam(b)
+    g.configure_run(space_charge=0, push=abi.push_options(abi.COMPACT_SWAP, abi.SCREEN_PARTICLE))
+    g.run_steps(1)
+    got = abi.Beam(b.capacity)
+    g.download_beam(got)
+    new_np = n - n_lost
+    assert got.np == new_np
+    ids = np.arange(1, n + 1)
+    is_lost = np.zeros(n, bool)
+    is_lost[lost] = True
+    holes = lost[lost < new_np]
+    donors = np.nonzero(~is_lost[new_np:])[0] + new_np
+    expect = ids[:new_np].copy()
+    expect[holes] = ids[donors]
+    assert np.array_equal(got["particleID"], expect)
+    g.close()
+
+
 def pillbox_run(precision, steps, sort_interval=20):
     cfg = workloads.PillboxConfig()
     f = geometry.fields_for(cfg.nz, cfg.nr, cfg.zmin, cfg.zmax, cfg.rmax, cfg.geo_text(),
