@@ -51,6 +51,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -730,8 +731,13 @@ void parallel_rows(int n, Fn fn)
   const int chunk = (n + nt - 1) / nt;
   for (int t = 0; t < nt; t++) {
     const int lo = t * chunk, hi = std::min(n, lo + chunk);
-    if (lo < hi)
+    if (lo >= hi)
+      continue;
+    try {
       pool.emplace_back(fn, lo, hi);
+    } catch (const std::system_error &) {
+      fn(lo, hi); // no thread to be had: this chunk on the caller's thread
+    }
   }
   for (std::thread &th : pool)
     th.join();
