@@ -85,6 +85,21 @@ def parse():
     return p.parse_args()
 
 
+def combine_ranks(dist, ms, e2e_ms, psteps, e2e_psteps, device):
+    """The job's figures from every rank's (replicas: each GPU runs the whole
+    workload): the slowest rank's times and the sum of the work.  dist is
+    torch.distributed with an initialised group, or None for one process."""
+    if not dist:
+        return ms, e2e_ms, float(psteps), float(e2e_psteps)
+    import torch
+
+    t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    w = torch.tensor([psteps, e2e_psteps], dtype=torch.float64, device=device)
+    dist.all_reduce(w, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(w[0]), float(w[1])
+
+
 def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
@@ -356,15 +371,7 @@ def gpu_arm(args):
                            "run; its K steps hold the same share of Poisson corrections (one per 20 steps)"}
         g3.close()
     # --- totals over ranks (max time, summed work)
-    if dist:
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        w = torch.tensor([psteps, e2e_psteps], dtype=torch.float64, device="cuda")
-        dist.all_reduce(w, op=dist.ReduceOp.SUM)
-        ms, e2e_ms = float(t[0]), float(t[1])
-        psteps_all, e2e_all = float(w[0]), float(w[1])
-    else:
-        psteps_all, e2e_all = psteps, e2e_psteps
+    ms, e2e_ms, psteps_all, e2e_all = combine_ranks(dist, ms, e2e_ms, psteps, e2e_psteps, "cuda")
     sec = ms / 1e3
     value = psteps_all / sec
     cells = cfg.nz * cfg.nr * K * world / sec
